@@ -1,0 +1,173 @@
+/*
+ * vp_b200.h - C ABI of the B200 (sm_100a) Vlasov-Poisson step and its discrete adjoint.
+ *
+ * This is the boundary a host binding (ctypes, cffi, a C/C++ driver) links against. It replaces
+ * the device side of Forgotten/warp_vp_solver: the Warp kernels of warp_vp_solver/kernels.py,
+ * the host FFT Poisson solve of warp_vp_solver/poisson.py and the per-step launch/transfer
+ * loops of warp_vp_solver/solver.py. Each entry point names the reference interface it replaces.
+ *
+ * Conventions
+ *  - Every call returns an int status: VP_OK (0) or one of the VP_ERR_* codes below. The text
+ *    of the last error on the calling thread is returned by vp_get_last_error().
+ *  - Array arguments are DEVICE pointers owned by the caller (for example torch tensors), laid
+ *    out row-major with x (index i, length nx) as rows and v (index j, length nv) as columns,
+ *    exactly like the reference's (nx, nv) arrays. "real" below means the plan's compute type:
+ *    float when the plan was created with VP_F32, double with VP_F64.
+ *  - Calls are asynchronous on the given cudaStream_t (passed as void*; NULL = legacy default
+ *    stream). They never synchronise the device and never allocate device memory: scratch space
+ *    is a caller-provided workspace of vp_workspace_bytes() bytes, and state kept from the
+ *    forward pass for the backward pass lives in a caller-provided tape of vp_tape_bytes()
+ *    bytes. Calls are therefore safe to capture in a CUDA graph.
+ *  - A plan is bound to the device that was current at vp_plan_create(). One plan must not be
+ *    used from two host threads at once, and two calls that share a workspace must not overlap
+ *    on the device (the reference's solver object is not re-entrant either,
+ *    warp_vp_solver/solver.py:169-203).
+ */
+#ifndef VP_B200_H
+#define VP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VP_ABI_VERSION 1
+
+/* status codes */
+#define VP_OK 0
+#define VP_ERR_ARG 1          /* invalid argument (shape, pointer, size, value)           */
+#define VP_ERR_CUDA 2         /* a CUDA runtime call failed                                */
+#define VP_ERR_TIMEOUT 3      /* a bounded device-side wait ran out                        */
+#define VP_ERR_UNSUPPORTED 4  /* valid request this build does not implement               */
+
+/* compute types */
+#define VP_F32 0
+#define VP_F64 1
+
+/* Mesh description: the fields of warp_vp_solver/mesh.py:10-23 (Mesh) that the step uses.
+ * xs and vs are HOST arrays of length nx and nv (float64), as produced by make_mesh
+ * (warp_vp_solver/mesh.py:26-56). period_v is the half width length_v; the v period of the
+ * advection is 2*period_v (warp_vp_solver/solver.py:241). */
+typedef struct vp_mesh_desc {
+    int32_t nx;
+    int32_t nv;
+    const double* xs;
+    const double* vs;
+    double dx;
+    double dv;
+    double period_x;
+    double period_v;
+} vp_mesh_desc;
+
+typedef struct vp_plan vp_plan;
+
+/* Builds a plan for one (mesh, dt, f_eq) triple. Replaces WarpVlasovPoissonSolver.__init__
+ * (warp_vp_solver/solver.py:92-206): validates the inputs, uploads f_eq, and precomputes the
+ * per-column x half-step shifts, the FFT twiddles and the spectral multiplier of
+ * fft_inv_multiplier (warp_vp_solver/poisson.py:34-45).
+ * f_eq_host: HOST float64 array of nx*nv values (row-major (nx, nv)).
+ * dtype: VP_F32 or VP_F64. The plan detects an x-invariant f_eq (every row equal) and then
+ * keeps only one row on the device. */
+int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host, int dtype,
+                   vp_plan** out_plan);
+
+/* Releases a plan and its device tables. */
+int vp_plan_destroy(vp_plan* plan);
+
+/* Number of time steps for t_final: int(t_final / dt), as WarpVlasovPoissonSolver.num_steps
+ * (warp_vp_solver/solver.py:212-213). */
+int vp_num_steps(const vp_plan* plan, double t_final, int32_t* out_steps);
+
+/* Bytes of caller-provided device workspace a forward or backward call of n_steps steps needs
+ * with the given checkpoint interval (0 = automatic). */
+int vp_workspace_bytes(const vp_plan* plan, int32_t n_steps, int32_t checkpoint_every,
+                       size_t* out_bytes);
+
+/* Bytes of the tape a forward call writes for a later backward call: the delta-f state after
+ * the leading x half-step at every checkpoint_every-th step, plus the self-consistent field E
+ * and the v-step shift of every step. Replaces the f_hist residual the reference keeps in host
+ * memory for its adjoint (warp_vp_solver/solver.py:1379-1392). */
+int vp_tape_bytes(const vp_plan* plan, int32_t n_steps, int32_t checkpoint_every,
+                  size_t* out_bytes);
+
+/* Checkpoint interval actually used for a request (resolves 0 = automatic to ceil(sqrt(n))). */
+int vp_resolve_checkpoint_every(const vp_plan* plan, int32_t n_steps, int32_t checkpoint_every,
+                                int32_t* out_every);
+
+/* Forward time loop of n_steps Strang steps. Replaces WarpVlasovPoissonSolver.run_forward
+ * (warp_vp_solver/solver.py:418-464; legacy loop 470-524, fused-E+H loop 530-612).
+ *   f_iv      double[nx*nv]     initial distribution (input).
+ *   H         real[nx]          external field (input).
+ *   f_final   double[nx*nv]     final distribution, or NULL.
+ *   f_hist    real[n_steps*nx*nv]  f after every step, or NULL (record_history=False).
+ *   E_hist    real[n_steps*nx]  E + H of every step, or NULL.
+ *   ee_hist   real[n_steps]     0.5*trapz(E^2)*dx of the self-consistent E, or NULL.
+ *   tape      vp_tape_bytes() bytes, or NULL when no backward pass will follow.
+ * n_steps == 0 copies f_iv to f_final. */
+int vp_forward(vp_plan* plan, const double* f_iv, const void* H, int32_t n_steps,
+               double* f_final, void* f_hist, void* E_hist, void* ee_hist,
+               void* tape, int32_t checkpoint_every,
+               void* workspace, size_t workspace_bytes, void* stream);
+
+/* Discrete adjoint of vp_forward. Replaces WarpVlasovPoissonSolver._run_backward
+ * (warp_vp_solver/solver.py:742-772; legacy adjoint 778-932, on-device adjoint 938-1105).
+ * Reads the tape written by the vp_forward call with the same (H, n_steps, checkpoint_every)
+ * and recomputes the states between checkpoints. Cotangents may be NULL (treated as zero):
+ *   g_f_final real[nx*nv], g_f_hist real[n_steps*nx*nv], g_E_hist real[n_steps*nx],
+ *   g_ee_hist real[n_steps].
+ * Outputs: g_f_iv real[nx*nv] and g_H real[nx] (both overwritten). */
+int vp_backward(vp_plan* plan, const void* H, int32_t n_steps,
+                const void* tape, int32_t checkpoint_every,
+                const void* g_f_final, const void* g_f_hist, const void* g_E_hist,
+                const void* g_ee_hist, void* g_f_iv, void* g_H,
+                void* workspace, size_t workspace_bytes, void* stream);
+
+/* --- single-stage operators (the reference's helper methods and unit-tested kernels) ------ */
+
+/* rho[i] = dv * trapz_j(f_eq[i,j] - f[i,j]). Replaces compute_rho (warp_vp_solver/solver.py:
+ * 393-397) and compute_rho_kernel (warp_vp_solver/kernels.py:156-172). f: double[nx*nv],
+ * rho: real[nx]. */
+int vp_compute_rho(vp_plan* plan, const double* f, void* rho, void* stream);
+
+/* E = real(ifft(m * fft(rho))) (adjoint=0) or real(ifft(conj(m) * fft(rho))) (adjoint=1) with
+ * the in-block shared-memory FFT. Replaces solve_poisson_host / solve_poisson_host_adjoint
+ * (warp_vp_solver/poisson.py:48-99) and compute_E_from_rho (warp_vp_solver/solver.py:399-404).
+ * in, out: real[nx]. */
+int vp_poisson(vp_plan* plan, const void* in, void* out, int adjoint, void* stream);
+
+/* ee = 0.5 * dx * trapz(E^2). Replaces compute_electric_energy (warp_vp_solver/solver.py:
+ * 409-412) and compute_ee_kernel (warp_vp_solver/kernels.py:175-197). E: real[nx], ee: real[1]. */
+int vp_electric_energy(vp_plan* plan, const void* E, void* ee, void* stream);
+
+/* x half-step advection by dt/2 (adjoint=0) or its transpose (adjoint=1) on an arbitrary
+ * real[nx*nv] array. Replaces semilag_x_kernel / semilag_x_adjoint_kernel
+ * (warp_vp_solver/kernels.py:109-130, 215-241). dt may differ from the plan's dt. */
+int vp_semilag_x(vp_plan* plan, const void* in, void* out, double dt, int adjoint, void* stream);
+
+/* v advection by dt with field E_total[nx] on an arbitrary real[nx*nv] array. adjoint=0:
+ * out = V(in) (semilag_v_kernel / semilag_v_fused_kernel, warp_vp_solver/kernels.py:133-153,
+ * 367-393). adjoint=1: out = V^T(in) and, when f_in and g_E are non-NULL,
+ * g_E[i] = sum_j -dt*(f_in[i,i1]-f_in[i,i0])/dv * in[i,j] (semilag_v_adjoint_kernel /
+ * semilag_v_fused_adjoint_kernel, warp_vp_solver/kernels.py:244-273, 396-429). */
+int vp_semilag_v(vp_plan* plan, const void* in, const void* E_total, void* out, double dt,
+                 int adjoint, const void* f_in, void* g_E, void* stream);
+
+/* --- diagnostics ------------------------------------------------------------------------ */
+
+/* Copies the last error message of the calling thread into buf (always NUL-terminated). */
+int vp_get_last_error(char* buf, size_t buf_len);
+
+/* Kernel launches issued by the calling thread since the last reset (for launch accounting). */
+int64_t vp_launch_count(void);
+void vp_reset_launch_count(void);
+
+/* ABI version (VP_ABI_VERSION). */
+int vp_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VP_B200_H */

@@ -1,0 +1,131 @@
+"""Parity of the CUDA path with the reference (golden vectors) and the float64 oracle.
+
+Bars (max-norm relative error, max|a-b| / max|b|):
+  * float64 plan vs reference: 1e-11 forward, 1e-10 adjoint (same scheme, re-associated);
+  * float32 plan vs reference: 1e-5 for f, E, ee (the stated requirement); the adjoint, which
+    accumulates cotangents over every step in float32, 1e-4.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+import vp_oracle as O
+from conftest import BACKWARD_CASES, FORWARD_CASES, two_stream_state
+from warp_vp_solver_b200 import WarpVlasovPoissonSolver, make_mesh
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("f_final", "f_hist", "E_hist", "ee_hist")
+TOL_FWD = {torch.float64: 1e-11, torch.float32: 1e-5}
+TOL_BWD = {torch.float64: 1e-10, torch.float32: 1e-4}
+DTYPES = [torch.float32, torch.float64]
+
+
+def _dt_id(d):
+    return "f32" if d == torch.float32 else "f64"
+
+
+@pytest.mark.parametrize("dtype", DTYPES, ids=_dt_id)
+@pytest.mark.parametrize("case", FORWARD_CASES, ids=lambda c: c.name)
+def test_forward_matches_reference_golden(case, dtype):
+    s = WarpVlasovPoissonSolver(case.mesh, float(case["dt"]), case["f_eq"], dtype=dtype)
+    out = s.run_forward(case["f_iv"], case["H"], float(case["t_final"]))
+    assert out[1].shape == case["f_hist"].shape
+    for arr, name in zip(out, FIELDS):
+        ref = case[name]
+        if case.name.startswith("fwd_equilibrium") and name in ("E_hist", "ee_hist"):
+            assert np.abs(arr).max() <= 1e-12
+            continue
+        err = O.rel_err(arr, ref)
+        assert err < TOL_FWD[dtype], f"{case.name}:{name} rel err {err:.2e}"
+
+
+@pytest.mark.parametrize("dtype", DTYPES, ids=_dt_id)
+@pytest.mark.parametrize("case", BACKWARD_CASES, ids=lambda c: c.name)
+def test_backward_matches_reference_golden(case, dtype):
+    s = WarpVlasovPoissonSolver(case.mesh, float(case["dt"]), case["f_eq"], dtype=dtype)
+    g_f, g_H = s._run_backward(case["f_iv"], case["H"], float(case["t_final"]), None,
+                               case["g_f_final"], case["g_f_hist"], case["g_E_hist"],
+                               case["g_ee_hist"])
+    e1, e2 = O.rel_err(g_f, case["g_f_iv"]), O.rel_err(g_H, case["g_H"])
+    assert e1 < TOL_BWD[dtype] and e2 < TOL_BWD[dtype], f"{case.name}: g_f {e1:.2e} g_H {e2:.2e}"
+
+
+@pytest.mark.parametrize("every", [1, 2, 3, 0])
+def test_checkpoint_interval_is_bitwise_neutral(every):
+    case = [c for c in BACKWARD_CASES if c.name == "bwd_random_16x32"][0]
+    outs = []
+    for ce in (1, every):
+        s = WarpVlasovPoissonSolver(case.mesh, float(case["dt"]), case["f_eq"], checkpoint_every=ce)
+        outs.append(s._run_backward(case["f_iv"], case["H"], float(case["t_final"]), None,
+                                    case["g_f_final"], case["g_f_hist"], case["g_E_hist"],
+                                    case["g_ee_hist"]))
+    np.testing.assert_array_equal(outs[0][0], outs[1][0])
+    np.testing.assert_array_equal(outs[0][1], outs[1][1])
+
+
+def test_record_history_false_and_determinism():
+    case = [c for c in FORWARD_CASES if c.name == "fwd_twostream_32x32"][0]
+    s = WarpVlasovPoissonSolver(case.mesh, float(case["dt"]), case["f_eq"])
+    a = s.run_forward(case["f_iv"], case["H"], float(case["t_final"]))
+    b = s.run_forward(case["f_iv"], case["H"], float(case["t_final"]), record_history=False)
+    assert b[1] is None
+    for x, y in zip((a[0], a[2], a[3]), (b[0], b[2], b[3])):
+        np.testing.assert_array_equal(x, y)
+    c = s.run_forward(case["f_iv"], case["H"], float(case["t_final"]))
+    for x, y in zip(a, c):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_zero_steps_returns_initial_state():
+    m = make_mesh(2 * np.pi, 6.0, 16, 32)
+    f_eq = np.exp(-0.5 * m.V ** 2)
+    f0 = f_eq * (1 + 1e-3 * np.cos(m.X))
+    s = WarpVlasovPoissonSolver(m, 0.1, f_eq)
+    f, fh, Eh, ee = s.run_forward(f0, np.zeros(16), 0.05)
+    np.testing.assert_array_equal(f, f0)
+    assert fh.shape == (0, 16, 32) and Eh.shape == (0, 16) and ee.shape == (0,)
+
+
+def test_config1_two_stream_128_100_steps():
+    """128x128 two-stream, dt 0.05, t_final 5 (100 steps), H = 0."""
+    m = make_mesh(10.0 * np.pi, 6.0, 128, 128)
+    f_eq, f_iv = two_stream_state(m)
+    H = np.zeros(m.nx)
+    g = O.grid_from(m)
+    ref = O.run_forward(g, 0.05, f_eq, f_iv, H, 5.0)
+    s = WarpVlasovPoissonSolver(m, 0.05, f_eq)
+    out = s.run_forward(f_iv, H, 5.0)
+    s64 = WarpVlasovPoissonSolver(m, 0.05, f_eq, dtype=torch.float64)
+    out64 = s64.run_forward(f_iv, H, 5.0)
+    for arr, arr64, r, name in zip(out, out64, ref, FIELDS):
+        assert O.rel_err(arr, r) < 1e-5, f"{name} {O.rel_err(arr, r):.2e}"
+        assert O.rel_err(arr64, r) < 1e-11, f"{name} f64 {O.rel_err(arr64, r):.2e}"
+
+
+def test_autograd_matches_oracle_adjoint():
+    """run_forward_torch + torch autograd gives the oracle's dJ/dH and dJ/df_iv."""
+    from warp_vp_solver_b200 import electric_energy_in_time
+
+    m = make_mesh(10.0 * np.pi, 6.0, 32, 64)
+    f_eq, f_iv = two_stream_state(m)
+    rng = np.random.default_rng(0)
+    H0 = 0.01 * rng.standard_normal(m.nx)
+    dt, tf = 0.05, 0.6
+    T = int(tf / dt)
+    s = WarpVlasovPoissonSolver(m, dt, f_eq, dtype=torch.float64)
+    H = torch.tensor(H0, dtype=torch.float64, device="cuda", requires_grad=True)
+    f0 = torch.tensor(f_iv, dtype=torch.float64, device="cuda", requires_grad=True)
+    f_final, f_hist, E_hist, ee = s.run_forward_torch(f0, H, tf)
+    J = electric_energy_in_time(ee, s) + (f_final ** 2).sum() * 1e-3 + (E_hist ** 2).sum()
+    J.backward()
+    g = O.grid_from(m)
+    fwd = O.run_forward(g, dt, f_eq, f_iv, H0, tf)
+    w = O.trapezoid_time_weights(T, dt)
+    gf, gH = O.run_backward(g, dt, f_eq, f_iv, H0, tf, fwd[1], 2e-3 * fwd[0],
+                            np.zeros((T, m.nx, m.nv)), 2.0 * fwd[2], w)
+    assert O.rel_err(H.grad.cpu().numpy(), gH) < 1e-10
+    assert O.rel_err(f0.grad.cpu().numpy(), gf) < 1e-10

@@ -1,0 +1,121 @@
+"""ctypes bindings to ``libvpb200.so`` (the C ABI declared in ``include/vp_b200.h``).
+
+The library is loaded from this package directory. There is no CPU fallback: if the library
+is missing or no CUDA device is present, the calls that need it raise.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+VP_OK = 0
+VP_ERR_ARG = 1
+VP_ERR_CUDA = 2
+VP_ERR_TIMEOUT = 3
+VP_ERR_UNSUPPORTED = 4
+VP_F32 = 0
+VP_F64 = 1
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libvpb200.so")
+
+_lib = None
+_lock = threading.Lock()
+
+c_int = ctypes.c_int
+c_i32 = ctypes.c_int32
+c_i64 = ctypes.c_int64
+c_dbl = ctypes.c_double
+c_size = ctypes.c_size_t
+c_vp = ctypes.c_void_p
+
+
+class MeshDesc(ctypes.Structure):
+    _fields_ = [
+        ("nx", c_i32),
+        ("nv", c_i32),
+        ("xs", ctypes.POINTER(c_dbl)),
+        ("vs", ctypes.POINTER(c_dbl)),
+        ("dx", c_dbl),
+        ("dv", c_dbl),
+        ("period_x", c_dbl),
+        ("period_v", c_dbl),
+    ]
+
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "vp_abi_version": (c_int, []),
+    "vp_get_last_error": (c_int, [ctypes.c_char_p, c_size]),
+    "vp_launch_count": (c_i64, []),
+    "vp_reset_launch_count": (None, []),
+    "vp_plan_create": (c_int, [ctypes.POINTER(MeshDesc), c_dbl, ctypes.POINTER(c_dbl), c_int,
+                               ctypes.POINTER(c_vp)]),
+    "vp_plan_destroy": (c_int, [c_vp]),
+    "vp_num_steps": (c_int, [c_vp, c_dbl, ctypes.POINTER(c_i32)]),
+    "vp_workspace_bytes": (c_int, [c_vp, c_i32, c_i32, ctypes.POINTER(c_size)]),
+    "vp_tape_bytes": (c_int, [c_vp, c_i32, c_i32, ctypes.POINTER(c_size)]),
+    "vp_resolve_checkpoint_every": (c_int, [c_vp, c_i32, c_i32, ctypes.POINTER(c_i32)]),
+    "vp_forward": (c_int, [c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp,
+                           c_size, c_vp]),
+    "vp_backward": (c_int, [c_vp, c_vp, c_i32, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
+                            c_vp, c_size, c_vp]),
+    "vp_compute_rho": (c_int, [c_vp, c_vp, c_vp, c_vp]),
+    "vp_poisson": (c_int, [c_vp, c_vp, c_vp, c_int, c_vp]),
+    "vp_electric_energy": (c_int, [c_vp, c_vp, c_vp, c_vp]),
+    "vp_semilag_x": (c_int, [c_vp, c_vp, c_vp, c_dbl, c_int, c_vp]),
+    "vp_semilag_v": (c_int, [c_vp, c_vp, c_vp, c_vp, c_dbl, c_int, c_vp, c_vp, c_vp]),
+}
+
+
+class VPError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(msg)
+        self.code = code
+
+
+def load():
+    """Load the library (once) and declare the C signatures."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    f"{LIB_PATH} is missing: build it with `python -m warp_vp_solver_b200.build` "
+                    "(there is no CPU fallback)")
+            lib = ctypes.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+    return _lib
+
+
+def last_error() -> str:
+    buf = ctypes.create_string_buffer(512)
+    load().vp_get_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int) -> None:
+    if rc == VP_OK:
+        return
+    msg = last_error()
+    if rc == VP_ERR_ARG:
+        raise ValueError(msg)
+    if rc == VP_ERR_UNSUPPORTED:
+        raise NotImplementedError(msg)
+    raise VPError(rc, msg)
+
+
+def ptr(t) -> int | None:
+    """Device pointer of a torch tensor (or None)."""
+    return None if t is None else int(t.data_ptr())
+
+
+def dbl_ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(c_dbl))

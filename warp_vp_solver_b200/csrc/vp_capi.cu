@@ -1,0 +1,763 @@
+// C ABI (include/vp_b200.h): plan set-up, validation, workspace/tape layout and the host-side
+// orchestration of the fused forward and adjoint launches. No device allocation and no device
+// synchronisation happen inside vp_forward / vp_backward; they only enqueue work on the
+// caller's stream.
+
+#include "../../include/vp_b200.h"
+#include "vp_internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+namespace vpb {
+
+static thread_local char g_err[512] = "";
+static thread_local int64_t g_launches = 0;
+
+void count_launch(int n) { g_launches += n; }
+
+static int set_err(int code, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+static int cuda_err(cudaError_t e, const char* what) {
+    return set_err(VP_ERR_CUDA, "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+}
+
+#define VP_CUDA(call, what)                        \
+    do {                                           \
+        cudaError_t e_ = (call);                   \
+        if (e_ != cudaSuccess) return cuda_err(e_, what); \
+    } while (0)
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace vpb
+
+using namespace vpb;
+
+struct vp_plan {
+    int nx = 0, nv = 0, dtype = VP_F32;
+    double dx = 0, dv = 0, dt = 0, period_x = 0, period_v = 0;
+    int feq2d = 0;
+    int device = 0;
+    int pow2 = 0, log2nx = 0;
+    int use_smem_poisson = 0;
+    LaunchCfg cfg{};
+    // device tables (owned)
+    double* d_feq = nullptr;   // nv (x-invariant) or nx*nv
+    double* d_vs = nullptr;    // nv
+    int* d_mx = nullptr;       // nv
+    void* d_tx = nullptr;      // nv reals
+    double* d_tx64 = nullptr;  // nv
+    void* d_tw = nullptr;      // nx/2 complex
+    void* d_mult = nullptr;    // nx reals (imaginary part)
+    void* d_circ = nullptr;    // nx reals
+};
+
+namespace vpb {
+
+static size_t real_size(const vp_plan* p) { return p->dtype == VP_F64 ? 8 : 4; }
+static size_t vshift_size(const vp_plan* p) { return p->dtype == VP_F64 ? 16 : 8; }
+
+static int check_dev_ptr(const void* ptr, const char* name, int device) {
+    if (ptr == nullptr) return set_err(VP_ERR_ARG, "%s must not be NULL", name);
+    cudaPointerAttributes at;
+    cudaError_t e = cudaPointerGetAttributes(&at, ptr);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(VP_ERR_ARG, "%s is not a CUDA-visible pointer (%s)", name, cudaGetErrorName(e));
+    }
+    if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)
+        return set_err(VP_ERR_ARG, "%s must be device memory (got host or unregistered memory)", name);
+    if (at.type == cudaMemoryTypeDevice && at.device != device)
+        return set_err(VP_ERR_ARG, "%s lives on device %d but the plan is bound to device %d", name,
+                       at.device, device);
+    return VP_OK;
+}
+
+static int check_opt_ptr(const void* ptr, const char* name, int device) {
+    return ptr == nullptr ? VP_OK : check_dev_ptr(ptr, name, device);
+}
+
+static LaunchCfg choose_cfg(int nx, int nv, int n_sms) {
+    LaunchCfg c{};
+    c.threads = nv >= 128 ? 128 : ((nv + 31) / 32) * 32;
+    int R = 1;
+    for (int r : {16, 8, 4, 2}) {
+        if (nx % r == 0 && r <= nx / 2) {
+            R = r;
+            break;
+        }
+    }
+    int chunks = 1;
+    int chunk_cols = nv;
+    const int target = 2 * n_sms;
+    while ((nx / R) * chunks < target) {
+        if (R > 4 && nx % (R / 2) == 0) {
+            R /= 2;
+        } else if ((chunk_cols + 1) / 2 >= c.threads) {
+            chunks *= 2;
+            chunk_cols = (nv + chunks - 1) / chunks;
+            chunk_cols = ((chunk_cols + 31) / 32) * 32;
+            chunks = (nv + chunk_cols - 1) / chunk_cols;
+        } else if (R > 1) {
+            R /= 2;
+        } else {
+            break;
+        }
+    }
+    c.R = R;
+    c.n_chunks = chunks;
+    c.chunk_cols = chunk_cols;
+    return c;
+}
+
+static size_t fused_smem(const vp_plan* p, int R) {
+    const size_t red = ((size_t)32 * R * real_size(p) + 15) & ~(size_t)15;
+    return red + (p->use_smem_poisson ? poisson_smem_bytes(p->nx, real_size(p)) : 0);
+}
+
+static int resolve_every(int n_steps, int every) {
+    if (n_steps <= 0) return 1;
+    if (every <= 0) {
+        int k = (int)std::ceil(std::sqrt((double)n_steps));
+        return std::max(1, std::min(k, n_steps));
+    }
+    return std::min(every, n_steps);
+}
+
+struct WsLayout {
+    size_t hbuf0, hbuf1, seg, part, counter, vsh, E, grho, gscratch, total;
+};
+
+static WsLayout ws_layout(const vp_plan* p, int n_steps, int every) {
+    const size_t nxnv = (size_t)p->nx * p->nv * real_size(p);
+    const int K = resolve_every(n_steps, every);
+    WsLayout L{};
+    size_t off = 0;
+    L.hbuf0 = off; off += align256(nxnv);
+    L.hbuf1 = off; off += align256(nxnv);
+    L.seg = off; off += align256(nxnv * (size_t)std::max(0, K - 1));
+    L.part = off; off += align256((size_t)p->cfg.n_chunks * p->nx * real_size(p));
+    L.counter = off; off += 256;
+    L.vsh = off; off += align256((size_t)p->nx * vshift_size(p));
+    L.E = off; off += align256((size_t)p->nx * real_size(p));
+    L.grho = off; off += align256((size_t)p->nx * real_size(p));
+    L.gscratch = off; off += align256((size_t)3 * p->nx * real_size(p));
+    L.total = off;
+    return L;
+}
+
+struct TapeLayout {
+    size_t ckpt, E, vsh, total;
+    int K, n_ckpt;
+};
+
+static TapeLayout tape_layout(const vp_plan* p, int n_steps, int every) {
+    TapeLayout L{};
+    L.K = resolve_every(n_steps, every);
+    L.n_ckpt = n_steps > 0 ? (n_steps + L.K - 1) / L.K : 0;
+    const size_t nxnv = (size_t)p->nx * p->nv * real_size(p);
+    size_t off = 0;
+    L.ckpt = off; off += align256(nxnv * (size_t)L.n_ckpt);
+    L.E = off; off += align256((size_t)n_steps * p->nx * real_size(p));
+    L.vsh = off; off += align256((size_t)n_steps * p->nx * vshift_size(p));
+    L.total = off;
+    return L;
+}
+
+template <typename T>
+static PoissonTables<T> poisson_tables(const vp_plan* p, unsigned char* ws, const WsLayout* L) {
+    PoissonTables<T> P{};
+    P.nx = p->nx;
+    P.log2nx = p->log2nx;
+    P.pow2 = p->pow2;
+    P.tw = static_cast<const typename Cplx<T>::type*>(p->d_tw);
+    P.mult_im = static_cast<const T*>(p->d_mult);
+    P.circ = static_cast<const T*>(p->d_circ);
+    P.gscratch = (ws != nullptr && L != nullptr) ? reinterpret_cast<T*>(ws + L->gscratch) : nullptr;
+    P.use_smem = p->use_smem_poisson;
+    return P;
+}
+
+// ---------------------------------------------------------------------------------------------
+// forward orchestration
+// ---------------------------------------------------------------------------------------------
+template <typename T>
+static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps, double* f_final,
+                        T* f_hist, T* E_hist, T* ee_hist, unsigned char* tape, int every,
+                        unsigned char* ws, cudaStream_t s) {
+    const int nx = p->nx, nv = p->nv;
+    const size_t nxnv = (size_t)nx * nv;
+    const WsLayout L = ws_layout(p, T_steps, every);
+    const TapeLayout TL = tape_layout(p, T_steps, every);
+    const int K = TL.K;
+    T* hbuf[2] = {reinterpret_cast<T*>(ws + L.hbuf0), reinterpret_cast<T*>(ws + L.hbuf1)};
+    unsigned* counter = reinterpret_cast<unsigned*>(ws + L.counter);
+    T* part = reinterpret_cast<T*>(ws + L.part);
+    VShift<T>* vsh_ws = reinterpret_cast<VShift<T>*>(ws + L.vsh);
+    T* E_ws = reinterpret_cast<T*>(ws + L.E);
+    T* ckpt = tape ? reinterpret_cast<T*>(tape + TL.ckpt) : nullptr;
+    T* E_all = tape ? reinterpret_cast<T*>(tape + TL.E) : nullptr;
+    VShift<T>* vsh_all = tape ? reinterpret_cast<VShift<T>*>(tape + TL.vsh) : nullptr;
+
+    VP_CUDA(cudaMemsetAsync(counter, 0, 256, s), "cudaMemsetAsync(counter)");
+
+    auto h_slot = [&](int n) -> T* {
+        if (ckpt != nullptr && n % K == 0) return ckpt + (size_t)(n / K) * nxnv;
+        return hbuf[n & 1];
+    };
+
+    FwdArgs<T> a{};
+    a.nx = nx;
+    a.nv = nv;
+    a.n_chunks = p->cfg.n_chunks;
+    a.chunk_cols = p->cfg.chunk_cols;
+    a.mx = p->d_mx;
+    a.tx = static_cast<const T*>(p->d_tx);
+    a.tx64 = p->d_tx64;
+    a.feq = p->d_feq;
+    a.feq_rs = p->feq2d ? nv : 0;
+    a.counter = counter;
+    a.P = poisson_tables<T>(p, ws, &L);
+    a.dv = (T)p->dv;
+    a.dx = (T)p->dx;
+    a.dtdv = (T)(p->dt / p->dv);
+    a.H = H;
+
+    // prologue: h_0, rho_0 -> E_0
+    a.f_iv = f_iv;
+    a.h_in = nullptr;
+    a.h_out = h_slot(0);
+    a.vsh = nullptr;
+    a.part = part;
+    a.E_out = E_all ? E_all : E_ws;
+    a.vsh_out = vsh_all ? vsh_all : vsh_ws;
+    a.E_hist_out = E_hist;
+    a.ee_out = ee_hist;
+    a.f_hist_n = nullptr;
+    a.f_final = nullptr;
+    VP_CUDA(launch_fwd<T>(a, p->cfg, 0, p->feq2d != 0, s), "forward prologue launch");
+
+    for (int n = 0; n < T_steps; ++n) {
+        const bool last = (n == T_steps - 1);
+        a.f_iv = nullptr;
+        a.h_in = h_slot(n);
+        a.h_out = last ? nullptr : h_slot(n + 1);
+        a.vsh = vsh_all ? vsh_all + (size_t)n * nx : vsh_ws;
+        a.f_hist_n = f_hist ? f_hist + (size_t)n * nxnv : nullptr;
+        a.f_final = last ? f_final : nullptr;
+        a.part = last ? nullptr : part;
+        a.E_out = E_all ? E_all + (size_t)(n + 1) * nx : E_ws;
+        a.vsh_out = vsh_all ? vsh_all + (size_t)(n + 1) * nx : vsh_ws;
+        a.E_hist_out = (E_hist && !last) ? E_hist + (size_t)(n + 1) * nx : nullptr;
+        a.ee_out = (ee_hist && !last) ? ee_hist + (n + 1) : nullptr;
+        VP_CUDA(launch_fwd<T>(a, p->cfg, 1, p->feq2d != 0, s), "forward step launch");
+    }
+    return VP_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// backward orchestration
+// ---------------------------------------------------------------------------------------------
+template <typename T>
+static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned char* tape, int every,
+                         const T* g_ff, const T* g_fh, const T* g_Eh, const T* g_ee, T* g_fiv,
+                         T* g_H, unsigned char* ws, cudaStream_t s) {
+    const int nx = p->nx, nv = p->nv;
+    const size_t nxnv = (size_t)nx * nv;
+    const WsLayout L = ws_layout(p, T_steps, every);
+    const TapeLayout TL = tape_layout(p, T_steps, every);
+    const int K = TL.K;
+    T* wbuf[2] = {reinterpret_cast<T*>(ws + L.hbuf0), reinterpret_cast<T*>(ws + L.hbuf1)};
+    T* seg = reinterpret_cast<T*>(ws + L.seg);
+    unsigned* counter = reinterpret_cast<unsigned*>(ws + L.counter);
+    T* part = reinterpret_cast<T*>(ws + L.part);
+    T* grho = reinterpret_cast<T*>(ws + L.grho);
+    const T* ckpt = reinterpret_cast<const T*>(tape + TL.ckpt);
+    const T* E_all = reinterpret_cast<const T*>(tape + TL.E);
+    const VShift<T>* vsh_all = reinterpret_cast<const VShift<T>*>(tape + TL.vsh);
+
+    VP_CUDA(cudaMemsetAsync(counter, 0, 256, s), "cudaMemsetAsync(counter)");
+    VP_CUDA(cudaMemsetAsync(g_H, 0, (size_t)nx * sizeof(T), s), "cudaMemsetAsync(g_H)");
+
+    auto h_ptr = [&](int n) -> const T* {
+        if (n % K == 0) return ckpt + (size_t)(n / K) * nxnv;
+        return seg + (size_t)((n % K) - 1) * nxnv;
+    };
+    auto h_mut = [&](int n) -> T* { return seg + (size_t)((n % K) - 1) * nxnv; };
+
+    FwdArgs<T> fa{};
+    fa.nx = nx;
+    fa.nv = nv;
+    fa.n_chunks = p->cfg.n_chunks;
+    fa.chunk_cols = p->cfg.chunk_cols;
+    fa.mx = p->d_mx;
+    fa.tx = static_cast<const T*>(p->d_tx);
+    fa.tx64 = p->d_tx64;
+    fa.feq = p->d_feq;
+    fa.feq_rs = p->feq2d ? nv : 0;
+    fa.counter = counter;
+    fa.P = poisson_tables<T>(p, ws, &L);
+    fa.dv = (T)p->dv;
+    fa.dx = (T)p->dx;
+    fa.dtdv = (T)(p->dt / p->dv);
+    fa.H = H;
+    fa.part = nullptr;  // propagation only
+
+    int current_seg = -1;
+    auto recompute = [&](int sgi) -> int {
+        if (sgi == current_seg) return VP_OK;
+        current_seg = sgi;
+        const int n0 = sgi * K;
+        const int n1 = std::min(n0 + K, T_steps);
+        for (int n = n0; n < n1 - 1; ++n) {
+            fa.h_in = h_ptr(n);
+            fa.h_out = h_mut(n + 1);
+            fa.vsh = vsh_all + (size_t)n * nx;
+            VP_CUDA(launch_fwd<T>(fa, p->cfg, 1, p->feq2d != 0, s), "recompute launch");
+        }
+        return VP_OK;
+    };
+
+    BwdArgs<T> b{};
+    b.nx = nx;
+    b.nv = nv;
+    b.n_chunks = p->cfg.n_chunks;
+    b.chunk_cols = p->cfg.chunk_cols;
+    b.mx = p->d_mx;
+    b.tx = static_cast<const T*>(p->d_tx);
+    b.feq = p->d_feq;
+    b.feq_rs = p->feq2d ? nv : 0;
+    b.part = part;
+    b.counter = counter;
+    b.P = poisson_tables<T>(p, ws, &L);
+    b.dv = (T)p->dv;
+    b.dx = (T)p->dx;
+    b.neg_dt_dv = (T)(-p->dt / p->dv);
+    b.gH = g_H;
+    b.grho_out = grho;
+
+    int rc;
+    // prologue (n = T)
+    if ((rc = recompute((T_steps - 1) / K)) != VP_OK) return rc;
+    b.c_src = g_ff;
+    b.c_src2 = g_fh ? g_fh + (size_t)(T_steps - 1) * nxnv : nullptr;
+    b.w_out = wbuf[(T_steps - 1) & 1];
+    b.h_prev = h_ptr(T_steps - 1);
+    b.vsh_prev = vsh_all + (size_t)(T_steps - 1) * nx;
+    b.E_prev = E_all + (size_t)(T_steps - 1) * nx;
+    b.gE_hist = g_Eh ? g_Eh + (size_t)(T_steps - 1) * nx : nullptr;
+    b.gee = g_ee ? g_ee + (T_steps - 1) : nullptr;
+    VP_CUDA(launch_bwd<T>(b, p->cfg, 0, p->feq2d != 0, s), "backward prologue launch");
+
+    b.c_src = nullptr;
+    b.c_src2 = nullptr;
+    for (int n = T_steps - 1; n >= 1; --n) {
+        if ((rc = recompute((n - 1) / K)) != VP_OK) return rc;
+        b.w_in = wbuf[n & 1];
+        b.grho = grho;
+        b.vsh_n = vsh_all + (size_t)n * nx;
+        b.gfh = g_fh ? g_fh + (size_t)(n - 1) * nxnv : nullptr;
+        b.w_out = wbuf[(n - 1) & 1];
+        b.h_prev = h_ptr(n - 1);
+        b.vsh_prev = vsh_all + (size_t)(n - 1) * nx;
+        b.E_prev = E_all + (size_t)(n - 1) * nx;
+        b.gE_hist = g_Eh ? g_Eh + (size_t)(n - 1) * nx : nullptr;
+        b.gee = g_ee ? g_ee + (n - 1) : nullptr;
+        VP_CUDA(launch_bwd<T>(b, p->cfg, 1, p->feq2d != 0, s), "backward step launch");
+    }
+    // epilogue (n = 0)
+    b.w_in = wbuf[0];
+    b.grho = grho;
+    b.vsh_n = vsh_all;
+    b.gfh = nullptr;
+    b.w_out = nullptr;
+    b.gfiv_out = g_fiv;
+    VP_CUDA(launch_bwd<T>(b, p->cfg, 2, p->feq2d != 0, s), "backward epilogue launch");
+    return VP_OK;
+}
+
+static void free_plan(vp_plan* p) {
+    if (!p) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(p->device);
+    cudaFree(p->d_feq);
+    cudaFree(p->d_vs);
+    cudaFree(p->d_mx);
+    cudaFree(p->d_tx);
+    cudaFree(p->d_tx64);
+    cudaFree(p->d_tw);
+    cudaFree(p->d_mult);
+    cudaFree(p->d_circ);
+    cudaSetDevice(prev);
+    delete p;
+}
+
+template <typename T>
+static int upload(void** dst, const std::vector<double>& src) {
+    std::vector<T> tmp(src.size());
+    for (size_t i = 0; i < src.size(); ++i) tmp[i] = (T)src[i];
+    VP_CUDA(cudaMalloc(dst, std::max<size_t>(1, tmp.size()) * sizeof(T)), "cudaMalloc(plan table)");
+    if (!tmp.empty())
+        VP_CUDA(cudaMemcpy(*dst, tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice),
+                "cudaMemcpy(plan table)");
+    return VP_OK;
+}
+
+static int upload_bytes(void** dst, const void* src, size_t bytes) {
+    VP_CUDA(cudaMalloc(dst, std::max<size_t>(1, bytes)), "cudaMalloc(plan table)");
+    if (bytes) VP_CUDA(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice), "cudaMemcpy(plan table)");
+    return VP_OK;
+}
+
+}  // namespace vpb
+
+// =============================================================================================
+// extern "C" entry points
+// =============================================================================================
+
+extern "C" {
+
+int vp_abi_version(void) { return VP_ABI_VERSION; }
+
+int vp_get_last_error(char* buf, size_t buf_len) {
+    if (buf == nullptr || buf_len == 0) return VP_ERR_ARG;
+    std::snprintf(buf, buf_len, "%s", g_err);
+    return VP_OK;
+}
+
+int64_t vp_launch_count(void) { return g_launches; }
+void vp_reset_launch_count(void) { g_launches = 0; }
+
+int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host, int dtype,
+                   vp_plan** out_plan) {
+    if (out_plan == nullptr) return set_err(VP_ERR_ARG, "out_plan must not be NULL");
+    *out_plan = nullptr;
+    if (mesh == nullptr || f_eq_host == nullptr || mesh->xs == nullptr || mesh->vs == nullptr)
+        return set_err(VP_ERR_ARG, "mesh, mesh->xs, mesh->vs and f_eq must not be NULL");
+    const int nx = mesh->nx, nv = mesh->nv;
+    if (nx < 2 || nv < 2) return set_err(VP_ERR_ARG, "nx and nv must be >= 2 (got %d, %d)", nx, nv);
+    if ((long long)nx * nv > (1LL << 31) - 1)
+        return set_err(VP_ERR_ARG, "nx*nv = %lld exceeds 2^31-1 cells", (long long)nx * nv);
+    if (!(mesh->dx > 0) || !(mesh->dv > 0) || !std::isfinite(mesh->dx) || !std::isfinite(mesh->dv))
+        return set_err(VP_ERR_ARG, "dx and dv must be finite and positive");
+    if (!(mesh->period_x > 0) || !(mesh->period_v > 0))
+        return set_err(VP_ERR_ARG, "period_x and period_v must be positive");
+    if (!std::isfinite(dt)) return set_err(VP_ERR_ARG, "dt must be finite");
+    if (dtype != VP_F32 && dtype != VP_F64) return set_err(VP_ERR_ARG, "dtype must be VP_F32 or VP_F64");
+    for (int j = 0; j < nv; ++j)
+        if (!std::isfinite(mesh->vs[j])) return set_err(VP_ERR_ARG, "vs[%d] is not finite", j);
+
+    vp_plan* p = new (std::nothrow) vp_plan();
+    if (!p) return set_err(VP_ERR_ARG, "out of host memory");
+    p->nx = nx;
+    p->nv = nv;
+    p->dtype = dtype;
+    p->dx = mesh->dx;
+    p->dv = mesh->dv;
+    p->dt = dt;
+    p->period_x = mesh->period_x;
+    p->period_v = mesh->period_v;
+    cudaError_t ce = cudaGetDevice(&p->device);
+    if (ce != cudaSuccess) {
+        delete p;
+        return cuda_err(ce, "cudaGetDevice");
+    }
+    int n_sms = 148;
+    cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, p->device);
+
+    // f_eq: x-invariant when every row equals the first one exactly
+    bool inv = true;
+    for (int i = 1; i < nx && inv; ++i)
+        inv = std::memcmp(f_eq_host + (size_t)i * nv, f_eq_host, (size_t)nv * sizeof(double)) == 0;
+    p->feq2d = inv ? 0 : 1;
+
+    // x half-step table: s_j = 0.5*v_j*dt/dx, m_j = floor(-s_j) mod nx, t_j = -s_j - floor(-s_j)
+    std::vector<int> mx(nv);
+    std::vector<double> tx(nv);
+    for (int j = 0; j < nv; ++j) {
+        const double sj = 0.5 * mesh->vs[j] * dt / mesh->dx;
+        const double mf = std::floor(-sj);
+        tx[j] = -sj - mf;
+        long long mi = (long long)mf % nx;
+        if (mi < 0) mi += nx;
+        mx[j] = (int)mi;
+    }
+
+    // Poisson: multiplier of fft_inv_multiplier (poisson.py:34-45): m_k = -1/(i*2*pi*f_k) = i/(2*pi*f_k)
+    p->pow2 = (nx & (nx - 1)) == 0;
+    p->log2nx = 0;
+    while ((1 << p->log2nx) < nx) ++p->log2nx;
+    std::vector<double> mult_im(nx, 0.0);
+    {
+        const double d = mesh->period_x / nx;
+        const double val = 1.0 / (nx * d);
+        const int npos = (nx - 1) / 2 + 1;
+        for (int k = 1; k < nx; ++k) {
+            const double kk = k < npos ? (double)k : (double)(k - nx);
+            const double f = kk * val;
+            mult_im[k] = 1.0 / ((2.0 * M_PI) * f);
+        }
+    }
+    std::vector<double> tw;  // interleaved (re, im)
+    if (p->pow2) {
+        tw.resize((size_t)std::max(1, nx / 2) * 2);
+        for (int q = 0; q < nx / 2; ++q) {
+            const double ang = 2.0 * M_PI * (double)q / (double)nx;
+            tw[2 * q] = std::cos(ang);
+            tw[2 * q + 1] = -std::sin(ang);
+        }
+    }
+    // circulant kernel c = real(ifft(m)): c[k] = -(1/nx) * sum_q mult_im[q] * sin(2*pi*q*k/nx)
+    std::vector<double> circ(nx, 0.0);
+    if (!p->pow2) {
+        for (int k = 0; k < nx; ++k) {
+            double s = 0.0;
+            for (int q = 0; q < nx; ++q) {
+                const long long r = ((long long)q * k) % nx;
+                s += mult_im[q] * std::sin(2.0 * M_PI * (double)r / (double)nx);
+            }
+            circ[k] = -s / nx;
+        }
+    }
+    const size_t rs = dtype == VP_F64 ? 8 : 4;
+    p->use_smem_poisson = poisson_smem_bytes(nx, rs) <= 24 * 1024 ? 1 : 0;
+    p->cfg = choose_cfg(nx, nv, n_sms);
+    p->cfg.smem = fused_smem(p, p->cfg.R);
+
+    int rc = VP_OK;
+    const size_t feq_count = inv ? (size_t)nv : (size_t)nx * nv;
+    std::vector<double> vs(mesh->vs, mesh->vs + nv);
+    if ((rc = upload_bytes((void**)&p->d_feq, f_eq_host, feq_count * sizeof(double))) ||
+        (rc = upload_bytes((void**)&p->d_vs, vs.data(), nv * sizeof(double))) ||
+        (rc = upload_bytes((void**)&p->d_mx, mx.data(), nv * sizeof(int))) ||
+        (rc = upload_bytes((void**)&p->d_tx64, tx.data(), nv * sizeof(double)))) {
+        free_plan(p);
+        return rc;
+    }
+    if (dtype == VP_F64) {
+        rc = upload<double>(&p->d_tx, tx);
+        if (!rc) rc = upload<double>(&p->d_tw, tw);
+        if (!rc) rc = upload<double>(&p->d_mult, mult_im);
+        if (!rc) rc = upload<double>(&p->d_circ, circ);
+    } else {
+        rc = upload<float>(&p->d_tx, tx);
+        if (!rc) rc = upload<float>(&p->d_tw, tw);
+        if (!rc) rc = upload<float>(&p->d_mult, mult_im);
+        if (!rc) rc = upload<float>(&p->d_circ, circ);
+    }
+    if (rc) {
+        free_plan(p);
+        return rc;
+    }
+    *out_plan = p;
+    return VP_OK;
+}
+
+int vp_plan_destroy(vp_plan* plan) {
+    free_plan(plan);
+    return VP_OK;
+}
+
+int vp_num_steps(const vp_plan* plan, double t_final, int32_t* out_steps) {
+    if (!plan || !out_steps) return set_err(VP_ERR_ARG, "plan and out_steps must not be NULL");
+    const double r = t_final / plan->dt;
+    if (!std::isfinite(r) || r > 2147483647.0 || r < -2147483648.0)
+        return set_err(VP_ERR_ARG, "t_final/dt = %g is out of range", r);
+    *out_steps = (int32_t)r;  // C truncation == Python int() for finite values
+    return VP_OK;
+}
+
+int vp_resolve_checkpoint_every(const vp_plan* plan, int32_t n_steps, int32_t every,
+                                int32_t* out_every) {
+    if (!plan || !out_every) return set_err(VP_ERR_ARG, "plan and out_every must not be NULL");
+    if (n_steps < 0) return set_err(VP_ERR_ARG, "n_steps must be >= 0");
+    *out_every = resolve_every(n_steps, every);
+    return VP_OK;
+}
+
+int vp_workspace_bytes(const vp_plan* plan, int32_t n_steps, int32_t every, size_t* out_bytes) {
+    if (!plan || !out_bytes) return set_err(VP_ERR_ARG, "plan and out_bytes must not be NULL");
+    if (n_steps < 0) return set_err(VP_ERR_ARG, "n_steps must be >= 0");
+    *out_bytes = ws_layout(plan, n_steps, every).total;
+    return VP_OK;
+}
+
+int vp_tape_bytes(const vp_plan* plan, int32_t n_steps, int32_t every, size_t* out_bytes) {
+    if (!plan || !out_bytes) return set_err(VP_ERR_ARG, "plan and out_bytes must not be NULL");
+    if (n_steps < 0) return set_err(VP_ERR_ARG, "n_steps must be >= 0");
+    *out_bytes = tape_layout(plan, n_steps, every).total;
+    return VP_OK;
+}
+
+static int check_ws(vp_plan* plan, int32_t n_steps, int32_t every, void* ws, size_t ws_bytes) {
+    size_t need = ws_layout(plan, n_steps, every).total;
+    if (ws_bytes < need)
+        return set_err(VP_ERR_ARG, "workspace has %zu bytes, %zu needed", ws_bytes, need);
+    if (((uintptr_t)ws & 255) != 0) return set_err(VP_ERR_ARG, "workspace must be 256-byte aligned");
+    return check_dev_ptr(ws, "workspace", plan->device);
+}
+
+int vp_forward(vp_plan* plan, const double* f_iv, const void* H, int32_t n_steps, double* f_final,
+               void* f_hist, void* E_hist, void* ee_hist, void* tape, int32_t every,
+               void* workspace, size_t workspace_bytes, void* stream) {
+    if (!plan) return set_err(VP_ERR_ARG, "plan must not be NULL");
+    if (n_steps < 0) return set_err(VP_ERR_ARG, "n_steps must be >= 0 (got %d)", n_steps);
+    int rc;
+    const int dev = plan->device;
+    if ((rc = check_dev_ptr(f_iv, "f_iv", dev)) || (rc = check_opt_ptr(f_final, "f_final", dev)))
+        return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t nxnv = (size_t)plan->nx * plan->nv;
+    if (n_steps == 0) {
+        if (f_final)
+            VP_CUDA(cudaMemcpyAsync(f_final, f_iv, nxnv * sizeof(double), cudaMemcpyDeviceToDevice, s),
+                    "cudaMemcpyAsync(f_final)");
+        return VP_OK;
+    }
+    if ((rc = check_dev_ptr(H, "H", dev)) || (rc = check_opt_ptr(f_hist, "f_hist", dev)) ||
+        (rc = check_opt_ptr(E_hist, "E_hist", dev)) || (rc = check_opt_ptr(ee_hist, "ee_hist", dev)) ||
+        (rc = check_opt_ptr(tape, "tape", dev)) ||
+        (rc = check_ws(plan, n_steps, every, workspace, workspace_bytes)))
+        return rc;
+    if (tape && ((uintptr_t)tape & 255) != 0) return set_err(VP_ERR_ARG, "tape must be 256-byte aligned");
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != dev) return set_err(VP_ERR_ARG, "current device %d differs from the plan's device %d", cur, dev);
+    unsigned char* ws = static_cast<unsigned char*>(workspace);
+    unsigned char* tp = static_cast<unsigned char*>(tape);
+    if (plan->dtype == VP_F64)
+        return forward_impl<double>(plan, f_iv, (const double*)H, n_steps, f_final, (double*)f_hist,
+                                    (double*)E_hist, (double*)ee_hist, tp, every, ws, s);
+    return forward_impl<float>(plan, f_iv, (const float*)H, n_steps, f_final, (float*)f_hist,
+                               (float*)E_hist, (float*)ee_hist, tp, every, ws, s);
+}
+
+int vp_backward(vp_plan* plan, const void* H, int32_t n_steps, const void* tape, int32_t every,
+                const void* g_f_final, const void* g_f_hist, const void* g_E_hist,
+                const void* g_ee_hist, void* g_f_iv, void* g_H, void* workspace,
+                size_t workspace_bytes, void* stream) {
+    if (!plan) return set_err(VP_ERR_ARG, "plan must not be NULL");
+    if (n_steps < 0) return set_err(VP_ERR_ARG, "n_steps must be >= 0 (got %d)", n_steps);
+    int rc;
+    const int dev = plan->device;
+    if ((rc = check_dev_ptr(g_f_iv, "g_f_iv", dev)) || (rc = check_dev_ptr(g_H, "g_H", dev)) ||
+        (rc = check_opt_ptr(g_f_final, "g_f_final", dev)))
+        return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t rsz = real_size(plan);
+    const size_t nxnv = (size_t)plan->nx * plan->nv;
+    if (n_steps == 0) {
+        if (g_f_final)
+            VP_CUDA(cudaMemcpyAsync(g_f_iv, g_f_final, nxnv * rsz, cudaMemcpyDeviceToDevice, s), "copy g_f_iv");
+        else
+            VP_CUDA(cudaMemsetAsync(g_f_iv, 0, nxnv * rsz, s), "zero g_f_iv");
+        VP_CUDA(cudaMemsetAsync(g_H, 0, (size_t)plan->nx * rsz, s), "zero g_H");
+        return VP_OK;
+    }
+    if ((rc = check_dev_ptr(H, "H", dev)) || (rc = check_dev_ptr(tape, "tape", dev)) ||
+        (rc = check_opt_ptr(g_f_hist, "g_f_hist", dev)) || (rc = check_opt_ptr(g_E_hist, "g_E_hist", dev)) ||
+        (rc = check_opt_ptr(g_ee_hist, "g_ee_hist", dev)) ||
+        (rc = check_ws(plan, n_steps, every, workspace, workspace_bytes)))
+        return rc;
+    if (((uintptr_t)tape & 255) != 0) return set_err(VP_ERR_ARG, "tape must be 256-byte aligned");
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != dev) return set_err(VP_ERR_ARG, "current device %d differs from the plan's device %d", cur, dev);
+    unsigned char* ws = static_cast<unsigned char*>(workspace);
+    const unsigned char* tp = static_cast<const unsigned char*>(tape);
+    if (plan->dtype == VP_F64)
+        return backward_impl<double>(plan, (const double*)H, n_steps, tp, every, (const double*)g_f_final,
+                                     (const double*)g_f_hist, (const double*)g_E_hist,
+                                     (const double*)g_ee_hist, (double*)g_f_iv, (double*)g_H, ws, s);
+    return backward_impl<float>(plan, (const float*)H, n_steps, tp, every, (const float*)g_f_final,
+                                (const float*)g_f_hist, (const float*)g_E_hist, (const float*)g_ee_hist,
+                                (float*)g_f_iv, (float*)g_H, ws, s);
+}
+
+int vp_compute_rho(vp_plan* plan, const double* f, void* rho, void* stream) {
+    if (!plan) return set_err(VP_ERR_ARG, "plan must not be NULL");
+    int rc;
+    if ((rc = check_dev_ptr(f, "f", plan->device)) || (rc = check_dev_ptr(rho, "rho", plan->device))) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int rs = plan->feq2d ? plan->nv : 0;
+    cudaError_t e = plan->dtype == VP_F64
+                        ? launch_compute_rho<double>(plan->nx, plan->nv, f, plan->d_feq, rs, plan->dv, (double*)rho, s)
+                        : launch_compute_rho<float>(plan->nx, plan->nv, f, plan->d_feq, rs, plan->dv, (float*)rho, s);
+    return e == cudaSuccess ? VP_OK : cuda_err(e, "compute_rho launch");
+}
+
+int vp_poisson(vp_plan* plan, const void* in, void* out, int adjoint, void* stream) {
+    if (!plan) return set_err(VP_ERR_ARG, "plan must not be NULL");
+    int rc;
+    if ((rc = check_dev_ptr(in, "in", plan->device)) || (rc = check_dev_ptr(out, "out", plan->device))) return rc;
+    if (!plan->use_smem_poisson)
+        return set_err(VP_ERR_UNSUPPORTED, "standalone Poisson solve supports nx up to the shared-memory limit; "
+                                           "nx=%d uses the fused path's global scratch", plan->nx);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e;
+    if (plan->dtype == VP_F64)
+        e = launch_poisson<double>(poisson_tables<double>(plan, nullptr, nullptr), (const double*)in, (double*)out, adjoint, s);
+    else
+        e = launch_poisson<float>(poisson_tables<float>(plan, nullptr, nullptr), (const float*)in, (float*)out, adjoint, s);
+    return e == cudaSuccess ? VP_OK : cuda_err(e, "poisson launch");
+}
+
+int vp_electric_energy(vp_plan* plan, const void* E, void* ee, void* stream) {
+    if (!plan) return set_err(VP_ERR_ARG, "plan must not be NULL");
+    int rc;
+    if ((rc = check_dev_ptr(E, "E", plan->device)) || (rc = check_dev_ptr(ee, "ee", plan->device))) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e = plan->dtype == VP_F64
+                        ? launch_electric_energy<double>(plan->nx, plan->dx, (const double*)E, (double*)ee, s)
+                        : launch_electric_energy<float>(plan->nx, plan->dx, (const float*)E, (float*)ee, s);
+    return e == cudaSuccess ? VP_OK : cuda_err(e, "electric energy launch");
+}
+
+int vp_semilag_x(vp_plan* plan, const void* in, void* out, double dt, int adjoint, void* stream) {
+    if (!plan) return set_err(VP_ERR_ARG, "plan must not be NULL");
+    if (!std::isfinite(dt)) return set_err(VP_ERR_ARG, "dt must be finite");
+    int rc;
+    if ((rc = check_dev_ptr(in, "in", plan->device)) || (rc = check_dev_ptr(out, "out", plan->device))) return rc;
+    if (in == out) return set_err(VP_ERR_ARG, "in and out must not alias");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e = plan->dtype == VP_F64
+                        ? launch_semilag_x<double>(plan->nx, plan->nv, plan->d_vs, plan->dx, dt, (const double*)in, (double*)out, adjoint, s)
+                        : launch_semilag_x<float>(plan->nx, plan->nv, plan->d_vs, plan->dx, dt, (const float*)in, (float*)out, adjoint, s);
+    return e == cudaSuccess ? VP_OK : cuda_err(e, "semilag_x launch");
+}
+
+int vp_semilag_v(vp_plan* plan, const void* in, const void* E_total, void* out, double dt,
+                 int adjoint, const void* f_in, void* g_E, void* stream) {
+    if (!plan) return set_err(VP_ERR_ARG, "plan must not be NULL");
+    if (!std::isfinite(dt)) return set_err(VP_ERR_ARG, "dt must be finite");
+    int rc;
+    const int dev = plan->device;
+    if ((rc = check_dev_ptr(in, "in", dev)) || (rc = check_dev_ptr(out, "out", dev)) ||
+        (rc = check_dev_ptr(E_total, "E_total", dev)) || (rc = check_opt_ptr(f_in, "f_in", dev)) ||
+        (rc = check_opt_ptr(g_E, "g_E", dev)))
+        return rc;
+    if (in == out) return set_err(VP_ERR_ARG, "in and out must not alias");
+    if ((g_E == nullptr) != (f_in == nullptr)) return set_err(VP_ERR_ARG, "f_in and g_E must be given together");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e = plan->dtype == VP_F64
+                        ? launch_semilag_v<double>(plan->nx, plan->nv, plan->dv, dt, (const double*)in, (const double*)E_total,
+                                                   (double*)out, adjoint, (const double*)f_in, (double*)g_E, s)
+                        : launch_semilag_v<float>(plan->nx, plan->nv, plan->dv, dt, (const float*)in, (const float*)E_total,
+                                                  (float*)out, adjoint, (const float*)f_in, (float*)g_E, s);
+    return e == cudaSuccess ? VP_OK : cuda_err(e, "semilag_v launch");
+}
+
+}  // extern "C"

@@ -1,0 +1,204 @@
+// Device helpers shared by the fused step kernels and the single-stage operators:
+// periodic index arithmetic, lerp, block reductions and the in-block radix-2 FFT Poisson solve.
+#pragma once
+
+#include "vp_internal.h"
+
+namespace vpb {
+
+__device__ __forceinline__ float vfloor(float x) { return floorf(x); }
+__device__ __forceinline__ double vfloor(double x) { return floor(x); }
+__device__ __forceinline__ float vabs(float x) { return fabsf(x); }
+__device__ __forceinline__ double vabs(double x) { return fabs(x); }
+
+template <typename T>
+__device__ __forceinline__ T lerp(T a, T b, T t) {
+    return (T(1) - t) * a + t * b;
+}
+
+// x in [0, 2n) -> [0, n)
+__device__ __forceinline__ int wrap1(int x, int n) { return x >= n ? x - n : x; }
+// x in [0, 3n) -> [0, n)
+__device__ __forceinline__ int wrap2(int x, int n) {
+    x = x >= n ? x - n : x;
+    return x >= n ? x - n : x;
+}
+// x in [-n, n) -> [0, n)
+__device__ __forceinline__ int wrapneg(int x, int n) { return x < 0 ? x + n : x; }
+
+// Trapezoid weight of index k in [0, n): 0.5 at both ends, 1 inside
+// (warp_vp_solver/kernels.py:167-172 and 192-197).
+template <typename T>
+__device__ __forceinline__ T trap_w(int k, int n) {
+    return (k == 0 || k == n - 1) ? T(0.5) : T(1);
+}
+
+// v-step shift of one row from the total field: s = E_total*dt/dv cells, m = floor(-s) reduced
+// mod nv, t = -s - floor(-s). This is the index-space form of the foot v_j - E_total*dt of
+// warp_vp_solver/kernels.py:150 and _periodic_indices (kernels.py:47-69).
+// A non-finite field gives m = 0 and a NaN weight: the NaN propagates into the results the way
+// it does in the reference, and every index stays in bounds.
+template <typename T>
+__device__ __forceinline__ VShift<T> make_vshift(T Et, T dtdv, int nv) {
+    const T s = Et * dtdv;
+    const T mf = vfloor(-s);
+    const T t = -s - mf;
+    int m = 0;
+    if (vabs(mf) < T(1.0e9)) {
+        long long r = ((long long)mf) % (long long)nv;
+        if (r < 0) r += nv;
+        m = (int)r;
+    }
+    VShift<T> v;
+    v.m = m;
+    v.t = t;
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sum over the block in a fixed order (deterministic). red: >= 32 elements of shared memory.
+template <typename T>
+__device__ T block_sum(T v, T* red) {
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+    __syncthreads();
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        T s = lane < nw ? red[lane] : T(0);
+        s = warp_sum(s);
+        if (lane == 0) red[0] = s;
+    }
+    __syncthreads();
+    return red[0];
+}
+
+// ---------------------------------------------------------------------------------------------
+// Poisson solve E = real(ifft(m * fft(rho))) (or its transpose with conj(m)) inside one CTA.
+// Power-of-two nx: iterative radix-2 decimation-in-time FFT on a complex buffer. The inverse
+// transform is a forward transform of the conjugated spectrum, so one twiddle table serves both.
+// Other nx: the equivalent real circulant product E_i = sum_k c[(i-k) mod nx] rho_k with
+// c = real(ifft(m)) (and c[(k-i) mod nx] for the transpose).
+// ---------------------------------------------------------------------------------------------
+
+template <typename C>
+__device__ __forceinline__ C cmake(decltype(C::x) a, decltype(C::x) b) {
+    C c;
+    c.x = a;
+    c.y = b;
+    return c;
+}
+
+__device__ __forceinline__ int bitrev(int i, int L) {
+    return L == 0 ? 0 : (int)(__brev((unsigned)i) >> (32 - L));
+}
+
+template <typename T>
+__device__ void fft_radix2(typename Cplx<T>::type* z, const typename Cplx<T>::type* tw, int n,
+                           int L) {
+    using C = typename Cplx<T>::type;
+    for (int s = 1; s <= L; ++s) {
+        const int half = 1 << (s - 1);
+        const int stride = n >> s;
+        for (int b = threadIdx.x; b < (n >> 1); b += blockDim.x) {
+            const int k = b & (half - 1);
+            const int i0 = ((b >> (s - 1)) << s) + k;
+            const int i1 = i0 + half;
+            const C w = tw[k * stride];
+            const C u = z[i0];
+            const C v = z[i1];
+            const T vr = v.x * w.x - v.y * w.y;
+            const T vi = v.x * w.y + v.y * w.x;
+            z[i0] = cmake<C>(u.x + vr, u.y + vi);
+            z[i1] = cmake<C>(u.x - vr, u.y - vi);
+        }
+        __syncthreads();
+    }
+}
+
+// x: nx reals (in/out). z: nx complex scratch. tw_s: nx/2 complex (may be a shared copy).
+// All threads of the block must call this. Ends with a __syncthreads().
+template <typename T>
+__device__ void poisson_block(const PoissonTables<T>& P, T* x, typename Cplx<T>::type* z,
+                              const typename Cplx<T>::type* tw_s, bool adjoint) {
+    using C = typename Cplx<T>::type;
+    const int nx = P.nx;
+    __syncthreads();
+    if (P.pow2) {
+        const int L = P.log2nx;
+        for (int i = threadIdx.x; i < nx; i += blockDim.x) z[bitrev(i, L)] = cmake<C>(x[i], T(0));
+        __syncthreads();
+        fft_radix2<T>(z, tw_s, nx, L);
+        const T sgn = adjoint ? T(-1) : T(1);
+        for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+            const int r = bitrev(i, L);
+            if (i <= r) {
+                const C a = z[i];
+                const C b = z[r];
+                const T mi = sgn * P.mult_im[i];
+                const T mr = sgn * P.mult_im[r];
+                // conj(m * z) with m purely imaginary: (0 + i*mi)(a.x + i*a.y) = (-mi*a.y, mi*a.x)
+                z[r] = cmake<C>(-mi * a.y, -mi * a.x);
+                z[i] = cmake<C>(-mr * b.y, -mr * b.x);
+            }
+        }
+        __syncthreads();
+        fft_radix2<T>(z, tw_s, nx, L);
+        const T scale = T(1) / T(nx);
+        for (int i = threadIdx.x; i < nx; i += blockDim.x) x[i] = z[i].x * scale;
+        __syncthreads();
+    } else {
+        for (int i = threadIdx.x; i < nx; i += blockDim.x) z[i].x = x[i];
+        __syncthreads();
+        for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+            T s = T(0);
+            for (int k = 0; k < nx; ++k) {
+                int d = adjoint ? (k - i) : (i - k);
+                d = wrapneg(d, nx);
+                s += P.circ[d] * z[k].x;
+            }
+            x[i] = s;
+        }
+        __syncthreads();
+    }
+}
+
+// Shared-memory layout of the Poisson work area: x (nx reals), z (nx complex), tw (nx/2 complex).
+template <typename T>
+struct PoissonSmem {
+    T* x;
+    typename Cplx<T>::type* z;
+    const typename Cplx<T>::type* tw;
+};
+
+template <typename T>
+__device__ PoissonSmem<T> poisson_workspace(const PoissonTables<T>& P, unsigned char* smem) {
+    using C = typename Cplx<T>::type;
+    PoissonSmem<T> w;
+    if (P.use_smem) {
+        C* z = reinterpret_cast<C*>(smem);
+        C* tw = z + P.nx;
+        T* x = reinterpret_cast<T*>(tw + (P.nx >> 1) + 1);
+        if (P.pow2) {
+            for (int i = threadIdx.x; i < (P.nx >> 1); i += blockDim.x) tw[i] = P.tw[i];
+        }
+        w.x = x;
+        w.z = z;
+        w.tw = tw;
+    } else {
+        C* z = reinterpret_cast<C*>(P.gscratch);
+        w.z = z;
+        w.x = P.gscratch + 2 * P.nx;
+        w.tw = P.tw;
+    }
+    return w;
+}
+
+}  // namespace vpb

@@ -1,0 +1,127 @@
+// Internal declarations shared by the host orchestration (vp_capi.cu) and the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include <string>
+
+namespace vpb {
+
+template <typename T> struct Cplx;
+template <> struct Cplx<float> { using type = float2; };
+template <> struct Cplx<double> { using type = double2; };
+
+// Per-row v-step shift: integer cell offset m (already reduced mod nv) and lerp weight t.
+template <typename T> struct alignas(2 * sizeof(T) >= 8 ? 2 * sizeof(T) : 8) VShift {
+    int m;
+    T t;
+};
+
+// Device tables of the Poisson solve for one nx.
+template <typename T> struct PoissonTables {
+    int nx;
+    int log2nx;        // valid when pow2
+    int pow2;
+    const typename Cplx<T>::type* tw;   // nx/2 twiddles exp(-2*pi*i*q/nx)        (pow2)
+    const T* mult_im;                   // imaginary part of the multiplier m_k   (pow2)
+    const T* circ;                      // c = real(ifft(m)): E = c (*) rho       (any nx)
+    T* gscratch;                        // 3*nx reals of global scratch, used when the shared
+                                        // buffer would exceed the dynamic shared-memory budget
+    int use_smem;
+};
+
+// Arguments of one fused forward launch (see vp_kernels.cu for the phase semantics).
+template <typename T> struct FwdArgs {
+    int nx, nv, n_chunks, chunk_cols;
+    const T* h_in;              // delta after the leading x half-step of step n
+    const double* f_iv;         // prologue only
+    T* h_out;                   // delta after the leading x half-step of step n+1 (or null)
+    const VShift<T>* vsh;       // v shifts of step n
+    const int* mx;              // x half-step offsets, reduced mod nx   [nv]
+    const T* tx;                // x half-step weights                   [nv]
+    const double* tx64;         // x half-step weights in float64        [nv]
+    const double* feq;          // f_eq (one row when feq_rs == 0)
+    int feq_rs;                 // f_eq row stride: 0 or nv
+    T* f_hist_n;                // f after step n, or null
+    double* f_final;            // f after the last step, or null
+    T* part;                    // rho partial sums [n_chunks][nx], or null (no tail)
+    unsigned* counter;
+    // tail (last CTA): Poisson for step n+1
+    PoissonTables<T> P;
+    T dv, dx, dtdv;
+    const T* H;
+    T* E_out;                   // raw E of step n+1
+    T* E_hist_out;              // E + H of step n+1, or null
+    T* ee_out;                  // ee of step n+1, or null
+    VShift<T>* vsh_out;         // v shifts of step n+1
+};
+
+// Arguments of one fused backward launch.
+template <typename T> struct BwdArgs {
+    int nx, nv, n_chunks, chunk_cols;
+    const T* w_in;              // cotangent on the v-step output of step n
+    const T* grho;              // cotangent on rho of step n
+    const VShift<T>* vsh_n;     // v shifts of step n
+    const T* gfh;               // cotangent on f_hist[n-1], or null
+    const T* c_src;             // prologue: cotangent on f_final, or null
+    const T* c_src2;            // prologue: cotangent on f_hist[T-1], or null
+    T* w_out;                   // cotangent on the v-step output of step n-1 (or null)
+    T* gfiv_out;                // epilogue: cotangent on f_iv
+    const T* h_prev;            // delta_half of step n-1
+    const VShift<T>* vsh_prev;  // v shifts of step n-1
+    const int* mx;
+    const T* tx;
+    const double* feq;
+    int feq_rs;
+    T* part;
+    unsigned* counter;
+    // tail
+    PoissonTables<T> P;
+    T dv, dx, neg_dt_dv;
+    const T* E_prev;            // raw E of step n-1
+    const T* gE_hist;           // cotangent on E_hist[n-1], or null
+    const T* gee;               // address of the cotangent on ee_hist[n-1], or null
+    T* gH;                      // accumulated cotangent on H
+    T* grho_out;                // cotangent on rho of step n-1
+};
+
+struct LaunchCfg {
+    int R;          // rows per CTA
+    int threads;    // threads per CTA (one column each)
+    int n_chunks;   // column chunks per row block
+    int chunk_cols; // columns per chunk
+    size_t smem;    // dynamic shared memory bytes
+};
+
+// Launchers (vp_kernels.cu). PHASE: 0 = prologue, 1 = step, 2 = epilogue (backward only).
+template <typename T>
+cudaError_t launch_fwd(const FwdArgs<T>& a, const LaunchCfg& c, int phase, bool feq2d,
+                       cudaStream_t s);
+template <typename T>
+cudaError_t launch_bwd(const BwdArgs<T>& a, const LaunchCfg& c, int phase, bool feq2d,
+                       cudaStream_t s);
+
+// Single-stage operators (vp_ops.cu).
+template <typename T>
+cudaError_t launch_compute_rho(int nx, int nv, const double* f, const double* feq, int feq_rs,
+                               double dv, T* rho, cudaStream_t s);
+template <typename T>
+cudaError_t launch_poisson(const PoissonTables<T>& P, const T* in, T* out, int adjoint,
+                           cudaStream_t s);
+template <typename T>
+cudaError_t launch_electric_energy(int nx, double dx, const T* E, T* ee, cudaStream_t s);
+template <typename T>
+cudaError_t launch_semilag_x(int nx, int nv, const double* vs, double dx, double dt,
+                             const T* in, T* out, int adjoint, cudaStream_t s);
+template <typename T>
+cudaError_t launch_semilag_v(int nx, int nv, double dv, double dt, const T* in,
+                             const T* E_total, T* out, int adjoint, const T* f_in, T* g_E,
+                             cudaStream_t s);
+
+size_t poisson_smem_bytes(int nx, size_t real_size);
+
+void count_launch(int n = 1);
+
+}  // namespace vpb

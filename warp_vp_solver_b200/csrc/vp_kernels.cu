@@ -1,0 +1,403 @@
+// Fused Strang-step kernels (forward and discrete adjoint) for sm_100a.
+//
+// Scheme (warp_vp_solver/solver.py:17-28, one step):
+//   f_half = X(f); rho = dv*trapz(f_eq - f_half); E = Poisson(rho); ee = 0.5*dx*trapz(E^2);
+//   f_one = V_{E+H}(f_half); f = X(f_one)
+// with X the periodic linear semi-Lagrangian half step along x (kernels.py:109-130) and V the
+// full step along v (kernels.py:133-153, 367-393).
+//
+// Representation. The state is delta = f - f_eq (float32 or float64). Each x half-step shifts
+// column j by a fixed s_j = 0.5*v_j*dt/dx cells (integer part m_j, weight t_j, precomputed on
+// the host in float64); the v step shifts row i by s_i = (E_i + H_i)*dt/dv cells. The pipeline
+// carries h_n = delta after the leading x half-step of step n (f_half - f_eq), so that one launch
+// per step reads h_n once and writes h_{n+1} once:
+//
+//   o  = V(h_n) + [V(f_eq) - f_eq]        rows around the block, per-row shift from E_n + H
+//   d  = X(o)   + [X(f_eq) - f_eq]        = f_{n+1} - f_eq      (history / final output)
+//   h' = X(d)   + [X(f_eq) - f_eq]        = h_{n+1}, and its row sums -> rho_{n+1}
+//
+// The f_eq corrections are formed in float64 from differences of f_eq and are exactly zero for
+// an x-invariant f_eq in the x direction.
+//
+// Thread mapping. A CTA owns R consecutive rows [r0, r0+R) and a chunk of columns; each thread
+// owns one column j at a time. Because the x shift of column j is one number, the rows column j
+// needs are a contiguous window offset by m_j: R+2 rows of o, R+1 rows of d, R rows of h'. The
+// windows live in registers with compile-time indices, so the two x half-steps need no shared
+// memory and no block barrier. The v step reads h_n straight from global memory (coalesced along
+// the row, each value reused by the neighbouring thread through L1).
+//
+// Step-global dependency. rho needs whole rows and E needs all of rho. Each CTA writes its rows'
+// partial sums; the last CTA to finish (threadfence + atomic counter, no spinning) reduces them
+// in a fixed order and runs the in-block FFT Poisson solve for the next step, writing E, E+H,
+// ee and the next v shifts. The next launch in the stream consumes them.
+//
+// The adjoint mirrors this with gathers instead of the reference's atomic scatters
+// (kernels.py:215-273): X^T g at row k is (1-t) g[k-m] + t g[k-m-1], V^T likewise along v, so
+// every output is written by exactly one thread and the result is bitwise reproducible.
+
+#include "vp_device.cuh"
+
+namespace vpb {
+
+template <typename T, bool FEQ2D>
+__device__ __forceinline__ double feq_at(const double* __restrict__ feq, int rs, int row, int col) {
+    return FEQ2D ? __ldg(feq + (size_t)row * rs + col) : __ldg(feq + col);
+}
+
+// V step of one cell: o[row, j] for the delta state h (plus the f_eq correction).
+template <typename T, bool FEQ2D>
+__device__ __forceinline__ T v_cell(const T* __restrict__ h, const double* __restrict__ feq,
+                                    int feq_rs, int nv, int row, int j, const VShift<T> s) {
+    int c0 = wrap1(j + s.m, nv);
+    int c1 = c0 + 1;
+    c1 = c1 == nv ? 0 : c1;
+    const T* hr = h + (size_t)row * nv;
+    const T a = __ldg(hr + c0);
+    const T b = __ldg(hr + c1);
+    T o = lerp(a, b, s.t);
+    const double fj = feq_at<T, FEQ2D>(feq, feq_rs, row, j);
+    const double f0 = feq_at<T, FEQ2D>(feq, feq_rs, row, c0) - fj;
+    const double f1 = feq_at<T, FEQ2D>(feq, feq_rs, row, c1) - fj;
+    const double tt = (double)s.t;
+    o += (T)((1.0 - tt) * f0 + tt * f1);
+    return o;
+}
+
+// X(f_eq) - f_eq at (row, j) for an x-dependent f_eq (zero otherwise).
+template <typename T, bool FEQ2D>
+__device__ __forceinline__ T x_corr(const double* __restrict__ feq, int feq_rs, int nx, int row,
+                                    int m, double t64, int j) {
+    if (!FEQ2D) return T(0);
+    int q0 = wrap1(row + m, nx);
+    int q1 = q0 + 1;
+    q1 = q1 == nx ? 0 : q1;
+    const double fj = __ldg(feq + (size_t)row * feq_rs + j);
+    const double a0 = __ldg(feq + (size_t)q0 * feq_rs + j) - fj;
+    const double a1 = __ldg(feq + (size_t)q1 * feq_rs + j) - fj;
+    return (T)((1.0 - t64) * a0 + t64 * a1);
+}
+
+// Reduce the R per-thread row accumulators over the block and store them as this chunk's
+// partial sums for rows [r0, r0+R).
+template <typename T, int R>
+__device__ __forceinline__ void store_row_partials(T (&acc)[R], T* red, T* part_row) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int e = 0; e < R; ++e) {
+        const T v = warp_sum(acc[e]);
+        if (lane == 0) red[wid * R + e] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < R) {
+        T s = T(0);
+        for (int w = 0; w < nw; ++w) s += red[w * R + threadIdx.x];
+        part_row[threadIdx.x] = s;
+    }
+}
+
+// Completion counter: returns true in every thread of the CTA that finished last.
+__device__ __forceinline__ bool last_cta_done(unsigned* counter, int* flag) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned total = gridDim.x * gridDim.y;
+        const unsigned prev = atomicAdd(counter, 1u);
+        *flag = (prev == total - 1) ? 1 : 0;
+    }
+    __syncthreads();
+    const bool last = *flag != 0;
+    if (last) __threadfence();
+    return last;
+}
+
+// ----------------------------------------------------------------------------------------------
+// Forward
+// PHASE 0 (prologue): h_0 = X(f_iv - f_eq) + Xcorr, rho_0, tail -> E_0.
+// PHASE 1 (step n):   h_n -> o -> d (= f_{n+1} - f_eq) -> [h_{n+1}, rho_{n+1}, tail -> E_{n+1}]
+//                     The bracket is skipped when h_out == null (last step). With part == null
+//                     the launch only propagates the state (segment recomputation in the adjoint).
+// ----------------------------------------------------------------------------------------------
+template <typename T, int R, bool FEQ2D, int PHASE>
+__global__ void __launch_bounds__(256) vp_fwd_kernel(const FwdArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    T* red = reinterpret_cast<T*>(smem);
+    __shared__ int s_last;
+
+    const int nx = a.nx, nv = a.nv;
+    const int r0 = blockIdx.x * R;
+    const int c_begin = blockIdx.y * a.chunk_cols;
+    const int c_end = min(nv, c_begin + a.chunk_cols);
+    const bool next = a.h_out != nullptr;
+
+    T acc[R];
+#pragma unroll
+    for (int e = 0; e < R; ++e) acc[e] = T(0);
+
+    for (int j = c_begin + (int)threadIdx.x; j < c_end; j += blockDim.x) {
+        const int m = __ldg(a.mx + j);
+        const T t = __ldg(a.tx + j);
+        const double t64 = FEQ2D ? __ldg(a.tx64 + j) : 0.0;
+        const T wj = trap_w<T>(j, nv);
+        T d[R + 1];
+        if (PHASE == 0) {
+            const int base = wrap1(r0 + m, nx);
+#pragma unroll
+            for (int k = 0; k < R + 1; ++k) {
+                const int row = wrap1(base + k, nx);
+                const double fv = __ldg(a.f_iv + (size_t)row * nv + j);
+                d[k] = (T)(fv - feq_at<T, FEQ2D>(a.feq, a.feq_rs, row, j));
+            }
+        } else {
+            const int base = wrap2(r0 + 2 * m, nx);
+            T o[R + 2];
+#pragma unroll
+            for (int k = 0; k < R + 2; ++k) {
+                const int row = wrap1(base + k, nx);
+                const VShift<T> vs = a.vsh[row];
+                o[k] = v_cell<T, FEQ2D>(a.h_in, a.feq, a.feq_rs, nv, row, j, vs);
+            }
+            const int dbase = wrap1(r0 + m, nx);
+#pragma unroll
+            for (int k = 0; k < R + 1; ++k) {
+                d[k] = lerp(o[k], o[k + 1], t);
+                if (FEQ2D) d[k] += x_corr<T, FEQ2D>(a.feq, a.feq_rs, nx, wrap1(dbase + k, nx), m, t64, j);
+            }
+            if (a.f_hist_n != nullptr || a.f_final != nullptr) {
+#pragma unroll
+                for (int k = 0; k < R; ++k) {
+                    const int row = wrap1(dbase + k, nx);
+                    const double f = feq_at<T, FEQ2D>(a.feq, a.feq_rs, row, j) + (double)d[k];
+                    if (a.f_hist_n != nullptr) a.f_hist_n[(size_t)row * nv + j] = (T)f;
+                    if (a.f_final != nullptr) a.f_final[(size_t)row * nv + j] = f;
+                }
+            }
+        }
+        if (PHASE == 0 || next) {
+#pragma unroll
+            for (int e = 0; e < R; ++e) {
+                T hv = lerp(d[e], d[e + 1], t);
+                if (FEQ2D) hv += x_corr<T, FEQ2D>(a.feq, a.feq_rs, nx, r0 + e, m, t64, j);
+                a.h_out[(size_t)(r0 + e) * nv + j] = hv;
+                acc[e] += wj * hv;
+            }
+        }
+    }
+
+    if (a.part == nullptr || (PHASE != 0 && !next)) return;
+    store_row_partials<T, R>(acc, red, a.part + (size_t)blockIdx.y * nx + r0);
+
+    if (!last_cta_done(a.counter, &s_last)) return;
+
+    // ---- tail: rho -> E, ee, E + H, next v shifts ----
+    const size_t red_bytes = (size_t)32 * R * sizeof(T);
+    PoissonSmem<T> w = poisson_workspace<T>(a.P, smem + ((red_bytes + 15) & ~(size_t)15));
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        T s = T(0);
+        for (int c = 0; c < a.n_chunks; ++c) s += __ldcg(a.part + (size_t)c * nx + i);
+        w.x[i] = -a.dv * s;
+    }
+    poisson_block<T>(a.P, w.x, w.z, w.tw, false);
+    T e2 = T(0);
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        const T E = w.x[i];
+        e2 += trap_w<T>(i, nx) * E * E;
+        const T Et = E + __ldg(a.H + i);
+        a.E_out[i] = E;
+        if (a.E_hist_out != nullptr) a.E_hist_out[i] = Et;
+        a.vsh_out[i] = make_vshift<T>(Et, a.dtdv, nv);
+    }
+    const T tot = block_sum<T>(e2, red);
+    if (threadIdx.x == 0) {
+        if (a.ee_out != nullptr) *a.ee_out = T(0.5) * tot * a.dx;
+        *a.counter = 0u;
+    }
+}
+
+// ----------------------------------------------------------------------------------------------
+// Backward (discrete adjoint, warp_vp_solver/solver.py:814-929 per step)
+// PHASE 0 (n = T):   c = g_f_final + g_f_hist[T-1]; w_{T-1} = X^T c; row sums for g_E_total.
+// PHASE 1 (n >= 1):  gh = V^T w_n + rho^T grho_n; c = X^T gh (+ g_f_hist[n-1]); w_{n-1} = X^T c.
+// PHASE 2 (n = 0):   g_f_iv = X^T (V^T w_0 + rho^T grho_0).
+// Tail (phases 0, 1), for step n-1: g_E_total = -dt/dv * sum_j slope*w + g_E_hist; g_H += g_E_total;
+// g_E = g_E_total + ee^T; grho_{n-1} = Poisson^T g_E.
+// ----------------------------------------------------------------------------------------------
+template <typename T, int R, bool FEQ2D, int PHASE>
+__global__ void __launch_bounds__(256) vp_bwd_kernel(const BwdArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    T* red = reinterpret_cast<T*>(smem);
+    __shared__ int s_last;
+
+    const int nx = a.nx, nv = a.nv;
+    const int r0 = blockIdx.x * R;
+    const int c_begin = blockIdx.y * a.chunk_cols;
+    const int c_end = min(nv, c_begin + a.chunk_cols);
+
+    T acc[R];
+#pragma unroll
+    for (int e = 0; e < R; ++e) acc[e] = T(0);
+
+    for (int j = c_begin + (int)threadIdx.x; j < c_end; j += blockDim.x) {
+        const int m = __ldg(a.mx + j);
+        const T t = __ldg(a.tx + j);
+        const T wr = -a.dv * trap_w<T>(j, nv);   // rho^T weight (kernels.py:292-299)
+        if (PHASE == 2) {
+            // gh rows r0 - m - 1 + k, k in [0, R+1); out rows r0 + e
+            int base = (r0 - m - 1) % nx;
+            base = wrapneg(base, nx);
+            T gh[R + 1];
+#pragma unroll
+            for (int k = 0; k < R + 1; ++k) {
+                const int row = wrap1(base + k, nx);
+                const VShift<T> vs = a.vsh_n[row];
+                int c0 = wrapneg(j - vs.m, nv);
+                int c1 = wrapneg(c0 - 1, nv);
+                const T* wrow = a.w_in + (size_t)row * nv;
+                gh[k] = lerp(__ldg(wrow + c0), __ldg(wrow + c1), vs.t) + wr * __ldg(a.grho + row);
+            }
+#pragma unroll
+            for (int e = 0; e < R; ++e) {
+                a.gfiv_out[(size_t)(r0 + e) * nv + j] = lerp(gh[e + 1], gh[e], t);
+            }
+            continue;
+        }
+        // c rows r0 - m - 1 + k, k in [0, R+1)
+        int cbase = (r0 - m - 1) % nx;
+        cbase = wrapneg(cbase, nx);
+        T c[R + 1];
+        if (PHASE == 0) {
+#pragma unroll
+            for (int k = 0; k < R + 1; ++k) {
+                const int row = wrap1(cbase + k, nx);
+                T v = T(0);
+                if (a.c_src != nullptr) v += __ldg(a.c_src + (size_t)row * nv + j);
+                if (a.c_src2 != nullptr) v += __ldg(a.c_src2 + (size_t)row * nv + j);
+                c[k] = v;
+            }
+        } else {
+            // gh rows r0 - 2m - 2 + k, k in [0, R+2)
+            int base = (r0 - 2 * m - 2) % nx;
+            base = wrapneg(base, nx);
+            T gh[R + 2];
+#pragma unroll
+            for (int k = 0; k < R + 2; ++k) {
+                const int row = wrap1(base + k, nx);
+                const VShift<T> vs = a.vsh_n[row];
+                int c0 = wrapneg(j - vs.m, nv);
+                int c1 = wrapneg(c0 - 1, nv);
+                const T* wrow = a.w_in + (size_t)row * nv;
+                gh[k] = lerp(__ldg(wrow + c0), __ldg(wrow + c1), vs.t) + wr * __ldg(a.grho + row);
+            }
+#pragma unroll
+            for (int k = 0; k < R + 1; ++k) {
+                c[k] = lerp(gh[k + 1], gh[k], t);
+                if (a.gfh != nullptr) c[k] += __ldg(a.gfh + (size_t)wrap1(cbase + k, nx) * nv + j);
+            }
+        }
+        // w rows r0 + e, and the slope reduction for g_E_total of step n-1
+#pragma unroll
+        for (int e = 0; e < R; ++e) {
+            const T wv = lerp(c[e + 1], c[e], t);
+            const int row = r0 + e;
+            a.w_out[(size_t)row * nv + j] = wv;
+            const VShift<T> vp = a.vsh_prev[row];
+            const int d0 = wrap1(j + vp.m, nv);
+            int d1 = d0 + 1;
+            d1 = d1 == nv ? 0 : d1;
+            const T* hr = a.h_prev + (size_t)row * nv;
+            const T sl = (__ldg(hr + d1) - __ldg(hr + d0)) +
+                         (T)(feq_at<T, FEQ2D>(a.feq, a.feq_rs, row, d1) -
+                             feq_at<T, FEQ2D>(a.feq, a.feq_rs, row, d0));
+            acc[e] += sl * wv;
+        }
+    }
+
+    if (PHASE == 2) return;
+    store_row_partials<T, R>(acc, red, a.part + (size_t)blockIdx.y * nx + r0);
+    if (!last_cta_done(a.counter, &s_last)) return;
+
+    // ---- tail for step n-1 ----
+    const size_t red_bytes = (size_t)32 * R * sizeof(T);
+    PoissonSmem<T> w = poisson_workspace<T>(a.P, smem + ((red_bytes + 15) & ~(size_t)15));
+    const T gee = a.gee != nullptr ? *a.gee : T(0);
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        T s = T(0);
+        for (int c = 0; c < a.n_chunks; ++c) s += __ldcg(a.part + (size_t)c * nx + i);
+        T gEt = a.neg_dt_dv * s;
+        if (a.gE_hist != nullptr) gEt += __ldg(a.gE_hist + i);
+        a.gH[i] += gEt;
+        // ee^T (kernels.py:302-322): dx * w_i * E_i * g_ee
+        w.x[i] = gEt + a.dx * trap_w<T>(i, nx) * __ldg(a.E_prev + i) * gee;
+    }
+    poisson_block<T>(a.P, w.x, w.z, w.tw, true);
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) a.grho_out[i] = w.x[i];
+    if (threadIdx.x == 0) *a.counter = 0u;
+}
+
+// ----------------------------------------------------------------------------------------------
+// Launchers
+// ----------------------------------------------------------------------------------------------
+
+template <typename T, int R, bool F2>
+static cudaError_t fwd_dispatch_phase(const FwdArgs<T>& a, const LaunchCfg& c, int phase,
+                                      cudaStream_t s) {
+    dim3 grid(a.nx / R, c.n_chunks);
+    if (phase == 0)
+        vp_fwd_kernel<T, R, F2, 0><<<grid, c.threads, c.smem, s>>>(a);
+    else
+        vp_fwd_kernel<T, R, F2, 1><<<grid, c.threads, c.smem, s>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename T, int R, bool F2>
+static cudaError_t bwd_dispatch_phase(const BwdArgs<T>& a, const LaunchCfg& c, int phase,
+                                      cudaStream_t s) {
+    dim3 grid(a.nx / R, c.n_chunks);
+    if (phase == 0)
+        vp_bwd_kernel<T, R, F2, 0><<<grid, c.threads, c.smem, s>>>(a);
+    else if (phase == 1)
+        vp_bwd_kernel<T, R, F2, 1><<<grid, c.threads, c.smem, s>>>(a);
+    else
+        vp_bwd_kernel<T, R, F2, 2><<<grid, c.threads, c.smem, s>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+#define VP_R_SWITCH(FN, ...)                                              \
+    switch (c.R) {                                                        \
+        case 1: return FN<T, 1, F2>(__VA_ARGS__);                         \
+        case 2: return FN<T, 2, F2>(__VA_ARGS__);                         \
+        case 4: return FN<T, 4, F2>(__VA_ARGS__);                         \
+        case 8: return FN<T, 8, F2>(__VA_ARGS__);                         \
+        case 16: return FN<T, 16, F2>(__VA_ARGS__);                       \
+        default: return cudaErrorInvalidValue;                            \
+    }
+
+template <typename T, bool F2>
+static cudaError_t fwd_r(const FwdArgs<T>& a, const LaunchCfg& c, int phase, cudaStream_t s) {
+    VP_R_SWITCH(fwd_dispatch_phase, a, c, phase, s)
+}
+template <typename T, bool F2>
+static cudaError_t bwd_r(const BwdArgs<T>& a, const LaunchCfg& c, int phase, cudaStream_t s) {
+    VP_R_SWITCH(bwd_dispatch_phase, a, c, phase, s)
+}
+
+template <typename T>
+cudaError_t launch_fwd(const FwdArgs<T>& a, const LaunchCfg& c, int phase, bool feq2d,
+                       cudaStream_t s) {
+    return feq2d ? fwd_r<T, true>(a, c, phase, s) : fwd_r<T, false>(a, c, phase, s);
+}
+
+template <typename T>
+cudaError_t launch_bwd(const BwdArgs<T>& a, const LaunchCfg& c, int phase, bool feq2d,
+                       cudaStream_t s) {
+    return feq2d ? bwd_r<T, true>(a, c, phase, s) : bwd_r<T, false>(a, c, phase, s);
+}
+
+template cudaError_t launch_fwd<float>(const FwdArgs<float>&, const LaunchCfg&, int, bool, cudaStream_t);
+template cudaError_t launch_fwd<double>(const FwdArgs<double>&, const LaunchCfg&, int, bool, cudaStream_t);
+template cudaError_t launch_bwd<float>(const BwdArgs<float>&, const LaunchCfg&, int, bool, cudaStream_t);
+template cudaError_t launch_bwd<double>(const BwdArgs<double>&, const LaunchCfg&, int, bool, cudaStream_t);
+
+}  // namespace vpb

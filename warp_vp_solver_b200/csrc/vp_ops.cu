@@ -1,0 +1,176 @@
+// Single-stage operators: the building blocks of the step exposed on their own, as the
+// reference exposes its kernels and helper methods (warp_vp_solver/kernels.py,
+// warp_vp_solver/solver.py:393-412, warp_vp_solver/poisson.py:48-99). They share the index
+// arithmetic and the in-block FFT with the fused kernels in vp_kernels.cu.
+
+#include "vp_device.cuh"
+
+namespace vpb {
+
+size_t poisson_smem_bytes(int nx, size_t real_size) {
+    const size_t c = 2 * real_size;
+    return (size_t)nx * c + (size_t)((nx >> 1) + 1) * c + (size_t)nx * real_size;
+}
+
+// rho[i] = dv * trapz_j(f_eq[i,j] - f[i,j]), accumulated in float64 (one CTA per row).
+template <typename T>
+__global__ void __launch_bounds__(256) rho_kernel(int nv, const double* __restrict__ f,
+                                                  const double* __restrict__ feq, int feq_rs,
+                                                  double dv, T* __restrict__ rho) {
+    __shared__ double red[32];
+    const int i = blockIdx.x;
+    double s = 0.0;
+    for (int j = threadIdx.x; j < nv; j += blockDim.x) {
+        const double d = feq[(size_t)i * feq_rs + j] - f[(size_t)i * nv + j];
+        s += trap_w<double>(j, nv) * d;
+    }
+    s = block_sum<double>(s, red);
+    if (threadIdx.x == 0) rho[i] = (T)(s * dv);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024) poisson_kernel(const PoissonTables<T> P, const T* in,
+                                                      T* out, int adjoint) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    PoissonSmem<T> w = poisson_workspace<T>(P, smem);
+    for (int i = threadIdx.x; i < P.nx; i += blockDim.x) w.x[i] = in[i];
+    poisson_block<T>(P, w.x, w.z, w.tw, adjoint != 0);
+    for (int i = threadIdx.x; i < P.nx; i += blockDim.x) out[i] = w.x[i];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) ee_kernel(int nx, double dx, const T* E, T* ee) {
+    __shared__ double red[32];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        const double e = (double)E[i];
+        s += trap_w<double>(i, nx) * e * e;
+    }
+    s = block_sum<double>(s, red);
+    if (threadIdx.x == 0) *ee = (T)(0.5 * s * dx);
+}
+
+// x half-step by dt/2 (or its transpose) of an arbitrary array, shift computed per column in
+// float64: s = 0.5*v_j*dt/dx (warp_vp_solver/kernels.py:127).
+template <typename T>
+__global__ void __launch_bounds__(256) semilag_x_kernel(int nx, int nv, const double* __restrict__ vs,
+                                                        double dx, double dt, const T* __restrict__ in,
+                                                        T* __restrict__ out, int adjoint) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y;
+    if (j >= nv) return;
+    const double s = 0.5 * vs[j] * dt / dx;
+    const double mf = floor(-s);
+    const T t = (T)(-s - mf);
+    long long mm = ((long long)mf) % nx;
+    if (mm < 0) mm += nx;
+    const int m = (int)mm;
+    if (!adjoint) {
+        const int q0 = wrap1(i + m, nx);
+        const int q1 = wrap1(q0 + 1, nx);
+        out[(size_t)i * nv + j] = lerp(in[(size_t)q0 * nv + j], in[(size_t)q1 * nv + j], t);
+    } else {
+        const int q0 = wrapneg(i - m, nx);
+        const int q1 = wrapneg(q0 - 1, nx);
+        out[(size_t)i * nv + j] = lerp(in[(size_t)q0 * nv + j], in[(size_t)q1 * nv + j], t);
+    }
+}
+
+// v step (or its transpose plus the field cotangent) of an arbitrary array, one CTA per row.
+template <typename T>
+__global__ void __launch_bounds__(256) semilag_v_kernel(int nv, T dtdv, const T* __restrict__ in,
+                                                        const T* __restrict__ Et,
+                                                        T* __restrict__ out, int adjoint,
+                                                        const T* __restrict__ f_in,
+                                                        T* __restrict__ g_E) {
+    __shared__ T red[32];
+    const int i = blockIdx.x;
+    const VShift<T> vs = make_vshift<T>(Et[i], dtdv, nv);
+    const T* row = in + (size_t)i * nv;
+    T acc = T(0);
+    for (int j = threadIdx.x; j < nv; j += blockDim.x) {
+        if (!adjoint) {
+            const int c0 = wrap1(j + vs.m, nv);
+            const int c1 = wrap1(c0 + 1, nv);
+            out[(size_t)i * nv + j] = lerp(row[c0], row[c1], vs.t);
+        } else {
+            const int c0 = wrapneg(j - vs.m, nv);
+            const int c1 = wrapneg(c0 - 1, nv);
+            out[(size_t)i * nv + j] = lerp(row[c0], row[c1], vs.t);
+            if (g_E != nullptr) {
+                const int d0 = wrap1(j + vs.m, nv);
+                const int d1 = wrap1(d0 + 1, nv);
+                const T* fr = f_in + (size_t)i * nv;
+                acc += (fr[d1] - fr[d0]) * row[j];
+            }
+        }
+    }
+    if (adjoint && g_E != nullptr) {
+        acc = block_sum<T>(acc, red);
+        if (threadIdx.x == 0) g_E[i] = -dtdv * acc;
+    }
+}
+
+template <typename T>
+cudaError_t launch_compute_rho(int nx, int nv, const double* f, const double* feq, int feq_rs,
+                               double dv, T* rho, cudaStream_t s) {
+    if (feq_rs == 0) {
+        // broadcast one row of f_eq: index with stride 0
+        rho_kernel<T><<<nx, 256, 0, s>>>(nv, f, feq, 0, dv, rho);
+    } else {
+        rho_kernel<T><<<nx, 256, 0, s>>>(nv, f, feq, feq_rs, dv, rho);
+    }
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_poisson(const PoissonTables<T>& P, const T* in, T* out, int adjoint,
+                           cudaStream_t s) {
+    int threads = P.nx >= 2048 ? 1024 : (P.nx >= 64 ? P.nx / 2 : 32);
+    if (threads > 1024) threads = 1024;
+    const size_t smem = P.use_smem ? poisson_smem_bytes(P.nx, sizeof(T)) : 0;
+    poisson_kernel<T><<<1, threads, smem, s>>>(P, in, out, adjoint);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_electric_energy(int nx, double dx, const T* E, T* ee, cudaStream_t s) {
+    ee_kernel<T><<<1, 256, 0, s>>>(nx, dx, E, ee);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_semilag_x(int nx, int nv, const double* vs, double dx, double dt,
+                             const T* in, T* out, int adjoint, cudaStream_t s) {
+    dim3 grid((nv + 127) / 128, nx);
+    semilag_x_kernel<T><<<grid, 128, 0, s>>>(nx, nv, vs, dx, dt, in, out, adjoint);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_semilag_v(int nx, int nv, double dv, double dt, const T* in,
+                             const T* E_total, T* out, int adjoint, const T* f_in, T* g_E,
+                             cudaStream_t s) {
+    semilag_v_kernel<T><<<nx, 256, 0, s>>>(nv, (T)(dt / dv), in, E_total, out, adjoint, f_in, g_E);
+    count_launch();
+    return cudaGetLastError();
+}
+
+#define VP_INST(T)                                                                              \
+    template cudaError_t launch_compute_rho<T>(int, int, const double*, const double*, int,     \
+                                               double, T*, cudaStream_t);                       \
+    template cudaError_t launch_poisson<T>(const PoissonTables<T>&, const T*, T*, int,          \
+                                           cudaStream_t);                                       \
+    template cudaError_t launch_electric_energy<T>(int, double, const T*, T*, cudaStream_t);    \
+    template cudaError_t launch_semilag_x<T>(int, int, const double*, double, double, const T*, \
+                                             T*, int, cudaStream_t);                            \
+    template cudaError_t launch_semilag_v<T>(int, int, double, double, const T*, const T*, T*,  \
+                                             int, const T*, T*, cudaStream_t);
+VP_INST(float)
+VP_INST(double)
+
+}  // namespace vpb
