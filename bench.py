@@ -1,0 +1,460 @@
+#!/usr/bin/env python
+"""Benchmark of the fused Vlasov-Poisson Strang step: phase-space cell-steps/s, forward + adjoint.
+
+Default workload (``--workload c2``): two-stream 256x256, dt 0.05, t_final 5 (100 time steps),
+8-mode external field, forward pass plus the discrete adjoint of J = sum(ee)*dt. One bench
+"step" is one such forward + adjoint; value = cell-steps processed / second = nx*nv*T per step
+(times the number of GPUs: every rank runs an independent replica, a single instance does not
+shard).
+
+Prints ONE JSON line on rank 0. ``--impl reference`` times the CPU restatement of the
+reference's own algorithm (the reference is pure Python over NVIDIA Warp/JAX, neither of which
+can run here) on the host cores instead.
+
+Launch for N>1: python -m torch.distributed.run --nnodes=1 --nproc-per-node N
+--master-addr 127.0.0.1 --master-port P bench.py --gpus N ...
+"""
+
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L2_FLUSH_BYTES = 256 << 20   # > 126 MB L2
+BYTES_FWD = 8                # algorithmic bytes per cell-step, forward (read + write delta)
+BYTES_BWD = 12               # adjoint: read f_half, read cotangent, write cotangent
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "roofline"])
+    ap.add_argument("--dtype", default="float32", choices=["float32", "float64"])
+    ap.add_argument("--checkpoint-every", type=int, default=None)
+    ap.add_argument("--no-graph", action="store_true", help="launch eagerly instead of replaying a CUDA graph")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample duration")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------------------------
+# helpers
+# ------------------------------------------------------------------------------------------------
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")),
+            int(os.environ.get("WORLD_SIZE", "1")))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch recorded by an ncu capture (profiles/<kernel>_<workload>.txt)."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.txt")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", f.read())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in (self.out or "").strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------------
+# CPU baseline: the float64 restatement of the reference's algorithm on the host cores
+# ------------------------------------------------------------------------------------------------
+
+def cpu_baseline(wl, target_s: float):
+    """Time the oracle (forward + adjoint, the reference's legacy loop) on a bounded sample.
+
+    Uses the OpenMP C restatement when it is built (oracle/libvporacle.so), else NumPy.
+    Returns (cell_steps_per_s, cores, kind, sample_description).
+    """
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import vp_oracle as O
+
+    g = O.grid_from(wl.mesh)
+    H = wl.H
+    cores = 1
+    impl = "numpy float64 restatement (1 thread)"
+    runner = None
+    try:
+        import vp_oracle_c as OC  # optional OpenMP build
+        if OC.available():
+            cores = OC.threads()
+            impl = f"C float64 restatement, OpenMP x{cores}"
+            runner = lambda T: OC.forward_backward(g, wl.dt, wl.f_eq, wl.f_iv, H, T)  # noqa: E731
+    except ImportError:
+        pass
+    if runner is None:
+        def runner(T):
+            tf = T * wl.dt * (1 + 1e-12)
+            Tn = O.num_steps(tf, wl.dt)
+            fwd = O.run_forward(g, wl.dt, wl.f_eq, wl.f_iv, H, tf)
+            if wl.adjoint:
+                O.run_backward(g, wl.dt, wl.f_eq, wl.f_iv, H, tf, fwd[1], np.zeros_like(wl.f_iv),
+                               np.zeros((Tn, g.nx, g.nv)), np.zeros((Tn, g.nx)), np.full(Tn, wl.dt))
+            return Tn
+    t0 = time.perf_counter()
+    runner(1)
+    one = max(time.perf_counter() - t0, 1e-4)
+    T = int(max(1, min(wl.n_steps, target_s / one)))
+    t0 = time.perf_counter()
+    runner(T)
+    el = time.perf_counter() - t0
+    value = g.nx * g.nv * T / el
+    what = "forward + adjoint" if wl.adjoint else "forward"
+    sample = f"{impl}: {what} of {T} of the {wl.n_steps} time steps at {g.nx}x{g.nv}"
+    return value, cores, "port", sample
+
+
+# ------------------------------------------------------------------------------------------------
+# GPU arm
+# ------------------------------------------------------------------------------------------------
+
+def run_ours(args, rank, local_rank, world):
+    import torch
+    import torch.distributed as dist
+
+    from warp_vp_solver_b200 import _capi
+    from warp_vp_solver_b200 import WarpVlasovPoissonSolver, electric_energy_in_time
+    from warp_vp_solver_b200 import external_electric_field
+    from warp_vp_solver_b200.workloads import make_workload
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    wl = make_workload(args.workload)
+    dtype = torch.float32 if args.dtype == "float32" else torch.float64
+    ce = args.checkpoint_every if args.checkpoint_every is not None else wl.checkpoint_every
+    solver = WarpVlasovPoissonSolver(wl.mesh, wl.dt, wl.f_eq, dtype=dtype, checkpoint_every=ce)
+    plan = solver.plan
+    lib = _capi.load()
+    nx, nv, T = wl.mesh.nx, wl.mesh.nv, wl.n_steps
+    every = plan.resolve_every(T, ce)
+
+    f_iv = torch.tensor(wl.f_iv, dtype=torch.float64, device=dev)
+    H = torch.tensor(wl.H, dtype=dtype, device=dev)
+    E_hist = torch.empty((T, nx), dtype=dtype, device=dev)
+    ee_hist = torch.empty((T,), dtype=dtype, device=dev)
+    tape = torch.empty(plan.tape_bytes(T, every), dtype=torch.uint8, device=dev)
+    ws = plan.workspace(T, every)
+    g_ee = torch.full((T,), wl.dt, dtype=dtype, device=dev)   # dJ/dee for J = sum(ee)*dt
+    g_fiv = torch.empty((nx, nv), dtype=dtype, device=dev)
+    g_H = torch.empty((nx,), dtype=dtype, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    def fwd():
+        stream = torch.cuda.current_stream().cuda_stream
+        _capi.check(lib.vp_forward(plan.handle, f_iv.data_ptr(), H.data_ptr(), T, None, None,
+                                   E_hist.data_ptr(), ee_hist.data_ptr(), tape.data_ptr(), every,
+                                   ws.data_ptr(), ws.numel(), stream))
+
+    def bwd():
+        stream = torch.cuda.current_stream().cuda_stream
+        if not wl.adjoint:
+            return
+        _capi.check(lib.vp_backward(plan.handle, H.data_ptr(), T, tape.data_ptr(), every, None,
+                                    None, None, g_ee.data_ptr(), g_fiv.data_ptr(), g_H.data_ptr(),
+                                    ws.data_ptr(), ws.numel(), stream))
+
+    # launches per step, counted on an eager call
+    lib.vp_reset_launch_count()
+    fwd()
+    n_fwd = lib.vp_launch_count()
+    lib.vp_reset_launch_count()
+    bwd()
+    n_bwd = lib.vp_launch_count()
+    torch.cuda.synchronize()
+
+    use_graph = not args.no_graph
+    if use_graph:
+        g_fwd, g_bwd = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            fwd()
+            bwd()
+        torch.cuda.current_stream().wait_stream(s)
+        torch.cuda.synchronize()
+        with torch.cuda.graph(g_fwd):
+            fwd()
+        if wl.adjoint:
+            with torch.cuda.graph(g_bwd):
+                bwd()
+        run_f = g_fwd.replay
+        run_b = g_bwd.replay if wl.adjoint else (lambda: None)
+    else:
+        run_f, run_b = fwd, bwd
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        run_f()
+        run_b()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local_rank) as clk:
+        for i in range(args.steps):
+            flush.zero_()                      # L2 flush between timed steps (not timed)
+            ev[i][0].record()
+            run_f()
+            ev[i][1].record()
+            run_b()
+            ev[i][2].record()
+        torch.cuda.synchronize()
+    t_f = [a.elapsed_time(b) for a, b, _ in ev]
+    t_b = [b.elapsed_time(c) for _, b, c in ev]
+    total_ms = sum(f + b for f, b in zip(t_f, t_b))
+    tt = torch.tensor([total_ms, sum(t_f), sum(t_b)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    total_ms, tf_ms, tb_ms = (float(x) for x in tt.cpu())
+
+    cells = nx * nv
+    cell_steps = cells * T * args.steps * world
+    value = cell_steps / (total_ms * 1e-3)
+
+    # roofline of the dominant kernel (per-launch average over the timed region)
+    peak, peak_kind = measured_peaks()
+    f_launch_ms = tf_ms / (args.steps * n_fwd)
+    b_launch_ms = tb_ms / (args.steps * max(n_bwd, 1)) if wl.adjoint else 0.0
+    if wl.adjoint and tb_ms >= tf_ms and every == 1:
+        kname, per_ms, alg = "vp_bwd_kernel", b_launch_ms, BYTES_BWD * cells
+    else:
+        kname, per_ms, alg = "vp_fwd_kernel", f_launch_ms, BYTES_FWD * cells
+    achieved = alg / (per_ms * 1e-3) / 1e9
+    traffic = profile_traffic(kname, wl.name)
+    roof = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": peak,
+            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+            "algorithmic_bytes_per_launch": alg, "avg_launch_us": round(per_ms * 1e3, 3),
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+            else "fallback 6650 GB/s",
+            "note": "per-launch average over graph replays of the timed steps"}
+
+    # end to end through the public API with host buffers (rank 0's replica measured on every rank)
+    e2e = None
+    if not args.no_e2e:
+        e2e = e2e_public_api(args, solver, wl, dev, flush)
+
+    clocks = clk.summary()
+    launches = (n_fwd + (n_bwd if wl.adjoint else 0)) * args.steps
+    line = {
+        "metric": "cell-steps/s fwd+adjoint" if wl.adjoint else "cell-steps/s fwd",
+        "value": round(value, 1),
+        "unit": "cell-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(total_ms / args.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32" if dtype == torch.float32 else "f64",
+        "data": "synthetic (seeded two-stream / bump-on-tail set-ups of the benchmark configs)",
+        "config": {"workload": wl.description, "nx": nx, "nv": nv, "n_time_steps": T,
+                   "checkpoint_every": every, "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "flushed between timed steps (256 MiB write, untimed)",
+                   "cuda_graph": use_graph,
+                   "fwd_ms_per_step": round(tf_ms / args.steps, 4),
+                   "bwd_ms_per_step": round(tb_ms / args.steps, 4)},
+        "roofline": roof,
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    return line, wl
+
+
+def e2e_public_api(args, solver, wl, dev, flush):
+    """Same metric through ``run_forward_torch`` + autograd with host inputs and outputs."""
+    import torch
+
+    from warp_vp_solver_b200 import electric_energy_in_time, external_electric_field
+
+    coeffs = wl.coeffs if wl.coeffs is not None else np.zeros((2, 1))
+    f_host = torch.from_numpy(np.ascontiguousarray(wl.f_iv)).pin_memory()
+    c_host = torch.from_numpy(np.ascontiguousarray(coeffs)).pin_memory()
+    J_out = torch.empty((), dtype=torch.float64).pin_memory()
+    g_out = torch.empty(c_host.shape, dtype=torch.float64).pin_memory()
+
+    def step():
+        f0 = f_host.to(dev, non_blocking=True)
+        ak = c_host.to(dev, non_blocking=True).requires_grad_(True)
+        H = external_electric_field(ak, wl.mesh, wl.k0)
+        f_final, _, _, ee = solver.run_forward_torch(f0, H, wl.t_final, record_history=False)
+        J = ee.double().sum() * wl.dt
+        if wl.adjoint:
+            J.backward()
+            g_out.copy_(ak.grad, non_blocking=True)
+        J_out.copy_(J.detach(), non_blocking=True)
+
+    for _ in range(max(2, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        step()
+        b.record()
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+    ms = sum(times) / len(times)
+    cells = wl.mesh.nx * wl.mesh.nv * wl.n_steps
+    world = dist_env()[2]
+    return {"value": round(cells * world / (ms * 1e-3), 1), "unit": "cell-steps/s",
+            "h2d_bytes_per_step": int(f_host.numel() * 8 + c_host.numel() * 8),
+            "d2h_bytes_per_step": int(8 + (g_out.numel() * 8 if wl.adjoint else 0)),
+            "ms_per_step": round(ms, 4),
+            "path": "WarpVlasovPoissonSolver.run_forward_torch + torch.autograd, pinned host f_iv "
+                    "and field coefficients in, J and dJ/dcoeffs out"}
+
+
+def run_reference(args, rank, world):
+    """CPU restatement of the reference algorithm on the host cores (rank 0 only)."""
+    from warp_vp_solver_b200.workloads import make_workload
+
+    wl = make_workload(args.workload)
+    vals = []
+    info = None
+    for _ in range(args.warmup):
+        cpu_baseline(wl, min(args.cpu_seconds, 2.0))
+    for _ in range(args.steps):
+        v, cores, kind, sample = cpu_baseline(wl, args.cpu_seconds / max(1, args.steps) * 4)
+        vals.append(v)
+        info = (cores, kind, sample)
+    value = statistics.median(vals)
+    cores, kind, sample = info
+    return {
+        "impl": "reference",
+        "metric": "cell-steps/s fwd+adjoint" if wl.adjoint else "cell-steps/s fwd",
+        "value": round(value, 1),
+        "unit": "cell-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": None,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": wl.description, "nx": wl.mesh.nx, "nv": wl.mesh.nv,
+                   "n_time_steps": wl.n_steps},
+        "cpu_baseline": {"value": round(value, 1), "unit": "cell-steps/s", "cores": cores,
+                         "kind": kind, "sample": sample},
+        "e2e": {"value": round(value, 1), "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": "the reference itself (Python over NVIDIA Warp and JAX) cannot be installed offline; "
+                "this arm times the float64 restatement of its legacy forward and adjoint",
+    }
+
+
+def main():
+    args = parse_args()
+    rank, local_rank, world = dist_env()
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args, rank, world)), flush=True)
+        return
+    import torch.distributed as dist
+
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        line, wl = run_ours(args, rank, local_rank, world)
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            v, cores, kind, sample = cpu_baseline(wl, args.cpu_seconds)
+            line["cpu_baseline"] = {"value": round(v, 1), "unit": "cell-steps/s", "cores": cores,
+                                    "kind": kind, "sample": sample}
+        else:
+            line["cpu_baseline"] = None
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -92,7 +92,10 @@ int vp_workspace_bytes(const vp_plan* plan, int32_t n_steps, int32_t checkpoint_
 int vp_tape_bytes(const vp_plan* plan, int32_t n_steps, int32_t checkpoint_every,
                   size_t* out_bytes);
 
-/* Checkpoint interval actually used for a request (resolves 0 = automatic to ceil(sqrt(n))). */
+/* Checkpoint interval actually used for a request. every > 0 is used as given (capped at
+ * n_steps). every == 0 (automatic) keeps the state of every step when that tape is at most
+ * 256 MiB and otherwise checkpoints every ceil(sqrt(n_steps)) steps, recomputing the states in
+ * between during the adjoint. */
 int vp_resolve_checkpoint_every(const vp_plan* plan, int32_t n_steps, int32_t checkpoint_every,
                                 int32_t* out_every);
 

@@ -69,8 +69,27 @@ namespace vpb {
 static size_t real_size(const vp_plan* p) { return p->dtype == VP_F64 ? 8 : 4; }
 static size_t vshift_size(const vp_plan* p) { return p->dtype == VP_F64 ? 16 : 8; }
 
+// Set while the calling thread's stream is being captured into a CUDA graph: pointer
+// attribute queries are skipped then (the same call is validated when run eagerly).
+static thread_local bool g_capturing = false;
+
+struct CaptureScope {
+    explicit CaptureScope(bool on) { g_capturing = on; }
+    ~CaptureScope() { g_capturing = false; }
+};
+
+static bool stream_capturing(cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &st) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return st != cudaStreamCaptureStatusNone;
+}
+
 static int check_dev_ptr(const void* ptr, const char* name, int device) {
     if (ptr == nullptr) return set_err(VP_ERR_ARG, "%s must not be NULL", name);
+    if (g_capturing) return VP_OK;
     cudaPointerAttributes at;
     cudaError_t e = cudaPointerGetAttributes(&at, ptr);
     if (e != cudaSuccess) {
@@ -127,9 +146,16 @@ static size_t fused_smem(const vp_plan* p, int R) {
     return red + (p->use_smem_poisson ? poisson_smem_bytes(p->nx, real_size(p)) : 0);
 }
 
-static int resolve_every(int n_steps, int every) {
+// Checkpoint interval. every > 0 is used as given (capped at n_steps). every == 0 (automatic)
+// keeps every step's state when that tape fits in kStoreAllBytes, and otherwise checkpoints every
+// ceil(sqrt(n_steps)) steps, recomputing the states in between during the adjoint.
+static const size_t kStoreAllBytes = (size_t)256 << 20;
+
+static int resolve_every(const vp_plan* p, int n_steps, int every) {
     if (n_steps <= 0) return 1;
     if (every <= 0) {
+        const size_t all = (size_t)n_steps * p->nx * p->nv * real_size(p);
+        if (all <= kStoreAllBytes) return 1;
         int k = (int)std::ceil(std::sqrt((double)n_steps));
         return std::max(1, std::min(k, n_steps));
     }
@@ -142,7 +168,7 @@ struct WsLayout {
 
 static WsLayout ws_layout(const vp_plan* p, int n_steps, int every) {
     const size_t nxnv = (size_t)p->nx * p->nv * real_size(p);
-    const int K = resolve_every(n_steps, every);
+    const int K = resolve_every(p, n_steps, every);
     WsLayout L{};
     size_t off = 0;
     L.hbuf0 = off; off += align256(nxnv);
@@ -165,7 +191,7 @@ struct TapeLayout {
 
 static TapeLayout tape_layout(const vp_plan* p, int n_steps, int every) {
     TapeLayout L{};
-    L.K = resolve_every(n_steps, every);
+    L.K = resolve_every(p, n_steps, every);
     L.n_ckpt = n_steps > 0 ? (n_steps + L.K - 1) / L.K : 0;
     const size_t nxnv = (size_t)p->nx * p->nv * real_size(p);
     size_t off = 0;
@@ -584,7 +610,7 @@ int vp_resolve_checkpoint_every(const vp_plan* plan, int32_t n_steps, int32_t ev
                                 int32_t* out_every) {
     if (!plan || !out_every) return set_err(VP_ERR_ARG, "plan and out_every must not be NULL");
     if (n_steps < 0) return set_err(VP_ERR_ARG, "n_steps must be >= 0");
-    *out_every = resolve_every(n_steps, every);
+    *out_every = resolve_every(plan, n_steps, every);
     return VP_OK;
 }
 
@@ -617,9 +643,10 @@ int vp_forward(vp_plan* plan, const double* f_iv, const void* H, int32_t n_steps
     if (n_steps < 0) return set_err(VP_ERR_ARG, "n_steps must be >= 0 (got %d)", n_steps);
     int rc;
     const int dev = plan->device;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    CaptureScope capture_scope(stream_capturing(s));
     if ((rc = check_dev_ptr(f_iv, "f_iv", dev)) || (rc = check_opt_ptr(f_final, "f_final", dev)))
         return rc;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     const size_t nxnv = (size_t)plan->nx * plan->nv;
     if (n_steps == 0) {
         if (f_final)
@@ -653,10 +680,11 @@ int vp_backward(vp_plan* plan, const void* H, int32_t n_steps, const void* tape,
     if (n_steps < 0) return set_err(VP_ERR_ARG, "n_steps must be >= 0 (got %d)", n_steps);
     int rc;
     const int dev = plan->device;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    CaptureScope capture_scope(stream_capturing(s));
     if ((rc = check_dev_ptr(g_f_iv, "g_f_iv", dev)) || (rc = check_dev_ptr(g_H, "g_H", dev)) ||
         (rc = check_opt_ptr(g_f_final, "g_f_final", dev)))
         return rc;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     const size_t rsz = real_size(plan);
     const size_t nxnv = (size_t)plan->nx * plan->nv;
     if (n_steps == 0) {

@@ -54,8 +54,9 @@ class WarpVlasovPoissonSolver:
         reference's refusal of ``record_history=False``. ``aggressive=True`` is accepted and
         raises ``NotImplementedError`` when run: the merged-Strang scheme is not built.
         ``record_history`` sets the default of ``run_forward``'s keyword of the same name.
-        ``checkpoint_every`` (None = ceil(sqrt(n_steps))) is the interval of the delta-f
-        checkpoints the adjoint recomputes from.
+        ``checkpoint_every`` is the interval of the delta-f checkpoints the adjoint recomputes
+        from; None keeps every step when that tape is at most 256 MiB and otherwise checkpoints
+        every ceil(sqrt(n_steps)) steps.
         """
         self.mesh = mesh
         self.dt = float(dt)
