@@ -157,6 +157,29 @@ int vp_semilag_x(vp_plan* plan, const void* in, void* out, double dt, int adjoin
 int vp_semilag_v(vp_plan* plan, const void* in, const void* E_total, void* out, double dt,
                  int adjoint, const void* f_in, void* g_E, void* stream);
 
+/* --- launch configuration (autotuning) ---------------------------------------------------- */
+
+/* Launch shape of a plan's fused step kernels. No reference counterpart: the reference launches
+ * one thread per cell (warp_vp_solver/solver.py:215-265) and has no tunables beyond
+ * aggressive_tile_size (solver.py:99-167). */
+typedef struct vp_launch_config {
+    int32_t rows_per_cta;     /* R: 1, 2, 4, 8 or 16; must divide nx and be <= nx/2 (or be 1) */
+    int32_t threads;          /* threads per CTA: a multiple of 32 in [32, 256], one column each */
+    int32_t n_chunks;         /* column chunks per row block, >= 1                                */
+    int32_t chunk_cols;       /* columns per chunk (derived: ceil(nv / n_chunks) rounded to 32)   */
+    int32_t tail_inline;      /* 1: the Poisson tail runs in the last CTA of the fused launch     */
+    int32_t tail_threads;     /* threads of the separate tail launch (tail_inline == 0)           */
+    int64_t fused_smem_bytes; /* dynamic shared memory of the fused launch                        */
+    int64_t tail_smem_bytes;  /* dynamic shared memory of the tail launch (0: global scratch)     */
+} vp_launch_config;
+
+/* Reads the plan's current launch shape. */
+int vp_plan_get_config(const vp_plan* plan, vp_launch_config* out);
+
+/* Sets rows_per_cta, threads and n_chunks (the other fields are derived and ignored). Workspace
+ * sizes depend on n_chunks: query vp_workspace_bytes() again after changing it. */
+int vp_plan_set_config(vp_plan* plan, const vp_launch_config* cfg);
+
 /* --- diagnostics ------------------------------------------------------------------------ */
 
 /* Copies the last error message of the calling thread into buf (always NUL-terminated). */

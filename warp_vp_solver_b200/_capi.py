@@ -46,6 +46,19 @@ class MeshDesc(ctypes.Structure):
     ]
 
 
+class LaunchConfig(ctypes.Structure):
+    _fields_ = [
+        ("rows_per_cta", c_i32),
+        ("threads", c_i32),
+        ("n_chunks", c_i32),
+        ("chunk_cols", c_i32),
+        ("tail_inline", c_i32),
+        ("tail_threads", c_i32),
+        ("fused_smem_bytes", c_i64),
+        ("tail_smem_bytes", c_i64),
+    ]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "vp_abi_version": (c_int, []),
@@ -55,6 +68,8 @@ SIGNATURES = {
     "vp_plan_create": (c_int, [ctypes.POINTER(MeshDesc), c_dbl, ctypes.POINTER(c_dbl), c_int,
                                ctypes.POINTER(c_vp)]),
     "vp_plan_destroy": (c_int, [c_vp]),
+    "vp_plan_get_config": (c_int, [c_vp, ctypes.POINTER(LaunchConfig)]),
+    "vp_plan_set_config": (c_int, [c_vp, ctypes.POINTER(LaunchConfig)]),
     "vp_num_steps": (c_int, [c_vp, c_dbl, ctypes.POINTER(c_i32)]),
     "vp_workspace_bytes": (c_int, [c_vp, c_i32, c_i32, ctypes.POINTER(c_size)]),
     "vp_tape_bytes": (c_int, [c_vp, c_i32, c_i32, ctypes.POINTER(c_size)]),

@@ -41,6 +41,12 @@ static int cuda_err(cudaError_t e, const char* what) {
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Poisson work area placement: inside the fused launch up to kInlineTailBytes of shared memory
+// (it is requested by every CTA of that launch), else in a separate single-CTA launch with up to
+// kTailSmemBytes of shared memory, else in global scratch.
+static const size_t kInlineTailBytes = 24 * 1024;
+static const size_t kTailSmemBytes = 200 * 1024;
+
 }  // namespace vpb
 
 using namespace vpb;
@@ -51,7 +57,9 @@ struct vp_plan {
     int feq2d = 0;
     int device = 0;
     int pow2 = 0, log2nx = 0;
-    int use_smem_poisson = 0;
+    int tail_inline = 0;       // Poisson tail inside the fused launch (small nx)
+    size_t tail_smem = 0;      // dynamic shared memory of the separate tail launch (0: global scratch)
+    int tail_threads = 0;
     LaunchCfg cfg{};
     // device tables (owned)
     double* d_feq = nullptr;   // nv (x-invariant) or nx*nv
@@ -108,6 +116,10 @@ static int check_opt_ptr(const void* ptr, const char* name, int device) {
     return ptr == nullptr ? VP_OK : check_dev_ptr(ptr, name, device);
 }
 
+// Launch shape of the fused kernels: R rows per CTA (largest of 16, 8, 4, 2 that divides nx and
+// leaves at least two row blocks, else 1), one column per thread, and enough column chunks per
+// row block for about eight CTAs per SM; R is lowered while the grid has fewer than two CTAs per
+// SM. Halo rows cost (R+2)/R V evaluations per output row, so larger R is preferred.
 static LaunchCfg choose_cfg(int nx, int nv, int n_sms) {
     LaunchCfg c{};
     c.threads = nv >= 128 ? 128 : ((nv + 31) / 32) * 32;
@@ -118,32 +130,27 @@ static LaunchCfg choose_cfg(int nx, int nv, int n_sms) {
             break;
         }
     }
-    int chunks = 1;
-    int chunk_cols = nv;
-    const int target = 2 * n_sms;
-    while ((nx / R) * chunks < target) {
-        if (R > 4 && nx % (R / 2) == 0) {
-            R /= 2;
-        } else if ((chunk_cols + 1) / 2 >= c.threads) {
-            chunks *= 2;
-            chunk_cols = (nv + chunks - 1) / chunks;
-            chunk_cols = ((chunk_cols + 31) / 32) * 32;
-            chunks = (nv + chunk_cols - 1) / chunk_cols;
-        } else if (R > 1) {
-            R /= 2;
-        } else {
-            break;
-        }
+    const int max_chunks = std::max(1, nv / c.threads);
+    auto chunks_for = [&](int rr) {
+        const int rows = nx / rr;
+        return std::max(1, std::min(max_chunks, (8 * n_sms + rows - 1) / rows));
+    };
+    int chunks = chunks_for(R);
+    while (R > 1 && (nx / R) * chunks < 2 * n_sms) {
+        R /= 2;
+        chunks = chunks_for(R);
     }
+    int chunk_cols = (nv + chunks - 1) / chunks;
+    chunk_cols = ((chunk_cols + 31) / 32) * 32;
     c.R = R;
-    c.n_chunks = chunks;
     c.chunk_cols = chunk_cols;
+    c.n_chunks = (nv + chunk_cols - 1) / chunk_cols;
     return c;
 }
 
 static size_t fused_smem(const vp_plan* p, int R) {
     const size_t red = ((size_t)32 * R * real_size(p) + 15) & ~(size_t)15;
-    return red + (p->use_smem_poisson ? poisson_smem_bytes(p->nx, real_size(p)) : 0);
+    return red + (p->tail_inline ? poisson_area_size(p->nx, real_size(p)) : 0);
 }
 
 // Checkpoint interval. every > 0 is used as given (capped at n_steps). every == 0 (automatic)
@@ -179,7 +186,7 @@ static WsLayout ws_layout(const vp_plan* p, int n_steps, int every) {
     L.vsh = off; off += align256((size_t)p->nx * vshift_size(p));
     L.E = off; off += align256((size_t)p->nx * real_size(p));
     L.grho = off; off += align256((size_t)p->nx * real_size(p));
-    L.gscratch = off; off += align256((size_t)3 * p->nx * real_size(p));
+    L.gscratch = off; off += align256((size_t)2 * p->nx * real_size(p));
     L.total = off;
     return L;
 }
@@ -203,7 +210,8 @@ static TapeLayout tape_layout(const vp_plan* p, int n_steps, int every) {
 }
 
 template <typename T>
-static PoissonTables<T> poisson_tables(const vp_plan* p, unsigned char* ws, const WsLayout* L) {
+static PoissonTables<T> poisson_tables(const vp_plan* p, unsigned char* ws, const WsLayout* L,
+                                       bool in_smem) {
     PoissonTables<T> P{};
     P.nx = p->nx;
     P.log2nx = p->log2nx;
@@ -212,7 +220,7 @@ static PoissonTables<T> poisson_tables(const vp_plan* p, unsigned char* ws, cons
     P.mult_im = static_cast<const T*>(p->d_mult);
     P.circ = static_cast<const T*>(p->d_circ);
     P.gscratch = (ws != nullptr && L != nullptr) ? reinterpret_cast<T*>(ws + L->gscratch) : nullptr;
-    P.use_smem = p->use_smem_poisson;
+    P.use_smem = in_smem ? 1 : 0;
     return P;
 }
 
@@ -254,8 +262,8 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
     a.tx64 = p->d_tx64;
     a.feq = p->d_feq;
     a.feq_rs = p->feq2d ? nv : 0;
-    a.counter = counter;
-    a.P = poisson_tables<T>(p, ws, &L);
+    a.counter = p->tail_inline ? counter : nullptr;
+    a.P = poisson_tables<T>(p, ws, &L, p->tail_inline || p->tail_smem > 0);
     a.dv = (T)p->dv;
     a.dx = (T)p->dx;
     a.dtdv = (T)(p->dt / p->dv);
@@ -274,6 +282,7 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
     a.f_hist_n = nullptr;
     a.f_final = nullptr;
     VP_CUDA(launch_fwd<T>(a, p->cfg, 0, p->feq2d != 0, s), "forward prologue launch");
+    if (!p->tail_inline) VP_CUDA(launch_fwd_tail<T>(a, p->tail_threads, p->tail_smem, s), "forward tail launch");
 
     for (int n = 0; n < T_steps; ++n) {
         const bool last = (n == T_steps - 1);
@@ -289,6 +298,8 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
         a.E_hist_out = (E_hist && !last) ? E_hist + (size_t)(n + 1) * nx : nullptr;
         a.ee_out = (ee_hist && !last) ? ee_hist + (n + 1) : nullptr;
         VP_CUDA(launch_fwd<T>(a, p->cfg, 1, p->feq2d != 0, s), "forward step launch");
+        if (!last && !p->tail_inline)
+            VP_CUDA(launch_fwd_tail<T>(a, p->tail_threads, p->tail_smem, s), "forward tail launch");
     }
     return VP_OK;
 }
@@ -333,8 +344,8 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
     fa.tx64 = p->d_tx64;
     fa.feq = p->d_feq;
     fa.feq_rs = p->feq2d ? nv : 0;
-    fa.counter = counter;
-    fa.P = poisson_tables<T>(p, ws, &L);
+    fa.counter = nullptr;
+    fa.P = poisson_tables<T>(p, ws, &L, true);
     fa.dv = (T)p->dv;
     fa.dx = (T)p->dx;
     fa.dtdv = (T)(p->dt / p->dv);
@@ -366,8 +377,8 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
     b.feq = p->d_feq;
     b.feq_rs = p->feq2d ? nv : 0;
     b.part = part;
-    b.counter = counter;
-    b.P = poisson_tables<T>(p, ws, &L);
+    b.counter = p->tail_inline ? counter : nullptr;
+    b.P = poisson_tables<T>(p, ws, &L, p->tail_inline || p->tail_smem > 0);
     b.dv = (T)p->dv;
     b.dx = (T)p->dx;
     b.neg_dt_dv = (T)(-p->dt / p->dv);
@@ -386,6 +397,7 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
     b.gE_hist = g_Eh ? g_Eh + (size_t)(T_steps - 1) * nx : nullptr;
     b.gee = g_ee ? g_ee + (T_steps - 1) : nullptr;
     VP_CUDA(launch_bwd<T>(b, p->cfg, 0, p->feq2d != 0, s), "backward prologue launch");
+    if (!p->tail_inline) VP_CUDA(launch_bwd_tail<T>(b, p->tail_threads, p->tail_smem, s), "backward tail launch");
 
     b.c_src = nullptr;
     b.c_src2 = nullptr;
@@ -402,6 +414,8 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
         b.gE_hist = g_Eh ? g_Eh + (size_t)(n - 1) * nx : nullptr;
         b.gee = g_ee ? g_ee + (n - 1) : nullptr;
         VP_CUDA(launch_bwd<T>(b, p->cfg, 1, p->feq2d != 0, s), "backward step launch");
+        if (!p->tail_inline)
+            VP_CUDA(launch_bwd_tail<T>(b, p->tail_threads, p->tail_smem, s), "backward tail launch");
     }
     // epilogue (n = 0)
     b.w_in = wbuf[0];
@@ -559,9 +573,22 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
         }
     }
     const size_t rs = dtype == VP_F64 ? 8 : 4;
-    p->use_smem_poisson = poisson_smem_bytes(nx, rs) <= 24 * 1024 ? 1 : 0;
+    const size_t area = poisson_area_size(nx, rs);
+    p->tail_inline = area <= kInlineTailBytes ? 1 : 0;
+    p->tail_smem = (!p->tail_inline && area <= kTailSmemBytes) ? area : 0;
+    p->tail_threads = nx >= 2048 ? 1024 : std::max(32, ((nx / 2 + 31) / 32) * 32);
     p->cfg = choose_cfg(nx, nv, n_sms);
     p->cfg.smem = fused_smem(p, p->cfg.R);
+    {
+        cudaError_t e1 = dtype == VP_F64 ? set_tail_smem_limit<double>(kTailSmemBytes)
+                                         : set_tail_smem_limit<float>(kTailSmemBytes);
+        cudaError_t e2 = dtype == VP_F64 ? set_poisson_smem_limit<double>(kTailSmemBytes)
+                                         : set_poisson_smem_limit<float>(kTailSmemBytes);
+        if (e1 != cudaSuccess || e2 != cudaSuccess) {
+            delete p;
+            return cuda_err(e1 != cudaSuccess ? e1 : e2, "cudaFuncSetAttribute(tail shared memory)");
+        }
+    }
 
     int rc = VP_OK;
     const size_t feq_count = inv ? (size_t)nv : (size_t)nx * nv;
@@ -589,6 +616,41 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
         return rc;
     }
     *out_plan = p;
+    return VP_OK;
+}
+
+int vp_plan_get_config(const vp_plan* plan, vp_launch_config* out) {
+    if (!plan || !out) return set_err(VP_ERR_ARG, "plan and out must not be NULL");
+    out->rows_per_cta = plan->cfg.R;
+    out->threads = plan->cfg.threads;
+    out->n_chunks = plan->cfg.n_chunks;
+    out->chunk_cols = plan->cfg.chunk_cols;
+    out->tail_inline = plan->tail_inline;
+    out->tail_threads = plan->tail_threads;
+    out->fused_smem_bytes = (int64_t)plan->cfg.smem;
+    out->tail_smem_bytes = (int64_t)plan->tail_smem;
+    return VP_OK;
+}
+
+int vp_plan_set_config(vp_plan* plan, const vp_launch_config* cfg) {
+    if (!plan || !cfg) return set_err(VP_ERR_ARG, "plan and cfg must not be NULL");
+    const int R = cfg->rows_per_cta, th = cfg->threads, ch = cfg->n_chunks;
+    if (!(R == 1 || R == 2 || R == 4 || R == 8 || R == 16))
+        return set_err(VP_ERR_ARG, "rows_per_cta must be 1, 2, 4, 8 or 16 (got %d)", R);
+    if (plan->nx % R != 0 || (R > 1 && R > plan->nx / 2))
+        return set_err(VP_ERR_ARG, "rows_per_cta=%d must divide nx=%d and be <= nx/2", R, plan->nx);
+    if (th < 32 || th > 256 || th % 32 != 0)
+        return set_err(VP_ERR_ARG, "threads must be a multiple of 32 in [32, 256] (got %d)", th);
+    if (ch < 1 || ch > plan->nv) return set_err(VP_ERR_ARG, "n_chunks must be in [1, nv] (got %d)", ch);
+    LaunchCfg c{};
+    c.R = R;
+    c.threads = th;
+    int cols = (plan->nv + ch - 1) / ch;
+    cols = ((cols + 31) / 32) * 32;
+    c.chunk_cols = cols;
+    c.n_chunks = (plan->nv + cols - 1) / cols;
+    plan->cfg = c;
+    plan->cfg.smem = fused_smem(plan, R);
     return VP_OK;
 }
 
@@ -731,15 +793,16 @@ int vp_poisson(vp_plan* plan, const void* in, void* out, int adjoint, void* stre
     if (!plan) return set_err(VP_ERR_ARG, "plan must not be NULL");
     int rc;
     if ((rc = check_dev_ptr(in, "in", plan->device)) || (rc = check_dev_ptr(out, "out", plan->device))) return rc;
-    if (!plan->use_smem_poisson)
-        return set_err(VP_ERR_UNSUPPORTED, "standalone Poisson solve supports nx up to the shared-memory limit; "
-                                           "nx=%d uses the fused path's global scratch", plan->nx);
+    if (poisson_area_size(plan->nx, real_size(plan)) > kTailSmemBytes)
+        return set_err(VP_ERR_UNSUPPORTED, "standalone Poisson solve needs nx*%zu bytes of shared memory; "
+                                           "nx=%d exceeds the %zu-byte limit", 3 * real_size(plan), plan->nx,
+                       kTailSmemBytes);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaError_t e;
     if (plan->dtype == VP_F64)
-        e = launch_poisson<double>(poisson_tables<double>(plan, nullptr, nullptr), (const double*)in, (double*)out, adjoint, s);
+        e = launch_poisson<double>(poisson_tables<double>(plan, nullptr, nullptr, true), (const double*)in, (double*)out, adjoint, s);
     else
-        e = launch_poisson<float>(poisson_tables<float>(plan, nullptr, nullptr), (const float*)in, (float*)out, adjoint, s);
+        e = launch_poisson<float>(poisson_tables<float>(plan, nullptr, nullptr, true), (const float*)in, (float*)out, adjoint, s);
     return e == cudaSuccess ? VP_OK : cuda_err(e, "poisson launch");
 }
 

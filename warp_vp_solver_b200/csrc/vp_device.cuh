@@ -123,18 +123,33 @@ __device__ void fft_radix2(typename Cplx<T>::type* z, const typename Cplx<T>::ty
     }
 }
 
-// x: nx reals (in/out). z: nx complex scratch. tw_s: nx/2 complex (may be a shared copy).
-// All threads of the block must call this. Ends with a __syncthreads().
+// In-place Poisson transform on a complex work buffer z (nx entries). The caller stores the
+// input with poisson_put and reads the result with poisson_get; poisson_core runs between them.
+// Power-of-two nx: the input goes to bit-reversed positions, z = fft(x); z = conj(m*z) (or
+// conj(conj(m)*z) for the transpose) written back in bit-reversed order; z = fft(z). The result
+// is real(z)/nx = real(ifft(m*fft(x))). Other nx: z[i].y = sum_k c[(i-k) mod nx] z[k].x.
+// All threads of the block must call poisson_core; it begins and ends with __syncthreads().
 template <typename T>
-__device__ void poisson_block(const PoissonTables<T>& P, T* x, typename Cplx<T>::type* z,
-                              const typename Cplx<T>::type* tw_s, bool adjoint) {
+__device__ __forceinline__ void poisson_put(const PoissonTables<T>& P, typename Cplx<T>::type* z,
+                                            int i, T v) {
+    using C = typename Cplx<T>::type;
+    z[P.pow2 ? bitrev(i, P.log2nx) : i] = cmake<C>(v, T(0));
+}
+
+template <typename T>
+__device__ __forceinline__ T poisson_get(const PoissonTables<T>& P, const typename Cplx<T>::type* z,
+                                         int i) {
+    return P.pow2 ? z[i].x * (T(1) / T(P.nx)) : z[i].y;
+}
+
+template <typename T>
+__device__ void poisson_core(const PoissonTables<T>& P, typename Cplx<T>::type* z,
+                             const typename Cplx<T>::type* tw_s, bool adjoint) {
     using C = typename Cplx<T>::type;
     const int nx = P.nx;
     __syncthreads();
     if (P.pow2) {
         const int L = P.log2nx;
-        for (int i = threadIdx.x; i < nx; i += blockDim.x) z[bitrev(i, L)] = cmake<C>(x[i], T(0));
-        __syncthreads();
         fft_radix2<T>(z, tw_s, nx, L);
         const T sgn = adjoint ? T(-1) : T(1);
         for (int i = threadIdx.x; i < nx; i += blockDim.x) {
@@ -151,12 +166,7 @@ __device__ void poisson_block(const PoissonTables<T>& P, T* x, typename Cplx<T>:
         }
         __syncthreads();
         fft_radix2<T>(z, tw_s, nx, L);
-        const T scale = T(1) / T(nx);
-        for (int i = threadIdx.x; i < nx; i += blockDim.x) x[i] = z[i].x * scale;
-        __syncthreads();
     } else {
-        for (int i = threadIdx.x; i < nx; i += blockDim.x) z[i].x = x[i];
-        __syncthreads();
         for (int i = threadIdx.x; i < nx; i += blockDim.x) {
             T s = T(0);
             for (int k = 0; k < nx; ++k) {
@@ -164,38 +174,34 @@ __device__ void poisson_block(const PoissonTables<T>& P, T* x, typename Cplx<T>:
                 d = wrapneg(d, nx);
                 s += P.circ[d] * z[k].x;
             }
-            x[i] = s;
+            z[i].y = s;
         }
         __syncthreads();
     }
 }
 
-// Shared-memory layout of the Poisson work area: x (nx reals), z (nx complex), tw (nx/2 complex).
 template <typename T>
-struct PoissonSmem {
-    T* x;
+struct PoissonArea {
     typename Cplx<T>::type* z;
     const typename Cplx<T>::type* tw;
 };
 
+// Work area in shared memory (when P.use_smem) or in the global scratch of the workspace.
+// Copies the twiddles into shared memory; the copy is complete after poisson_core's first barrier.
 template <typename T>
-__device__ PoissonSmem<T> poisson_workspace(const PoissonTables<T>& P, unsigned char* smem) {
+__device__ PoissonArea<T> poisson_area(const PoissonTables<T>& P, unsigned char* smem) {
     using C = typename Cplx<T>::type;
-    PoissonSmem<T> w;
+    PoissonArea<T> w;
     if (P.use_smem) {
         C* z = reinterpret_cast<C*>(smem);
         C* tw = z + P.nx;
-        T* x = reinterpret_cast<T*>(tw + (P.nx >> 1) + 1);
         if (P.pow2) {
             for (int i = threadIdx.x; i < (P.nx >> 1); i += blockDim.x) tw[i] = P.tw[i];
         }
-        w.x = x;
         w.z = z;
         w.tw = tw;
     } else {
-        C* z = reinterpret_cast<C*>(P.gscratch);
-        w.z = z;
-        w.x = P.gscratch + 2 * P.nx;
+        w.z = reinterpret_cast<C*>(P.gscratch);
         w.tw = P.tw;
     }
     return w;

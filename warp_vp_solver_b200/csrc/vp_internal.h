@@ -27,9 +27,9 @@ template <typename T> struct PoissonTables {
     const typename Cplx<T>::type* tw;   // nx/2 twiddles exp(-2*pi*i*q/nx)        (pow2)
     const T* mult_im;                   // imaginary part of the multiplier m_k   (pow2)
     const T* circ;                      // c = real(ifft(m)): E = c (*) rho       (any nx)
-    T* gscratch;                        // 3*nx reals of global scratch, used when the shared
-                                        // buffer would exceed the dynamic shared-memory budget
-    int use_smem;
+    T* gscratch;                        // nx complex of global scratch, used when the work area
+                                        // does not fit in the launch's shared memory
+    int use_smem;                       // work area in dynamic shared memory
 };
 
 // Arguments of one fused forward launch (see vp_kernels.cu for the phase semantics).
@@ -120,7 +120,19 @@ cudaError_t launch_semilag_v(int nx, int nv, double dv, double dt, const T* in,
                              const T* E_total, T* out, int adjoint, const T* f_in, T* g_E,
                              cudaStream_t s);
 
-size_t poisson_smem_bytes(int nx, size_t real_size);
+template <typename T>
+cudaError_t launch_fwd_tail(const FwdArgs<T>& a, int threads, size_t smem, cudaStream_t s);
+template <typename T>
+cudaError_t launch_bwd_tail(const BwdArgs<T>& a, int threads, size_t smem, cudaStream_t s);
+template <typename T>
+cudaError_t set_tail_smem_limit(size_t bytes);
+template <typename T>
+cudaError_t set_poisson_smem_limit(size_t bytes);
+
+// Bytes of the Poisson work area (nx complex values plus nx/2+1 complex twiddles).
+inline size_t poisson_area_size(int nx, size_t real_size) {
+    return (size_t)nx * 2 * real_size + (size_t)((nx >> 1) + 1) * 2 * real_size;
+}
 
 void count_launch(int n = 1);
 

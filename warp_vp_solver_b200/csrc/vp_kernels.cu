@@ -111,6 +111,49 @@ __device__ __forceinline__ bool last_cta_done(unsigned* counter, int* flag) {
     return last;
 }
 
+// Forward tail (one CTA): rho_{n+1} from the chunk partial sums, E_{n+1} = Poisson(rho), ee, and
+// the next step's E + H and v shifts.
+template <typename T>
+__device__ void fwd_tail(const FwdArgs<T>& a, PoissonArea<T> w, T* red) {
+    const int nx = a.nx;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        T s = T(0);
+        for (int c = 0; c < a.n_chunks; ++c) s += __ldcg(a.part + (size_t)c * nx + i);
+        poisson_put<T>(a.P, w.z, i, -a.dv * s);
+    }
+    poisson_core<T>(a.P, w.z, w.tw, false);
+    T e2 = T(0);
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        const T E = poisson_get<T>(a.P, w.z, i);
+        e2 += trap_w<T>(i, nx) * E * E;
+        const T Et = E + __ldg(a.H + i);
+        a.E_out[i] = E;
+        if (a.E_hist_out != nullptr) a.E_hist_out[i] = Et;
+        a.vsh_out[i] = make_vshift<T>(Et, a.dtdv, a.nv);
+    }
+    const T tot = block_sum<T>(e2, red);
+    if (threadIdx.x == 0 && a.ee_out != nullptr) *a.ee_out = T(0.5) * tot * a.dx;
+}
+
+// Backward tail (one CTA), for step n-1: g_E_total = -dt/dv * sum_j slope*w + g_E_hist;
+// g_H += g_E_total; g_E = g_E_total + ee^T; grho_{n-1} = Poisson^T g_E.
+template <typename T>
+__device__ void bwd_tail(const BwdArgs<T>& a, PoissonArea<T> w) {
+    const int nx = a.nx;
+    const T gee = a.gee != nullptr ? *a.gee : T(0);
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        T s = T(0);
+        for (int c = 0; c < a.n_chunks; ++c) s += __ldcg(a.part + (size_t)c * nx + i);
+        T gEt = a.neg_dt_dv * s;
+        if (a.gE_hist != nullptr) gEt += __ldg(a.gE_hist + i);
+        a.gH[i] += gEt;
+        // ee^T (kernels.py:302-322): dx * w_i * E_i * g_ee
+        poisson_put<T>(a.P, w.z, i, gEt + a.dx * trap_w<T>(i, nx) * __ldg(a.E_prev + i) * gee);
+    }
+    poisson_core<T>(a.P, w.z, w.tw, true);
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) a.grho_out[i] = poisson_get<T>(a.P, w.z, i);
+}
+
 // ----------------------------------------------------------------------------------------------
 // Forward
 // PHASE 0 (prologue): h_0 = X(f_iv - f_eq) + Xcorr, rho_0, tail -> E_0.
@@ -186,32 +229,12 @@ __global__ void __launch_bounds__(256) vp_fwd_kernel(const FwdArgs<T> a) {
 
     if (a.part == nullptr || (PHASE != 0 && !next)) return;
     store_row_partials<T, R>(acc, red, a.part + (size_t)blockIdx.y * nx + r0);
-
+    if (a.counter == nullptr) return;   // the tail runs as its own launch (large nx)
     if (!last_cta_done(a.counter, &s_last)) return;
 
-    // ---- tail: rho -> E, ee, E + H, next v shifts ----
     const size_t red_bytes = (size_t)32 * R * sizeof(T);
-    PoissonSmem<T> w = poisson_workspace<T>(a.P, smem + ((red_bytes + 15) & ~(size_t)15));
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-        T s = T(0);
-        for (int c = 0; c < a.n_chunks; ++c) s += __ldcg(a.part + (size_t)c * nx + i);
-        w.x[i] = -a.dv * s;
-    }
-    poisson_block<T>(a.P, w.x, w.z, w.tw, false);
-    T e2 = T(0);
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-        const T E = w.x[i];
-        e2 += trap_w<T>(i, nx) * E * E;
-        const T Et = E + __ldg(a.H + i);
-        a.E_out[i] = E;
-        if (a.E_hist_out != nullptr) a.E_hist_out[i] = Et;
-        a.vsh_out[i] = make_vshift<T>(Et, a.dtdv, nv);
-    }
-    const T tot = block_sum<T>(e2, red);
-    if (threadIdx.x == 0) {
-        if (a.ee_out != nullptr) *a.ee_out = T(0.5) * tot * a.dx;
-        *a.counter = 0u;
-    }
+    fwd_tail<T>(a, poisson_area<T>(a.P, smem + ((red_bytes + 15) & ~(size_t)15)), red);
+    if (threadIdx.x == 0) *a.counter = 0u;
 }
 
 // ----------------------------------------------------------------------------------------------
@@ -314,24 +337,27 @@ __global__ void __launch_bounds__(256) vp_bwd_kernel(const BwdArgs<T> a) {
 
     if (PHASE == 2) return;
     store_row_partials<T, R>(acc, red, a.part + (size_t)blockIdx.y * nx + r0);
+    if (a.counter == nullptr) return;   // the tail runs as its own launch (large nx)
     if (!last_cta_done(a.counter, &s_last)) return;
 
-    // ---- tail for step n-1 ----
     const size_t red_bytes = (size_t)32 * R * sizeof(T);
-    PoissonSmem<T> w = poisson_workspace<T>(a.P, smem + ((red_bytes + 15) & ~(size_t)15));
-    const T gee = a.gee != nullptr ? *a.gee : T(0);
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-        T s = T(0);
-        for (int c = 0; c < a.n_chunks; ++c) s += __ldcg(a.part + (size_t)c * nx + i);
-        T gEt = a.neg_dt_dv * s;
-        if (a.gE_hist != nullptr) gEt += __ldg(a.gE_hist + i);
-        a.gH[i] += gEt;
-        // ee^T (kernels.py:302-322): dx * w_i * E_i * g_ee
-        w.x[i] = gEt + a.dx * trap_w<T>(i, nx) * __ldg(a.E_prev + i) * gee;
-    }
-    poisson_block<T>(a.P, w.x, w.z, w.tw, true);
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) a.grho_out[i] = w.x[i];
+    bwd_tail<T>(a, poisson_area<T>(a.P, smem + ((red_bytes + 15) & ~(size_t)15)));
     if (threadIdx.x == 0) *a.counter = 0u;
+}
+
+// Tails as their own single-CTA launches (used when the Poisson work area does not fit in the
+// fused kernels' shared-memory budget).
+template <typename T>
+__global__ void __launch_bounds__(1024) vp_fwd_tail_kernel(const FwdArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ T red[32];
+    fwd_tail<T>(a, poisson_area<T>(a.P, smem), red);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024) vp_bwd_tail_kernel(const BwdArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    bwd_tail<T>(a, poisson_area<T>(a.P, smem));
 }
 
 // ----------------------------------------------------------------------------------------------
@@ -394,6 +420,35 @@ cudaError_t launch_bwd(const BwdArgs<T>& a, const LaunchCfg& c, int phase, bool 
                        cudaStream_t s) {
     return feq2d ? bwd_r<T, true>(a, c, phase, s) : bwd_r<T, false>(a, c, phase, s);
 }
+
+template <typename T>
+cudaError_t launch_fwd_tail(const FwdArgs<T>& a, int threads, size_t smem, cudaStream_t s) {
+    vp_fwd_tail_kernel<T><<<1, threads, smem, s>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_bwd_tail(const BwdArgs<T>& a, int threads, size_t smem, cudaStream_t s) {
+    vp_bwd_tail_kernel<T><<<1, threads, smem, s>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t set_tail_smem_limit(size_t bytes) {
+    cudaError_t e = cudaFuncSetAttribute(vp_fwd_tail_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)bytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(vp_bwd_tail_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template cudaError_t launch_fwd_tail<float>(const FwdArgs<float>&, int, size_t, cudaStream_t);
+template cudaError_t launch_fwd_tail<double>(const FwdArgs<double>&, int, size_t, cudaStream_t);
+template cudaError_t launch_bwd_tail<float>(const BwdArgs<float>&, int, size_t, cudaStream_t);
+template cudaError_t launch_bwd_tail<double>(const BwdArgs<double>&, int, size_t, cudaStream_t);
+template cudaError_t set_tail_smem_limit<float>(size_t);
+template cudaError_t set_tail_smem_limit<double>(size_t);
 
 template cudaError_t launch_fwd<float>(const FwdArgs<float>&, const LaunchCfg&, int, bool, cudaStream_t);
 template cudaError_t launch_fwd<double>(const FwdArgs<double>&, const LaunchCfg&, int, bool, cudaStream_t);

@@ -7,11 +7,6 @@
 
 namespace vpb {
 
-size_t poisson_smem_bytes(int nx, size_t real_size) {
-    const size_t c = 2 * real_size;
-    return (size_t)nx * c + (size_t)((nx >> 1) + 1) * c + (size_t)nx * real_size;
-}
-
 // rho[i] = dv * trapz_j(f_eq[i,j] - f[i,j]), accumulated in float64 (one CTA per row).
 template <typename T>
 __global__ void __launch_bounds__(256) rho_kernel(int nv, const double* __restrict__ f,
@@ -32,10 +27,10 @@ template <typename T>
 __global__ void __launch_bounds__(1024) poisson_kernel(const PoissonTables<T> P, const T* in,
                                                       T* out, int adjoint) {
     extern __shared__ __align__(16) unsigned char smem[];
-    PoissonSmem<T> w = poisson_workspace<T>(P, smem);
-    for (int i = threadIdx.x; i < P.nx; i += blockDim.x) w.x[i] = in[i];
-    poisson_block<T>(P, w.x, w.z, w.tw, adjoint != 0);
-    for (int i = threadIdx.x; i < P.nx; i += blockDim.x) out[i] = w.x[i];
+    PoissonArea<T> w = poisson_area<T>(P, smem);
+    for (int i = threadIdx.x; i < P.nx; i += blockDim.x) poisson_put<T>(P, w.z, i, in[i]);
+    poisson_core<T>(P, w.z, w.tw, adjoint != 0);
+    for (int i = threadIdx.x; i < P.nx; i += blockDim.x) out[i] = poisson_get<T>(P, w.z, i);
 }
 
 template <typename T>
@@ -128,8 +123,7 @@ template <typename T>
 cudaError_t launch_poisson(const PoissonTables<T>& P, const T* in, T* out, int adjoint,
                            cudaStream_t s) {
     int threads = P.nx >= 2048 ? 1024 : (P.nx >= 64 ? P.nx / 2 : 32);
-    if (threads > 1024) threads = 1024;
-    const size_t smem = P.use_smem ? poisson_smem_bytes(P.nx, sizeof(T)) : 0;
+    const size_t smem = poisson_area_size(P.nx, sizeof(T));
     poisson_kernel<T><<<1, threads, smem, s>>>(P, in, out, adjoint);
     count_launch();
     return cudaGetLastError();
@@ -159,6 +153,13 @@ cudaError_t launch_semilag_v(int nx, int nv, double dv, double dt, const T* in,
     count_launch();
     return cudaGetLastError();
 }
+
+template <typename T>
+cudaError_t set_poisson_smem_limit(size_t bytes) {
+    return cudaFuncSetAttribute(poisson_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+template cudaError_t set_poisson_smem_limit<float>(size_t);
+template cudaError_t set_poisson_smem_limit<double>(size_t);
 
 #define VP_INST(T)                                                                              \
     template cudaError_t launch_compute_rho<T>(int, int, const double*, const double*, int,     \

@@ -75,6 +75,16 @@ class Plan:
     def handle(self):
         return self._h
 
+    def get_config(self) -> dict:
+        c = _capi.LaunchConfig()
+        _capi.check(self.lib.vp_plan_get_config(self._h, ctypes.byref(c)))
+        return {f: getattr(c, f) for f, _ in _capi.LaunchConfig._fields_}
+
+    def set_config(self, rows_per_cta: int, threads: int, n_chunks: int) -> None:
+        c = _capi.LaunchConfig(rows_per_cta, threads, n_chunks, 0, 0, 0, 0, 0)
+        _capi.check(self.lib.vp_plan_set_config(self._h, ctypes.byref(c)))
+        self._ws = {}   # workspace size depends on n_chunks
+
     def num_steps(self, t_final: float) -> int:
         out = ctypes.c_int32()
         _capi.check(self.lib.vp_num_steps(self._h, float(t_final), ctypes.byref(out)))
