@@ -127,6 +127,26 @@ int vp_backward(vp_plan* plan, const void* H, int32_t n_steps,
                 const void* g_ee_hist, void* g_f_iv, void* g_H,
                 void* workspace, size_t workspace_bytes, void* stream);
 
+/* Maximum scratch of vp_forward_noalloc: 8 MiB of device memory per GPU that loads the library. */
+#define VP_NOALLOC_SCRATCH_BYTES ((size_t)8 << 20)
+
+/* Forward time loop that allocates nothing: the same computation and outputs as vp_forward
+ * without a tape, for callers that cannot allocate device memory when they run the solver
+ * (for example code that must not call cudaMalloc, or must not go through an allocator, while
+ * it is being captured into a CUDA graph or runs inside a host that owns all device memory).
+ * No counterpart in the reference, which allocates Warp arrays per solver
+ * (warp_vp_solver/solver.py:169-203).
+ * The scratch this needs (two delta-f buffers of nx*nv reals plus O(nx) vectors) lives in one
+ * statically allocated device array of VP_NOALLOC_SCRATCH_BYTES bytes that every GPU loading
+ * this library holds until the process exits; requests that need more return VP_ERR_ARG (the
+ * two buffers take 8*nx*nv bytes in float32: 512x1024 fits, 1024x1024 does not). The first call on a device looks up
+ * that array's device address, so make the first call on each device before any stream
+ * capture. All calls share the one array and it keeps the previous call's contents: the call
+ * clears what must start at zero itself, but two calls whose work overlaps on the GPU (other
+ * streams, other host threads, other plans on the same device) race and corrupt each other. */
+int vp_forward_noalloc(vp_plan* plan, const double* f_iv, const void* H, int32_t n_steps,
+                       double* f_final, void* f_hist, void* E_hist, void* ee_hist, void* stream);
+
 /* --- single-stage operators (the reference's helper methods and unit-tested kernels) ------ */
 
 /* rho[i] = dv * trapz_j(f_eq[i,j] - f[i,j]). Replaces compute_rho (warp_vp_solver/solver.py:

@@ -78,6 +78,7 @@ SIGNATURES = {
                            c_size, c_vp]),
     "vp_backward": (c_int, [c_vp, c_vp, c_i32, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
                             c_vp, c_size, c_vp]),
+    "vp_forward_noalloc": (c_int, [c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "vp_compute_rho": (c_int, [c_vp, c_vp, c_vp, c_vp]),
     "vp_poisson": (c_int, [c_vp, c_vp, c_vp, c_int, c_vp]),
     "vp_electric_energy": (c_int, [c_vp, c_vp, c_vp, c_vp]),

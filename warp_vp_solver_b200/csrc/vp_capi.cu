@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -775,6 +776,79 @@ int vp_backward(vp_plan* plan, const void* H, int32_t n_steps, const void* tape,
     return backward_impl<float>(plan, (const float*)H, n_steps, tp, every, (const float*)g_f_final,
                                 (const float*)g_f_hist, (const float*)g_E_hist, (const float*)g_ee_hist,
                                 (float*)g_f_iv, (float*)g_H, ws, s);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// vp_forward_noalloc: the forward loop with its scratch in a static device array, for callers
+// that cannot allocate device memory at call time.
+// ---------------------------------------------------------------------------------------------
+namespace vpb {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[VP_NOALLOC_SCRATCH_BYTES];
+
+static const int kMaxDevices = 64;
+static std::once_flag g_noalloc_once[kMaxDevices];
+static void* g_noalloc_ptr[kMaxDevices] = {};
+static cudaError_t g_noalloc_err[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device. In host code the array's name is
+// only a host-side stand-in; the address comes from cudaGetSymbolAddress, looked up once per
+// device with that device current.
+static int noalloc_scratch(int device, void** out) {
+    if (device < 0 || device >= kMaxDevices) return set_err(VP_ERR_UNSUPPORTED, "device %d out of range", device);
+    std::call_once(g_noalloc_once[device], [device]() {
+        void* ptr = nullptr;
+        g_noalloc_err[device] = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        g_noalloc_ptr[device] = ptr;
+    });
+    if (g_noalloc_err[device] != cudaSuccess) return cuda_err(g_noalloc_err[device], "cudaGetSymbolAddress(noalloc scratch)");
+    *out = g_noalloc_ptr[device];
+    return VP_OK;
+}
+
+}  // namespace vpb
+
+extern "C" {
+
+int vp_forward_noalloc(vp_plan* plan, const double* f_iv, const void* H, int32_t n_steps,
+                       double* f_final, void* f_hist, void* E_hist, void* ee_hist, void* stream) {
+    if (!plan) return set_err(VP_ERR_ARG, "plan must not be NULL");
+    if (n_steps < 0) return set_err(VP_ERR_ARG, "n_steps must be >= 0 (got %d)", n_steps);
+    int rc;
+    const int dev = plan->device;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != dev) return set_err(VP_ERR_ARG, "current device %d differs from the plan's device %d", cur, dev);
+    CaptureScope capture_scope(stream_capturing(s));
+    if ((rc = check_dev_ptr(f_iv, "f_iv", dev)) || (rc = check_opt_ptr(f_final, "f_final", dev)))
+        return rc;
+    const size_t nxnv = (size_t)plan->nx * plan->nv;
+    if (n_steps == 0) {
+        if (f_final)
+            VP_CUDA(cudaMemcpyAsync(f_final, f_iv, nxnv * sizeof(double), cudaMemcpyDeviceToDevice, s),
+                    "cudaMemcpyAsync(f_final)");
+        return VP_OK;
+    }
+    if ((rc = check_dev_ptr(H, "H", dev)) || (rc = check_opt_ptr(f_hist, "f_hist", dev)) ||
+        (rc = check_opt_ptr(E_hist, "E_hist", dev)) || (rc = check_opt_ptr(ee_hist, "ee_hist", dev)))
+        return rc;
+    const size_t need = ws_layout(plan, n_steps, 1).total;
+    if (need > VP_NOALLOC_SCRATCH_BYTES)
+        return set_err(VP_ERR_ARG,
+                       "vp_forward_noalloc: an %dx%d grid needs %zu bytes of scratch, more than the "
+                       "%zu-byte static scratch; use vp_forward with a caller-provided workspace",
+                       plan->nx, plan->nv, need, (size_t)VP_NOALLOC_SCRATCH_BYTES);
+    void* scratch = nullptr;
+    if ((rc = noalloc_scratch(dev, &scratch)) != VP_OK) return rc;
+    unsigned char* ws = static_cast<unsigned char*>(scratch);
+    if (plan->dtype == VP_F64)
+        return forward_impl<double>(plan, f_iv, (const double*)H, n_steps, f_final, (double*)f_hist,
+                                    (double*)E_hist, (double*)ee_hist, nullptr, 1, ws, s);
+    return forward_impl<float>(plan, f_iv, (const float*)H, n_steps, f_final, (float*)f_hist,
+                               (float*)E_hist, (float*)ee_hist, nullptr, 1, ws, s);
 }
 
 int vp_compute_rho(vp_plan* plan, const double* f, void* rho, void* stream) {
