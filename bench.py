@@ -46,6 +46,8 @@ def parse_args():
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "roofline"])
     ap.add_argument("--dtype", default="float32", choices=["float32", "float64"])
     ap.add_argument("--checkpoint-every", type=int, default=None)
+    ap.add_argument("--cluster-size", type=int, default=None,
+                    help="force the cluster size of the resident path (0: streaming path)")
     ap.add_argument("--no-graph", action="store_true", help="launch eagerly instead of replaying a CUDA graph")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -201,6 +203,8 @@ def run_ours(args, rank, local_rank, world):
     ce = args.checkpoint_every if args.checkpoint_every is not None else wl.checkpoint_every
     solver = WarpVlasovPoissonSolver(wl.mesh, wl.dt, wl.f_eq, dtype=dtype, checkpoint_every=ce)
     plan = solver.plan
+    if args.cluster_size is not None:
+        plan.set_config(cluster_size=args.cluster_size)
     lib = _capi.load()
     nx, nv, T = wl.mesh.nx, wl.mesh.nv, wl.n_steps
     every = plan.resolve_every(T, ce)
@@ -292,29 +296,40 @@ def run_ours(args, rank, local_rank, world):
     cell_steps = cells * T * args.steps * world
     value = cell_steps / (total_ms * 1e-3)
 
-    # roofline of the dominant kernel: average time per fused launch over the timed region; when
-    # the Poisson tail is a separate launch its time is charged to the fused launch (conservative)
+    # roofline of the dominant kernel. Streaming path: one fused launch per time step (any
+    # separate Poisson tail launch is charged to it, conservatively). Cluster-resident path: one
+    # launch runs the whole time loop with the state in distributed shared memory, so its
+    # "achieved" figure is an effective bandwidth (the state never travels through HBM).
     peak, peak_kind = measured_peaks()
     cfg = plan.get_config()
-    n_fused_f = T + 1
-    n_recompute = 0 if every == 1 else sum(max(0, min(s0 + every, T) - s0 - 1) for s0 in range(0, T, every))
-    n_fused_b = T + 1
-    f_launch_ms = tf_ms / (args.steps * n_fused_f)
-    b_launch_ms = (tb_ms / (args.steps * (n_fused_b + n_recompute))) if wl.adjoint else 0.0
-    if wl.adjoint and tb_ms >= tf_ms and every == 1:
-        kname, per_ms, alg = "vp_bwd_kernel", b_launch_ms, BYTES_BWD * cells
+    resident = cfg["cluster_size"] > 0 and every == 1
+    if resident:
+        n_fused_f, n_fused_b = 1, 1
+        alg_f, alg_b = BYTES_FWD * cells * T, BYTES_BWD * cells * T
+        kf, kb = "vp_res_fwd_kernel", "vp_res_bwd_kernel"
     else:
-        kname, per_ms, alg = "vp_fwd_kernel", f_launch_ms, BYTES_FWD * cells
+        n_recompute = 0 if every == 1 else sum(max(0, min(s0 + every, T) - s0 - 1) for s0 in range(0, T, every))
+        n_fused_f, n_fused_b = T + 1, T + 1 + n_recompute
+        alg_f, alg_b = BYTES_FWD * cells, BYTES_BWD * cells
+        kf, kb = "vp_fwd_kernel", "vp_bwd_kernel"
+    f_launch_ms = tf_ms / (args.steps * n_fused_f)
+    b_launch_ms = (tb_ms / (args.steps * n_fused_b)) if wl.adjoint else 0.0
+    if wl.adjoint and tb_ms >= tf_ms and (resident or every == 1):
+        kname, per_ms, alg = kb, b_launch_ms, alg_b
+    else:
+        kname, per_ms, alg = kf, f_launch_ms, alg_f
     achieved = alg / (per_ms * 1e-3) / 1e9
     traffic = profile_traffic(kname, wl.name)
+    note = ("one launch per forward (adjoint) time loop, state resident in distributed shared "
+            "memory: achieved is an effective bandwidth over the algorithmic bytes" if resident else
+            "time per fused launch averaged over graph replays of the timed steps, including launch gaps"
+            + ("" if cfg["tail_inline"] else " and the separate Poisson tail launch"))
     roof = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": peak,
             "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
             "algorithmic_bytes_per_launch": alg, "avg_launch_us": round(per_ms * 1e3, 3),
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
             else "fallback 6650 GB/s",
-            "note": "time per fused launch averaged over graph replays of the timed steps, "
-                    "including launch gaps" + ("" if cfg["tail_inline"] else
-                                               " and the separate Poisson tail launch")}
+            "note": note}
 
     # end to end through the public API with host buffers (rank 0's replica measured on every rank)
     e2e = None
@@ -340,7 +355,9 @@ def run_ours(args, rank, local_rank, world):
                    "checkpoint_every": every, "parallelism": "replicas" if world > 1 else "single",
                    "l2": "flushed between timed steps (256 MiB write, untimed)",
                    "cuda_graph": use_graph,
-                   "launch": {k: cfg[k] for k in ("rows_per_cta", "threads", "n_chunks", "tail_inline")},
+                   "launch": {k: cfg[k] for k in ("rows_per_cta", "threads", "n_chunks", "tail_inline",
+                                                  "cluster_size", "cluster_threads")},
+                   "path": "cluster-resident" if resident else "streaming",
                    "fwd_ms_per_step": round(tf_ms / args.steps, 4),
                    "bwd_ms_per_step": round(tb_ms / args.steps, 4)},
         "roofline": roof,

@@ -191,13 +191,21 @@ typedef struct vp_launch_config {
     int32_t tail_threads;     /* threads of the separate tail launch (tail_inline == 0)           */
     int64_t fused_smem_bytes; /* dynamic shared memory of the fused launch                        */
     int64_t tail_smem_bytes;  /* dynamic shared memory of the tail launch (0: global scratch)     */
+    int32_t cluster_size;     /* > 0: whole time loops run in one launch of one cluster of this   */
+                              /* many CTAs with the state in distributed shared memory            */
+                              /* (cluster-resident path); 0: one fused launch per step            */
+    int32_t cluster_threads;  /* threads per CTA of the cluster-resident kernels                  */
+    int64_t cluster_smem_bytes; /* dynamic shared memory per CTA of the cluster-resident kernels  */
 } vp_launch_config;
 
 /* Reads the plan's current launch shape. */
 int vp_plan_get_config(const vp_plan* plan, vp_launch_config* out);
 
-/* Sets rows_per_cta, threads and n_chunks (the other fields are derived and ignored). Workspace
- * sizes depend on n_chunks: query vp_workspace_bytes() again after changing it. */
+/* Sets rows_per_cta, threads, n_chunks and cluster_size (the other fields are derived and
+ * ignored). cluster_size must be 0 or a power of two in [2, 16] that splits nx into 1, 2, 4, 8,
+ * 16 or 32 rows per CTA whose state fits in shared memory; the cluster-resident path is used for forward calls without a tape or with
+ * checkpoint interval 1, and for backward calls with checkpoint interval 1. Workspace sizes
+ * depend on n_chunks: query vp_workspace_bytes() again after changing it. */
 int vp_plan_set_config(vp_plan* plan, const vp_launch_config* cfg);
 
 /* --- diagnostics ------------------------------------------------------------------------ */

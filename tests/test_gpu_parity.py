@@ -24,14 +24,27 @@ TOL_BWD = {torch.float64: 1e-10, torch.float32: 1e-4}
 DTYPES = [torch.float32, torch.float64]
 
 
+PATHS = ["auto", "stream"]
+
+
 def _dt_id(d):
     return "f32" if d == torch.float32 else "f64"
 
 
+def make_solver(mesh, dt, f_eq, path="auto", **kw):
+    """Solver on the plan's automatic path (cluster-resident where the grid fits) or forced onto
+    the per-step streaming kernels."""
+    s = WarpVlasovPoissonSolver(mesh, dt, f_eq, **kw)
+    if path == "stream":
+        s.plan.set_config(cluster_size=0)
+    return s
+
+
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("dtype", DTYPES, ids=_dt_id)
 @pytest.mark.parametrize("case", FORWARD_CASES, ids=lambda c: c.name)
-def test_forward_matches_reference_golden(case, dtype):
-    s = WarpVlasovPoissonSolver(case.mesh, float(case["dt"]), case["f_eq"], dtype=dtype)
+def test_forward_matches_reference_golden(case, dtype, path):
+    s = make_solver(case.mesh, float(case["dt"]), case["f_eq"], path, dtype=dtype)
     out = s.run_forward(case["f_iv"], case["H"], float(case["t_final"]))
     assert out[1].shape == case["f_hist"].shape
     for arr, name in zip(out, FIELDS):
@@ -43,10 +56,11 @@ def test_forward_matches_reference_golden(case, dtype):
         assert err < TOL_FWD[dtype], f"{case.name}:{name} rel err {err:.2e}"
 
 
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("dtype", DTYPES, ids=_dt_id)
 @pytest.mark.parametrize("case", BACKWARD_CASES, ids=lambda c: c.name)
-def test_backward_matches_reference_golden(case, dtype):
-    s = WarpVlasovPoissonSolver(case.mesh, float(case["dt"]), case["f_eq"], dtype=dtype)
+def test_backward_matches_reference_golden(case, dtype, path):
+    s = make_solver(case.mesh, float(case["dt"]), case["f_eq"], path, dtype=dtype)
     g_f, g_H = s._run_backward(case["f_iv"], case["H"], float(case["t_final"]), None,
                                case["g_f_final"], case["g_f_hist"], case["g_E_hist"],
                                case["g_ee_hist"])
@@ -59,7 +73,8 @@ def test_checkpoint_interval_is_bitwise_neutral(every):
     case = [c for c in BACKWARD_CASES if c.name == "bwd_random_16x32"][0]
     outs = []
     for ce in (1, every):
-        s = WarpVlasovPoissonSolver(case.mesh, float(case["dt"]), case["f_eq"], checkpoint_every=ce)
+        # both on the streaming path: the interval must not change a single bit
+        s = make_solver(case.mesh, float(case["dt"]), case["f_eq"], "stream", checkpoint_every=ce)
         outs.append(s._run_backward(case["f_iv"], case["H"], float(case["t_final"]), None,
                                     case["g_f_final"], case["g_f_hist"], case["g_E_hist"],
                                     case["g_ee_hist"]))
@@ -67,9 +82,10 @@ def test_checkpoint_interval_is_bitwise_neutral(every):
     np.testing.assert_array_equal(outs[0][1], outs[1][1])
 
 
-def test_record_history_false_and_determinism():
+@pytest.mark.parametrize("path", PATHS)
+def test_record_history_false_and_determinism(path):
     case = [c for c in FORWARD_CASES if c.name == "fwd_twostream_32x32"][0]
-    s = WarpVlasovPoissonSolver(case.mesh, float(case["dt"]), case["f_eq"])
+    s = make_solver(case.mesh, float(case["dt"]), case["f_eq"], path)
     a = s.run_forward(case["f_iv"], case["H"], float(case["t_final"]))
     b = s.run_forward(case["f_iv"], case["H"], float(case["t_final"]), record_history=False)
     assert b[1] is None
@@ -90,23 +106,25 @@ def test_zero_steps_returns_initial_state():
     assert fh.shape == (0, 16, 32) and Eh.shape == (0, 16) and ee.shape == (0,)
 
 
-def test_config1_two_stream_128_100_steps():
-    """128x128 two-stream, dt 0.05, t_final 5 (100 steps), H = 0."""
+@pytest.mark.parametrize("path", PATHS)
+def test_config1_two_stream_128_100_steps(path):
+    """Configuration 1: 128x128 two-stream, dt 0.05, t_final 5 (100 steps), H = 0."""
     m = make_mesh(10.0 * np.pi, 6.0, 128, 128)
     f_eq, f_iv = two_stream_state(m)
     H = np.zeros(m.nx)
     g = O.grid_from(m)
     ref = O.run_forward(g, 0.05, f_eq, f_iv, H, 5.0)
-    s = WarpVlasovPoissonSolver(m, 0.05, f_eq)
+    s = make_solver(m, 0.05, f_eq, path)
     out = s.run_forward(f_iv, H, 5.0)
-    s64 = WarpVlasovPoissonSolver(m, 0.05, f_eq, dtype=torch.float64)
+    s64 = make_solver(m, 0.05, f_eq, path, dtype=torch.float64)
     out64 = s64.run_forward(f_iv, H, 5.0)
     for arr, arr64, r, name in zip(out, out64, ref, FIELDS):
         assert O.rel_err(arr, r) < 1e-5, f"{name} {O.rel_err(arr, r):.2e}"
         assert O.rel_err(arr64, r) < 1e-11, f"{name} f64 {O.rel_err(arr64, r):.2e}"
 
 
-def test_autograd_matches_oracle_adjoint():
+@pytest.mark.parametrize("path", PATHS)
+def test_autograd_matches_oracle_adjoint(path):
     """run_forward_torch + torch autograd gives the oracle's dJ/dH and dJ/df_iv."""
     from warp_vp_solver_b200 import electric_energy_in_time
 
@@ -116,7 +134,7 @@ def test_autograd_matches_oracle_adjoint():
     H0 = 0.01 * rng.standard_normal(m.nx)
     dt, tf = 0.05, 0.6
     T = int(tf / dt)
-    s = WarpVlasovPoissonSolver(m, dt, f_eq, dtype=torch.float64)
+    s = make_solver(m, dt, f_eq, path, dtype=torch.float64)
     H = torch.tensor(H0, dtype=torch.float64, device="cuda", requires_grad=True)
     f0 = torch.tensor(f_iv, dtype=torch.float64, device="cuda", requires_grad=True)
     f_final, f_hist, E_hist, ee = s.run_forward_torch(f0, H, tf)
@@ -129,3 +147,36 @@ def test_autograd_matches_oracle_adjoint():
                             np.zeros((T, m.nx, m.nv)), 2.0 * fwd[2], w)
     assert O.rel_err(H.grad.cpu().numpy(), gH) < 1e-10
     assert O.rel_err(f0.grad.cpu().numpy(), gf) < 1e-10
+
+
+def test_plan_picks_cluster_resident_path_for_small_grids():
+    m = make_mesh(10.0 * np.pi, 6.0, 256, 256)
+    f_eq, _ = two_stream_state(m)
+    cfg = WarpVlasovPoissonSolver(m, 0.05, f_eq).plan.get_config()
+    assert cfg["cluster_size"] in (2, 4, 8, 16) and cfg["cluster_smem_bytes"] > 0
+    big = make_mesh(2 * np.pi / 0.3, 8.0, 512, 1024)
+    cfg = WarpVlasovPoissonSolver(big, 0.05, np.ones((512, 1024))).plan.get_config()
+    assert cfg["cluster_size"] == 0   # 2 MB of state does not fit one cluster
+
+
+@pytest.mark.parametrize("cn", [2, 4, 8, 16])
+def test_cluster_sizes_agree_with_oracle(cn):
+    m = make_mesh(10.0 * np.pi, 6.0, 64, 64)
+    f_eq, f_iv = two_stream_state(m, eps=1e-2)
+    H = 0.02 * np.random.default_rng(5).standard_normal(m.nx)
+    g = O.grid_from(m)
+    ref = O.run_forward(g, 0.1, f_eq, f_iv, H, 1.0)
+    s = WarpVlasovPoissonSolver(m, 0.1, f_eq, dtype=torch.float64)
+    s.plan.set_config(cluster_size=cn)
+    out = s.run_forward(f_iv, H, 1.0)
+    for arr, r, name in zip(out, ref, FIELDS):
+        assert O.rel_err(arr, r) < 1e-11, f"cn={cn} {name}"
+    T = 10
+    w = O.trapezoid_time_weights(T, 0.1)
+    rg = np.random.default_rng(6)
+    gff = rg.standard_normal((m.nx, m.nv))
+    gfh = 0.1 * rg.standard_normal((T, m.nx, m.nv))
+    gEh = rg.standard_normal((T, m.nx))
+    gf, gH = s._run_backward(f_iv, H, 1.0, None, gff, gfh, gEh, w)
+    gf_r, gH_r = O.run_backward(g, 0.1, f_eq, f_iv, H, 1.0, ref[1], gff, gfh, gEh, w)
+    assert O.rel_err(gf, gf_r) < 1e-10 and O.rel_err(gH, gH_r) < 1e-10

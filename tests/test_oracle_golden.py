@@ -8,6 +8,8 @@ evaluate) must agree to float64 round-off.
 
 from __future__ import annotations
 
+import os
+
 import numpy as np
 import pytest
 
@@ -85,3 +87,35 @@ def test_literal_kernels_bit_exact(golden_kernels):
     np.testing.assert_array_equal(O.solve_poisson(k["poisson_rho"], g.period_x), k["poisson_E"])
     np.testing.assert_array_equal(O.solve_poisson_adjoint(k["poisson_g_E"], g.period_x),
                                   k["poisson_adj"])
+
+
+def _c_oracle():
+    import subprocess
+
+    import vp_oracle_c as OC
+    if not OC.available():
+        subprocess.run(["make", "-C", os.path.join(os.path.dirname(__file__), "..", "oracle")],
+                       check=True, capture_output=True)
+    assert OC.available(), "oracle/_build/libvporacle.so did not build"
+    return OC
+
+
+@pytest.mark.parametrize("case", FORWARD_CASES, ids=lambda c: c.name)
+def test_c_oracle_forward_matches_reference(case):
+    """The OpenMP C restatement (the timed CPU baseline) reproduces the reference's outputs."""
+    OC = _c_oracle()
+    out = OC.forward(case.grid, float(case["dt"]), case["f_eq"], case["f_iv"], case["H"],
+                     int(case["n_steps"]))
+    for arr, name in zip(out, FIELDS):
+        assert O.rel_err(arr, case[name]) < 1e-13, name
+
+
+@pytest.mark.parametrize("case", BACKWARD_CASES, ids=lambda c: c.name)
+def test_c_oracle_backward_matches_reference(case):
+    OC = _c_oracle()
+    T, dt = int(case["n_steps"]), float(case["dt"])
+    fwd = OC.forward(case.grid, dt, case["f_eq"], case["f_iv"], case["H"], T)
+    g_f, g_H = OC.backward(case.grid, dt, case["f_eq"], case["f_iv"], case["H"], T, fwd[1],
+                           case["g_f_final"], case["g_f_hist"], case["g_E_hist"], case["g_ee_hist"])
+    assert O.rel_err(g_f, case["g_f_iv"]) < 1e-13
+    assert O.rel_err(g_H, case["g_H"]) < 1e-13

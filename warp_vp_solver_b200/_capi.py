@@ -56,6 +56,9 @@ class LaunchConfig(ctypes.Structure):
         ("tail_threads", c_i32),
         ("fused_smem_bytes", c_i64),
         ("tail_smem_bytes", c_i64),
+        ("cluster_size", c_i32),
+        ("cluster_threads", c_i32),
+        ("cluster_smem_bytes", c_i64),
     ]
 
 

@@ -62,6 +62,10 @@ struct vp_plan {
     size_t tail_smem = 0;      // dynamic shared memory of the separate tail launch (0: global scratch)
     int tail_threads = 0;
     LaunchCfg cfg{};
+    int res_cn = 0;            // cluster size of the cluster-resident path (0: not used)
+    long long mx_lo = 0, mx_hi = 0;  // extremes of the unreduced x half-step offsets floor(-s_j)
+    int res_threads = 0;
+    size_t res_smem = 0;
     // device tables (owned)
     double* d_feq = nullptr;   // nv (x-invariant) or nx*nv
     double* d_vs = nullptr;    // nv
@@ -147,6 +151,37 @@ static LaunchCfg choose_cfg(int nx, int nv, int n_sms) {
     c.chunk_cols = chunk_cols;
     c.n_chunks = (nv + chunk_cols - 1) / chunk_cols;
     return c;
+}
+
+// Largest shared memory a CTA may request on sm_100.
+static const size_t kMaxSmemPerCta = 227 * 1024;
+
+// Checks that a cluster-resident configuration of cn CTAs can launch; returns its shared memory
+// (0 when it cannot).
+static size_t res_config_ok(const vp_plan* p, int cn) {
+    if (cn < 2 || cn > 16 || (cn & (cn - 1)) != 0 || p->nx % cn != 0) return 0;
+    const int Rc = p->nx / cn;
+    if (!res_rows_supported(Rc)) return 0;
+    const size_t smem = res_smem_size(p->nx, p->nv, Rc, real_size(p));
+    if (smem > kMaxSmemPerCta) return 0;
+    if (res_threads(Rc, p->nv) > 1024) return 0;
+    const int n = p->dtype == VP_F64 ? res_max_clusters<double>(p->feq2d != 0, cn, Rc, p->nv, smem)
+                                     : res_max_clusters<float>(p->feq2d != 0, cn, Rc, p->nv, smem);
+    return n > 0 ? smem : 0;
+}
+
+// Rows whose field a resident CTA needs besides its own: 2*max|x offset| + 2 around them
+// (see the window comment in vp_resident.cu); capped at nx.
+static void res_window_rows(const vp_plan* p, int Rc, bool adjoint, int* lo, int* n) {
+    const long long span = (long long)Rc + 2 * (p->mx_hi - p->mx_lo) + 2;
+    if (span >= p->nx) {
+        *lo = 0;
+        *n = p->nx;
+        return;
+    }
+    const long long l = adjoint ? -2 * p->mx_hi - 2 : 2 * p->mx_lo;
+    *lo = (int)(l % p->nx);
+    *n = (int)span;
 }
 
 static size_t fused_smem(const vp_plan* p, int R) {
@@ -246,6 +281,36 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
     T* E_all = tape ? reinterpret_cast<T*>(tape + TL.E) : nullptr;
     VShift<T>* vsh_all = tape ? reinterpret_cast<VShift<T>*>(tape + TL.vsh) : nullptr;
 
+    if (p->res_cn > 0 && (tape == nullptr || K == 1)) {
+        ResFwdArgs<T> r{};
+        r.nx = nx;
+        r.nv = nv;
+        r.n_steps = T_steps;
+        r.Rc = nx / p->res_cn;
+        r.f_iv = f_iv;
+        r.H = H;
+        r.mx = p->d_mx;
+        r.tx = static_cast<const T*>(p->d_tx);
+        r.tx64 = p->d_tx64;
+        r.feq = p->d_feq;
+        r.feq_rs = p->feq2d ? nv : 0;
+        r.f_final = f_final;
+        r.f_hist = f_hist;
+        r.E_hist = E_hist;
+        r.ee_hist = ee_hist;
+        r.h_tape = ckpt;
+        r.E_tape = E_all;
+        r.vsh_tape = vsh_all;
+        r.P = poisson_tables<T>(p, nullptr, nullptr, true);
+        r.dv = (T)p->dv;
+        r.dx = (T)p->dx;
+        r.dtdv = (T)(p->dt / p->dv);
+        res_window_rows(p, r.Rc, false, &r.win_lo, &r.win_n);
+        VP_CUDA(launch_res_fwd<T>(r, p->feq2d != 0, p->res_cn, p->res_threads, p->res_smem, s),
+                "cluster-resident forward launch");
+        return VP_OK;
+    }
+
     VP_CUDA(cudaMemsetAsync(counter, 0, 256, s), "cudaMemsetAsync(counter)");
 
     auto h_slot = [&](int n) -> T* {
@@ -325,6 +390,36 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
     const T* ckpt = reinterpret_cast<const T*>(tape + TL.ckpt);
     const T* E_all = reinterpret_cast<const T*>(tape + TL.E);
     const VShift<T>* vsh_all = reinterpret_cast<const VShift<T>*>(tape + TL.vsh);
+
+    if (p->res_cn > 0 && K == 1) {
+        ResBwdArgs<T> r{};
+        r.nx = nx;
+        r.nv = nv;
+        r.n_steps = T_steps;
+        r.Rc = nx / p->res_cn;
+        r.H = H;
+        r.mx = p->d_mx;
+        r.tx = static_cast<const T*>(p->d_tx);
+        r.feq = p->d_feq;
+        r.feq_rs = p->feq2d ? nv : 0;
+        r.h_tape = ckpt;
+        r.E_tape = E_all;
+        r.vsh_tape = vsh_all;
+        r.g_ff = g_ff;
+        r.g_fh = g_fh;
+        r.g_Eh = g_Eh;
+        r.g_ee = g_ee;
+        r.g_fiv = g_fiv;
+        r.g_H = g_H;
+        r.P = poisson_tables<T>(p, nullptr, nullptr, true);
+        r.dv = (T)p->dv;
+        r.dx = (T)p->dx;
+        r.neg_dt_dv = (T)(-p->dt / p->dv);
+        res_window_rows(p, r.Rc, true, &r.win_lo, &r.win_n);
+        VP_CUDA(launch_res_bwd<T>(r, p->feq2d != 0, p->res_cn, p->res_threads, p->res_smem, s),
+                "cluster-resident backward launch");
+        return VP_OK;
+    }
 
     VP_CUDA(cudaMemsetAsync(counter, 0, 256, s), "cudaMemsetAsync(counter)");
     VP_CUDA(cudaMemsetAsync(g_H, 0, (size_t)nx * sizeof(T), s), "cudaMemsetAsync(g_H)");
@@ -532,6 +627,8 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
         const double sj = 0.5 * mesh->vs[j] * dt / mesh->dx;
         const double mf = std::floor(-sj);
         tx[j] = -sj - mf;
+        if (j == 0 || (long long)mf < p->mx_lo) p->mx_lo = (long long)mf;
+        if (j == 0 || (long long)mf > p->mx_hi) p->mx_hi = (long long)mf;
         long long mi = (long long)mf % nx;
         if (mi < 0) mi += nx;
         mx[j] = (int)mi;
@@ -562,8 +659,9 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
         }
     }
     // circulant kernel c = real(ifft(m)): c[k] = -(1/nx) * sum_q mult_im[q] * sin(2*pi*q*k/nx)
+    // (needed by the non-power-of-two FFT fallback and by the cluster-resident path, nx <= 512)
     std::vector<double> circ(nx, 0.0);
-    if (!p->pow2) {
+    if (!p->pow2 || nx <= 512) {
         for (int k = 0; k < nx; ++k) {
             double s = 0.0;
             for (int q = 0; q < nx; ++q) {
@@ -580,6 +678,17 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
     p->tail_threads = nx >= 2048 ? 1024 : std::max(32, ((nx / 2 + 31) / 32) * 32);
     p->cfg = choose_cfg(nx, nv, n_sms);
     p->cfg.smem = fused_smem(p, p->cfg.R);
+    // cluster-resident path: the largest cluster (16, 8, 4, 2 CTAs) whose per-CTA share of the
+    // state fits in shared memory and that the occupancy calculator accepts
+    for (int cn : {16, 8, 4, 2}) {
+        const size_t smem = res_config_ok(p, cn);
+        if (smem > 0) {
+            p->res_cn = cn;
+            p->res_threads = res_threads(nx / cn, nv);
+            p->res_smem = smem;
+            break;
+        }
+    }
     {
         cudaError_t e1 = dtype == VP_F64 ? set_tail_smem_limit<double>(kTailSmemBytes)
                                          : set_tail_smem_limit<float>(kTailSmemBytes);
@@ -630,6 +739,9 @@ int vp_plan_get_config(const vp_plan* plan, vp_launch_config* out) {
     out->tail_threads = plan->tail_threads;
     out->fused_smem_bytes = (int64_t)plan->cfg.smem;
     out->tail_smem_bytes = (int64_t)plan->tail_smem;
+    out->cluster_size = plan->res_cn;
+    out->cluster_threads = plan->res_threads;
+    out->cluster_smem_bytes = (int64_t)plan->res_smem;
     return VP_OK;
 }
 
@@ -643,6 +755,19 @@ int vp_plan_set_config(vp_plan* plan, const vp_launch_config* cfg) {
     if (th < 32 || th > 256 || th % 32 != 0)
         return set_err(VP_ERR_ARG, "threads must be a multiple of 32 in [32, 256] (got %d)", th);
     if (ch < 1 || ch > plan->nv) return set_err(VP_ERR_ARG, "n_chunks must be in [1, nv] (got %d)", ch);
+    const int cn = cfg->cluster_size;
+    size_t res_smem = 0;
+    if (cn != 0) {
+        res_smem = res_config_ok(plan, cn);
+        if (res_smem == 0)
+            return set_err(VP_ERR_ARG, "cluster_size=%d is not usable for a %dx%d grid (must be a power of two "
+                                       "in [2,16] dividing nx into 1, 2, 4, 8, 16 or 32 rows per CTA whose "
+                                       "state fits in shared memory)",
+                           cn, plan->nx, plan->nv);
+    }
+    plan->res_cn = cn;
+    plan->res_smem = res_smem;
+    plan->res_threads = cn ? res_threads(plan->nx / cn, plan->nv) : 0;
     LaunchCfg c{};
     c.R = R;
     c.threads = th;

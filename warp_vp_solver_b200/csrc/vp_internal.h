@@ -134,6 +134,62 @@ inline size_t poisson_area_size(int nx, size_t real_size) {
     return (size_t)nx * 2 * real_size + (size_t)((nx >> 1) + 1) * 2 * real_size;
 }
 
+// Cluster-resident kernels (vp_resident.cu): one cluster runs a whole time loop.
+template <typename T> struct ResFwdArgs {
+    int nx, nv, n_steps, Rc;
+    const double* f_iv;
+    const T* H;
+    const int* mx;
+    const T* tx;
+    const double* tx64;
+    const double* feq;
+    int feq_rs;
+    double* f_final;
+    T* f_hist;
+    T* E_hist;
+    T* ee_hist;
+    T* h_tape;              // h_n for every step (or null)
+    T* E_tape;              // raw E_n for every step (or null)
+    VShift<T>* vsh_tape;    // v shifts for every step (or null)
+    PoissonTables<T> P;
+    T dv, dx, dtdv;
+    int win_lo, win_n;      // rows whose field a CTA needs: gr0 + win_lo .. + win_n - 1 (mod nx)
+};
+
+template <typename T> struct ResBwdArgs {
+    int nx, nv, n_steps, Rc;
+    const T* H;
+    const int* mx;
+    const T* tx;
+    const double* feq;
+    int feq_rs;
+    const T* h_tape;
+    const T* E_tape;
+    const VShift<T>* vsh_tape;
+    const T* g_ff;
+    const T* g_fh;
+    const T* g_Eh;
+    const T* g_ee;
+    T* g_fiv;
+    T* g_H;
+    PoissonTables<T> P;
+    T dv, dx, neg_dt_dv;
+    int win_lo, win_n;      // rows whose grho a CTA needs: gr0 + win_lo .. + win_n - 1 (mod nx)
+};
+
+template <typename T>
+cudaError_t launch_res_fwd(const ResFwdArgs<T>& a, bool feq2d, int cn, int threads, size_t smem,
+                           cudaStream_t s);
+template <typename T>
+cudaError_t launch_res_bwd(const ResBwdArgs<T>& a, bool feq2d, int cn, int threads, size_t smem,
+                           cudaStream_t s);
+size_t res_smem_size(int nx, int nv, int Rc, size_t real_size);
+template <typename T>
+int res_max_clusters(bool feq2d, int cn, int rc, int nv, size_t smem);
+bool res_rows_supported(int rc);
+int res_rows_per_thread(int rc, int nv);
+int res_threads(int rc, int nv);
+
 void count_launch(int n = 1);
 
 }  // namespace vpb

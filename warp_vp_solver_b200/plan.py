@@ -80,8 +80,14 @@ class Plan:
         _capi.check(self.lib.vp_plan_get_config(self._h, ctypes.byref(c)))
         return {f: getattr(c, f) for f, _ in _capi.LaunchConfig._fields_}
 
-    def set_config(self, rows_per_cta: int, threads: int, n_chunks: int) -> None:
-        c = _capi.LaunchConfig(rows_per_cta, threads, n_chunks, 0, 0, 0, 0, 0)
+    def set_config(self, rows_per_cta: int | None = None, threads: int | None = None,
+                   n_chunks: int | None = None, cluster_size: int | None = None) -> None:
+        cur = self.get_config()
+        c = _capi.LaunchConfig()
+        c.rows_per_cta = cur["rows_per_cta"] if rows_per_cta is None else int(rows_per_cta)
+        c.threads = cur["threads"] if threads is None else int(threads)
+        c.n_chunks = cur["n_chunks"] if n_chunks is None else int(n_chunks)
+        c.cluster_size = cur["cluster_size"] if cluster_size is None else int(cluster_size)
         _capi.check(self.lib.vp_plan_set_config(self._h, ctypes.byref(c)))
         self._ws = {}   # workspace size depends on n_chunks
 
