@@ -48,6 +48,7 @@ template <typename T> struct ResSmem {
     T* dfeq;         // nv: f_eq[j+1] - f_eq[j] rounded from float64 (periodic)
     T* red;          // 32
     double* eep;     // 2 x 16 partial energies (read by CTA 0)
+    T* own;          // RC: accumulated g_H of the own rows (adjoint)
 };
 
 __host__ __device__ inline size_t res_align(size_t x) { return (x + 15) & ~(size_t)15; }
@@ -61,6 +62,7 @@ __host__ __device__ inline size_t res_smem_bytes(int nx, int nv, int RC, size_t 
     b += res_align((size_t)nv * rs);
     b += res_align((size_t)32 * rs);
     b += res_align((size_t)32 * 8);
+    b += res_align((size_t)RC * rs);
     return b;
 }
 
@@ -86,6 +88,7 @@ __device__ ResSmem<T> res_carve(unsigned char* smem, int nx, int nv, int RC) {
     s.dfeq = reinterpret_cast<T*>(take((size_t)nv * sizeof(T)));
     s.red = reinterpret_cast<T*>(take((size_t)32 * sizeof(T)));
     s.eep = reinterpret_cast<double*>(take((size_t)32 * sizeof(double)));
+    s.own = reinterpret_cast<T*>(take((size_t)RC * sizeof(T)));
     return s;
 }
 
@@ -140,7 +143,17 @@ __device__ __forceinline__ const T* res_row(cg::cluster_group& cl, const T* plan
     const int cta = q / RC;
     const int l = q - cta * RC;
     const T* base = (cta == me) ? plane : cl.map_shared_rank(plane, cta);
-    return base + (size_t)l * nv;
+    return base + l * nv;
+}
+
+// Split cluster barrier: arrive (release: this thread's earlier shared/global writes become
+// visible cluster-wide) ... wait (acquire). Work placed between the two overlaps the barrier;
+// the global writes of the outputs go there so the release does not wait for them.
+__device__ __forceinline__ void cluster_arrive() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait() {
+    asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
 }
 
 // Row sums of the plane `vals` (RC x nv, already weighted) for the CTA's own rows, written to
@@ -304,27 +317,58 @@ __global__ void __launch_bounds__(1024) vp_res_fwd_kernel(const ResFwdArgs<T> a)
         const T* cur = Hb[n & 1];
         T* nxt = Hb[(n + 1) & 1];
         const bool last = (n == a.n_steps - 1);
+        T d[RPT + 1];
+        T hv[RPT];
+        int dq = 0;
         if (colv) {
-            // o on rows g+2m .. g+2m+RPT+1 (h of those rows read from the owning CTAs)
+            // o on rows g+2m .. g+2m+RPT+1 (h of those rows, from the owning CTAs)
             T o[RPT + 2];
             const int q0 = wrap2(g + 2 * m, nx);
+            if (q0 >= gr0 && q0 + RPT + 1 < gr0 + RC) {
+                // the whole window lies in this CTA: plain shared-memory loads
 #pragma unroll
-            for (int k = 0; k < RPT + 2; ++k) {
-                const int q = wrap1(q0 + k, nx);
-                const VShift<T> v = S.vsh[q];
-                const T* hr = res_row<T, RC>(cluster, cur, q, nv, me);
-                const int c0 = wrap1(j + v.m, nv);
-                const int c1 = c0 + 1 == nv ? 0 : c0 + 1;
-                o[k] = lerp(hr[c0], hr[c1], v.t) + res_vcorr<T, FEQ2D>(S, a.feq, a.feq_rs, q, j, c0, c1, v, nv);
+                for (int k = 0; k < RPT + 2; ++k) {
+                    const int q = q0 + k;
+                    const VShift<T> v = S.vsh[q];
+                    const T* hr = cur + (q - gr0) * nv;
+                    const int c0 = wrap1(j + v.m, nv);
+                    const int c1 = c0 + 1 == nv ? 0 : c0 + 1;
+                    o[k] = lerp(hr[c0], hr[c1], v.t) + res_vcorr<T, FEQ2D>(S, a.feq, a.feq_rs, q, j, c0, c1, v, nv);
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < RPT + 2; ++k) {
+                    const int q = wrap1(q0 + k, nx);
+                    const VShift<T> v = S.vsh[q];
+                    const T* hr = res_row<T, RC>(cluster, cur, q, nv, me);
+                    const int c0 = wrap1(j + v.m, nv);
+                    const int c1 = c0 + 1 == nv ? 0 : c0 + 1;
+                    o[k] = lerp(hr[c0], hr[c1], v.t) + res_vcorr<T, FEQ2D>(S, a.feq, a.feq_rs, q, j, c0, c1, v, nv);
+                }
             }
             // d on rows g+m .. g+m+RPT (= f_{n+1} - f_eq)
-            T d[RPT + 1];
-            const int dq = wrap1(g + m, nx);
+            dq = wrap1(g + m, nx);
 #pragma unroll
             for (int k = 0; k <= RPT; ++k) {
                 d[k] = lerp(o[k], o[k + 1], t);
                 if (FEQ2D) d[k] += (T)res_xcorr(a.feq, a.feq_rs, nx, wrap1(dq + k, nx), m, t64, j);
             }
+            if (!last) {
+#pragma unroll
+                for (int k = 0; k < RPT; ++k) {
+                    T h = lerp(d[k], d[k + 1], t);
+                    if (FEQ2D) h += (T)res_xcorr(a.feq, a.feq_rs, nx, g + k, m, t64, j);
+                    hv[k] = h;
+                    nxt[(rt + k) * nv + j] = h;
+                    Wt[(rt + k) * nv + j] = wj * h;
+                }
+            }
+        }
+        T* rs = ((n + 1) & 1) ? S.vec1 : S.vec0;
+        if (!last) res_rowsum_broadcast<T, RC>(cluster, Wt, rs, nv, gr0, CN);
+        cluster_arrive();
+        // outputs to global memory, overlapped with the barrier
+        if (colv) {
             if (a.f_hist != nullptr || (a.f_final != nullptr && last)) {
 #pragma unroll
                 for (int k = 0; k < RPT; ++k) {
@@ -335,21 +379,12 @@ __global__ void __launch_bounds__(1024) vp_res_fwd_kernel(const ResFwdArgs<T> a)
                     if (a.f_final != nullptr && last) a.f_final[(size_t)q * nv + j] = f;
                 }
             }
-            if (!last) {
+            if (!last && a.h_tape != nullptr) {
 #pragma unroll
-                for (int k = 0; k < RPT; ++k) {
-                    const int i = g + k;
-                    T h = lerp(d[k], d[k + 1], t);
-                    if (FEQ2D) h += (T)res_xcorr(a.feq, a.feq_rs, nx, i, m, t64, j);
-                    nxt[(size_t)(rt + k) * nv + j] = h;
-                    Wt[(size_t)(rt + k) * nv + j] = wj * h;
-                    if (a.h_tape != nullptr) a.h_tape[((size_t)(n + 1) * nx + i) * nv + j] = h;
-                }
+                for (int k = 0; k < RPT; ++k) a.h_tape[((size_t)(n + 1) * nx + g + k) * nv + j] = hv[k];
             }
         }
-        T* rs = ((n + 1) & 1) ? S.vec1 : S.vec0;
-        if (!last) res_rowsum_broadcast<T, RC>(cluster, Wt, rs, nv, gr0, CN);
-        cluster.sync();
+        cluster_wait();
         if (!last) res_fwd_field<T>(a, S, cluster, rs, n + 1, gr0, RC, me, CN);
     }
     // energy of the last step (its partials were stored before the last barrier)
@@ -376,7 +411,7 @@ __device__ void res_bwd_field(const ResBwdArgs<T>& a, ResSmem<T>& S, const T* su
     for (int i = threadIdx.x; i < nx; i += blockDim.x) {
         T gEt = a.neg_dt_dv * sums[i];
         if (a.g_Eh != nullptr) gEt += __ldg(a.g_Eh + (size_t)s * nx + i);
-        if (i >= gr0 && i < gr0 + RC) a.g_H[i] += gEt;
+        if (i >= gr0 && i < gr0 + RC) S.own[i - gr0] += gEt;
         S.aux[i] = gEt + a.dx * trap_w<T>(i, nx) * __ldg(a.E_tape + (size_t)s * nx + i) * gee;
     }
     const int first = ((gr0 + a.win_lo) % nx + nx) % nx;
@@ -430,7 +465,7 @@ __global__ void __launch_bounds__(1024) vp_res_bwd_kernel(const ResBwdArgs<T> a)
     T* Wb[2] = {S.p0, S.p1};   // cotangent on the v-step output of even / odd steps, own rows
     T* Wt = S.p2;              // slope * w for the row sums
     res_init_tables<T>(S, a.P, a.feq, FEQ2D, nx, nv);
-    for (int r = threadIdx.x; r < RC; r += blockDim.x) a.g_H[gr0 + r] = T(0);
+    for (int r = threadIdx.x; r < RC; r += blockDim.x) S.own[r] = T(0);
     int m = 0;
     T t = T(0), wr = T(0);
     if (colv) {
@@ -503,9 +538,11 @@ __global__ void __launch_bounds__(1024) vp_res_bwd_kernel(const ResBwdArgs<T> a)
         }
         T* rs = ((n - 1) & 1) ? S.vec1 : S.vec0;
         if (n > 0) res_rowsum_broadcast<T, RC>(cluster, Wt, rs, nv, gr0, CN);
-        cluster.sync();
+        cluster_arrive();
+        cluster_wait();
         if (n > 0) res_bwd_field<T>(a, S, rs, n - 1, gr0, RC);
     }
+    for (int r = threadIdx.x; r < RC; r += blockDim.x) a.g_H[gr0 + r] = S.own[r];
 }
 
 // ---------------------------------------------------------------------------------------------
