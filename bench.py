@@ -43,7 +43,8 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "roofline"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "roofline"])
+    ap.add_argument("--instances", type=int, default=256, help="c4: instances per GPU")
     ap.add_argument("--dtype", default="float32", choices=["float32", "float64"])
     ap.add_argument("--checkpoint-every", type=int, default=None)
     ap.add_argument("--cluster-size", type=int, default=None,
@@ -414,17 +415,247 @@ def e2e_public_api(args, solver, wl, dev, flush):
                     "and field coefficients in, J and dJ/dcoeffs out"}
 
 
+def cpu_baseline_ensemble(ew, target_s: float):
+    """The oracle's forward + adjoint over the ensemble's instances in order, each for the
+    ensemble's full step count, until about ``target_s`` seconds have passed."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import vp_oracle as O
+
+    cores, impl, OC = 1, "numpy float64 restatement (1 thread)", None
+    try:
+        import vp_oracle_c as OC  # optional OpenMP build
+        if OC.available():
+            cores = OC.threads()
+            impl = f"C float64 restatement, OpenMP x{cores}"
+        else:
+            OC = None
+    except ImportError:
+        OC = None
+    T = ew.n_steps
+    done_cells = 0
+    n_done = 0
+    t0 = time.perf_counter()
+    for i in range(ew.n):
+        g = O.grid_from(ew.meshes[i])
+        H = ew.H(i)
+        if OC is not None:
+            OC.forward_backward(g, ew.dt, ew.f_eqs[i], ew.f_ivs[i], H, T)
+        else:
+            fwd = O.delta_forward(g, ew.dt, ew.f_eqs[i], ew.f_ivs[i], H, T)
+            O.delta_backward(g, ew.dt, ew.f_eqs[i], ew.f_ivs[i], H, T, np.zeros((g.nx, g.nv)),
+                             None, np.zeros((T, g.nx)), np.full(T, ew.dt))
+            del fwd
+        done_cells += g.nx * g.nv * T
+        n_done += 1
+        if time.perf_counter() - t0 > target_s:
+            break
+    el = time.perf_counter() - t0
+    sample = (f"{impl}: forward + adjoint of the first {n_done} of the {ew.n} instances, "
+              f"{T} time steps each")
+    return done_cells / el, cores, "port", sample
+
+
+def run_ensemble(args, rank, local_rank, world):
+    """C4: the uneven ensemble, one persistent launch per time step, the forward and the adjoint
+    loops each replayed as one CUDA graph. Weak scaling: every rank takes an LPT shard of an
+    ensemble of ``instances * world`` instances."""
+    import torch
+    import torch.distributed as dist
+
+    from warp_vp_solver_b200 import _capi
+    from warp_vp_solver_b200.ensemble import Ensemble
+    from warp_vp_solver_b200.sharding import lpt_shards
+    from warp_vp_solver_b200.workloads import make_ensemble_workload
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dtype = torch.float32 if args.dtype == "float32" else torch.float64
+    full = make_ensemble_workload("c4", args.instances * world, seed=0)
+    shards = lpt_shards([m.nx * m.nv for m in full.meshes], world)
+    ew = full.subset(shards[rank])
+    ens = Ensemble(ew.meshes, ew.dt, ew.f_eqs, dtype=dtype, device=dev)
+    lib = _capi.load()
+    T = ew.n_steps
+    f_iv = ens.pack_cells(ew.f_ivs)
+    H = ens.pack_rows([ew.H(i) for i in range(ew.n)])
+    out = ens.alloc_outputs(T, want_tape=True, want_f_final=False)
+    g_ee = torch.full((ens.n * T,), ew.dt, dtype=dtype, device=dev)
+    g_fiv = torch.empty(ens.total_cells, dtype=dtype, device=dev)
+    g_H = torch.empty(ens.total_rows, dtype=dtype, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    def fwd():
+        ens.forward_into(f_iv, H, T, out)
+
+    def bwd():
+        ens.backward_into(H, T, out["tape"], None, None, g_ee, g_fiv, g_H)
+
+    lib.vp_reset_launch_count()
+    fwd()
+    n_fwd = lib.vp_launch_count()
+    lib.vp_reset_launch_count()
+    bwd()
+    n_bwd = lib.vp_launch_count()
+    torch.cuda.synchronize()
+    use_graph = not args.no_graph
+    if use_graph:
+        g_fwd, g_bwd = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g_fwd):
+            fwd()
+        with torch.cuda.graph(g_bwd):
+            bwd()
+        run_f, run_b = g_fwd.replay, g_bwd.replay
+    else:
+        run_f, run_b = fwd, bwd
+    for _ in range(args.warmup):
+        flush.zero_()
+        run_f()
+        run_b()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local_rank) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            ev[i][0].record()
+            run_f()
+            ev[i][1].record()
+            run_b()
+            ev[i][2].record()
+        torch.cuda.synchronize()
+    tf_ms = sum(a.elapsed_time(b) for a, b, _ in ev)
+    tb_ms = sum(b.elapsed_time(c) for _, b, c in ev)
+    cells_all = torch.tensor([float(ens.total_cells)], dtype=torch.float64, device=dev)
+    tt = torch.tensor([tf_ms + tb_ms, tf_ms, tb_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dist.all_reduce(cells_all, op=dist.ReduceOp.SUM)
+        dist.barrier()
+    total_ms, tf_ms, tb_ms = (float(x) for x in tt.cpu())
+    cells = ens.total_cells
+    value = float(cells_all.item()) * T * args.steps / (total_ms * 1e-3)
+
+    peak, peak_kind = measured_peaks()
+    n_launch = T + 1   # prologue + T steps (forward); prologue + T-1 steps + epilogue (adjoint)
+    f_launch_ms, b_launch_ms = tf_ms / (args.steps * n_launch), tb_ms / (args.steps * n_launch)
+    if b_launch_ms >= f_launch_ms:
+        kname, per_ms, alg = "vp_batch_bwd_kernel", b_launch_ms, BYTES_BWD * cells
+    else:
+        kname, per_ms, alg = "vp_batch_fwd_kernel", f_launch_ms, BYTES_FWD * cells
+    achieved = alg / (per_ms * 1e-3) / 1e9
+    roof = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": peak,
+            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": profile_traffic(kname, "c4"),
+            "algorithmic_bytes_per_launch": alg, "avg_launch_us": round(per_ms * 1e3, 3),
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+            else "fallback 6650 GB/s",
+            "note": "time per persistent ensemble launch averaged over graph replays of the timed "
+                    "steps; the packed state of all instances is read and written once per launch"}
+    e2e = None if args.no_e2e else e2e_ensemble(args, ens, ew, dev, flush)
+    shapes = {}
+    for m in ew.meshes:
+        shapes[f"{m.nx}x{m.nv}"] = shapes.get(f"{m.nx}x{m.nv}", 0) + 1
+    line = {
+        "metric": "cell-steps/s fwd+adjoint",
+        "value": round(value, 1),
+        "unit": "cell-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(total_ms / args.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32" if dtype == torch.float32 else "f64",
+        "data": "synthetic (seeded uneven two-stream ensemble)",
+        "config": {"workload": full.description if world == 1 else
+                   f"{args.instances} instances per GPU (LPT shard of {full.n}); " + full.description,
+                   "instances": ew.n, "cells_per_step": cells, "n_time_steps": T,
+                   "shapes": shapes, "parallelism": f"ensemble shards x{world}" if world > 1 else "single",
+                   "l2": "flushed between timed steps (256 MiB write, untimed)",
+                   "cuda_graph": use_graph, "path": "ensemble persistent launch per time step",
+                   "fwd_ms_per_step": round(tf_ms / args.steps, 4),
+                   "bwd_ms_per_step": round(tb_ms / args.steps, 4)},
+        "roofline": roof,
+        "e2e": e2e,
+        "gpu_launches": int((n_fwd + n_bwd) * args.steps),
+        "clocks": clk.summary(),
+    }
+    return line, ew
+
+
+def e2e_ensemble(args, ens, ew, dev, flush):
+    """Same metric through ``Ensemble.run_forward_torch`` + autograd: pinned host f_iv and
+    per-instance field coefficients in, J and dJ/dcoefficients out."""
+    import torch
+
+    rows_inst = np.repeat(np.arange(ew.n), [m.nx for m in ew.meshes])
+    basis = np.concatenate([
+        np.concatenate([np.cos(ew.k0(i) * np.arange(1, 9)[None, :] * m.xs[:, None]),
+                        np.sin(ew.k0(i) * np.arange(1, 9)[None, :] * m.xs[:, None])], axis=1)
+        for i, m in enumerate(ew.meshes)])
+    B = torch.tensor(basis, dtype=ens.dtype, device=dev)
+    ri = torch.tensor(rows_inst, device=dev)
+    f_host = torch.from_numpy(np.concatenate([np.asarray(f).reshape(-1) for f in ew.f_ivs])).pin_memory()
+    c_host = torch.from_numpy(np.stack([np.asarray(c).reshape(-1) for c in ew.coeffs])).pin_memory()
+    J_out = torch.empty((), dtype=torch.float64).pin_memory()
+    g_out = torch.empty(c_host.shape, dtype=torch.float64).pin_memory()
+    T = ew.n_steps
+
+    def step():
+        f0 = f_host.to(dev, non_blocking=True)
+        c = c_host.to(dev, non_blocking=True).requires_grad_(True)
+        Hp = (B * c.to(ens.dtype)[ri]).sum(1)
+        _, _, ee = ens.run_forward_torch(f0, Hp, T)
+        J = ee.double().sum() * ew.dt
+        J.backward()
+        g_out.copy_(c.grad, non_blocking=True)
+        J_out.copy_(J.detach(), non_blocking=True)
+
+    for _ in range(max(2, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        step()
+        b.record()
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+    ms = sum(times) / len(times)
+    world = dist_env()[2]
+    return {"value": round(ens.total_cells * T * world / (ms * 1e-3), 1), "unit": "cell-steps/s",
+            "h2d_bytes_per_step": int(f_host.numel() * 8 + c_host.numel() * 8),
+            "d2h_bytes_per_step": int(8 + g_out.numel() * 8),
+            "ms_per_step": round(ms, 4),
+            "path": "Ensemble.run_forward_torch + torch.autograd, pinned host f_iv and field "
+                    "coefficients in, J and dJ/dcoefficients out"}
+
+
 def run_reference(args, rank, world):
     """CPU restatement of the reference algorithm on the host cores (rank 0 only)."""
-    from warp_vp_solver_b200.workloads import make_workload
+    from warp_vp_solver_b200.workloads import make_ensemble_workload, make_workload
 
-    wl = make_workload(args.workload)
+    if args.workload == "c4":
+        wl = make_ensemble_workload("c4", args.instances, seed=0)
+        base = cpu_baseline_ensemble
+        desc = {"workload": wl.description, "instances": wl.n, "cells_per_step": wl.cells,
+                "n_time_steps": wl.n_steps}
+    else:
+        wl = make_workload(args.workload)
+        base = cpu_baseline
+        desc = {"workload": wl.description, "nx": wl.mesh.nx, "nv": wl.mesh.nv,
+                "n_time_steps": wl.n_steps}
     vals = []
     info = None
     for _ in range(args.warmup):
-        cpu_baseline(wl, min(args.cpu_seconds, 2.0))
+        base(wl, min(args.cpu_seconds, 2.0))
     for _ in range(args.steps):
-        v, cores, kind, sample = cpu_baseline(wl, args.cpu_seconds / max(1, args.steps) * 4)
+        v, cores, kind, sample = base(wl, args.cpu_seconds / max(1, args.steps) * 4)
         vals.append(v)
         info = (cores, kind, sample)
     value = statistics.median(vals)
@@ -443,8 +674,7 @@ def run_reference(args, rank, world):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": wl.description, "nx": wl.mesh.nx, "nv": wl.mesh.nv,
-                   "n_time_steps": wl.n_steps},
+        "config": desc,
         "cpu_baseline": {"value": round(value, 1), "unit": "cell-steps/s", "cores": cores,
                          "kind": kind, "sample": sample},
         "e2e": {"value": round(value, 1), "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
@@ -467,9 +697,14 @@ def main():
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        line, wl = run_ours(args, rank, local_rank, world)
+        if args.workload == "c4":
+            line, wl = run_ensemble(args, rank, local_rank, world)
+            base = cpu_baseline_ensemble
+        else:
+            line, wl = run_ours(args, rank, local_rank, world)
+            base = cpu_baseline
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
-            v, cores, kind, sample = cpu_baseline(wl, args.cpu_seconds)
+            v, cores, kind, sample = base(wl, args.cpu_seconds)
             line["cpu_baseline"] = {"value": round(v, 1), "unit": "cell-steps/s", "cores": cores,
                                     "kind": kind, "sample": sample}
         else:

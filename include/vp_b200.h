@@ -147,6 +147,42 @@ int vp_backward(vp_plan* plan, const void* H, int32_t n_steps,
 int vp_forward_noalloc(vp_plan* plan, const double* f_iv, const void* H, int32_t n_steps,
                        double* f_final, void* f_hist, void* E_hist, void* ee_hist, void* stream);
 
+/* --- ensembles ------------------------------------------------------------------------------
+ * Many instances (each with its own mesh, dt, f_eq, initial state and field) advanced together:
+ * one persistent launch per time step covers every instance. No counterpart in the reference,
+ * which advances one WarpVlasovPoissonSolver at a time (warp_vp_solver/solver.py:418-612,
+ * 742-1105); each instance's numerics are exactly those of vp_forward / vp_backward.
+ * Packed layouts (instance i, in the order given to vp_batch_create):
+ *   cell arrays (f_iv, f_final, g_f_final, g_f_iv): the (nx_i, nv_i) block at cell offset i;
+ *   row arrays (H, g_H): the nx_i block at row offset i;
+ *   E_hist / g_E_hist: the (n_steps, nx_i) block at n_steps * row offset i;
+ *   ee_hist / g_ee_hist: the n_steps entries at i * n_steps.
+ * Offsets come from vp_batch_offsets. The adjoint needs the tape of the forward call. */
+typedef struct vp_batch vp_batch;
+
+int vp_batch_create(int32_t n_instances, const vp_mesh_desc* meshes, const double* dts,
+                    const double* const* f_eq_host, int dtype, vp_batch** out_batch);
+int vp_batch_destroy(vp_batch* batch);
+
+/* Total packed sizes (cells and rows) and the per-instance offsets (arrays of n_instances;
+ * either may be NULL). */
+int vp_batch_offsets(const vp_batch* batch, int64_t* total_cells, int64_t* total_rows,
+                     int64_t* cell_offsets, int64_t* row_offsets);
+int vp_batch_workspace_bytes(const vp_batch* batch, int32_t n_steps, size_t* out_bytes);
+int vp_batch_tape_bytes(const vp_batch* batch, int32_t n_steps, size_t* out_bytes);
+
+/* Forward of every instance for n_steps steps (all pointers device memory, packed as above).
+ * f_final, E_hist, ee_hist and tape may be NULL. */
+int vp_batch_forward(vp_batch* batch, const double* f_iv, const void* H, int32_t n_steps,
+                     double* f_final, void* E_hist, void* ee_hist, void* tape,
+                     void* workspace, size_t workspace_bytes, void* stream);
+
+/* Adjoint of every instance; cotangents may be NULL (zero). Outputs g_f_iv and g_H. */
+int vp_batch_backward(vp_batch* batch, const void* H, int32_t n_steps, const void* tape,
+                      const void* g_f_final, const void* g_E_hist, const void* g_ee_hist,
+                      void* g_f_iv, void* g_H, void* workspace, size_t workspace_bytes,
+                      void* stream);
+
 /* --- single-stage operators (the reference's helper methods and unit-tested kernels) ------ */
 
 /* rho[i] = dv * trapz_j(f_eq[i,j] - f[i,j]). Replaces compute_rho (warp_vp_solver/solver.py:

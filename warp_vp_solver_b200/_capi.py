@@ -82,6 +82,17 @@ SIGNATURES = {
     "vp_backward": (c_int, [c_vp, c_vp, c_i32, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
                             c_vp, c_size, c_vp]),
     "vp_forward_noalloc": (c_int, [c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "vp_batch_create": (c_int, [c_i32, ctypes.POINTER(MeshDesc), ctypes.POINTER(c_dbl),
+                                ctypes.POINTER(ctypes.POINTER(c_dbl)), c_int, ctypes.POINTER(c_vp)]),
+    "vp_batch_destroy": (c_int, [c_vp]),
+    "vp_batch_offsets": (c_int, [c_vp, ctypes.POINTER(c_i64), ctypes.POINTER(c_i64),
+                                 ctypes.POINTER(c_i64), ctypes.POINTER(c_i64)]),
+    "vp_batch_workspace_bytes": (c_int, [c_vp, c_i32, ctypes.POINTER(c_size)]),
+    "vp_batch_tape_bytes": (c_int, [c_vp, c_i32, ctypes.POINTER(c_size)]),
+    "vp_batch_forward": (c_int, [c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_size,
+                                 c_vp]),
+    "vp_batch_backward": (c_int, [c_vp, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                  c_size, c_vp]),
     "vp_compute_rho": (c_int, [c_vp, c_vp, c_vp, c_vp]),
     "vp_poisson": (c_int, [c_vp, c_vp, c_vp, c_int, c_vp]),
     "vp_electric_energy": (c_int, [c_vp, c_vp, c_vp, c_vp]),

@@ -62,6 +62,8 @@ struct vp_plan {
     size_t tail_smem = 0;      // dynamic shared memory of the separate tail launch (0: global scratch)
     int tail_threads = 0;
     LaunchCfg cfg{};
+    std::vector<double> host_feq;  // f_eq as given (host), for recognising identical plans
+    std::vector<double> host_vs;
     int res_cn = 0;            // cluster size of the cluster-resident path (0: not used)
     long long mx_lo = 0, mx_hi = 0;  // extremes of the unreduced x half-step offsets floor(-s_j)
     int res_threads = 0;
@@ -619,6 +621,8 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
     for (int i = 1; i < nx && inv; ++i)
         inv = std::memcmp(f_eq_host + (size_t)i * nv, f_eq_host, (size_t)nv * sizeof(double)) == 0;
     p->feq2d = inv ? 0 : 1;
+    p->host_feq.assign(f_eq_host, f_eq_host + (size_t)nx * nv);
+    p->host_vs.assign(mesh->vs, mesh->vs + nv);
 
     // x half-step table: s_j = 0.5*v_j*dt/dx, m_j = floor(-s_j) mod nx, t_j = -s_j - floor(-s_j)
     std::vector<int> mx(nv);
@@ -1048,6 +1052,428 @@ int vp_semilag_v(vp_plan* plan, const void* in, const void* E_total, void* out, 
                         : launch_semilag_v<float>(plan->nx, plan->nv, plan->dv, dt, (const float*)in, (const float*)E_total,
                                                   (float*)out, adjoint, (const float*)f_in, (float*)g_E, s);
     return e == cudaSuccess ? VP_OK : cuda_err(e, "semilag_v launch");
+}
+
+}  // extern "C"
+
+// =============================================================================================
+// Ensembles
+// =============================================================================================
+
+struct vp_batch {
+    int n = 0, dtype = VP_F32, device = 0, R = 1, threads = 128, feq2d = 0;
+    std::vector<vp_plan*> owned;          // distinct plans
+    std::vector<vp_plan*> plan_of;        // plan of each instance (caller order)
+    std::vector<long long> off_f;         // caller order
+    std::vector<long long> off_x;
+    long long total_f = 0, total_x = 0, total_part = 0;
+    int n_tiles = 0, grid_fwd = 0, grid_bwd = 0;
+    size_t smem = 0;
+    void* d_inst = nullptr;
+};
+
+namespace vpb {
+
+struct BatchWs {
+    size_t h0, h1, part, counters, vsh, E, grho, total;
+};
+
+static BatchWs batch_ws(const vp_batch* b) {
+    const size_t rs = b->dtype == VP_F64 ? 8 : 4, vs = b->dtype == VP_F64 ? 16 : 8;
+    BatchWs L{};
+    size_t off = 0;
+    L.h0 = off; off += align256((size_t)b->total_f * rs);
+    L.h1 = off; off += align256((size_t)b->total_f * rs);
+    L.part = off; off += align256((size_t)b->total_part * rs);
+    L.counters = off; off += align256((size_t)b->n * sizeof(unsigned));
+    L.vsh = off; off += align256((size_t)b->total_x * vs);
+    L.E = off; off += align256((size_t)b->total_x * rs);
+    L.grho = off; off += align256((size_t)b->total_x * rs);
+    L.total = off;
+    return L;
+}
+
+struct BatchTape {
+    size_t h, E, vsh, total;
+};
+
+static BatchTape batch_tape(const vp_batch* b, int T) {
+    const size_t rs = b->dtype == VP_F64 ? 8 : 4, vs = b->dtype == VP_F64 ? 16 : 8;
+    BatchTape L{};
+    size_t off = 0;
+    L.h = off; off += align256((size_t)T * b->total_f * rs);
+    L.E = off; off += align256((size_t)T * b->total_x * rs);
+    L.vsh = off; off += align256((size_t)T * b->total_x * vs);
+    L.total = off;
+    return L;
+}
+
+template <typename T>
+static void batch_fill(const vp_batch* b, std::vector<BatchInst<T>>& out, const std::vector<int>& order,
+                       const std::vector<int>& chunk_cols) {
+    out.clear();
+    int tile = 0;
+    long long part = 0;
+    for (int k : order) {
+        const vp_plan* p = b->plan_of[k];
+        BatchInst<T> I{};
+        I.nx = p->nx;
+        I.nv = p->nv;
+        I.chunk_cols = chunk_cols[k];
+        I.n_chunks = (p->nv + I.chunk_cols - 1) / I.chunk_cols;
+        I.n_tiles = (p->nx / b->R) * I.n_chunks;
+        I.tile_begin = tile;
+        tile += I.n_tiles;
+        I.off_f = b->off_f[k];
+        I.off_x = (int)b->off_x[k];
+        I.off_part = (int)part;
+        part += (long long)I.n_chunks * p->nx;
+        I.index = k;
+        I.mx = p->d_mx;
+        I.tx = static_cast<const T*>(p->d_tx);
+        I.tx64 = p->d_tx64;
+        I.feq = p->d_feq;
+        I.feq_rs = p->feq2d ? p->nv : 0;
+        I.P = poisson_tables<T>(p, nullptr, nullptr, true);
+        I.dv = (T)p->dv;
+        I.dx = (T)p->dx;
+        I.dtdv = (T)(p->dt / p->dv);
+        I.neg_dt_dv = (T)(-p->dt / p->dv);
+        out.push_back(I);
+    }
+}
+
+static void free_batch(vp_batch* b) {
+    if (!b) return;
+    for (vp_plan* p : b->owned) free_plan(p);
+    if (b->d_inst) {
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(b->device);
+        cudaFree(b->d_inst);
+        cudaSetDevice(prev);
+    }
+    delete b;
+}
+
+template <typename T>
+static int batch_forward_impl(vp_batch* b, const double* f_iv, const T* H, int Ts, double* f_final,
+                              T* E_hist, T* ee_hist, unsigned char* tape, unsigned char* ws, cudaStream_t s) {
+    const BatchWs L = batch_ws(b);
+    const BatchTape TL = batch_tape(b, Ts);
+    T* hb[2] = {reinterpret_cast<T*>(ws + L.h0), reinterpret_cast<T*>(ws + L.h1)};
+    VShift<T>* vsh_ws = reinterpret_cast<VShift<T>*>(ws + L.vsh);
+    T* E_ws = reinterpret_cast<T*>(ws + L.E);
+    T* th = tape ? reinterpret_cast<T*>(tape + TL.h) : nullptr;
+    T* tE = tape ? reinterpret_cast<T*>(tape + TL.E) : nullptr;
+    VShift<T>* tv = tape ? reinterpret_cast<VShift<T>*>(tape + TL.vsh) : nullptr;
+    VP_CUDA(cudaMemsetAsync(ws + L.counters, 0, (size_t)b->n * sizeof(unsigned), s), "memset(counters)");
+    BatchStep<T> st{};
+    st.inst = static_cast<const BatchInst<T>*>(b->d_inst);
+    st.n_inst = b->n;
+    st.n_tiles = b->n_tiles;
+    st.n_steps = Ts;
+    st.H = H;
+    st.part = reinterpret_cast<T*>(ws + L.part);
+    st.counters = reinterpret_cast<unsigned*>(ws + L.counters);
+    st.E_hist = E_hist;
+    st.ee_hist = ee_hist;
+    auto set_out = [&](int n) {   // slots written for step n (h_n, shifts/E of step n)
+        if (tape) {
+            st.c_out = th; st.c_out_mul = Ts; st.c_out_step = n;
+            st.vsh_out = tv; st.vsh_out_mul = Ts; st.vsh_out_step = n;
+            st.E_out = tE; st.E_out_mul = Ts; st.E_out_step = n;
+        } else {
+            st.c_out = hb[n & 1]; st.c_out_mul = 1; st.c_out_step = 0;
+            st.vsh_out = vsh_ws; st.vsh_out_mul = 1; st.vsh_out_step = 0;
+            st.E_out = E_ws; st.E_out_mul = 1; st.E_out_step = 0;
+        }
+    };
+    // prologue
+    st.f_iv = f_iv;
+    st.last = 0;
+    st.hist_step = 0;
+    set_out(0);
+    VP_CUDA(launch_batch_fwd<T>(st, b->R, 0, b->feq2d != 0, b->grid_fwd, b->threads, b->smem, s), "batch prologue");
+    st.f_iv = nullptr;
+    for (int n = 0; n < Ts; ++n) {
+        const bool last = (n == Ts - 1);
+        if (tape) {
+            st.c_in = th; st.c_in_mul = Ts; st.c_in_step = n;
+            st.vsh_in = tv; st.vsh_in_mul = Ts; st.vsh_in_step = n;
+        } else {
+            st.c_in = hb[n & 1]; st.c_in_mul = 1; st.c_in_step = 0;
+            st.vsh_in = vsh_ws; st.vsh_in_mul = 1; st.vsh_in_step = 0;
+        }
+        if (last) {
+            st.c_out = nullptr;
+        } else {
+            set_out(n + 1);
+        }
+        st.last = last ? 1 : 0;
+        st.hist_step = n + 1;
+        st.f_final = last ? f_final : nullptr;
+        VP_CUDA(launch_batch_fwd<T>(st, b->R, 1, b->feq2d != 0, b->grid_fwd, b->threads, b->smem, s), "batch step");
+    }
+    return VP_OK;
+}
+
+template <typename T>
+static int batch_backward_impl(vp_batch* b, const T* H, int Ts, const unsigned char* tape, const T* g_ff,
+                               const T* g_Eh, const T* g_ee, T* g_fiv, T* g_H, unsigned char* ws,
+                               cudaStream_t s) {
+    const BatchWs L = batch_ws(b);
+    const BatchTape TL = batch_tape(b, Ts);
+    T* wb[2] = {reinterpret_cast<T*>(ws + L.h0), reinterpret_cast<T*>(ws + L.h1)};
+    const T* th = reinterpret_cast<const T*>(tape + TL.h);
+    const T* tE = reinterpret_cast<const T*>(tape + TL.E);
+    const VShift<T>* tv = reinterpret_cast<const VShift<T>*>(tape + TL.vsh);
+    T* grho = reinterpret_cast<T*>(ws + L.grho);
+    VP_CUDA(cudaMemsetAsync(ws + L.counters, 0, (size_t)b->n * sizeof(unsigned), s), "memset(counters)");
+    VP_CUDA(cudaMemsetAsync(g_H, 0, (size_t)b->total_x * sizeof(T), s), "memset(g_H)");
+    BatchStep<T> st{};
+    st.inst = static_cast<const BatchInst<T>*>(b->d_inst);
+    st.n_inst = b->n;
+    st.n_tiles = b->n_tiles;
+    st.n_steps = Ts;
+    st.H = H;
+    st.part = reinterpret_cast<T*>(ws + L.part);
+    st.counters = reinterpret_cast<unsigned*>(ws + L.counters);
+    st.g_Eh = g_Eh;
+    st.g_ee = g_ee;
+    st.g_H = g_H;
+    st.grho_out = grho;
+    // prologue (n = T)
+    st.g_ff = g_ff;
+    st.c_out = wb[(Ts - 1) & 1]; st.c_out_mul = 1; st.c_out_step = 0;
+    st.h_prev = th; st.h_prev_step = Ts - 1;
+    st.vsh_prev = tv; st.vsh_prev_step = Ts - 1;
+    st.E_prev = tE; st.E_prev_step = Ts - 1;
+    st.g_step = Ts - 1;
+    VP_CUDA(launch_batch_bwd<T>(st, b->R, 0, b->feq2d != 0, b->grid_bwd, b->threads, b->smem, s), "batch bwd prologue");
+    st.g_ff = nullptr;
+    st.grho = grho;
+    for (int n = Ts - 1; n >= 1; --n) {
+        st.c_in = wb[n & 1]; st.c_in_mul = 1; st.c_in_step = 0;
+        st.c_out = wb[(n - 1) & 1];
+        st.vsh_in = tv; st.vsh_in_mul = Ts; st.vsh_in_step = n;
+        st.h_prev_step = n - 1;
+        st.vsh_prev_step = n - 1;
+        st.E_prev_step = n - 1;
+        st.g_step = n - 1;
+        VP_CUDA(launch_batch_bwd<T>(st, b->R, 1, b->feq2d != 0, b->grid_bwd, b->threads, b->smem, s), "batch bwd step");
+    }
+    st.c_in = wb[0]; st.c_in_mul = 1; st.c_in_step = 0;
+    st.c_out = nullptr;
+    st.vsh_in = tv; st.vsh_in_mul = Ts; st.vsh_in_step = 0;
+    st.g_fiv = g_fiv;
+    VP_CUDA(launch_batch_bwd<T>(st, b->R, 2, b->feq2d != 0, b->grid_bwd, b->threads, b->smem, s), "batch bwd epilogue");
+    return VP_OK;
+}
+
+}  // namespace vpb
+
+extern "C" {
+
+int vp_batch_create(int32_t n, const vp_mesh_desc* meshes, const double* dts,
+                    const double* const* f_eq_host, int dtype, vp_batch** out) {
+    if (!out) return set_err(VP_ERR_ARG, "out_batch must not be NULL");
+    *out = nullptr;
+    if (n < 1) return set_err(VP_ERR_ARG, "n_instances must be >= 1 (got %d)", n);
+    if (!meshes || !dts || !f_eq_host) return set_err(VP_ERR_ARG, "meshes, dts and f_eq_host must not be NULL");
+    vp_batch* b = new (std::nothrow) vp_batch();
+    if (!b) return set_err(VP_ERR_ARG, "out of host memory");
+    b->n = n;
+    b->dtype = dtype;
+    cudaGetDevice(&b->device);
+    // one plan per distinct (mesh, dt, f_eq)
+    for (int i = 0; i < n; ++i) {
+        vp_plan* found = nullptr;
+        const vp_mesh_desc& m = meshes[i];
+        for (vp_plan* p : b->owned) {
+            if (p->nx == m.nx && p->nv == m.nv && p->dx == m.dx && p->dv == m.dv && p->dt == dts[i] &&
+                p->period_x == m.period_x && p->period_v == m.period_v && p->host_feq.size() == (size_t)m.nx * m.nv &&
+                std::memcmp(p->host_feq.data(), f_eq_host[i], sizeof(double) * (size_t)m.nx * m.nv) == 0 &&
+                std::memcmp(p->host_vs.data(), m.vs, sizeof(double) * (size_t)m.nv) == 0) {
+                found = p;
+                break;
+            }
+        }
+        if (!found) {
+            int rc = vp_plan_create(&m, dts[i], f_eq_host[i], dtype, &found);
+            if (rc != VP_OK) {
+                free_batch(b);
+                return rc;
+            }
+            b->owned.push_back(found);
+        }
+        b->plan_of.push_back(found);
+    }
+    // common rows-per-tile and per-instance column chunks
+    int R = 8;
+    for (;;) {
+        bool ok = true;
+        for (vp_plan* p : b->plan_of) ok = ok && (p->nx % R == 0) && (R == 1 || R <= p->nx / 2);
+        if (ok || R == 1) break;
+        R /= 2;
+    }
+    b->R = R;
+    int max_nx = 0;
+    bool feq2d = false;
+    std::vector<int> chunk_cols(n);
+    for (int i = 0; i < n; ++i) {
+        vp_plan* p = b->plan_of[i];
+        chunk_cols[i] = p->nv >= 128 ? 128 : ((p->nv + 31) / 32) * 32;
+        max_nx = std::max(max_nx, p->nx);
+        feq2d = feq2d || p->feq2d;
+        b->off_f.push_back(b->total_f);
+        b->off_x.push_back(b->total_x);
+        b->total_f += (long long)p->nx * p->nv;
+        b->total_x += p->nx;
+        b->total_part += (long long)((p->nv + chunk_cols[i] - 1) / chunk_cols[i]) * p->nx;
+    }
+    if (b->total_x > 2147483647LL) {
+        free_batch(b);
+        return set_err(VP_ERR_ARG, "ensemble has more than 2^31 rows");
+    }
+    b->feq2d = feq2d ? 1 : 0;
+    b->threads = 128;
+    const size_t rs = dtype == VP_F64 ? 8 : 4;
+    const size_t area = poisson_area_size(max_nx, rs);
+    if (area > 40 * 1024) {
+        free_batch(b);
+        return set_err(VP_ERR_UNSUPPORTED, "ensembles support nx up to the in-kernel Poisson limit (got nx=%d)", max_nx);
+    }
+    b->smem = (((size_t)32 * R * rs + 15) & ~(size_t)15) + area;
+    // longest instances first
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+        return (long long)b->plan_of[a]->nx * b->plan_of[a]->nv > (long long)b->plan_of[c]->nx * b->plan_of[c]->nv;
+    });
+    size_t bytes = 0;
+    std::vector<unsigned char> host;
+    if (dtype == VP_F64) {
+        std::vector<BatchInst<double>> v;
+        batch_fill<double>(b, v, order, chunk_cols);
+        b->n_tiles = v.back().tile_begin + v.back().n_tiles;
+        bytes = v.size() * sizeof(BatchInst<double>);
+        host.assign(reinterpret_cast<unsigned char*>(v.data()), reinterpret_cast<unsigned char*>(v.data()) + bytes);
+    } else {
+        std::vector<BatchInst<float>> v;
+        batch_fill<float>(b, v, order, chunk_cols);
+        b->n_tiles = v.back().tile_begin + v.back().n_tiles;
+        bytes = v.size() * sizeof(BatchInst<float>);
+        host.assign(reinterpret_cast<unsigned char*>(v.data()), reinterpret_cast<unsigned char*>(v.data()) + bytes);
+    }
+    int rc = upload_bytes(&b->d_inst, host.data(), bytes);
+    if (rc != VP_OK) {
+        free_batch(b);
+        return rc;
+    }
+    int n_sms = 148;
+    cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, b->device);
+    const int bf = dtype == VP_F64 ? batch_blocks_per_sm<double>(R, true, feq2d, b->threads, b->smem)
+                                   : batch_blocks_per_sm<float>(R, true, feq2d, b->threads, b->smem);
+    const int bb = dtype == VP_F64 ? batch_blocks_per_sm<double>(R, false, feq2d, b->threads, b->smem)
+                                   : batch_blocks_per_sm<float>(R, false, feq2d, b->threads, b->smem);
+    b->grid_fwd = std::max(1, std::min(b->n_tiles, std::max(1, bf) * n_sms));
+    b->grid_bwd = std::max(1, std::min(b->n_tiles, std::max(1, bb) * n_sms));
+    *out = b;
+    return VP_OK;
+}
+
+int vp_batch_destroy(vp_batch* b) {
+    free_batch(b);
+    return VP_OK;
+}
+
+int vp_batch_offsets(const vp_batch* b, int64_t* total_cells, int64_t* total_rows, int64_t* cell_offsets,
+                     int64_t* row_offsets) {
+    if (!b) return set_err(VP_ERR_ARG, "batch must not be NULL");
+    if (total_cells) *total_cells = b->total_f;
+    if (total_rows) *total_rows = b->total_x;
+    for (int i = 0; i < b->n; ++i) {
+        if (cell_offsets) cell_offsets[i] = b->off_f[i];
+        if (row_offsets) row_offsets[i] = b->off_x[i];
+    }
+    return VP_OK;
+}
+
+int vp_batch_workspace_bytes(const vp_batch* b, int32_t n_steps, size_t* out) {
+    if (!b || !out) return set_err(VP_ERR_ARG, "batch and out_bytes must not be NULL");
+    if (n_steps < 0) return set_err(VP_ERR_ARG, "n_steps must be >= 0");
+    *out = batch_ws(b).total;
+    return VP_OK;
+}
+
+int vp_batch_tape_bytes(const vp_batch* b, int32_t n_steps, size_t* out) {
+    if (!b || !out) return set_err(VP_ERR_ARG, "batch and out_bytes must not be NULL");
+    if (n_steps < 0) return set_err(VP_ERR_ARG, "n_steps must be >= 0");
+    *out = batch_tape(b, n_steps).total;
+    return VP_OK;
+}
+
+static int batch_check_ws(vp_batch* b, void* ws, size_t ws_bytes) {
+    const size_t need = batch_ws(b).total;
+    if (ws_bytes < need) return set_err(VP_ERR_ARG, "workspace has %zu bytes, %zu needed", ws_bytes, need);
+    if (((uintptr_t)ws & 255) != 0) return set_err(VP_ERR_ARG, "workspace must be 256-byte aligned");
+    return check_dev_ptr(ws, "workspace", b->device);
+}
+
+int vp_batch_forward(vp_batch* b, const double* f_iv, const void* H, int32_t n_steps, double* f_final,
+                     void* E_hist, void* ee_hist, void* tape, void* ws, size_t ws_bytes, void* stream) {
+    if (!b) return set_err(VP_ERR_ARG, "batch must not be NULL");
+    if (n_steps < 1) return set_err(VP_ERR_ARG, "ensembles need n_steps >= 1 (got %d)", n_steps);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    CaptureScope capture_scope(stream_capturing(s));
+    int rc;
+    const int dev = b->device;
+    if ((rc = check_dev_ptr(f_iv, "f_iv", dev)) || (rc = check_dev_ptr(H, "H", dev)) ||
+        (rc = check_opt_ptr(f_final, "f_final", dev)) || (rc = check_opt_ptr(E_hist, "E_hist", dev)) ||
+        (rc = check_opt_ptr(ee_hist, "ee_hist", dev)) || (rc = check_opt_ptr(tape, "tape", dev)) ||
+        (rc = batch_check_ws(b, ws, ws_bytes)))
+        return rc;
+    if (tape && ((uintptr_t)tape & 255) != 0) return set_err(VP_ERR_ARG, "tape must be 256-byte aligned");
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != dev) return set_err(VP_ERR_ARG, "current device %d differs from the batch's device %d", cur, dev);
+    unsigned char* w = static_cast<unsigned char*>(ws);
+    unsigned char* t = static_cast<unsigned char*>(tape);
+    if (b->dtype == VP_F64)
+        return batch_forward_impl<double>(b, f_iv, (const double*)H, n_steps, f_final, (double*)E_hist,
+                                          (double*)ee_hist, t, w, s);
+    return batch_forward_impl<float>(b, f_iv, (const float*)H, n_steps, f_final, (float*)E_hist,
+                                     (float*)ee_hist, t, w, s);
+}
+
+int vp_batch_backward(vp_batch* b, const void* H, int32_t n_steps, const void* tape, const void* g_f_final,
+                      const void* g_E_hist, const void* g_ee_hist, void* g_f_iv, void* g_H, void* ws,
+                      size_t ws_bytes, void* stream) {
+    if (!b) return set_err(VP_ERR_ARG, "batch must not be NULL");
+    if (n_steps < 1) return set_err(VP_ERR_ARG, "ensembles need n_steps >= 1 (got %d)", n_steps);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    CaptureScope capture_scope(stream_capturing(s));
+    int rc;
+    const int dev = b->device;
+    if ((rc = check_dev_ptr(H, "H", dev)) || (rc = check_dev_ptr(tape, "tape", dev)) ||
+        (rc = check_opt_ptr(g_f_final, "g_f_final", dev)) || (rc = check_opt_ptr(g_E_hist, "g_E_hist", dev)) ||
+        (rc = check_opt_ptr(g_ee_hist, "g_ee_hist", dev)) || (rc = check_dev_ptr(g_f_iv, "g_f_iv", dev)) ||
+        (rc = check_dev_ptr(g_H, "g_H", dev)) || (rc = batch_check_ws(b, ws, ws_bytes)))
+        return rc;
+    if (((uintptr_t)tape & 255) != 0) return set_err(VP_ERR_ARG, "tape must be 256-byte aligned");
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != dev) return set_err(VP_ERR_ARG, "current device %d differs from the batch's device %d", cur, dev);
+    unsigned char* w = static_cast<unsigned char*>(ws);
+    const unsigned char* t = static_cast<const unsigned char*>(tape);
+    if (b->dtype == VP_F64)
+        return batch_backward_impl<double>(b, (const double*)H, n_steps, t, (const double*)g_f_final,
+                                           (const double*)g_E_hist, (const double*)g_ee_hist, (double*)g_f_iv,
+                                           (double*)g_H, w, s);
+    return batch_backward_impl<float>(b, (const float*)H, n_steps, t, (const float*)g_f_final,
+                                      (const float*)g_E_hist, (const float*)g_ee_hist, (float*)g_f_iv,
+                                      (float*)g_H, w, s);
 }
 
 }  // extern "C"

@@ -87,6 +87,61 @@ template <typename T> struct BwdArgs {
     T* grho_out;                // cotangent on rho of step n-1
 };
 
+// ---- ensembles: many instances (any nx, nv, dt, f_eq) advanced together -----------------------
+// Packed layouts: per-instance (nx, nv) blocks at off_f, nx blocks at off_x. The per-instance
+// device tables (shift tables, f_eq, FFT tables) belong to one vp_plan per instance.
+template <typename T> struct BatchInst {
+    int nx, nv, n_chunks, chunk_cols;
+    int tile_begin, n_tiles;    // tiles of this instance in a step launch
+    long long off_f;            // offset of the (nx, nv) block in packed cell buffers
+    int off_x;                  // offset of the nx block in packed row buffers
+    int off_part;               // offset of its n_chunks*nx partial sums
+    int index;                  // position of the instance in the caller's order
+    const int* mx;
+    const T* tx;
+    const double* tx64;
+    const double* feq;
+    int feq_rs;
+    PoissonTables<T> P;
+    T dv, dx, dtdv, neg_dt_dv;
+};
+
+// One step launch of an ensemble. A cell pointer of instance i is base + mul*off_f[i] + step*nx*nv
+// (a row pointer: base + mul*off_x[i] + step*nx): mul/step select a ping-pong slot (1, 0) or a
+// tape slot (n_steps, n).
+template <typename T> struct BatchStep {
+    const BatchInst<T>* inst;
+    int n_inst, n_tiles;
+    int last;                   // forward: the last step (no h_out, no tail)
+    int n_steps;
+    const double* f_iv;         // prologue (forward)
+    const T* H;
+    const T* c_in; int c_in_mul, c_in_step;   // forward h_n / adjoint w_n
+    T* c_out; int c_out_mul, c_out_step;      // forward h_{n+1} / adjoint w_{n-1}
+    const VShift<T>* vsh_in; int vsh_in_mul, vsh_in_step;     // shifts of step n
+    VShift<T>* vsh_out; int vsh_out_mul, vsh_out_step;        // forward: shifts of step n+1
+    T* E_out; int E_out_mul, E_out_step;                      // forward: raw E of step n+1
+    double* f_final;            // forward, last step
+    T* E_hist;                  // forward: [inst][n_steps][nx], row n+1 (or 0 in the prologue)
+    T* ee_hist;                 // forward: [inst][n_steps]
+    int hist_step;
+    T* part;
+    unsigned* counters;
+    // adjoint
+    const T* grho;              // packed rows, cotangent on rho of step n
+    T* grho_out;
+    const T* h_prev; int h_prev_step;            // tape h of step n-1 (mul = n_steps)
+    const VShift<T>* vsh_prev; int vsh_prev_step; // tape shifts of step n-1
+    const T* E_prev; int E_prev_step;            // tape E of step n-1
+    const double* unused_;
+    const T* g_ff;              // prologue: cotangent on f_final (packed cells)
+    const T* g_Eh;              // [inst][n_steps][nx], row n-1
+    const T* g_ee;              // [inst][n_steps], entry n-1
+    int g_step;
+    T* g_H;
+    T* g_fiv;                   // epilogue
+};
+
 struct LaunchCfg {
     int R;          // rows per CTA
     int threads;    // threads per CTA (one column each)
@@ -189,6 +244,15 @@ int res_max_clusters(bool feq2d, int cn, int rc, int nv, size_t smem);
 bool res_rows_supported(int rc);
 int res_rows_per_thread(int rc, int nv);
 int res_threads(int rc, int nv);
+
+template <typename T>
+cudaError_t launch_batch_fwd(const BatchStep<T>& b, int R, int phase, bool feq2d, int grid,
+                             int threads, size_t smem, cudaStream_t s);
+template <typename T>
+cudaError_t launch_batch_bwd(const BatchStep<T>& b, int R, int phase, bool feq2d, int grid,
+                             int threads, size_t smem, cudaStream_t s);
+template <typename T>
+int batch_blocks_per_sm(int R, bool fwd, bool feq2d, int threads, size_t smem);
 
 void count_launch(int n = 1);
 

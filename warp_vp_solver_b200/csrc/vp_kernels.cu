@@ -96,6 +96,21 @@ __device__ __forceinline__ void store_row_partials(T (&acc)[R], T* red, T* part_
     }
 }
 
+// Completion counter: returns true in every thread of the CTA that finished the last of
+// `total` units of work counted on `counter`.
+__device__ __forceinline__ bool last_unit_done(unsigned* counter, unsigned total, int* flag) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned prev = atomicAdd(counter, 1u);
+        *flag = (prev == total - 1) ? 1 : 0;
+    }
+    __syncthreads();
+    const bool last = *flag != 0;
+    if (last) __threadfence();
+    return last;
+}
+
 // Completion counter: returns true in every thread of the CTA that finished last.
 __device__ __forceinline__ bool last_cta_done(unsigned* counter, int* flag) {
     __threadfence();
@@ -161,22 +176,13 @@ __device__ void bwd_tail(const BwdArgs<T>& a, PoissonArea<T> w) {
 //                     The bracket is skipped when h_out == null (last step). With part == null
 //                     the launch only propagates the state (segment recomputation in the adjoint).
 // ----------------------------------------------------------------------------------------------
+// One tile of the fused forward: rows [r0, r0+R) x columns [c_begin, c_end), one column per
+// thread at a time; accumulates the trapezoid-weighted row sums of h_{n+1} into acc.
 template <typename T, int R, bool FEQ2D, int PHASE>
-__global__ void __launch_bounds__(256) vp_fwd_kernel(const FwdArgs<T> a) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    T* red = reinterpret_cast<T*>(smem);
-    __shared__ int s_last;
-
+__device__ __forceinline__ void fwd_tile(const FwdArgs<T>& a, int r0, int c_begin, int c_end,
+                                         T (&acc)[R]) {
     const int nx = a.nx, nv = a.nv;
-    const int r0 = blockIdx.x * R;
-    const int c_begin = blockIdx.y * a.chunk_cols;
-    const int c_end = min(nv, c_begin + a.chunk_cols);
     const bool next = a.h_out != nullptr;
-
-    T acc[R];
-#pragma unroll
-    for (int e = 0; e < R; ++e) acc[e] = T(0);
-
     for (int j = c_begin + (int)threadIdx.x; j < c_end; j += blockDim.x) {
         const int m = __ldg(a.mx + j);
         const T t = __ldg(a.tx + j);
@@ -227,6 +233,25 @@ __global__ void __launch_bounds__(256) vp_fwd_kernel(const FwdArgs<T> a) {
         }
     }
 
+}
+
+template <typename T, int R, bool FEQ2D, int PHASE>
+__global__ void __launch_bounds__(256) vp_fwd_kernel(const FwdArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    T* red = reinterpret_cast<T*>(smem);
+    __shared__ int s_last;
+
+    const int nx = a.nx, nv = a.nv;
+    const int r0 = blockIdx.x * R;
+    const int c_begin = blockIdx.y * a.chunk_cols;
+    const int c_end = min(nv, c_begin + a.chunk_cols);
+    const bool next = a.h_out != nullptr;
+
+    T acc[R];
+#pragma unroll
+    for (int e = 0; e < R; ++e) acc[e] = T(0);
+    fwd_tile<T, R, FEQ2D, PHASE>(a, r0, c_begin, c_end, acc);
+
     if (a.part == nullptr || (PHASE != 0 && !next)) return;
     store_row_partials<T, R>(acc, red, a.part + (size_t)blockIdx.y * nx + r0);
     if (a.counter == nullptr) return;   // the tail runs as its own launch (large nx)
@@ -245,21 +270,12 @@ __global__ void __launch_bounds__(256) vp_fwd_kernel(const FwdArgs<T> a) {
 // Tail (phases 0, 1), for step n-1: g_E_total = -dt/dv * sum_j slope*w + g_E_hist; g_H += g_E_total;
 // g_E = g_E_total + ee^T; grho_{n-1} = Poisson^T g_E.
 // ----------------------------------------------------------------------------------------------
+// One tile of the fused adjoint: rows [r0, r0+R) x columns [c_begin, c_end); accumulates the
+// slope-weighted row sums for g_E_total into acc (phases 0 and 1).
 template <typename T, int R, bool FEQ2D, int PHASE>
-__global__ void __launch_bounds__(256) vp_bwd_kernel(const BwdArgs<T> a) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    T* red = reinterpret_cast<T*>(smem);
-    __shared__ int s_last;
-
+__device__ __forceinline__ void bwd_tile(const BwdArgs<T>& a, int r0, int c_begin, int c_end,
+                                         T (&acc)[R]) {
     const int nx = a.nx, nv = a.nv;
-    const int r0 = blockIdx.x * R;
-    const int c_begin = blockIdx.y * a.chunk_cols;
-    const int c_end = min(nv, c_begin + a.chunk_cols);
-
-    T acc[R];
-#pragma unroll
-    for (int e = 0; e < R; ++e) acc[e] = T(0);
-
     for (int j = c_begin + (int)threadIdx.x; j < c_end; j += blockDim.x) {
         const int m = __ldg(a.mx + j);
         const T t = __ldg(a.tx + j);
@@ -334,6 +350,24 @@ __global__ void __launch_bounds__(256) vp_bwd_kernel(const BwdArgs<T> a) {
             acc[e] += sl * wv;
         }
     }
+
+}
+
+template <typename T, int R, bool FEQ2D, int PHASE>
+__global__ void __launch_bounds__(256) vp_bwd_kernel(const BwdArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    T* red = reinterpret_cast<T*>(smem);
+    __shared__ int s_last;
+
+    const int nx = a.nx, nv = a.nv;
+    const int r0 = blockIdx.x * R;
+    const int c_begin = blockIdx.y * a.chunk_cols;
+    const int c_end = min(nv, c_begin + a.chunk_cols);
+
+    T acc[R];
+#pragma unroll
+    for (int e = 0; e < R; ++e) acc[e] = T(0);
+    bwd_tile<T, R, FEQ2D, PHASE>(a, r0, c_begin, c_end, acc);
 
     if (PHASE == 2) return;
     store_row_partials<T, R>(acc, red, a.part + (size_t)blockIdx.y * nx + r0);
@@ -454,5 +488,224 @@ template cudaError_t launch_fwd<float>(const FwdArgs<float>&, const LaunchCfg&, 
 template cudaError_t launch_fwd<double>(const FwdArgs<double>&, const LaunchCfg&, int, bool, cudaStream_t);
 template cudaError_t launch_bwd<float>(const BwdArgs<float>&, const LaunchCfg&, int, bool, cudaStream_t);
 template cudaError_t launch_bwd<double>(const BwdArgs<double>&, const LaunchCfg&, int, bool, cudaStream_t);
+
+// ----------------------------------------------------------------------------------------------
+// Ensembles: one persistent launch per time step advances every instance. CTAs stride over the
+// instances' tiles (instances ordered longest first); the CTA that completes an instance's last
+// tile runs that instance's Poisson tail. Per-tile arithmetic is fwd_tile / bwd_tile above.
+// ----------------------------------------------------------------------------------------------
+
+template <typename T>
+__device__ __forceinline__ int batch_find(const BatchInst<T>* inst, int n, int tile) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&inst[mid].tile_begin) <= tile) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <typename T>
+__device__ __forceinline__ FwdArgs<T> batch_fwd_args(const BatchStep<T>& b, const BatchInst<T>& I) {
+    FwdArgs<T> a{};
+    const long long nn = (long long)I.nx * I.nv;
+    a.nx = I.nx;
+    a.nv = I.nv;
+    a.n_chunks = I.n_chunks;
+    a.chunk_cols = I.chunk_cols;
+    a.mx = I.mx;
+    a.tx = I.tx;
+    a.tx64 = I.tx64;
+    a.feq = I.feq;
+    a.feq_rs = I.feq_rs;
+    a.P = I.P;
+    a.dv = I.dv;
+    a.dx = I.dx;
+    a.dtdv = I.dtdv;
+    a.H = b.H + I.off_x;
+    a.f_iv = b.f_iv ? b.f_iv + I.off_f : nullptr;
+    a.h_in = b.c_in ? b.c_in + b.c_in_mul * I.off_f + (long long)b.c_in_step * nn : nullptr;
+    a.h_out = b.c_out ? b.c_out + b.c_out_mul * I.off_f + (long long)b.c_out_step * nn : nullptr;
+    a.vsh = b.vsh_in ? b.vsh_in + (long long)b.vsh_in_mul * I.off_x + (long long)b.vsh_in_step * I.nx : nullptr;
+    a.vsh_out = b.vsh_out ? b.vsh_out + (long long)b.vsh_out_mul * I.off_x + (long long)b.vsh_out_step * I.nx : nullptr;
+    a.E_out = b.E_out ? b.E_out + (long long)b.E_out_mul * I.off_x + (long long)b.E_out_step * I.nx : nullptr;
+    a.f_final = b.f_final ? b.f_final + I.off_f : nullptr;
+    a.f_hist_n = nullptr;
+    a.E_hist_out = b.E_hist ? b.E_hist + (long long)b.n_steps * I.off_x + (long long)b.hist_step * I.nx : nullptr;
+    a.ee_out = b.ee_hist ? b.ee_hist + (long long)I.index * b.n_steps + b.hist_step : nullptr;
+    a.part = b.part + I.off_part;
+    a.counter = b.counters + I.index;
+    return a;
+}
+
+template <typename T>
+__device__ __forceinline__ BwdArgs<T> batch_bwd_args(const BatchStep<T>& b, const BatchInst<T>& I) {
+    BwdArgs<T> a{};
+    const long long nn = (long long)I.nx * I.nv;
+    a.nx = I.nx;
+    a.nv = I.nv;
+    a.n_chunks = I.n_chunks;
+    a.chunk_cols = I.chunk_cols;
+    a.mx = I.mx;
+    a.tx = I.tx;
+    a.feq = I.feq;
+    a.feq_rs = I.feq_rs;
+    a.P = I.P;
+    a.dv = I.dv;
+    a.dx = I.dx;
+    a.neg_dt_dv = I.neg_dt_dv;
+    a.w_in = b.c_in ? b.c_in + b.c_in_mul * I.off_f + (long long)b.c_in_step * nn : nullptr;
+    a.w_out = b.c_out ? b.c_out + b.c_out_mul * I.off_f + (long long)b.c_out_step * nn : nullptr;
+    a.grho = b.grho ? b.grho + I.off_x : nullptr;
+    a.grho_out = b.grho_out ? b.grho_out + I.off_x : nullptr;
+    a.vsh_n = b.vsh_in ? b.vsh_in + (long long)b.vsh_in_mul * I.off_x + (long long)b.vsh_in_step * I.nx : nullptr;
+    a.h_prev = b.h_prev ? b.h_prev + (long long)b.n_steps * I.off_f + (long long)b.h_prev_step * nn : nullptr;
+    a.vsh_prev = b.vsh_prev ? b.vsh_prev + (long long)b.n_steps * I.off_x + (long long)b.vsh_prev_step * I.nx : nullptr;
+    a.E_prev = b.E_prev ? b.E_prev + (long long)b.n_steps * I.off_x + (long long)b.E_prev_step * I.nx : nullptr;
+    a.gfh = nullptr;
+    a.c_src = b.g_ff ? b.g_ff + I.off_f : nullptr;
+    a.c_src2 = nullptr;
+    a.gE_hist = b.g_Eh ? b.g_Eh + (long long)b.n_steps * I.off_x + (long long)b.g_step * I.nx : nullptr;
+    a.gee = b.g_ee ? b.g_ee + (long long)I.index * b.n_steps + b.g_step : nullptr;
+    a.gH = b.g_H + I.off_x;
+    a.gfiv_out = b.g_fiv ? b.g_fiv + I.off_f : nullptr;
+    a.part = b.part + I.off_part;
+    a.counter = b.counters + I.index;
+    return a;
+}
+
+template <typename T, int R, bool FEQ2D, int PHASE>
+__global__ void __launch_bounds__(256) vp_batch_fwd_kernel(const BatchStep<T> b) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    T* red = reinterpret_cast<T*>(smem);
+    __shared__ int s_last;
+    const size_t red_bytes = (((size_t)32 * R * sizeof(T)) + 15) & ~(size_t)15;
+    for (int tile = blockIdx.x; tile < b.n_tiles; tile += gridDim.x) {
+        const BatchInst<T> I = b.inst[batch_find<T>(b.inst, b.n_inst, tile)];
+        const FwdArgs<T> a = batch_fwd_args<T>(b, I);
+        const int lt = tile - I.tile_begin;
+        const int rb = lt / I.n_chunks, ch = lt - rb * I.n_chunks;
+        const int r0 = rb * R, c_begin = ch * I.chunk_cols;
+        const int c_end = min(I.nv, c_begin + I.chunk_cols);
+        T acc[R];
+#pragma unroll
+        for (int e = 0; e < R; ++e) acc[e] = T(0);
+        fwd_tile<T, R, FEQ2D, PHASE>(a, r0, c_begin, c_end, acc);
+        if (PHASE == 0 || !b.last) {
+            store_row_partials<T, R>(acc, red, a.part + (size_t)ch * I.nx + r0);
+            if (last_unit_done(a.counter, (unsigned)I.n_tiles, &s_last)) {
+                fwd_tail<T>(a, poisson_area<T>(a.P, smem + red_bytes), red);
+                if (threadIdx.x == 0) *a.counter = 0u;
+            }
+        }
+        __syncthreads();   // shared scratch is reused by the next tile
+    }
+}
+
+template <typename T, int R, bool FEQ2D, int PHASE>
+__global__ void __launch_bounds__(256) vp_batch_bwd_kernel(const BatchStep<T> b) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    T* red = reinterpret_cast<T*>(smem);
+    __shared__ int s_last;
+    const size_t red_bytes = (((size_t)32 * R * sizeof(T)) + 15) & ~(size_t)15;
+    for (int tile = blockIdx.x; tile < b.n_tiles; tile += gridDim.x) {
+        const BatchInst<T> I = b.inst[batch_find<T>(b.inst, b.n_inst, tile)];
+        const BwdArgs<T> a = batch_bwd_args<T>(b, I);
+        const int lt = tile - I.tile_begin;
+        const int rb = lt / I.n_chunks, ch = lt - rb * I.n_chunks;
+        const int r0 = rb * R, c_begin = ch * I.chunk_cols;
+        const int c_end = min(I.nv, c_begin + I.chunk_cols);
+        T acc[R];
+#pragma unroll
+        for (int e = 0; e < R; ++e) acc[e] = T(0);
+        bwd_tile<T, R, FEQ2D, PHASE>(a, r0, c_begin, c_end, acc);
+        if (PHASE != 2) {
+            store_row_partials<T, R>(acc, red, a.part + (size_t)ch * I.nx + r0);
+            if (last_unit_done(a.counter, (unsigned)I.n_tiles, &s_last)) {
+                bwd_tail<T>(a, poisson_area<T>(a.P, smem + red_bytes));
+                if (threadIdx.x == 0) *a.counter = 0u;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T, int R, bool F2>
+static cudaError_t batch_fwd_phase(const BatchStep<T>& b, int phase, int grid, int threads, size_t smem,
+                                   cudaStream_t s) {
+    if (phase == 0)
+        vp_batch_fwd_kernel<T, R, F2, 0><<<grid, threads, smem, s>>>(b);
+    else
+        vp_batch_fwd_kernel<T, R, F2, 1><<<grid, threads, smem, s>>>(b);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename T, int R, bool F2>
+static cudaError_t batch_bwd_phase(const BatchStep<T>& b, int phase, int grid, int threads, size_t smem,
+                                   cudaStream_t s) {
+    if (phase == 0)
+        vp_batch_bwd_kernel<T, R, F2, 0><<<grid, threads, smem, s>>>(b);
+    else if (phase == 1)
+        vp_batch_bwd_kernel<T, R, F2, 1><<<grid, threads, smem, s>>>(b);
+    else
+        vp_batch_bwd_kernel<T, R, F2, 2><<<grid, threads, smem, s>>>(b);
+    count_launch();
+    return cudaGetLastError();
+}
+
+#define VP_BATCH_R(FN, ...)                                                    \
+    switch (R) {                                                               \
+        case 1: return feq2d ? FN<T, 1, true>(__VA_ARGS__) : FN<T, 1, false>(__VA_ARGS__); \
+        case 2: return feq2d ? FN<T, 2, true>(__VA_ARGS__) : FN<T, 2, false>(__VA_ARGS__); \
+        case 4: return feq2d ? FN<T, 4, true>(__VA_ARGS__) : FN<T, 4, false>(__VA_ARGS__); \
+        case 8: return feq2d ? FN<T, 8, true>(__VA_ARGS__) : FN<T, 8, false>(__VA_ARGS__); \
+        default: return cudaErrorInvalidValue;                                 \
+    }
+
+template <typename T>
+cudaError_t launch_batch_fwd(const BatchStep<T>& b, int R, int phase, bool feq2d, int grid,
+                             int threads, size_t smem, cudaStream_t s) {
+    VP_BATCH_R(batch_fwd_phase, b, phase, grid, threads, smem, s)
+}
+
+template <typename T>
+cudaError_t launch_batch_bwd(const BatchStep<T>& b, int R, int phase, bool feq2d, int grid,
+                             int threads, size_t smem, cudaStream_t s) {
+    VP_BATCH_R(batch_bwd_phase, b, phase, grid, threads, smem, s)
+}
+
+template <typename K>
+static int occ(K kernel, int threads, size_t smem) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+// Resident CTAs per SM of the ensemble kernels (the persistent grid is this times the SM count).
+template <typename T>
+int batch_blocks_per_sm(int R, bool fwd, bool feq2d, int threads, size_t smem) {
+#define VP_OCC(RR)                                                                                     \
+    if (R == RR) {                                                                                     \
+        if (fwd) return feq2d ? occ(vp_batch_fwd_kernel<T, RR, true, 1>, threads, smem)                 \
+                              : occ(vp_batch_fwd_kernel<T, RR, false, 1>, threads, smem);               \
+        return feq2d ? occ(vp_batch_bwd_kernel<T, RR, true, 1>, threads, smem)                          \
+                     : occ(vp_batch_bwd_kernel<T, RR, false, 1>, threads, smem);                        \
+    }
+    VP_OCC(1) VP_OCC(2) VP_OCC(4) VP_OCC(8)
+#undef VP_OCC
+    return 0;
+}
+
+template cudaError_t launch_batch_fwd<float>(const BatchStep<float>&, int, int, bool, int, int, size_t, cudaStream_t);
+template cudaError_t launch_batch_fwd<double>(const BatchStep<double>&, int, int, bool, int, int, size_t, cudaStream_t);
+template cudaError_t launch_batch_bwd<float>(const BatchStep<float>&, int, int, bool, int, int, size_t, cudaStream_t);
+template cudaError_t launch_batch_bwd<double>(const BatchStep<double>&, int, int, bool, int, int, size_t, cudaStream_t);
+template int batch_blocks_per_sm<float>(int, bool, bool, int, size_t);
+template int batch_blocks_per_sm<double>(int, bool, bool, int, size_t);
 
 }  // namespace vpb

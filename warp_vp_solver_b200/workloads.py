@@ -67,7 +67,7 @@ class Workload:
 
 
 def make_workload(name: str) -> Workload:
-    """The benchmark configurations by name: c1, c2, c3, roofline."""
+    """The single-instance benchmark configurations by name: c1, c2, c3, roofline."""
     if name == "c1":
         m = make_mesh(10.0 * np.pi, 6.0, 128, 128)
         f_eq, f_iv = two_stream(m)
@@ -94,3 +94,67 @@ def make_workload(name: str) -> Workload:
                         1.0, f_eq, f_iv, fourier_coefficients(8, 1e-2, 0), 2 * np.pi / m.period_x,
                         True, None)
     raise ValueError(f"unknown workload {name!r}")
+
+
+@dataclasses.dataclass
+class EnsembleWorkload:
+    """Independent instances sharing dt and the number of steps."""
+    name: str
+    description: str
+    dt: float
+    t_final: float
+    meshes: list
+    f_eqs: list
+    f_ivs: list
+    coeffs: list
+    adjoint: bool = True
+
+    @property
+    def n(self) -> int:
+        return len(self.meshes)
+
+    @property
+    def n_steps(self) -> int:
+        return int(self.t_final / self.dt)
+
+    @property
+    def cells(self) -> int:
+        return int(sum(m.nx * m.nv for m in self.meshes))
+
+    def k0(self, i: int) -> float:
+        return 2 * np.pi / self.meshes[i].period_x
+
+    def H(self, i: int) -> np.ndarray:
+        return fourier_field(self.coeffs[i], self.meshes[i].xs, self.k0(i))
+
+    def subset(self, idx) -> "EnsembleWorkload":
+        idx = list(idx)
+        return EnsembleWorkload(self.name, self.description, self.dt, self.t_final,
+                                [self.meshes[i] for i in idx], [self.f_eqs[i] for i in idx],
+                                [self.f_ivs[i] for i in idx], [self.coeffs[i] for i in idx],
+                                self.adjoint)
+
+
+def make_ensemble_workload(name: str = "c4", n_instances: int = 256, seed: int = 0) -> EnsembleWorkload:
+    """Uneven two-stream ensemble: nx ~ U{64,128,256}, nv ~ U{128,256,512}, mu ~ U[2,3],
+    perturbation amplitude ~ U[1e-4,1e-2] on cos(0.2 x), L_x = 10 pi, v in [-6, 6), 8-mode H
+    with coefficients of standard deviation 1e-2; dt 0.05, 100 steps, forward + adjoint."""
+    if name != "c4":
+        raise ValueError(f"unknown ensemble workload {name!r}")
+    rng = np.random.default_rng(seed)
+    meshes, f_eqs, f_ivs, coeffs = [], [], [], []
+    cache: dict = {}
+    for _ in range(n_instances):
+        nx = int(rng.choice([64, 128, 256]))
+        nv = int(rng.choice([128, 256, 512]))
+        mu = float(rng.uniform(2.0, 3.0))
+        eps = float(rng.uniform(1e-4, 1e-2))
+        m = cache.setdefault((nx, nv), make_mesh(10.0 * np.pi, 6.0, nx, nv))
+        f_eq, f_iv = two_stream(m, mu=mu, eps=eps)
+        meshes.append(m)
+        f_eqs.append(f_eq)
+        f_ivs.append(f_iv)
+        coeffs.append(1e-2 * rng.standard_normal((2, 8)))
+    return EnsembleWorkload("c4", f"{n_instances} uneven two-stream instances, nx in {{64,128,256}}, "
+                            "nv in {128,256,512}, dt 0.05, 100 steps, 8-mode H, forward + adjoint "
+                            "of J = sum(ee)*dt per instance", 0.05, 5.0, meshes, f_eqs, f_ivs, coeffs)
