@@ -183,6 +183,48 @@ int vp_batch_backward(vp_batch* batch, const void* H, int32_t n_steps, const voi
                       void* g_f_iv, void* g_H, void* workspace, size_t workspace_bytes,
                       void* stream);
 
+/* --- surrogate MLP ----------------------------------------------------------------------------
+ * Fully connected network widths[0] -> ... -> widths[n_layers] with GELU (erf form) between
+ * layers and none on the output: BF16 operands, FP32 accumulation on the tensor cores, FP32
+ * master weights and Adam state. No counterpart in the reference, whose control optimisation
+ * uses the adjoint gradient alone; the network is the learned surrogate of the map from the
+ * external field's Fourier coefficients to the log electric-energy history.
+ * Parameters are packed per layer: W_l [widths[l+1], widths[l]] row-major, then b_l
+ * [widths[l+1]]. All pointers are device memory; row-major inputs take a leading dimension and
+ * an optional row-index array (rows[m] selects the input row of batch entry m). */
+typedef struct vp_mlp vp_mlp;
+
+int vp_mlp_create(int32_t n_layers, const int32_t* widths, int32_t max_batch, vp_mlp** out_mlp);
+int vp_mlp_destroy(vp_mlp* mlp);
+int vp_mlp_param_count(const vp_mlp* mlp, int64_t* count);
+/* Copies FP32 parameters in, zeroes the Adam moments and step count, refreshes the BF16 copies. */
+int vp_mlp_set_params(vp_mlp* mlp, const float* params, void* stream);
+/* Copies the FP32 parameters and/or the last parameter gradients out (either may be NULL). */
+int vp_mlp_get_params(const vp_mlp* mlp, float* params, float* grads, void* stream);
+/* Y[m, :] = net(X[rows ? rows[m] : m, :]) for m < M; Y may be NULL (activations are kept for a
+ * following backward). */
+int vp_mlp_forward(vp_mlp* mlp, const float* X, int64_t ldx, const int32_t* rows, int32_t M, float* Y,
+                   int64_t ldy, void* stream);
+/* Backward of the last forward (same M) from the output cotangent g_Y: parameter gradients
+ * when param_grads != 0 and, when g_X is not NULL, the input cotangent. */
+int vp_mlp_backward(vp_mlp* mlp, const float* g_Y, int64_t ldg, int32_t M, int32_t param_grads, float* g_X,
+                    int64_t ldgx, void* stream);
+/* Mean-squared-error loss of the last forward against target rows (gathered like X) and its
+ * parameter gradients; loss (one float, device) may be NULL. */
+int vp_mlp_mse_backward(vp_mlp* mlp, const float* target, int64_t ldt, const int32_t* rows, int32_t M,
+                        float* loss, void* stream);
+/* One Adam step (Kingma and Ba) on the last parameter gradients; the step count lives on the
+ * device, so the call can be captured in a CUDA graph. */
+int vp_mlp_adam(vp_mlp* mlp, float lr, float beta1, float beta2, float eps, void* stream);
+/* Nonzero bit 0: a tensor-core wait gave up (results of that call are invalid). Synchronous. */
+int vp_mlp_status(vp_mlp* mlp, uint32_t* flags);
+/* One BF16 tile GEMM with the MLP's epilogues: C = act(A[M,K] . B[N,K]^T + bias), act 0 none,
+ * 1 GELU, 2 multiply by GELU'(aux[m, n]); outputs FP32 C32, BF16 C16 and BF16 transposed C16T
+ * (each may be NULL). K, lda, ldb multiples of 8; A, B 16-byte aligned. */
+int vp_gemm_bf16(const void* A, int64_t lda, const void* B, int64_t ldb, int32_t M, int32_t N, int32_t K,
+                 const float* bias, int32_t act, const float* aux, int64_t ldaux, float* C32, int64_t ldc32,
+                 void* C16, int64_t ldc16, void* C16T, int64_t ldc16t, uint32_t* err, void* stream);
+
 /* --- single-stage operators (the reference's helper methods and unit-tested kernels) ------ */
 
 /* rho[i] = dv * trapz_j(f_eq[i,j] - f[i,j]). Replaces compute_rho (warp_vp_solver/solver.py:

@@ -93,6 +93,18 @@ SIGNATURES = {
                                  c_vp]),
     "vp_batch_backward": (c_int, [c_vp, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
                                   c_size, c_vp]),
+    "vp_mlp_create": (c_int, [c_i32, ctypes.POINTER(c_i32), c_i32, ctypes.POINTER(c_vp)]),
+    "vp_mlp_destroy": (c_int, [c_vp]),
+    "vp_mlp_param_count": (c_int, [c_vp, ctypes.POINTER(c_i64)]),
+    "vp_mlp_set_params": (c_int, [c_vp, c_vp, c_vp]),
+    "vp_mlp_get_params": (c_int, [c_vp, c_vp, c_vp, c_vp]),
+    "vp_mlp_forward": (c_int, [c_vp, c_vp, c_i64, c_vp, c_i32, c_vp, c_i64, c_vp]),
+    "vp_mlp_backward": (c_int, [c_vp, c_vp, c_i64, c_i32, c_i32, c_vp, c_i64, c_vp]),
+    "vp_mlp_mse_backward": (c_int, [c_vp, c_vp, c_i64, c_vp, c_i32, c_vp, c_vp]),
+    "vp_mlp_adam": (c_int, [c_vp, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, c_vp]),
+    "vp_mlp_status": (c_int, [c_vp, ctypes.POINTER(ctypes.c_uint32)]),
+    "vp_gemm_bf16": (c_int, [c_vp, c_i64, c_vp, c_i64, c_i32, c_i32, c_i32, c_vp, c_i32, c_vp, c_i64,
+                             c_vp, c_i64, c_vp, c_i64, c_vp, c_i64, c_vp, c_vp]),
     "vp_compute_rho": (c_int, [c_vp, c_vp, c_vp, c_vp]),
     "vp_poisson": (c_int, [c_vp, c_vp, c_vp, c_int, c_vp]),
     "vp_electric_energy": (c_int, [c_vp, c_vp, c_vp, c_vp]),

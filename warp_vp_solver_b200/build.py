@@ -17,7 +17,7 @@ LIB_NAME = "libvpb200.so"
 LIB_PATH = os.path.join(PKG_DIR, LIB_NAME)
 INCLUDE_DIR = os.path.join(os.path.dirname(PKG_DIR), "include")
 
-SOURCES = ["vp_capi.cu", "vp_kernels.cu", "vp_ops.cu", "vp_resident.cu"]
+SOURCES = ["vp_capi.cu", "vp_kernels.cu", "vp_ops.cu", "vp_resident.cu", "vp_mlp.cu"]
 HEADERS = ["vp_internal.h", "vp_device.cuh"]
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -22,7 +22,7 @@ static thread_local int64_t g_launches = 0;
 
 void count_launch(int n) { g_launches += n; }
 
-static int set_err(int code, const char* fmt, ...) {
+int set_err(int code, const char* fmt, ...) {
     va_list ap;
     va_start(ap, fmt);
     vsnprintf(g_err, sizeof(g_err), fmt, ap);

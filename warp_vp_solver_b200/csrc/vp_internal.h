@@ -255,5 +255,7 @@ template <typename T>
 int batch_blocks_per_sm(int R, bool fwd, bool feq2d, int threads, size_t smem);
 
 void count_launch(int n = 1);
+// Records the message returned by vp_get_last_error and returns code.
+int set_err(int code, const char* fmt, ...);
 
 }  // namespace vpb
