@@ -43,8 +43,9 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "roofline"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "roofline"])
     ap.add_argument("--instances", type=int, default=256, help="c4: instances per GPU")
+    ap.add_argument("--seeds", type=int, default=3, help="c5: random initial controls compared")
     ap.add_argument("--dtype", default="float32", choices=["float32", "float64"])
     ap.add_argument("--checkpoint-every", type=int, default=None)
     ap.add_argument("--cluster-size", type=int, default=None,
@@ -636,6 +637,64 @@ def e2e_ensemble(args, ens, ew, dev, flush):
                     "coefficients in, J and dJ/dcoefficients out"}
 
 
+def run_surrogate(args, rank, local_rank, world):
+    """C5: 4096 batched two-stream solves (256x256, dt 0.05, 100 steps, 16-mode field with
+    coefficients of standard deviation 0.05) generate (coefficients -> log ee); the tensor-core
+    MLP 32->256->256->100 trains for 2000 Adam steps (lr 1e-3); then, from random initial
+    coefficients, plain Adam on the true adjoint gradient until J stops improving, against the
+    surrogate-warm-started loop refined until J <= 1.01 J*."""
+    import torch
+
+    from warp_vp_solver_b200 import _capi
+    from warp_vp_solver_b200.surrogate import c5_setup, run_comparison
+
+    torch.cuda.set_device(local_rank)
+    lib = _capi.load()
+    setup = c5_setup()
+    lib.vp_reset_launch_count()
+    with ClockSampler(local_rank) as clk:
+        res = run_comparison(setup, n_samples=4096, coeff_std=0.05, train_steps=2000,
+                             seeds=list(range(11, 11 + args.seeds)))
+    launches = lib.vp_launch_count()
+    ratios = [r["time_ratio"] for r in res["runs"]]
+    data = res["data"]
+    line = {
+        "metric": "cell-steps/s fwd",
+        "value": round(data["cell_steps_per_s"] * world, 1),
+        "unit": "cell-steps/s",
+        "n_gpus": world,
+        "steps": 1,
+        "warmup": 0,
+        "ms_per_step": round(data["seconds"] * 1e3, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 solver, bf16-in/f32-accumulate MLP",
+        "data": "synthetic (seeded two-stream set-up, random field coefficients)",
+        "config": {"workload": "C5 surrogate control: 4096 x 256^2 two-stream solves, dt 0.05, "
+                               "100 steps, 16 modes ~ N(0, 0.05 std); MLP 32-256-256-100 GELU, "
+                               "Adam lr 1e-3, 2000 steps",
+                   "instances": data["instances"], "parallelism": "single" if world == 1 else "replicas"},
+        "surrogate": {
+            "train_seconds": round(res["train_seconds"], 3),
+            "train_steps": res["train_steps"],
+            "final_loss": res["final_loss"],
+            "holdout_mae_log_ee": res["holdout_mae_log_ee"],
+            "holdout_mae_mean_predictor": res["holdout_mae_mean_predictor"],
+            "runs": res["runs"] and [{k: (round(v, 6) if isinstance(v, float) else v)
+                                      for k, v in r.items()} for r in res["runs"]],
+            "time_ratio_mean": round(float(np.mean(ratios)), 4),
+            "time_ratio_max": round(float(np.max(ratios)), 4),
+            "note": "warm time = surrogate search + true-gradient refinement until J <= 1.01 J*; "
+                    "data generation and training are reported separately (amortised)",
+        },
+        "e2e": None,
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    return line, None
+
+
 def run_reference(args, rank, world):
     """CPU restatement of the reference algorithm on the host cores (rank 0 only)."""
     from warp_vp_solver_b200.workloads import make_ensemble_workload, make_workload
@@ -697,13 +756,16 @@ def main():
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        if args.workload == "c4":
+        if args.workload == "c5":
+            line, wl = run_surrogate(args, rank, local_rank, world)
+            base = None
+        elif args.workload == "c4":
             line, wl = run_ensemble(args, rank, local_rank, world)
             base = cpu_baseline_ensemble
         else:
             line, wl = run_ours(args, rank, local_rank, world)
             base = cpu_baseline
-        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        if rank == 0 and world == 1 and not args.no_cpu_baseline and base is not None:
             v, cores, kind, sample = base(wl, args.cpu_seconds)
             line["cpu_baseline"] = {"value": round(v, 1), "unit": "cell-steps/s", "cores": cores,
                                     "kind": kind, "sample": sample}

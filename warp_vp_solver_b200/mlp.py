@@ -115,6 +115,12 @@ class MLP:
             int(g_X.stride(0)) if g_X is not None else 0, self._s()))
         return g_X
 
+    def backward_into(self, g_Y: torch.Tensor, g_X: torch.Tensor | None, param_grads: bool) -> None:
+        """Capture-safe backward into preallocated tensors."""
+        _capi.check(self.lib.vp_mlp_backward(
+            self._h, _capi.ptr(g_Y), int(g_Y.stride(0)), int(g_Y.shape[0]), int(bool(param_grads)),
+            _capi.ptr(g_X), int(g_X.stride(0)) if g_X is not None else 0, self._s()))
+
     def mse_backward_into(self, T: torch.Tensor, rows, M: int, loss: torch.Tensor | None) -> None:
         _capi.check(self.lib.vp_mlp_mse_backward(self._h, _capi.ptr(T), int(T.stride(0)),
                                                  _capi.ptr(rows), int(M), _capi.ptr(loss), self._s()))

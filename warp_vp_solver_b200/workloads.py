@@ -67,7 +67,8 @@ class Workload:
 
 
 def make_workload(name: str) -> Workload:
-    """The single-instance benchmark configurations by name: c1, c2, c3, roofline."""
+    """The single-instance benchmark configurations by name: c1, c2, c3, c5 (one instance of the
+    surrogate's training data), roofline."""
     if name == "c1":
         m = make_mesh(10.0 * np.pi, 6.0, 128, 128)
         f_eq, f_iv = two_stream(m)
@@ -86,6 +87,12 @@ def make_workload(name: str) -> Workload:
         return Workload("c3", "bump-on-tail 512x1024, dt 0.05, 600 steps, 16-mode H (std 1e-2, seed 0), "
                         "sqrt(n)-checkpointed forward + adjoint of J = sum(ee)*dt", m, 0.05, 30.0,
                         f_eq, f_iv, fourier_coefficients(16, 1e-2, 0), 2 * np.pi / lx, True, 25)
+    if name == "c5":
+        m = make_mesh(10.0 * np.pi, 6.0, 256, 256)
+        f_eq, f_iv = two_stream(m)
+        return Workload("c5", "one surrogate training sample: two-stream 256x256, dt 0.05, 100 steps, "
+                        "16-mode H (std 0.05, seed 0), forward", m, 0.05, 5.0, f_eq, f_iv,
+                        fourier_coefficients(16, 0.05, 0), 2 * np.pi / m.period_x, False, None)
     if name == "roofline":
         m = make_mesh(10.0 * np.pi, 6.0, 8192, 8192)
         f_eq, f_iv = two_stream(m)
