@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define VP_ABI_VERSION 1
+#define VP_ABI_VERSION 2
 
 /* status codes */
 #define VP_OK 0
@@ -274,13 +274,18 @@ typedef struct vp_launch_config {
                               /* (cluster-resident path); 0: one fused launch per step            */
     int32_t cluster_threads;  /* threads per CTA of the cluster-resident kernels                  */
     int64_t cluster_smem_bytes; /* dynamic shared memory per CTA of the cluster-resident kernels  */
+    int32_t stage_rows;       /* > 0: per-step forward launches use the staged kernel with this   */
+                              /* many rows per CTA (4, 8, 16 or 32; x-invariant f_eq only); 0: off */
+    int32_t stage_threads;    /* columns (= threads) per CTA of the staged kernel, dividing nv    */
+    int32_t stage_span;       /* rows of its shared-memory staging buffer (derived)               */
+    int64_t stage_smem_bytes; /* dynamic shared memory of the staged kernel (derived)             */
 } vp_launch_config;
 
 /* Reads the plan's current launch shape. */
 int vp_plan_get_config(const vp_plan* plan, vp_launch_config* out);
 
-/* Sets rows_per_cta, threads, n_chunks and cluster_size (the other fields are derived and
- * ignored). cluster_size must be 0 or a power of two in [2, 16] that splits nx into 1, 2, 4, 8,
+/* Sets rows_per_cta, threads, n_chunks, cluster_size, stage_rows and stage_threads (the other
+ * fields are derived and ignored). cluster_size must be 0 or a power of two in [2, 16] that splits nx into 1, 2, 4, 8,
  * 16 or 32 rows per CTA whose state fits in shared memory; the cluster-resident path is used for forward calls without a tape or with
  * checkpoint interval 1, and for backward calls with checkpoint interval 1. Workspace sizes
  * depend on n_chunks: query vp_workspace_bytes() again after changing it. */

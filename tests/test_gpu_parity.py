@@ -180,3 +180,68 @@ def test_cluster_sizes_agree_with_oracle(cn):
     gf, gH = s._run_backward(f_iv, H, 1.0, None, gff, gfh, gEh, w)
     gf_r, gH_r = O.run_backward(g, 0.1, f_eq, f_iv, H, 1.0, ref[1], gff, gfh, gEh, w)
     assert O.rel_err(gf, gf_r) < 1e-10 and O.rel_err(gH, gH_r) < 1e-10
+
+
+# Per-step staged kernel (x-invariant f_eq, nv a multiple of 128): field strengths from a
+# fraction of a cell per step up to several cells (rows beyond the staging halo take the exact
+# scalar form), with histories, a tape and a recomputing checkpoint interval.
+STAGED = [(64, 256, 0.05, 0.02), (128, 128, 0.05, 0.05), (32, 512, 0.1, 0.3), (32, 512, 0.1, 1.0)]
+
+
+@pytest.mark.parametrize("dtype", DTYPES, ids=_dt_id)
+@pytest.mark.parametrize("shape", STAGED, ids=lambda s: f"{s[0]}x{s[1]}_H{s[3]}")
+def test_staged_step_matches_oracle(shape, dtype):
+    nx, nv, dt, amp = shape
+    m = make_mesh(10.0 * np.pi, 6.0, nx, nv)
+    f_eq, f_iv = two_stream_state(m, eps=1e-2)
+    H = amp * np.random.default_rng(nx + nv).standard_normal(nx)
+    T = 8
+    s = make_solver(m, dt, f_eq, "stream", dtype=dtype, checkpoint_every=3)
+    cfg = s.plan.get_config()
+    assert cfg["stage_rows"] > 0 and cfg["stage_span"] >= cfg["stage_rows"] + 2
+    out = s.run_forward(f_iv, H, T * dt)
+    g = O.grid_from(m)
+    ref = O.delta_forward(g, dt, f_eq, f_iv, H, T)
+    for arr, r, name in zip(out, ref, FIELDS):
+        assert O.rel_err(arr, r) < TOL_FWD[dtype], f"{name}: {O.rel_err(arr, r):.2e}"
+    w = O.trapezoid_time_weights(T, dt)
+    rg = np.random.default_rng(3)
+    gff = rg.standard_normal((nx, nv))
+    gEh = rg.standard_normal((T, nx))
+    gf, gH = s._run_backward(f_iv, H, T * dt, None, gff, None, gEh, w)
+    rf, rH = O.delta_backward(g, dt, f_eq, f_iv, H, T, gff, None, gEh, w)
+    assert O.rel_err(gf, rf) < TOL_BWD[dtype] and O.rel_err(gH, rH) < TOL_BWD[dtype]
+
+
+@pytest.mark.parametrize("rows,cols", [(4, 128), (8, 128), (16, 256), (32, 256), (0, 0)])
+def test_staged_shapes_agree(rows, cols):
+    """Every staged tile shape (and the per-column kernel, stage_rows=0) gives the oracle's
+    result; the checkpoint interval stays bitwise neutral on each."""
+    m = make_mesh(10.0 * np.pi, 6.0, 128, 512)
+    f_eq, f_iv = two_stream_state(m, eps=1e-2)
+    H = 0.3 * np.random.default_rng(1).standard_normal(m.nx)
+    T, dt = 6, 0.1
+    ref = O.delta_forward(O.grid_from(m), dt, f_eq, f_iv, H, T)
+    outs = []
+    for ce in (1, 4):
+        s = make_solver(m, dt, f_eq, "stream", checkpoint_every=ce)
+        s.plan.set_config(stage_rows=rows, stage_threads=cols)
+        assert s.plan.get_config()["stage_rows"] == rows
+        out = s.run_forward(f_iv, H, T * dt)
+        assert O.rel_err(out[0], ref[0]) < 1e-5 and O.rel_err(out[3], ref[3]) < 1e-5
+        outs.append(s._run_backward(f_iv, H, T * dt, None, None, None, None,
+                                    O.trapezoid_time_weights(T, dt)))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+
+
+def test_staged_shape_rejects_unusable_values():
+    m = make_mesh(10.0 * np.pi, 6.0, 64, 256)
+    f_eq, _ = two_stream_state(m)
+    s = make_solver(m, 0.05, f_eq, "stream")
+    before = s.plan.get_config()
+    for rows, cols in [(3, 128), (8, 96), (64, 128), (8, 512)]:
+        with pytest.raises(ValueError):
+            s.plan.set_config(stage_rows=rows, stage_threads=cols)
+    assert s.plan.get_config() == before
+    s2 = make_solver(m, 0.05, np.ones((64, 256)) + np.arange(64)[:, None] * 1e-3, "stream")
+    assert s2.plan.get_config()["stage_rows"] == 0   # x-dependent f_eq: per-column kernel

@@ -19,6 +19,7 @@ VP_ERR_TIMEOUT = 3
 VP_ERR_UNSUPPORTED = 4
 VP_F32 = 0
 VP_F64 = 1
+ABI_VERSION = 2   # VP_ABI_VERSION of the header these bindings follow
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libvpb200.so")
 
@@ -59,6 +60,10 @@ class LaunchConfig(ctypes.Structure):
         ("cluster_size", c_i32),
         ("cluster_threads", c_i32),
         ("cluster_smem_bytes", c_i64),
+        ("stage_rows", c_i32),
+        ("stage_threads", c_i32),
+        ("stage_span", c_i32),
+        ("stage_smem_bytes", c_i64),
     ]
 
 
@@ -133,6 +138,9 @@ def load():
                 fn = getattr(lib, name)
                 fn.restype = res
                 fn.argtypes = args
+            if lib.vp_abi_version() != ABI_VERSION:
+                raise RuntimeError(f"{LIB_PATH} has ABI version {lib.vp_abi_version()}, the bindings "
+                                   f"expect {ABI_VERSION}: rebuild with `python -m warp_vp_solver_b200.build`")
             _lib = lib
     return _lib
 

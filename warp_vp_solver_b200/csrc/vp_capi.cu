@@ -73,6 +73,10 @@ struct vp_plan {
     double* d_vs = nullptr;    // nv
     int* d_mx = nullptr;       // nv
     void* d_tx = nullptr;      // nv reals
+    void* d_vtab = nullptr;    // staged step: [2][2*kStageHalo][nv] reals (x-invariant f_eq only)
+    LaunchCfg scfg{};          // staged forward step (R rows x threads columns per CTA)
+    int stage_span = 0;        // rows its staging buffer holds (0: staged step not used)
+    std::vector<int> host_mx;  // x half-step offsets (host copy, for staged shapes)
     double* d_tx64 = nullptr;  // nv
     void* d_tw = nullptr;      // nx/2 complex
     void* d_mult = nullptr;    // nx reals (imaginary part)
@@ -191,6 +195,80 @@ static size_t fused_smem(const vp_plan* p, int R) {
     return red + (p->tail_inline ? poisson_area_size(p->nx, real_size(p)) : 0);
 }
 
+// Staged forward step with R rows x C columns per CTA (C divides nv): its staging buffer holds
+// the widest x window of any column block, R + 2 + 2 * (max - min signed x offset over the
+// block's columns) rows. Returns false (and leaves the plan unchanged) when the shape is not
+// usable.
+static bool staged_config(vp_plan* p, int R, int C, int blocks_per_cta = 0) {
+    const int nx = p->nx, nv = p->nv;
+    if (p->d_vtab == nullptr || (C != 128 && C != 256) || nv % C != 0) return false;
+    if (!(R == 4 || R == 8 || R == 16 || R == 32) || nx % R != 0 || R > nx / 4) return false;
+    int dmax = 0;
+    for (int c0 = 0; c0 < nv; c0 += C) {
+        int lo = 1 << 30, hi = -(1 << 30);
+        for (int j = c0; j < c0 + C; ++j) {
+            const int sm = p->host_mx[j] > nx / 2 ? p->host_mx[j] - nx : p->host_mx[j];
+            lo = std::min(lo, sm);
+            hi = std::max(hi, sm);
+        }
+        dmax = std::max(dmax, hi - lo);
+    }
+    const int span = R + 2 + 2 * dmax;
+    if (span > nx) return false;
+    const size_t rs = real_size(p);
+    const size_t red = ((size_t)32 * R * rs + 15) & ~(size_t)15;
+    const size_t stage = staged_smem_bytes(span, C, rs);
+    const size_t tail = p->tail_inline ? poisson_area_size(nx, rs) : 0;
+    const size_t smem = red + std::max(stage, tail);
+    if (smem > 160 * 1024) return false;
+    // column blocks per CTA: enough CTAs for two per SM, at most 8 blocks
+    const int n_blocks = nv / C;
+    int nb = blocks_per_cta;
+    if (nb <= 0) {
+        int sms = 148;
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        nb = 1;
+        while (nb < 8 && n_blocks % (2 * nb) == 0 && (long long)(nx / R) * (n_blocks / (2 * nb)) >= 2LL * sms)
+            nb *= 2;
+    }
+    if (nb < 1 || n_blocks % nb != 0) return false;
+    const cudaError_t e = p->dtype == VP_F64 ? set_staged_smem_limit<double>(smem) : set_staged_smem_limit<float>(smem);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    p->scfg.R = R;
+    p->scfg.threads = C;
+    p->scfg.chunk_cols = C * nb;
+    p->scfg.n_chunks = n_blocks / nb;
+    p->scfg.smem = smem;
+    p->stage_span = span;
+    return true;
+}
+
+// Default staged shape: C = 256 (or 128) columns, and the largest R of 32, 16, 8, 4 that still
+// gives two CTAs per SM.
+static void choose_staged(vp_plan* p, int n_sms) {
+    p->stage_span = 0;
+    for (int C : {256, 128}) {
+        if (p->nv % C != 0) continue;
+        int best = 0;
+        for (int r : {32, 16, 8, 4}) {
+            if (p->nx % r != 0 || r > p->nx / 4) continue;
+            if (best == 0) best = r;
+            if ((long long)(p->nx / r) * (p->nv / C) >= 2LL * n_sms) {
+                best = r;
+                break;
+            }
+        }
+        if (best == 0) continue;
+        for (int r = best; r >= 4; r /= 2)
+            if (staged_config(p, r, C)) return;
+    }
+}
+
 // Checkpoint interval. every > 0 is used as given (capped at n_steps). every == 0 (automatic)
 // keeps every step's state when that tape fits in kStoreAllBytes, and otherwise checkpoints every
 // ceil(sqrt(n_steps)) steps, recomputing the states in between during the adjoint.
@@ -219,7 +297,8 @@ static WsLayout ws_layout(const vp_plan* p, int n_steps, int every) {
     L.hbuf0 = off; off += align256(nxnv);
     L.hbuf1 = off; off += align256(nxnv);
     L.seg = off; off += align256(nxnv * (size_t)std::max(0, K - 1));
-    L.part = off; off += align256((size_t)p->cfg.n_chunks * p->nx * real_size(p));
+    const int part_chunks = std::max(p->cfg.n_chunks, p->stage_span > 0 ? p->scfg.n_chunks : 0);
+    L.part = off; off += align256((size_t)part_chunks * p->nx * real_size(p));
     L.counter = off; off += 256;
     L.vsh = off; off += align256((size_t)p->nx * vshift_size(p));
     L.E = off; off += align256((size_t)p->nx * real_size(p));
@@ -336,6 +415,8 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
     a.dx = (T)p->dx;
     a.dtdv = (T)(p->dt / p->dv);
     a.H = H;
+    a.vtab = static_cast<const T*>(p->d_vtab);
+    a.stage_span = p->stage_span;
 
     // prologue: h_0, rho_0 -> E_0
     a.f_iv = f_iv;
@@ -365,7 +446,13 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
         a.vsh_out = vsh_all ? vsh_all + (size_t)(n + 1) * nx : vsh_ws;
         a.E_hist_out = (E_hist && !last) ? E_hist + (size_t)(n + 1) * nx : nullptr;
         a.ee_out = (ee_hist && !last) ? ee_hist + (n + 1) : nullptr;
-        VP_CUDA(launch_fwd<T>(a, p->cfg, 1, p->feq2d != 0, s), "forward step launch");
+        if (p->stage_span > 0) {
+            a.n_chunks = p->scfg.n_chunks;
+            a.chunk_cols = p->scfg.chunk_cols;
+            VP_CUDA(launch_fwd_staged<T>(a, p->scfg, s), "forward step launch");
+        } else {
+            VP_CUDA(launch_fwd<T>(a, p->cfg, 1, p->feq2d != 0, s), "forward step launch");
+        }
         if (!last && !p->tail_inline)
             VP_CUDA(launch_fwd_tail<T>(a, p->tail_threads, p->tail_smem, s), "forward tail launch");
     }
@@ -448,6 +535,8 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
     fa.dx = (T)p->dx;
     fa.dtdv = (T)(p->dt / p->dv);
     fa.H = H;
+    fa.vtab = static_cast<const T*>(p->d_vtab);
+    fa.stage_span = p->stage_span;
     fa.part = nullptr;  // propagation only
 
     int current_seg = -1;
@@ -460,7 +549,10 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
             fa.h_in = h_ptr(n);
             fa.h_out = h_mut(n + 1);
             fa.vsh = vsh_all + (size_t)n * nx;
-            VP_CUDA(launch_fwd<T>(fa, p->cfg, 1, p->feq2d != 0, s), "recompute launch");
+            if (p->stage_span > 0)
+                VP_CUDA(launch_fwd_staged<T>(fa, p->scfg, s), "recompute launch");
+            else
+                VP_CUDA(launch_fwd<T>(fa, p->cfg, 1, p->feq2d != 0, s), "recompute launch");
         }
         return VP_OK;
     };
@@ -536,6 +628,7 @@ static void free_plan(vp_plan* p) {
     cudaFree(p->d_mx);
     cudaFree(p->d_tx);
     cudaFree(p->d_tx64);
+    cudaFree(p->d_vtab);
     cudaFree(p->d_tw);
     cudaFree(p->d_mult);
     cudaFree(p->d_circ);
@@ -682,6 +775,7 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
     p->tail_threads = nx >= 2048 ? 1024 : std::max(32, ((nx / 2 + 31) / 32) * 32);
     p->cfg = choose_cfg(nx, nv, n_sms);
     p->cfg.smem = fused_smem(p, p->cfg.R);
+    p->host_mx = mx;
     // cluster-resident path: the largest cluster (16, 8, 4, 2 CTAs) whose per-CTA share of the
     // state fits in shared memory and that the occupancy calculator accepts
     for (int cn : {16, 8, 4, 2}) {
@@ -714,13 +808,31 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
         free_plan(p);
         return rc;
     }
+    // staged-step correction tables, m in [-kStageHalo, kStageHalo):
+    // A_m[j] = f_eq[j+m] - f_eq[j], B_m[j] = f_eq[j+m+1] - f_eq[j+m] (periodic, float64)
+    std::vector<double> vtab;
+    const bool stage_tables = inv && nv % 32 == 0;
+    if (stage_tables) {
+        const int NM = 2 * kStageHalo;
+        vtab.assign((size_t)2 * NM * nv, 0.0);
+        auto fq = [&](long long c) { return f_eq_host[((c % nv) + nv) % nv]; };
+        for (int q = 0; q < NM; ++q) {
+            const int m = q - kStageHalo;
+            for (int j = 0; j < nv; ++j) {
+                vtab[(size_t)q * nv + j] = fq(j + m) - fq(j);
+                vtab[(size_t)(NM + q) * nv + j] = fq(j + m + 1) - fq(j + m);
+            }
+        }
+    }
     if (dtype == VP_F64) {
-        rc = upload<double>(&p->d_tx, tx);
+        if (stage_tables) rc = upload<double>(&p->d_vtab, vtab);
+        if (!rc) rc = upload<double>(&p->d_tx, tx);
         if (!rc) rc = upload<double>(&p->d_tw, tw);
         if (!rc) rc = upload<double>(&p->d_mult, mult_im);
         if (!rc) rc = upload<double>(&p->d_circ, circ);
     } else {
-        rc = upload<float>(&p->d_tx, tx);
+        if (stage_tables) rc = upload<float>(&p->d_vtab, vtab);
+        if (!rc) rc = upload<float>(&p->d_tx, tx);
         if (!rc) rc = upload<float>(&p->d_tw, tw);
         if (!rc) rc = upload<float>(&p->d_mult, mult_im);
         if (!rc) rc = upload<float>(&p->d_circ, circ);
@@ -729,6 +841,7 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
         free_plan(p);
         return rc;
     }
+    choose_staged(p, n_sms);
     *out_plan = p;
     return VP_OK;
 }
@@ -746,6 +859,10 @@ int vp_plan_get_config(const vp_plan* plan, vp_launch_config* out) {
     out->cluster_size = plan->res_cn;
     out->cluster_threads = plan->res_threads;
     out->cluster_smem_bytes = (int64_t)plan->res_smem;
+    out->stage_rows = plan->stage_span > 0 ? plan->scfg.R : 0;
+    out->stage_threads = plan->stage_span > 0 ? plan->scfg.threads : 0;
+    out->stage_span = plan->stage_span;
+    out->stage_smem_bytes = plan->stage_span > 0 ? (int64_t)plan->scfg.smem : 0;
     return VP_OK;
 }
 
@@ -768,6 +885,21 @@ int vp_plan_set_config(vp_plan* plan, const vp_launch_config* cfg) {
                                        "in [2,16] dividing nx into 1, 2, 4, 8, 16 or 32 rows per CTA whose "
                                        "state fits in shared memory)",
                            cn, plan->nx, plan->nv);
+    }
+    if (cfg->stage_rows != 0) {
+        const LaunchCfg keep = plan->scfg;
+        const int keep_span = plan->stage_span;
+        if (!staged_config(plan, cfg->stage_rows, cfg->stage_threads)) {
+            plan->scfg = keep;
+            plan->stage_span = keep_span;
+            return set_err(VP_ERR_ARG, "stage_rows=%d, stage_threads=%d is not usable for this plan (needs an "
+                                       "x-invariant f_eq, stage_threads a multiple of 32 in [32, 256] dividing nv, "
+                                       "stage_rows 4, 8, 16 or 32 dividing nx and <= nx/4, and a staging buffer "
+                                       "that fits in shared memory)",
+                           cfg->stage_rows, cfg->stage_threads);
+        }
+    } else {
+        plan->stage_span = 0;
     }
     plan->res_cn = cn;
     plan->res_smem = res_smem;

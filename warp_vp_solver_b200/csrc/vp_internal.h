@@ -56,7 +56,13 @@ template <typename T> struct FwdArgs {
     T* E_hist_out;              // E + H of step n+1, or null
     T* ee_out;                  // ee of step n+1, or null
     VShift<T>* vsh_out;         // v shifts of step n+1
+    const T* vtab;              // staged step: v-step f_eq correction tables A_m, B_m, or null
+    int stage_span;             // staged step: rows the staging buffer holds
 };
+
+// v halo of the staged step kernels (cells on each side of a CTA's columns), and the shifts the
+// correction tables cover: m in [-kStageHalo, kStageHalo).
+constexpr int kStageHalo = 4;
 
 // Arguments of one fused backward launch.
 template <typename T> struct BwdArgs {
@@ -157,6 +163,14 @@ cudaError_t launch_fwd(const FwdArgs<T>& a, const LaunchCfg& c, int phase, bool 
 template <typename T>
 cudaError_t launch_bwd(const BwdArgs<T>& a, const LaunchCfg& c, int phase, bool feq2d,
                        cudaStream_t s);
+// Staged forward step (x-invariant f_eq, C = c.threads in {128, 256} dividing nv, c.chunk_cols
+// columns per CTA in blocks of C); c.smem covers the buffers for a.stage_span rows.
+template <typename T>
+cudaError_t launch_fwd_staged(const FwdArgs<T>& a, const LaunchCfg& c, cudaStream_t s);
+template <typename T>
+cudaError_t set_staged_smem_limit(size_t bytes);
+// Shared memory of the staged kernel's buffers for a staging span of `span` rows and C columns.
+size_t staged_smem_bytes(int span, int C, size_t real_size);
 
 // Single-stage operators (vp_ops.cu).
 template <typename T>

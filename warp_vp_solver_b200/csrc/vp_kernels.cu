@@ -395,6 +395,225 @@ __global__ void __launch_bounds__(1024) vp_bwd_tail_kernel(const BwdArgs<T> a) {
 }
 
 // ----------------------------------------------------------------------------------------------
+// Staged forward step (x-invariant f_eq). The arithmetic of fwd_tile PHASE 1, organised for
+// throughput on large grids:
+//  * a CTA owns rows [r0, r0+R) and C = blockDim.x columns [c0, c0+C) (one column per thread);
+//  * the rows its columns' x windows touch, [r0 + 2 min m, r0 + 2 max m + R + 2), are staged in
+//    shared memory with a halo of kStageHalo cells on each side along v, by coalesced 16-byte
+//    loads (each staged value is read from global memory once per CTA);
+//  * the v step reads its two source cells from shared memory at any offset and adds the f_eq
+//    correction from per-shift tables A_m[j] = f_eq[j+m] - f_eq[j], B_m[j] = f_eq[j+m+1] -
+//    f_eq[j+m] (float64 differences rounded once on the host): V(f_eq) - f_eq = A_m + t B_m;
+//  * the x window is walked row by row with a rolling (o, d) pair.
+// Rows whose v shift lies outside [-kStageHalo, kStageHalo) take the float64 scalar form.
+// ----------------------------------------------------------------------------------------------
+template <typename T>
+struct Vec16 {
+    using type = float4;
+};
+template <>
+struct Vec16<double> {
+    using type = double2;
+};
+
+// Shared memory of the staged kernel, after the row-partial scratch: the staged rows
+// [span][C + 2 kStageHalo], the per-row shift records [span], and the correction tables of the
+// CTA's columns [2][2 kStageHalo][C].
+template <typename T>
+__host__ __device__ constexpr size_t staged_bytes(int span, int C) {
+    return (size_t)span * (C + 2 * kStageHalo) * sizeof(T) + (((size_t)span * 8 + 15) & ~(size_t)15) +
+           (size_t)4 * kStageHalo * C * sizeof(T);
+}
+
+template <typename T, int R, int C>
+__global__ void __launch_bounds__(C) vp_fwds_kernel(const FwdArgs<T> a) {
+    using V = typename Vec16<T>::type;
+    constexpr int VE = 16 / sizeof(T);
+    constexpr int HV = kStageHalo;
+    constexpr int W = C + 2 * HV;
+    constexpr int PER_ROW = W / VE;
+    constexpr int NM = 2 * HV;
+    extern __shared__ __align__(16) unsigned char smem[];
+    T* red = reinterpret_cast<T*>(smem);
+    const size_t red_bytes = (((size_t)32 * R * sizeof(T)) + 15) & ~(size_t)15;
+    const int span_max = a.stage_span;
+    T* stage = reinterpret_cast<T*>(smem + red_bytes);
+    int2* rinfo = reinterpret_cast<int2*>(smem + red_bytes + (size_t)span_max * W * sizeof(T));
+    T* tabs = reinterpret_cast<T*>(reinterpret_cast<unsigned char*>(rinfo) + (((size_t)span_max * 8 + 15) & ~(size_t)15));
+    __shared__ int s_last, s_min, s_max;
+
+    const int nx = a.nx, nv = a.nv;
+    const int r0 = blockIdx.x * R;
+    const int tid = threadIdx.x;
+    const bool next = a.h_out != nullptr;
+    const bool outf = a.f_hist_n != nullptr || a.f_final != nullptr;
+    const int g_begin = blockIdx.y * a.chunk_cols;
+    const int g_end = min(nv, g_begin + a.chunk_cols);
+
+    T acc[R];
+#pragma unroll
+    for (int e = 0; e < R; ++e) acc[e] = T(0);
+
+    for (int c0 = g_begin; c0 < g_end; c0 += C) {
+        const int j = c0 + tid;   // C divides nv and the group width
+        const int m = __ldg(a.mx + j);
+        const int sm = m > nx / 2 ? m - nx : m;   // signed x offset
+        int mn = sm, mxv = sm;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+            mxv = max(mxv, __shfl_xor_sync(0xffffffffu, mxv, o));
+        }
+        if (tid == 0) {
+            s_min = mn;
+            s_max = mxv;
+        }
+        __syncthreads();
+        if ((tid & 31) == 0 && tid != 0) {
+            atomicMin(&s_min, mn);
+            atomicMax(&s_max, mxv);
+        }
+        __syncthreads();
+        const int lo = r0 + 2 * s_min;
+        const int span = 2 * (s_max - s_min) + R + 2;
+        const bool staged = span <= span_max;
+        const int lo_w = ((lo % nx) + nx) % nx;
+        if (staged) {
+            for (int idx = tid; idx < span * PER_ROW; idx += C) {
+                const int q = idx / PER_ROW, v = idx - q * PER_ROW;
+                int row = lo_w + q;
+                row -= row >= nx ? nx : 0;
+                int col = c0 - HV + v * VE;
+                col += col < 0 ? nv : 0;
+                col -= col >= nv ? nv : 0;
+                reinterpret_cast<V*>(stage + q * W)[v] =
+                    __ldg(reinterpret_cast<const V*>(a.h_in + (size_t)row * nv + col));
+            }
+            for (int q = tid; q < span; q += C) {
+                int row = lo_w + q;
+                row -= row >= nx ? nx : 0;
+                const VShift<T> vs = a.vsh[row];
+                const int ms = vs.m >= nv / 2 ? vs.m - nv : vs.m;
+                int2 info;
+                info.x = (ms >= -HV && ms < HV) ? ms + HV : -1;
+                if constexpr (sizeof(T) == 4) {
+                    info.y = __float_as_int((float)vs.t);
+                } else {
+                    info.y = row;   // float64: the weight is read back from the shift record
+                }
+                rinfo[q] = info;
+            }
+#pragma unroll
+            for (int r = 0; r < 2 * NM; ++r) tabs[r * C + tid] = __ldg(a.vtab + (size_t)r * nv + j);
+        }
+        __syncthreads();
+        {
+            const T t = __ldg(a.tx + j);
+            const T wj = trap_w<T>(j, nv);
+            const int gbase = wrap2(r0 + 2 * m, nx);
+            const int sbase = r0 + 2 * sm - lo;
+            const int dbase = wrap1(r0 + m, nx);
+            const double fe = outf ? __ldg(a.feq + j) : 0.0;
+            const T* srow = stage + sbase * W + tid + HV;
+            auto vstep = [&](int k) -> T {
+                if (staged) {
+                    const int2 info = rinfo[sbase + k];
+                    if (info.x >= 0) {
+                        T tv;
+                        if constexpr (sizeof(T) == 4) tv = __int_as_float(info.y);
+                        else tv = a.vsh[info.y].t;
+                        const T* sr = srow + k * W + (info.x - HV);
+                        const T corr = tabs[info.x * C + tid] + tv * tabs[(NM + info.x) * C + tid];
+                        return lerp(sr[0], sr[1], tv) + corr;
+                    }
+                }
+                const int grow = wrap1(gbase + k, nx);
+                return v_cell<T, false>(a.h_in, a.feq, 0, nv, grow, j, a.vsh[grow]);
+            };
+            T o0 = vstep(0);
+            const T o1 = vstep(1);
+            T dp = lerp(o0, o1, t);
+            o0 = o1;
+            T* hout = next ? a.h_out + (size_t)r0 * nv + j : nullptr;
+#pragma unroll
+            for (int k = 2; k < R + 2; ++k) {
+                const T on = vstep(k);
+                const T dn = lerp(o0, on, t);
+                if (outf) {
+                    const int fr = wrap1(dbase + k - 2, nx);
+                    const double f = fe + (double)dp;
+                    if (a.f_hist_n != nullptr) a.f_hist_n[(size_t)fr * nv + j] = (T)f;
+                    if (a.f_final != nullptr) a.f_final[(size_t)fr * nv + j] = f;
+                }
+                if (next) {
+                    const T hv = lerp(dp, dn, t);
+                    hout[(size_t)(k - 2) * nv] = hv;
+                    acc[k - 2] += wj * hv;
+                }
+                o0 = on;
+                dp = dn;
+            }
+        }
+        __syncthreads();   // the next column block restages
+    }
+
+    if (a.part == nullptr || !next) return;
+    store_row_partials<T, R>(acc, red, a.part + (size_t)blockIdx.y * nx + r0);
+    if (a.counter == nullptr) return;
+    if (!last_cta_done(a.counter, &s_last)) return;
+    // the Poisson work area reuses the staging buffer (every thread of this CTA is past it)
+    fwd_tail<T>(a, poisson_area<T>(a.P, smem + red_bytes), red);
+    if (threadIdx.x == 0) *a.counter = 0u;
+}
+
+template <typename T, int R, int C>
+static cudaError_t fwds_launch(const FwdArgs<T>& args, const LaunchCfg& c, cudaStream_t s) {
+    // the column groups are the staged shape's (multiples of C), whatever the caller's args hold
+    FwdArgs<T> a = args;
+    a.chunk_cols = c.chunk_cols;
+    a.n_chunks = c.n_chunks;
+    if (a.chunk_cols < C || a.chunk_cols % C != 0 || a.nv % a.chunk_cols != 0) return cudaErrorInvalidValue;
+    dim3 grid(a.nx / R, a.nv / a.chunk_cols);
+    vp_fwds_kernel<T, R, C><<<grid, C, c.smem, s>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+#define VP_FWDS_C(RR)                                                             \
+    if (c.R == RR) return c.threads == 256 ? fwds_launch<T, RR, 256>(a, c, s) :   \
+                                             fwds_launch<T, RR, 128>(a, c, s);
+
+template <typename T>
+cudaError_t launch_fwd_staged(const FwdArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
+    if (c.threads != 128 && c.threads != 256) return cudaErrorInvalidValue;
+    VP_FWDS_C(4) VP_FWDS_C(8) VP_FWDS_C(16) VP_FWDS_C(32)
+    return cudaErrorInvalidValue;
+}
+#undef VP_FWDS_C
+
+size_t staged_smem_bytes(int span, int C, size_t real_size) {
+    return real_size == 8 ? staged_bytes<double>(span, C) : staged_bytes<float>(span, C);
+}
+
+template <typename T>
+cudaError_t set_staged_smem_limit(size_t bytes) {
+#define VP_SET(R, C)                                                                                 \
+    if (cudaError_t e = cudaFuncSetAttribute(vp_fwds_kernel<T, R, C>,                               \
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes); \
+        e != cudaSuccess)                                                                           \
+        return e;
+    VP_SET(4, 128) VP_SET(8, 128) VP_SET(16, 128) VP_SET(32, 128)
+    VP_SET(4, 256) VP_SET(8, 256) VP_SET(16, 256) VP_SET(32, 256)
+#undef VP_SET
+    return cudaSuccess;
+}
+
+template cudaError_t launch_fwd_staged<float>(const FwdArgs<float>&, const LaunchCfg&, cudaStream_t);
+template cudaError_t launch_fwd_staged<double>(const FwdArgs<double>&, const LaunchCfg&, cudaStream_t);
+template cudaError_t set_staged_smem_limit<float>(size_t);
+template cudaError_t set_staged_smem_limit<double>(size_t);
+
+// ----------------------------------------------------------------------------------------------
 // Launchers
 // ----------------------------------------------------------------------------------------------
 

@@ -81,13 +81,18 @@ class Plan:
         return {f: getattr(c, f) for f, _ in _capi.LaunchConfig._fields_}
 
     def set_config(self, rows_per_cta: int | None = None, threads: int | None = None,
-                   n_chunks: int | None = None, cluster_size: int | None = None) -> None:
+                   n_chunks: int | None = None, cluster_size: int | None = None,
+                   stage_rows: int | None = None, stage_threads: int | None = None) -> None:
+        """Change the launch shape; arguments left as None keep their current values.
+        ``stage_rows=0`` turns the staged forward step off."""
         cur = self.get_config()
         c = _capi.LaunchConfig()
         c.rows_per_cta = cur["rows_per_cta"] if rows_per_cta is None else int(rows_per_cta)
         c.threads = cur["threads"] if threads is None else int(threads)
         c.n_chunks = cur["n_chunks"] if n_chunks is None else int(n_chunks)
         c.cluster_size = cur["cluster_size"] if cluster_size is None else int(cluster_size)
+        c.stage_rows = cur["stage_rows"] if stage_rows is None else int(stage_rows)
+        c.stage_threads = cur["stage_threads"] if stage_threads is None else int(stage_threads)
         _capi.check(self.lib.vp_plan_set_config(self._h, ctypes.byref(c)))
         self._ws = {}   # workspace size depends on n_chunks
 
