@@ -86,55 +86,91 @@ def profile_traffic(kernel: str, workload: str):
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle sampling during the timed region."""
+    """SM clock and clock-event reasons sampled every 2 ms through NVML (read-only queries) in a
+    background thread while the timed region runs; falls back to `nvidia-smi -lms 200`."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake_slowdown", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, period_s: float = 0.002):
         self.gpu = gpu_index
-        self.proc = None
+        self.period = period_s
+        self.samples = []
+        self.reasons = set()
+        self.smax = None
+        self._stop = None
+        self._thread = None
+        self._proc = None
+
+    def _nvml_loop(self, nv, h):
+        masks = [(name, getattr(nv, attr)) for name, attr in self.REASONS if hasattr(nv, attr)]
+        while not self._stop.is_set():
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                for name, mask in masks:
+                    if r & mask:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            self._stop.wait(self.period)
 
     def __enter__(self):
+        import threading
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except (OSError, ValueError):
-            self.proc = None
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self._stop = threading.Event()
+            self._thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self._thread.start()
+        except Exception:
+            self._thread = None
+            try:
+                self._proc = subprocess.Popen(
+                    ["nvidia-smi", f"--id={self.gpu}", "--query-gpu=clocks.sm,clocks.max.sm,"
+                     "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                     "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                     "--format=csv,noheader,nounits", "-lms", "200"],
+                    stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            except (OSError, ValueError):
+                self._proc = None
         return self
 
     def __exit__(self, *exc):
-        self.out = ""
-        if self.proc is not None:
-            self.proc.terminate()
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=5)
+        if self._proc is not None:
+            self._proc.terminate()
             try:
-                self.out, _ = self.proc.communicate(timeout=5)
+                out, _ = self._proc.communicate(timeout=5)
             except subprocess.TimeoutExpired:
-                self.proc.kill()
-                self.out, _ = self.proc.communicate()
+                self._proc.kill()
+                out, _ = self._proc.communicate()
+            names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+            for line in (out or "").strip().splitlines():
+                parts = [p.strip() for p in line.split(",")]
+                try:
+                    self.samples.append(float(parts[0]))
+                    self.smax = float(parts[1])
+                except (ValueError, IndexError):
+                    continue
+                for name, val in zip(names, parts[2:6]):
+                    if val.lower().startswith("active"):
+                        self.reasons.add(name)
 
     def summary(self):
-        sm, smax, reasons = [], None, set()
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for line in (self.out or "").strip().splitlines():
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax = float(parts[2])
-            except ValueError:
-                continue
-            for name, val in zip(names, parts[5:9]):
-                if val.lower().startswith("active"):
-                    reasons.add(name)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.smax, "reasons": sorted(self.reasons),
+                    "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.smax,
+                "reasons": sorted(self.reasons), "samples": len(self.samples),
+                "source": "nvml" if self._proc is None else "nvidia-smi"}
 
 
 # ------------------------------------------------------------------------------------------------
@@ -313,7 +349,8 @@ def run_ours(args, rank, local_rank, world):
         n_recompute = 0 if every == 1 else sum(max(0, min(s0 + every, T) - s0 - 1) for s0 in range(0, T, every))
         n_fused_f, n_fused_b = T + 1, T + 1 + n_recompute
         alg_f, alg_b = BYTES_FWD * cells, BYTES_BWD * cells
-        kf, kb = "vp_fwd_kernel", "vp_bwd_kernel"
+        kf = "vp_fwds_kernel" if cfg["stage_rows"] > 0 else "vp_fwd_kernel"
+        kb = "vp_bwd_kernel"
     f_launch_ms = tf_ms / (args.steps * n_fused_f)
     b_launch_ms = (tb_ms / (args.steps * n_fused_b)) if wl.adjoint else 0.0
     if wl.adjoint and tb_ms >= tf_ms and (resident or every == 1):
