@@ -207,9 +207,10 @@ def test_staged_step_matches_oracle(shape, dtype):
     w = O.trapezoid_time_weights(T, dt)
     rg = np.random.default_rng(3)
     gff = rg.standard_normal((nx, nv))
+    gfh = 0.1 * rg.standard_normal((T, nx, nv))
     gEh = rg.standard_normal((T, nx))
-    gf, gH = s._run_backward(f_iv, H, T * dt, None, gff, None, gEh, w)
-    rf, rH = O.delta_backward(g, dt, f_eq, f_iv, H, T, gff, None, gEh, w)
+    gf, gH = s._run_backward(f_iv, H, T * dt, None, gff, gfh, gEh, w)
+    rf, rH = O.delta_backward(g, dt, f_eq, f_iv, H, T, gff, gfh, gEh, w)
     assert O.rel_err(gf, rf) < TOL_BWD[dtype] and O.rel_err(gH, rH) < TOL_BWD[dtype]
 
 

@@ -77,6 +77,7 @@ struct vp_plan {
     LaunchCfg scfg{};          // staged forward step (R rows x threads columns per CTA)
     int stage_span = 0;        // rows its staging buffer holds (0: staged step not used)
     std::vector<int> host_mx;  // x half-step offsets (host copy, for staged shapes)
+    size_t sb_smem = 0;        // staged adjoint step's shared memory (0: adjoint not staged)
     double* d_tx64 = nullptr;  // nv
     void* d_tw = nullptr;      // nx/2 complex
     void* d_mult = nullptr;    // nx reals (imaginary part)
@@ -239,12 +240,25 @@ static bool staged_config(vp_plan* p, int R, int C, int blocks_per_cta = 0) {
         cudaGetLastError();
         return false;
     }
+    // the adjoint step stages the same window of w plus the CTA's own rows of h_{n-1}
+    size_t sb = red + std::max(staged_bwd_smem_bytes(span, R, C, rs), tail);
+    if (sb > 200 * 1024) {
+        sb = 0;
+    } else {
+        const cudaError_t eb = p->dtype == VP_F64 ? set_staged_bwd_smem_limit<double>(sb)
+                                                  : set_staged_bwd_smem_limit<float>(sb);
+        if (eb != cudaSuccess) {
+            cudaGetLastError();
+            sb = 0;
+        }
+    }
     p->scfg.R = R;
     p->scfg.threads = C;
     p->scfg.chunk_cols = C * nb;
     p->scfg.n_chunks = n_blocks / nb;
     p->scfg.smem = smem;
     p->stage_span = span;
+    p->sb_smem = sb;
     return true;
 }
 
@@ -574,6 +588,8 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
     b.neg_dt_dv = (T)(-p->dt / p->dv);
     b.gH = g_H;
     b.grho_out = grho;
+    b.vtab = static_cast<const T*>(p->d_vtab);
+    b.stage_span = p->stage_span;
 
     int rc;
     // prologue (n = T)
@@ -603,7 +619,15 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
         b.E_prev = E_all + (size_t)(n - 1) * nx;
         b.gE_hist = g_Eh ? g_Eh + (size_t)(n - 1) * nx : nullptr;
         b.gee = g_ee ? g_ee + (n - 1) : nullptr;
-        VP_CUDA(launch_bwd<T>(b, p->cfg, 1, p->feq2d != 0, s), "backward step launch");
+        if (p->stage_span > 0 && p->sb_smem > 0) {
+            LaunchCfg bc = p->scfg;
+            bc.smem = p->sb_smem;
+            b.n_chunks = bc.n_chunks;
+            b.chunk_cols = bc.chunk_cols;
+            VP_CUDA(launch_bwd_staged<T>(b, bc, s), "backward step launch");
+        } else {
+            VP_CUDA(launch_bwd<T>(b, p->cfg, 1, p->feq2d != 0, s), "backward step launch");
+        }
         if (!p->tail_inline)
             VP_CUDA(launch_bwd_tail<T>(b, p->tail_threads, p->tail_smem, s), "backward tail launch");
     }

@@ -91,6 +91,8 @@ template <typename T> struct BwdArgs {
     const T* gee;               // address of the cotangent on ee_hist[n-1], or null
     T* gH;                      // accumulated cotangent on H
     T* grho_out;                // cotangent on rho of step n-1
+    const T* vtab;              // staged step: correction tables (B_m is the f_eq slope), or null
+    int stage_span;             // staged step: rows of w the staging buffer holds
 };
 
 // ---- ensembles: many instances (any nx, nv, dt, f_eq) advanced together -----------------------
@@ -171,6 +173,12 @@ template <typename T>
 cudaError_t set_staged_smem_limit(size_t bytes);
 // Shared memory of the staged kernel's buffers for a staging span of `span` rows and C columns.
 size_t staged_smem_bytes(int span, int C, size_t real_size);
+// Staged adjoint step (same shape rules as the staged forward step).
+template <typename T>
+cudaError_t launch_bwd_staged(const BwdArgs<T>& a, const LaunchCfg& c, cudaStream_t s);
+template <typename T>
+cudaError_t set_staged_bwd_smem_limit(size_t bytes);
+size_t staged_bwd_smem_bytes(int span, int R, int C, size_t real_size);
 
 // Single-stage operators (vp_ops.cu).
 template <typename T>

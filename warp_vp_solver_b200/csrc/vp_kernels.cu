@@ -595,6 +595,234 @@ size_t staged_smem_bytes(int span, int C, size_t real_size) {
     return real_size == 8 ? staged_bytes<double>(span, C) : staged_bytes<float>(span, C);
 }
 
+// ----------------------------------------------------------------------------------------------
+// Staged adjoint step (PHASE 1 of vp_bwd_kernel, x-invariant f_eq). Per column block of C
+// columns a CTA stages (a) the rows of w_n its columns' windows touch, [r0 - 2 max m - 2,
+// r0 - 2 min m + R), with a 4-cell halo along v, each with its shift record (m, t) and rho
+// cotangent; (b) its own R rows of h_{n-1} with the same halo and step n-1's shift records; (c) the
+// f_eq slope tables B_m of its columns. Then each thread walks its column: gh = V^T w + rho^T,
+// c = X^T gh (+ g_f_hist), w_{n-1} = X^T c, and the slope row sums for g_E_total of step n-1.
+// Rows whose shift leaves the halo use the global-memory form of bwd_tile.
+// ----------------------------------------------------------------------------------------------
+template <typename T>
+__host__ __device__ constexpr size_t staged_bwd_bytes(int span, int R, int C) {
+    return (size_t)(span + R) * (C + 2 * kStageHalo) * sizeof(T) + (((size_t)(span + R) * 8 + 15) & ~(size_t)15) +
+           (((size_t)span * sizeof(T) + 15) & ~(size_t)15) + (size_t)2 * kStageHalo * C * sizeof(T);
+}
+
+template <typename T, int R, int C>
+__global__ void __launch_bounds__(C) vp_bwds_kernel(const BwdArgs<T> a) {
+    using V = typename Vec16<T>::type;
+    constexpr int VE = 16 / sizeof(T);
+    constexpr int HV = kStageHalo;
+    constexpr int W = C + 2 * HV;
+    constexpr int PER_ROW = W / VE;
+    constexpr int NM = 2 * HV;
+    extern __shared__ __align__(16) unsigned char smem[];
+    T* red = reinterpret_cast<T*>(smem);
+    const size_t red_bytes = (((size_t)32 * R * sizeof(T)) + 15) & ~(size_t)15;
+    const int span_max = a.stage_span;
+    T* sw = reinterpret_cast<T*>(smem + red_bytes);               // [span_max][W]
+    T* sh = sw + (size_t)span_max * W;                               // [R][W]
+    int2* iw = reinterpret_cast<int2*>(sh + (size_t)R * W);          // [span_max]
+    int2* ih = iw + span_max;                                        // [R]
+    T* sg = reinterpret_cast<T*>(reinterpret_cast<unsigned char*>(iw) +
+                                 (((size_t)(span_max + R) * 8 + 15) & ~(size_t)15));   // [span_max]
+    T* tabB = reinterpret_cast<T*>(reinterpret_cast<unsigned char*>(sg) +
+                                   (((size_t)span_max * sizeof(T) + 15) & ~(size_t)15));  // [NM][C]
+    __shared__ int s_last, s_min, s_max;
+
+    const int nx = a.nx, nv = a.nv;
+    const int r0 = blockIdx.x * R;
+    const int tid = threadIdx.x;
+    const int g_begin = blockIdx.y * a.chunk_cols;
+    const int g_end = min(nv, g_begin + a.chunk_cols);
+    const T* vB = a.vtab + (size_t)NM * nv;
+
+    T acc[R];
+#pragma unroll
+    for (int e = 0; e < R; ++e) acc[e] = T(0);
+
+    for (int c0 = g_begin; c0 < g_end; c0 += C) {
+        const int j = c0 + tid;
+        const int m = __ldg(a.mx + j);
+        const int sm = m > nx / 2 ? m - nx : m;
+        int mn = sm, mxv = sm;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+            mxv = max(mxv, __shfl_xor_sync(0xffffffffu, mxv, o));
+        }
+        if (tid == 0) {
+            s_min = mn;
+            s_max = mxv;
+        }
+        __syncthreads();
+        if ((tid & 31) == 0 && tid != 0) {
+            atomicMin(&s_min, mn);
+            atomicMax(&s_max, mxv);
+        }
+        __syncthreads();
+        const int lo = r0 - 2 * s_max - 2;
+        const int span = 2 * (s_max - s_min) + R + 2;
+        const bool staged = span <= span_max;
+        const int lo_w = ((lo % nx) + nx) % nx;
+        if (staged) {
+            for (int idx = tid; idx < (span + R) * PER_ROW; idx += C) {
+                const int q = idx / PER_ROW, v = idx - q * PER_ROW;
+                int col = c0 - HV + v * VE;
+                col += col < 0 ? nv : 0;
+                col -= col >= nv ? nv : 0;
+                const T* src;
+                if (q < span) {
+                    int row = lo_w + q;
+                    row -= row >= nx ? nx : 0;
+                    src = a.w_in + (size_t)row * nv + col;
+                } else {
+                    src = a.h_prev + (size_t)(r0 + q - span) * nv + col;
+                }
+                const int dst_row = q < span ? q : span_max + (q - span);
+                reinterpret_cast<V*>(sw + (size_t)dst_row * W)[v] = __ldg(reinterpret_cast<const V*>(src));
+            }
+            for (int q = tid; q < span + R; q += C) {
+                int row;
+                VShift<T> vs;
+                if (q < span) {
+                    row = lo_w + q;
+                    row -= row >= nx ? nx : 0;
+                    vs = a.vsh_n[row];
+                    sg[q] = __ldg(a.grho + row);
+                } else {
+                    row = r0 + q - span;
+                    vs = a.vsh_prev[row];
+                }
+                const int ms = vs.m >= nv / 2 ? vs.m - nv : vs.m;
+                int2 info;
+                info.x = (ms >= -HV && ms < HV) ? ms + HV : -1;
+                if constexpr (sizeof(T) == 4) info.y = __float_as_int((float)vs.t);
+                else info.y = row;
+                if (q < span) iw[q] = info;
+                else ih[q - span] = info;
+            }
+#pragma unroll
+            for (int r = 0; r < NM; ++r) tabB[r * C + tid] = __ldg(vB + (size_t)r * nv + j);
+        }
+        __syncthreads();
+        {
+            const T t = __ldg(a.tx + j);
+            const T wr = -a.dv * trap_w<T>(j, nv);
+            const int sbase = 2 * (s_max - sm);            // staged row of gh[0]
+            const int gbase = wrapneg((r0 - 2 * m - 2) % nx, nx);
+            const int cbase = wrapneg((r0 - m - 1) % nx, nx);
+            auto ghstep = [&](int k) -> T {
+                if (staged) {
+                    const int2 info = iw[sbase + k];
+                    if (info.x >= 0) {
+                        T tv;
+                        if constexpr (sizeof(T) == 4) tv = __int_as_float(info.y);
+                        else tv = a.vsh_n[info.y].t;
+                        const T* sr = sw + (size_t)(sbase + k) * W + tid + 2 * HV - info.x;
+                        return lerp(sr[0], sr[-1], tv) + wr * sg[sbase + k];
+                    }
+                }
+                const int row = wrap1(gbase + k, nx);
+                const VShift<T> vs = a.vsh_n[row];
+                const int cc0 = wrapneg(j - vs.m, nv);
+                const int cc1 = wrapneg(cc0 - 1, nv);
+                const T* wrow = a.w_in + (size_t)row * nv;
+                return lerp(__ldg(wrow + cc0), __ldg(wrow + cc1), vs.t) + wr * __ldg(a.grho + row);
+            };
+            auto slope = [&](int e) -> T {
+                if (staged) {
+                    const int2 info = ih[e];
+                    if (info.x >= 0) {
+                        const T* hr = sh + (size_t)e * W + tid + info.x;   // column j + ms
+                        return (hr[1] - hr[0]) + tabB[info.x * C + tid];
+                    }
+                }
+                const int row = r0 + e;
+                const VShift<T> vp = a.vsh_prev[row];
+                const int d0 = wrap1(j + vp.m, nv);
+                int d1 = d0 + 1;
+                d1 = d1 == nv ? 0 : d1;
+                const T* hr = a.h_prev + (size_t)row * nv;
+                return (__ldg(hr + d1) - __ldg(hr + d0)) +
+                       (T)(feq_at<T, false>(a.feq, 0, row, d1) - feq_at<T, false>(a.feq, 0, row, d0));
+            };
+            T g0 = ghstep(0);
+            T g1 = ghstep(1);
+            T cp = lerp(g1, g0, t);
+            if (a.gfh != nullptr) cp += __ldg(a.gfh + (size_t)cbase * nv + j);
+            g0 = g1;
+            T* wout = a.w_out + (size_t)r0 * nv + j;
+#pragma unroll
+            for (int k = 2; k < R + 2; ++k) {
+                const T gk = ghstep(k);
+                T cn = lerp(gk, g0, t);
+                if (a.gfh != nullptr) cn += __ldg(a.gfh + (size_t)wrap1(cbase + k - 1, nx) * nv + j);
+                const T wv = lerp(cn, cp, t);
+                wout[(size_t)(k - 2) * nv] = wv;
+                acc[k - 2] += slope(k - 2) * wv;
+                g0 = gk;
+                cp = cn;
+            }
+        }
+        __syncthreads();
+    }
+
+    store_row_partials<T, R>(acc, red, a.part + (size_t)blockIdx.y * nx + r0);
+    if (a.counter == nullptr) return;
+    if (!last_cta_done(a.counter, &s_last)) return;
+    bwd_tail<T>(a, poisson_area<T>(a.P, smem + red_bytes));
+    if (threadIdx.x == 0) *a.counter = 0u;
+}
+
+template <typename T, int R, int C>
+static cudaError_t bwds_launch(const BwdArgs<T>& args, const LaunchCfg& c, cudaStream_t s) {
+    BwdArgs<T> a = args;
+    a.chunk_cols = c.chunk_cols;
+    a.n_chunks = c.n_chunks;
+    if (a.chunk_cols < C || a.chunk_cols % C != 0 || a.nv % a.chunk_cols != 0) return cudaErrorInvalidValue;
+    dim3 grid(a.nx / R, a.nv / a.chunk_cols);
+    vp_bwds_kernel<T, R, C><<<grid, C, c.smem, s>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+#define VP_BWDS_C(RR)                                                             \
+    if (c.R == RR) return c.threads == 256 ? bwds_launch<T, RR, 256>(a, c, s) :   \
+                                             bwds_launch<T, RR, 128>(a, c, s);
+
+template <typename T>
+cudaError_t launch_bwd_staged(const BwdArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
+    if (c.threads != 128 && c.threads != 256) return cudaErrorInvalidValue;
+    VP_BWDS_C(4) VP_BWDS_C(8) VP_BWDS_C(16) VP_BWDS_C(32)
+    return cudaErrorInvalidValue;
+}
+#undef VP_BWDS_C
+
+size_t staged_bwd_smem_bytes(int span, int R, int C, size_t real_size) {
+    return real_size == 8 ? staged_bwd_bytes<double>(span, R, C) : staged_bwd_bytes<float>(span, R, C);
+}
+
+template <typename T>
+cudaError_t set_staged_bwd_smem_limit(size_t bytes) {
+#define VP_SET(R, C)                                                                                 \
+    if (cudaError_t e = cudaFuncSetAttribute(vp_bwds_kernel<T, R, C>,                               \
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes); \
+        e != cudaSuccess)                                                                           \
+        return e;
+    VP_SET(4, 128) VP_SET(8, 128) VP_SET(16, 128) VP_SET(32, 128)
+    VP_SET(4, 256) VP_SET(8, 256) VP_SET(16, 256) VP_SET(32, 256)
+#undef VP_SET
+    return cudaSuccess;
+}
+
+template cudaError_t launch_bwd_staged<float>(const BwdArgs<float>&, const LaunchCfg&, cudaStream_t);
+template cudaError_t launch_bwd_staged<double>(const BwdArgs<double>&, const LaunchCfg&, cudaStream_t);
+template cudaError_t set_staged_bwd_smem_limit<float>(size_t);
+template cudaError_t set_staged_bwd_smem_limit<double>(size_t);
+
 template <typename T>
 cudaError_t set_staged_smem_limit(size_t bytes) {
 #define VP_SET(R, C)                                                                                 \
