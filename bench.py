@@ -51,6 +51,7 @@ def parse_args():
     ap.add_argument("--cluster-size", type=int, default=None,
                     help="force the cluster size of the resident path (0: streaming path)")
     ap.add_argument("--no-graph", action="store_true", help="launch eagerly instead of replaying a CUDA graph")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample duration")
@@ -241,8 +242,13 @@ def run_ours(args, rank, local_rank, world):
     ce = args.checkpoint_every if args.checkpoint_every is not None else wl.checkpoint_every
     solver = WarpVlasovPoissonSolver(wl.mesh, wl.dt, wl.f_eq, dtype=dtype, checkpoint_every=ce)
     plan = solver.plan
+    tuned = None
     if args.cluster_size is not None:
         plan.set_config(cluster_size=args.cluster_size)
+    elif not args.no_autotune:
+        t = solver.autotune(steps=min(8, wl.n_steps))
+        tuned = {"config": t["config"], "ms_per_candidate_run": t["ms"], "cached": t["cached"],
+                 "candidates": len(t.get("tried", []))}
     lib = _capi.load()
     nx, nv, T = wl.mesh.nx, wl.mesh.nv, wl.n_steps
     every = plan.resolve_every(T, ce)
@@ -397,6 +403,7 @@ def run_ours(args, rank, local_rank, world):
                    "launch": {k: cfg[k] for k in ("rows_per_cta", "threads", "n_chunks", "tail_inline",
                                                   "cluster_size", "cluster_threads")},
                    "path": "cluster-resident" if resident else "streaming",
+                   "autotune": tuned,
                    "fwd_ms_per_step": round(tf_ms / args.steps, 4),
                    "bwd_ms_per_step": round(tb_ms / args.steps, 4)},
         "roofline": roof,
@@ -512,6 +519,12 @@ def run_ensemble(args, rank, local_rank, world):
     shards = lpt_shards([m.nx * m.nv for m in full.meshes], world)
     ew = full.subset(shards[rank])
     ens = Ensemble(ew.meshes, ew.dt, ew.f_eqs, dtype=dtype, device=dev)
+    tuned = None
+    if not args.no_autotune:
+        from warp_vp_solver_b200.autotune import tune_ensemble
+        t = tune_ensemble(ens, steps=6)
+        tuned = {"config": t["config"], "ms_per_candidate_run": t["ms"], "cached": t["cached"],
+                 "candidates": len(t.get("tried", []))}
     lib = _capi.load()
     T = ew.n_steps
     f_iv = ens.pack_cells(ew.f_ivs)
@@ -614,6 +627,7 @@ def run_ensemble(args, rank, local_rank, world):
                    "shapes": shapes, "parallelism": f"ensemble shards x{world}" if world > 1 else "single",
                    "l2": "flushed between timed steps (256 MiB write, untimed)",
                    "cuda_graph": use_graph, "path": "ensemble persistent launch per time step",
+                   "autotune": tuned, "tile": ens.get_config(),
                    "fwd_ms_per_step": round(tf_ms / args.steps, 4),
                    "bwd_ms_per_step": round(tb_ms / args.steps, 4)},
         "roofline": roof,

@@ -183,6 +183,22 @@ int vp_batch_backward(vp_batch* batch, const void* H, int32_t n_steps, const voi
                       void* g_f_iv, void* g_H, void* workspace, size_t workspace_bytes,
                       void* stream);
 
+/* Tile shape of an ensemble's step launches (the autotuner's knobs). */
+typedef struct vp_batch_config {
+    int32_t rows_per_tile;    /* 1, 2, 4 or 8; divides every instance's nx and is <= nx/2        */
+    int32_t chunk_cols;       /* columns per tile: a multiple of 32 in [32, 256]                  */
+    int32_t threads;          /* threads per CTA: a multiple of 32 in [32, 256]                   */
+    int32_t ctas_per_sm;      /* persistent CTAs per SM (0: as many as fit)                       */
+    int32_t n_tiles;          /* derived: tiles per step over all instances                       */
+    int32_t grid_fwd;         /* derived: persistent grid of the forward launches                 */
+    int32_t grid_bwd;         /* derived: persistent grid of the adjoint launches                 */
+} vp_batch_config;
+
+int vp_batch_get_config(const vp_batch* batch, vp_batch_config* out);
+/* Sets rows_per_tile, chunk_cols, threads and ctas_per_sm. Workspace sizes depend on chunk_cols
+ * (query vp_batch_workspace_bytes again); graphs captured before the call must be re-captured. */
+int vp_batch_set_config(vp_batch* batch, const vp_batch_config* cfg);
+
 /* --- surrogate MLP ----------------------------------------------------------------------------
  * Fully connected network widths[0] -> ... -> widths[n_layers] with GELU (erf form) between
  * layers and none on the output: BF16 operands, FP32 accumulation on the tensor cores, FP32

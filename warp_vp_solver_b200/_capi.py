@@ -67,6 +67,18 @@ class LaunchConfig(ctypes.Structure):
     ]
 
 
+class BatchConfig(ctypes.Structure):
+    _fields_ = [
+        ("rows_per_tile", c_i32),
+        ("chunk_cols", c_i32),
+        ("threads", c_i32),
+        ("ctas_per_sm", c_i32),
+        ("n_tiles", c_i32),
+        ("grid_fwd", c_i32),
+        ("grid_bwd", c_i32),
+    ]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "vp_abi_version": (c_int, []),
@@ -90,6 +102,8 @@ SIGNATURES = {
     "vp_batch_create": (c_int, [c_i32, ctypes.POINTER(MeshDesc), ctypes.POINTER(c_dbl),
                                 ctypes.POINTER(ctypes.POINTER(c_dbl)), c_int, ctypes.POINTER(c_vp)]),
     "vp_batch_destroy": (c_int, [c_vp]),
+    "vp_batch_get_config": (c_int, [c_vp, ctypes.POINTER(BatchConfig)]),
+    "vp_batch_set_config": (c_int, [c_vp, ctypes.POINTER(BatchConfig)]),
     "vp_batch_offsets": (c_int, [c_vp, ctypes.POINTER(c_i64), ctypes.POINTER(c_i64),
                                  ctypes.POINTER(c_i64), ctypes.POINTER(c_i64)]),
     "vp_batch_workspace_bytes": (c_int, [c_vp, c_i32, ctypes.POINTER(c_size)]),

@@ -262,14 +262,14 @@ static bool staged_config(vp_plan* p, int R, int C, int blocks_per_cta = 0) {
     return true;
 }
 
-// Default staged shape: C = 256 (or 128) columns, and the largest R of 32, 16, 8, 4 that still
-// gives two CTAs per SM.
+// Default staged shape: C = 256 (or 128) columns, and the largest R of 16, 8, 4 that still gives
+// two CTAs per SM (R = 32 widens the staged window; an autotuned shape may still choose it).
 static void choose_staged(vp_plan* p, int n_sms) {
     p->stage_span = 0;
     for (int C : {256, 128}) {
         if (p->nv % C != 0) continue;
         int best = 0;
-        for (int r : {32, 16, 8, 4}) {
+        for (int r : {16, 8, 4}) {
             if (p->nx % r != 0 || r > p->nx / 4) continue;
             if (best == 0) best = r;
             if ((long long)(p->nx / r) * (p->nv / C) >= 2LL * n_sms) {
@@ -1217,7 +1217,7 @@ int vp_semilag_v(vp_plan* plan, const void* in, const void* E_total, void* out, 
 // =============================================================================================
 
 struct vp_batch {
-    int n = 0, dtype = VP_F32, device = 0, R = 1, threads = 128, feq2d = 0;
+    int n = 0, dtype = VP_F32, device = 0, R = 1, threads = 128, feq2d = 0, chunk = 128, per_sm = 0;
     std::vector<vp_plan*> owned;          // distinct plans
     std::vector<vp_plan*> plan_of;        // plan of each instance (caller order)
     std::vector<long long> off_f;         // caller order
@@ -1310,6 +1310,90 @@ static void free_batch(vp_batch* b) {
         cudaSetDevice(prev);
     }
     delete b;
+}
+
+// Tile shape of an ensemble: R rows x up to `chunk` columns per tile (instances narrower than the
+// chunk use their nv rounded up to 32), `threads` per CTA, and a persistent grid of `per_sm`
+// CTAs per SM (0: as many as the occupancy calculator allows). Rebuilds the device instance
+// table (longest instances first); a CUDA graph captured before this call is stale after it.
+static int batch_layout(vp_batch* b, int R, int chunk, int threads, int per_sm) {
+    if (!(R == 1 || R == 2 || R == 4 || R == 8)) return set_err(VP_ERR_ARG, "rows_per_tile must be 1, 2, 4 or 8");
+    for (vp_plan* p : b->plan_of)
+        if (p->nx % R != 0 || (R > 1 && R > p->nx / 2))
+            return set_err(VP_ERR_ARG, "rows_per_tile=%d must divide every nx and be <= nx/2 (nx=%d)", R, p->nx);
+    if (chunk < 32 || chunk > 256 || chunk % 32 != 0)
+        return set_err(VP_ERR_ARG, "chunk_cols must be a multiple of 32 in [32, 256] (got %d)", chunk);
+    if (threads < 32 || threads > 256 || threads % 32 != 0)
+        return set_err(VP_ERR_ARG, "threads must be a multiple of 32 in [32, 256] (got %d)", threads);
+    if (per_sm < 0) return set_err(VP_ERR_ARG, "ctas_per_sm must be >= 0");
+    const int n = b->n;
+    std::vector<int> chunk_cols(n);
+    int max_nx = 0;
+    long long part = 0;
+    for (int i = 0; i < n; ++i) {
+        vp_plan* p = b->plan_of[i];
+        chunk_cols[i] = std::min(chunk, ((p->nv + 31) / 32) * 32);
+        max_nx = std::max(max_nx, p->nx);
+        part += (long long)((p->nv + chunk_cols[i] - 1) / chunk_cols[i]) * p->nx;
+    }
+    const size_t rs = b->dtype == VP_F64 ? 8 : 4;
+    const size_t area = poisson_area_size(max_nx, rs);
+    if (area > 40 * 1024)
+        return set_err(VP_ERR_UNSUPPORTED, "ensembles support nx up to the in-kernel Poisson limit (got nx=%d)", max_nx);
+    const size_t smem = (((size_t)32 * R * rs + 15) & ~(size_t)15) + area;
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+        return (long long)b->plan_of[a]->nx * b->plan_of[a]->nv > (long long)b->plan_of[c]->nx * b->plan_of[c]->nv;
+    });
+    const int old_R = b->R;
+    b->R = R;   // batch_fill reads it
+    size_t bytes = 0;
+    int n_tiles = 0;
+    std::vector<unsigned char> host;
+    if (b->dtype == VP_F64) {
+        std::vector<BatchInst<double>> v;
+        batch_fill<double>(b, v, order, chunk_cols);
+        n_tiles = v.back().tile_begin + v.back().n_tiles;
+        bytes = v.size() * sizeof(BatchInst<double>);
+        host.assign(reinterpret_cast<unsigned char*>(v.data()), reinterpret_cast<unsigned char*>(v.data()) + bytes);
+    } else {
+        std::vector<BatchInst<float>> v;
+        batch_fill<float>(b, v, order, chunk_cols);
+        n_tiles = v.back().tile_begin + v.back().n_tiles;
+        bytes = v.size() * sizeof(BatchInst<float>);
+        host.assign(reinterpret_cast<unsigned char*>(v.data()), reinterpret_cast<unsigned char*>(v.data()) + bytes);
+    }
+    void* d_inst = nullptr;
+    const int rc = upload_bytes(&d_inst, host.data(), bytes);
+    if (rc != VP_OK) {
+        b->R = old_R;
+        return rc;
+    }
+    if (b->d_inst) cudaFree(b->d_inst);
+    b->d_inst = d_inst;
+    const bool f2 = b->feq2d != 0;
+    int n_sms = 148;
+    cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, b->device);
+    int bf = b->dtype == VP_F64 ? batch_blocks_per_sm<double>(R, true, f2, threads, smem)
+                                : batch_blocks_per_sm<float>(R, true, f2, threads, smem);
+    int bb = b->dtype == VP_F64 ? batch_blocks_per_sm<double>(R, false, f2, threads, smem)
+                                : batch_blocks_per_sm<float>(R, false, f2, threads, smem);
+    bf = std::max(1, bf);
+    bb = std::max(1, bb);
+    if (per_sm > 0) {
+        bf = std::min(bf, per_sm);
+        bb = std::min(bb, per_sm);
+    }
+    b->chunk = chunk;
+    b->threads = threads;
+    b->per_sm = per_sm;
+    b->smem = smem;
+    b->total_part = part;
+    b->n_tiles = n_tiles;
+    b->grid_fwd = std::max(1, std::min(n_tiles, bf * n_sms));
+    b->grid_bwd = std::max(1, std::min(n_tiles, bb * n_sms));
+    return VP_OK;
 }
 
 template <typename T>
@@ -1465,78 +1549,51 @@ int vp_batch_create(int32_t n, const vp_mesh_desc* meshes, const double* dts,
         }
         b->plan_of.push_back(found);
     }
-    // common rows-per-tile and per-instance column chunks
-    int R = 8;
+    int R = 8;   // largest common rows-per-tile
     for (;;) {
         bool ok = true;
         for (vp_plan* p : b->plan_of) ok = ok && (p->nx % R == 0) && (R == 1 || R <= p->nx / 2);
         if (ok || R == 1) break;
         R /= 2;
     }
-    b->R = R;
-    int max_nx = 0;
     bool feq2d = false;
-    std::vector<int> chunk_cols(n);
     for (int i = 0; i < n; ++i) {
         vp_plan* p = b->plan_of[i];
-        chunk_cols[i] = p->nv >= 128 ? 128 : ((p->nv + 31) / 32) * 32;
-        max_nx = std::max(max_nx, p->nx);
         feq2d = feq2d || p->feq2d;
         b->off_f.push_back(b->total_f);
         b->off_x.push_back(b->total_x);
         b->total_f += (long long)p->nx * p->nv;
         b->total_x += p->nx;
-        b->total_part += (long long)((p->nv + chunk_cols[i] - 1) / chunk_cols[i]) * p->nx;
     }
     if (b->total_x > 2147483647LL) {
         free_batch(b);
         return set_err(VP_ERR_ARG, "ensemble has more than 2^31 rows");
     }
     b->feq2d = feq2d ? 1 : 0;
-    b->threads = 128;
-    const size_t rs = dtype == VP_F64 ? 8 : 4;
-    const size_t area = poisson_area_size(max_nx, rs);
-    if (area > 40 * 1024) {
-        free_batch(b);
-        return set_err(VP_ERR_UNSUPPORTED, "ensembles support nx up to the in-kernel Poisson limit (got nx=%d)", max_nx);
-    }
-    b->smem = (((size_t)32 * R * rs + 15) & ~(size_t)15) + area;
-    // longest instances first
-    std::vector<int> order(n);
-    for (int i = 0; i < n; ++i) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
-        return (long long)b->plan_of[a]->nx * b->plan_of[a]->nv > (long long)b->plan_of[c]->nx * b->plan_of[c]->nv;
-    });
-    size_t bytes = 0;
-    std::vector<unsigned char> host;
-    if (dtype == VP_F64) {
-        std::vector<BatchInst<double>> v;
-        batch_fill<double>(b, v, order, chunk_cols);
-        b->n_tiles = v.back().tile_begin + v.back().n_tiles;
-        bytes = v.size() * sizeof(BatchInst<double>);
-        host.assign(reinterpret_cast<unsigned char*>(v.data()), reinterpret_cast<unsigned char*>(v.data()) + bytes);
-    } else {
-        std::vector<BatchInst<float>> v;
-        batch_fill<float>(b, v, order, chunk_cols);
-        b->n_tiles = v.back().tile_begin + v.back().n_tiles;
-        bytes = v.size() * sizeof(BatchInst<float>);
-        host.assign(reinterpret_cast<unsigned char*>(v.data()), reinterpret_cast<unsigned char*>(v.data()) + bytes);
-    }
-    int rc = upload_bytes(&b->d_inst, host.data(), bytes);
+    const int rc = batch_layout(b, R, 128, 128, 0);
     if (rc != VP_OK) {
         free_batch(b);
         return rc;
     }
-    int n_sms = 148;
-    cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, b->device);
-    const int bf = dtype == VP_F64 ? batch_blocks_per_sm<double>(R, true, feq2d, b->threads, b->smem)
-                                   : batch_blocks_per_sm<float>(R, true, feq2d, b->threads, b->smem);
-    const int bb = dtype == VP_F64 ? batch_blocks_per_sm<double>(R, false, feq2d, b->threads, b->smem)
-                                   : batch_blocks_per_sm<float>(R, false, feq2d, b->threads, b->smem);
-    b->grid_fwd = std::max(1, std::min(b->n_tiles, std::max(1, bf) * n_sms));
-    b->grid_bwd = std::max(1, std::min(b->n_tiles, std::max(1, bb) * n_sms));
     *out = b;
     return VP_OK;
+}
+
+int vp_batch_get_config(const vp_batch* b, vp_batch_config* out) {
+    if (!b || !out) return set_err(VP_ERR_ARG, "batch and out must not be NULL");
+    out->rows_per_tile = b->R;
+    out->chunk_cols = b->chunk;
+    out->threads = b->threads;
+    out->ctas_per_sm = b->per_sm;
+    out->n_tiles = b->n_tiles;
+    out->grid_fwd = b->grid_fwd;
+    out->grid_bwd = b->grid_bwd;
+    return VP_OK;
+}
+
+int vp_batch_set_config(vp_batch* b, const vp_batch_config* cfg) {
+    if (!b || !cfg) return set_err(VP_ERR_ARG, "batch and cfg must not be NULL");
+    return batch_layout(b, cfg->rows_per_tile, cfg->chunk_cols, cfg->threads, cfg->ctas_per_sm);
 }
 
 int vp_batch_destroy(vp_batch* b) {

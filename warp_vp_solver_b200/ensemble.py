@@ -102,6 +102,24 @@ class Ensemble:
         except Exception:
             pass
 
+    def get_config(self) -> dict:
+        c = _capi.BatchConfig()
+        _capi.check(self.lib.vp_batch_get_config(self._h, ctypes.byref(c)))
+        return {f: getattr(c, f) for f, _ in _capi.BatchConfig._fields_}
+
+    def set_config(self, rows_per_tile: int | None = None, chunk_cols: int | None = None,
+                   threads: int | None = None, ctas_per_sm: int | None = None) -> None:
+        """Change the tile shape (None keeps the current value). Invalidates captured graphs."""
+        cur = self.get_config()
+        c = _capi.BatchConfig()
+        c.rows_per_tile = cur["rows_per_tile"] if rows_per_tile is None else int(rows_per_tile)
+        c.chunk_cols = cur["chunk_cols"] if chunk_cols is None else int(chunk_cols)
+        c.threads = cur["threads"] if threads is None else int(threads)
+        c.ctas_per_sm = cur["ctas_per_sm"] if ctas_per_sm is None else int(ctas_per_sm)
+        with torch.cuda.device(self.device):
+            _capi.check(self.lib.vp_batch_set_config(self._h, ctypes.byref(c)))
+        self._ws = {}
+
     @property
     def cells_per_step(self) -> int:
         return self.total_cells

@@ -46,6 +46,7 @@ class Plan:
         f_eq = np.ascontiguousarray(np.asarray(f_eq, dtype=np.float64))
         if f_eq.shape != (self.nx, self.nv):
             raise ValueError(f"f_eq shape {f_eq.shape} != ({self.nx}, {self.nv})")
+        self.f_eq = f_eq
         self._xs = np.ascontiguousarray(np.asarray(mesh.xs, dtype=np.float64))
         self._vs = np.ascontiguousarray(np.asarray(mesh.vs, dtype=np.float64))
         desc = _capi.MeshDesc(self.nx, self.nv, _capi.dbl_ptr(self._xs), _capi.dbl_ptr(self._vs),

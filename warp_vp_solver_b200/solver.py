@@ -133,6 +133,12 @@ class WarpVlasovPoissonSolver:
         return float(self.plan.electric_energy(E).double().cpu()[0])
 
     # ------------------------------------------------------------------ forward
+    def autotune(self, steps: int = 8, force: bool = False, cache_path: str | None = None) -> dict:
+        """Time the candidate launch shapes on this solver's grid and keep the fastest (cached
+        per device and shape; see ``warp_vp_solver_b200.autotune``)."""
+        from .autotune import TuneCache, tune_plan
+        return tune_plan(self.plan, steps=steps, force=force, cache=TuneCache(cache_path))
+
     def run_forward(self, f_iv, H, t_final: float, *, record_history: bool | None = None):
         """Strang-split time loop (solver.py:418-464).
 
