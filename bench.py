@@ -52,6 +52,9 @@ def parse_args():
                     help="force the cluster size of the resident path (0: streaming path)")
     ap.add_argument("--no-graph", action="store_true", help="launch eagerly instead of replaying a CUDA graph")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape")
+    ap.add_argument("--stage-rows", type=int, default=None,
+                    help="force the staged step's rows per CTA (0: per-column kernel); skips autotuning")
+    ap.add_argument("--stage-threads", type=int, default=None, help="with --stage-rows: threads per CTA")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample duration")
@@ -243,8 +246,11 @@ def run_ours(args, rank, local_rank, world):
     solver = WarpVlasovPoissonSolver(wl.mesh, wl.dt, wl.f_eq, dtype=dtype, checkpoint_every=ce)
     plan = solver.plan
     tuned = None
-    if args.cluster_size is not None:
-        plan.set_config(cluster_size=args.cluster_size)
+    if args.cluster_size is not None or args.stage_rows is not None:
+        if args.cluster_size is not None:
+            plan.set_config(cluster_size=args.cluster_size)
+        if args.stage_rows is not None:
+            plan.set_config(cluster_size=0, stage_rows=args.stage_rows, stage_threads=args.stage_threads)
     elif not args.no_autotune:
         t = solver.autotune(steps=min(8, wl.n_steps))
         tuned = {"config": t["config"], "ms_per_candidate_run": t["ms"], "cached": t["cached"],
