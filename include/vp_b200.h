@@ -307,6 +307,18 @@ int vp_plan_get_config(const vp_plan* plan, vp_launch_config* out);
  * depend on n_chunks: query vp_workspace_bytes() again after changing it. */
 int vp_plan_set_config(vp_plan* plan, const vp_launch_config* cfg);
 
+/* Time-splitting scheme of a plan's forward and adjoint loops.
+ * VP_SCHEME_STRANG: X(dt/2) V(dt) X(dt/2) every step (the reference's default path,
+ *   warp_vp_solver/solver.py:418-612, 742-1105).
+ * VP_SCHEME_MERGED: the reference's aggressive path (`aggressive=True`, solver.py:618-736,
+ *   1111-1338): the trailing X(dt/2) of a step and the leading X(dt/2) of the next are one
+ *   X(dt); f_hist[t] holds the state after that X(dt) (f_final for the last step). Runs on the
+ *   per-column kernels (the cluster-resident and staged paths are Strang only). */
+#define VP_SCHEME_STRANG 0
+#define VP_SCHEME_MERGED 1
+int vp_plan_set_scheme(vp_plan* plan, int32_t scheme);
+int vp_plan_get_scheme(const vp_plan* plan, int32_t* scheme);
+
 /* --- diagnostics ------------------------------------------------------------------------ */
 
 /* Copies the last error message of the calling thread into buf (always NUL-terminated). */

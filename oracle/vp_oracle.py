@@ -266,6 +266,65 @@ def run_backward(g: Grid, dt, f_eq, f_iv, H, t_final, f_hist,
 # ---------------------------------------------------------------------------
 
 
+def run_forward_aggressive(g: Grid, dt, f_eq, f_iv, H, t_final):
+    """Merged-Strang forward, warp_vp_solver/solver.py:618-736: the trailing X(dt/2) of a step and
+    the leading X(dt/2) of the next are one X(dt) (``semilag_x_full_kernel``, kernels.py:535-556;
+    a full step is the half-step form with 2*dt). ``f_hist[t]`` is the state after the merged
+    X(dt) (``f_final`` for the last step). Returns ``(f_final, f_hist, E_hist, ee_hist)``."""
+    T = num_steps(t_final, dt)
+    f_eq = np.asarray(f_eq, np.float64)
+    H = np.asarray(H, np.float64)
+    f_hist = np.empty((T, g.nx, g.nv))
+    E_hist = np.empty((T, g.nx))
+    ee_hist = np.empty(T)
+    f_half = semilag_x(np.asarray(f_iv, np.float64), g, dt)
+    rho = compute_rho(f_eq, f_half, g.dv)
+    f_final = f_half
+    for t in range(T):
+        E = solve_poisson(rho, g.period_x)
+        ee = compute_ee(E, g.dx)
+        post_v = semilag_v(f_half, E + H, g, dt)
+        if t < T - 1:
+            f_half = semilag_x(post_v, g, 2.0 * dt)
+            rho = compute_rho(f_eq, f_half, g.dv)
+            f_hist[t] = f_half
+        else:
+            f_final = semilag_x(post_v, g, dt)
+            f_hist[t] = f_final
+        E_hist[t] = E + H
+        ee_hist[t] = ee
+    return f_final, f_hist, E_hist, ee_hist
+
+
+def run_backward_aggressive(g: Grid, dt, f_eq, f_iv, H, t_final, f_hist,
+                            g_f_final, g_f_hist, g_E_hist, g_ee_hist):
+    """Discrete adjoint of :func:`run_forward_aggressive`, warp_vp_solver/solver.py:1111-1338:
+    X(dt/2)^T for the last step, X(dt)^T for the merged inner steps, V^T, the E_total, ee,
+    Poisson and rho transposes, and X(dt/2)^T of the leading half step. Returns
+    ``(g_f_iv, g_H)``."""
+    T = num_steps(t_final, dt)
+    f_eq = np.asarray(f_eq, np.float64)
+    f_iv = np.asarray(f_iv, np.float64)
+    H = np.asarray(H, np.float64)
+    g_f = np.array(g_f_final, dtype=np.float64, copy=True) + np.asarray(g_f_hist[T - 1], np.float64)
+    g_H = np.zeros(g.nx)
+    g_f_half = None
+    for t in range(T - 1, -1, -1):
+        f_half = semilag_x(f_iv, g, dt) if t == 0 else np.asarray(f_hist[t - 1], np.float64)
+        rho = compute_rho(f_eq, f_half, g.dv)
+        E = solve_poisson(rho, g.period_x)
+        g_in = semilag_x_adjoint(g_f, g, dt if t == T - 1 else 2.0 * dt)
+        g_f_half, g_E_total = semilag_v_adjoint(g_in, f_half, E + H, g, dt)
+        g_E_total = g_E_total + np.asarray(g_E_hist[t], np.float64)
+        g_H = g_H + g_E_total
+        g_E_back = g_E_total + compute_ee_adjoint(float(g_ee_hist[t]), E, g.dx)
+        g_rho = solve_poisson_adjoint(g_E_back, g.period_x)
+        g_f_half = g_f_half + compute_rho_adjoint(g_rho, g.nv, g.dv)
+        if t > 0:
+            g_f = g_f_half + np.asarray(g_f_hist[t - 1], np.float64)
+    return semilag_x_adjoint(g_f_half, g, dt), g_H
+
+
 def x_shift_table(g: Grid, dt):
     """Per-column x half-step: integer offset m_j and weight t_j (float64)."""
     s = 0.5 * g.vs * dt / g.dx

@@ -19,7 +19,9 @@ matplotlib), and calls:
   (``warp_vp_solver/solver.py:742-932``),
 * the single-stage kernels of ``warp_vp_solver/kernels.py:109-322`` through
   ``wp.launch`` exactly as ``tests/test_kernels.py`` launches them,
-* ``warp_vp_solver/poisson.py:34-99``.
+* ``warp_vp_solver/poisson.py:34-99``,
+* ``WarpVlasovPoissonSolver(..., optimized=True, aggressive=True)`` forward and
+  ``_run_backward`` (``warp_vp_solver/solver.py:618-736, 1111-1338``).
 
 The outputs are written to ``tests/golden/golden_*.npz`` (float64). The cases
 mirror the reference's own test fixtures (``tests/conftest.py``,
@@ -158,6 +160,33 @@ def backward_cases(ref):
     H6 = 0.05 * np.random.default_rng(14).standard_normal(m6.nx)
     cases.append(("bwd_odd_24x40", m6, f_eq6, f06, H6, 0.1, 4 * 0.1, "random"))
     return cases
+
+
+def aggressive_cases(ref):
+    """The merged-Strang (aggressive) path, solver.py:618-736 and 1111-1338."""
+    mk = ref.mesh.make_mesh
+    m = mk(2.0 * np.pi, 6.0, 16, 32)
+    f_eq, f0 = maxwell(m)
+    m2 = mk(10.0 * np.pi, 6.0, 32, 32)
+    f_eq2, f02 = two_stream(m2, eps=1e-2)
+    f_eq3 = np.exp(-0.5 * m.V ** 2) * (1.0 + 0.2 * np.cos(m.X))
+    f03 = f_eq3 * (1.0 + 0.003 * np.sin(2.0 * m.X))
+    m5 = mk(10.0 * np.pi, 6.0, 24, 40)
+    f_eq5, f05 = two_stream(m5, eps=1e-2)
+    return [
+        ("agg_twostream_32x32", m2, f_eq2, f02, 0.02 * np.random.default_rng(31).standard_normal(m2.nx),
+         0.1, 8 * 0.1, "cpu_fused"),
+        ("agg_maxwell_H_16x32", m, f_eq, f0, 0.01 * np.random.default_rng(32).standard_normal(m.nx),
+         0.05, 6 * 0.05, "gpu_safe"),
+        ("agg_feq2d_16x32", m, f_eq3, f03, 0.02 * np.random.default_rng(33).standard_normal(m.nx),
+         0.05, 5 * 0.05, "cpu_fused"),
+        ("agg_bigshift_16x32", m, f_eq, f0, 2.0 * np.random.default_rng(34).standard_normal(m.nx),
+         0.9, 3 * 0.9, "cpu_fused"),
+        ("agg_odd_24x40", m5, f_eq5, f05, 0.05 * np.random.default_rng(35).standard_normal(m5.nx),
+         0.1, 4 * 0.1, "gpu_safe"),
+        ("agg_single_16x32", m, f_eq, f0, 0.01 * np.random.default_rng(36).standard_normal(m.nx),
+         0.05, 1 * 0.05, "cpu_fused"),
+    ]
 
 
 def cotangents(kind, outs, nx, nv, T, dt, seed):
@@ -312,6 +341,23 @@ def main():
     kern = kernel_case(ref)
     np.savez_compressed(os.path.join(args.out, "golden_kernels.npz"), **kern)
     print(f"kernels ({time.time() - t0:.1f}s)")
+
+    agg = {}
+    for i, (name, m, f_eq, f_iv, H, dt, t_final, layout) in enumerate(aggressive_cases(ref)):
+        s = Solver(mesh=m, dt=dt, f_eq=f_eq, optimized=True, aggressive=True, aggressive_layout=layout)
+        outs = s.run_forward(f_iv, H, t_final)
+        T = s.num_steps(t_final)
+        g_ff, g_fh, g_Eh, g_ee = cotangents("random", outs, m.nx, m.nv, T, dt, 200 + i)
+        g_f_iv, g_H = s._run_backward(f_iv, H, t_final, outs[1], g_ff, g_fh, g_Eh, g_ee)
+        d = dict(f_eq=f_eq, f_iv=f_iv, H=H, dt=dt, t_final=t_final, n_steps=T,
+                 f_final=outs[0], f_hist=outs[1], E_hist=outs[2], ee_hist=outs[3],
+                 g_f_final=g_ff, g_f_hist=g_fh, g_E_hist=g_Eh, g_ee_hist=g_ee,
+                 g_f_iv=g_f_iv, g_H=g_H, layout=layout,
+                 **{"mesh_" + k: v for k, v in mesh_dict(m).items()})
+        for k, v in d.items():
+            agg[f"{name}/{k}"] = np.asarray(v)
+        print(f"{name}: T={T} ({time.time() - t0:.1f}s)")
+    np.savez_compressed(os.path.join(args.out, "golden_aggressive.npz"), **agg)
 
 
 if __name__ == "__main__":

@@ -69,10 +69,11 @@ def test_legacy_rejects_record_history_false(small_mesh):
         s.run_forward(np.zeros((16, 32)), np.zeros(16), 5 * 0.001, record_history=False)
 
 
-def test_aggressive_not_built(small_mesh):
-    s = WarpVlasovPoissonSolver(small_mesh, 0.001, np.zeros((16, 32)), aggressive=True)
-    with pytest.raises(NotImplementedError):
-        s.run_forward(np.zeros((16, 32)), np.zeros(16), 0.005)
+@pytest.mark.parametrize("layout", ["cpu_fused", "gpu_safe", "tiled"])
+def test_aggressive_layouts_are_accepted(small_mesh, layout):
+    s = WarpVlasovPoissonSolver(small_mesh, 0.001, np.zeros((16, 32)), aggressive=True,
+                                aggressive_layout=layout)
+    assert s.aggressive and s.aggressive_layout == layout
 
 
 def test_num_steps_matches_python_int():

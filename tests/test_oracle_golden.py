@@ -119,3 +119,25 @@ def test_c_oracle_backward_matches_reference(case):
                            case["g_f_final"], case["g_f_hist"], case["g_E_hist"], case["g_ee_hist"])
     assert O.rel_err(g_f, case["g_f_iv"]) < 1e-13
     assert O.rel_err(g_H, case["g_H"]) < 1e-13
+
+
+
+def _aggressive_cases():
+    from conftest import load_golden
+    return load_golden("aggressive")
+
+
+@pytest.mark.parametrize("case", _aggressive_cases(), ids=lambda c: c.name)
+def test_literal_aggressive_forward_and_backward_bit_exact(case):
+    """The merged-Strang (aggressive) loops of the reference, solver.py:618-736 and 1111-1338,
+    recorded for the cpu_fused and gpu_safe layouts."""
+    g = case.grid
+    dt, t_final = float(case["dt"]), float(case["t_final"])
+    out = O.run_forward_aggressive(g, dt, case["f_eq"], case["f_iv"], case["H"], t_final)
+    for arr, name in zip(out, FIELDS):
+        np.testing.assert_array_equal(arr, case[name], err_msg=f"{case.name}:{name}")
+    g_f, g_H = O.run_backward_aggressive(g, dt, case["f_eq"], case["f_iv"], case["H"], t_final,
+                                         out[1], case["g_f_final"], case["g_f_hist"],
+                                         case["g_E_hist"], case["g_ee_hist"])
+    np.testing.assert_array_equal(g_f, case["g_f_iv"])
+    np.testing.assert_array_equal(g_H, case["g_H"])

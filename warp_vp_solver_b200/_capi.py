@@ -19,6 +19,8 @@ VP_ERR_TIMEOUT = 3
 VP_ERR_UNSUPPORTED = 4
 VP_F32 = 0
 VP_F64 = 1
+VP_SCHEME_STRANG = 0
+VP_SCHEME_MERGED = 1
 ABI_VERSION = 2   # VP_ABI_VERSION of the header these bindings follow
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libvpb200.so")
@@ -89,6 +91,8 @@ SIGNATURES = {
                                ctypes.POINTER(c_vp)]),
     "vp_plan_destroy": (c_int, [c_vp]),
     "vp_plan_get_config": (c_int, [c_vp, ctypes.POINTER(LaunchConfig)]),
+    "vp_plan_set_scheme": (c_int, [c_vp, c_i32]),
+    "vp_plan_get_scheme": (c_int, [c_vp, ctypes.POINTER(c_i32)]),
     "vp_plan_set_config": (c_int, [c_vp, ctypes.POINTER(LaunchConfig)]),
     "vp_num_steps": (c_int, [c_vp, c_dbl, ctypes.POINTER(c_i32)]),
     "vp_workspace_bytes": (c_int, [c_vp, c_i32, c_i32, ctypes.POINTER(c_size)]),

@@ -73,6 +73,10 @@ struct vp_plan {
     double* d_vs = nullptr;    // nv
     int* d_mx = nullptr;       // nv
     void* d_tx = nullptr;      // nv reals
+    int* d_mxf = nullptr;      // merged scheme: full-step x offsets (mod nx)      [nv]
+    void* d_txf = nullptr;     // merged scheme: full-step x weights               [nv]
+    double* d_txf64 = nullptr; // merged scheme: full-step x weights in float64    [nv]
+    int merged = 0;            // 1: merged-Strang (aggressive) scheme
     void* d_vtab = nullptr;    // staged step: [2][2*kStageHalo][nv] reals (x-invariant f_eq only)
     LaunchCfg scfg{};          // staged forward step (R rows x threads columns per CTA)
     int stage_span = 0;        // rows its staging buffer holds (0: staged step not used)
@@ -376,7 +380,7 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
     T* E_all = tape ? reinterpret_cast<T*>(tape + TL.E) : nullptr;
     VShift<T>* vsh_all = tape ? reinterpret_cast<VShift<T>*>(tape + TL.vsh) : nullptr;
 
-    if (p->res_cn > 0 && (tape == nullptr || K == 1)) {
+    if (p->res_cn > 0 && !p->merged && (tape == nullptr || K == 1)) {
         ResFwdArgs<T> r{};
         r.nx = nx;
         r.nv = nv;
@@ -460,7 +464,15 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
         a.vsh_out = vsh_all ? vsh_all + (size_t)(n + 1) * nx : vsh_ws;
         a.E_hist_out = (E_hist && !last) ? E_hist + (size_t)(n + 1) * nx : nullptr;
         a.ee_out = (ee_hist && !last) ? ee_hist + (n + 1) : nullptr;
-        if (p->stage_span > 0) {
+        if (p->merged && !last) {
+            // merged-Strang inner step: one X(dt) with the full-step tables
+            FwdArgs<T> am = a;
+            am.mx = p->d_mxf;
+            am.tx = static_cast<const T*>(p->d_txf);
+            am.tx64 = p->d_txf64;
+            am.f_hist_n = f_hist ? f_hist + (size_t)n * nxnv : nullptr;
+            VP_CUDA(launch_fwd<T>(am, p->cfg, 3, p->feq2d != 0, s), "forward merged step launch");
+        } else if (p->stage_span > 0 && !p->merged) {
             a.n_chunks = p->scfg.n_chunks;
             a.chunk_cols = p->scfg.chunk_cols;
             VP_CUDA(launch_fwd_staged<T>(a, p->scfg, s), "forward step launch");
@@ -494,7 +506,7 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
     const T* E_all = reinterpret_cast<const T*>(tape + TL.E);
     const VShift<T>* vsh_all = reinterpret_cast<const VShift<T>*>(tape + TL.vsh);
 
-    if (p->res_cn > 0 && K == 1) {
+    if (p->res_cn > 0 && !p->merged && K == 1) {
         ResBwdArgs<T> r{};
         r.nx = nx;
         r.nv = nv;
@@ -563,10 +575,17 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
             fa.h_in = h_ptr(n);
             fa.h_out = h_mut(n + 1);
             fa.vsh = vsh_all + (size_t)n * nx;
-            if (p->stage_span > 0)
+            if (p->merged) {
+                FwdArgs<T> am = fa;
+                am.mx = p->d_mxf;
+                am.tx = static_cast<const T*>(p->d_txf);
+                am.tx64 = p->d_txf64;
+                VP_CUDA(launch_fwd<T>(am, p->cfg, 3, p->feq2d != 0, s), "recompute launch");
+            } else if (p->stage_span > 0) {
                 VP_CUDA(launch_fwd_staged<T>(fa, p->scfg, s), "recompute launch");
-            else
+            } else {
                 VP_CUDA(launch_fwd<T>(fa, p->cfg, 1, p->feq2d != 0, s), "recompute launch");
+            }
         }
         return VP_OK;
     };
@@ -619,7 +638,12 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
         b.E_prev = E_all + (size_t)(n - 1) * nx;
         b.gE_hist = g_Eh ? g_Eh + (size_t)(n - 1) * nx : nullptr;
         b.gee = g_ee ? g_ee + (n - 1) : nullptr;
-        if (p->stage_span > 0 && p->sb_smem > 0) {
+        if (p->merged) {
+            BwdArgs<T> bm = b;
+            bm.mx = p->d_mxf;
+            bm.tx = static_cast<const T*>(p->d_txf);
+            VP_CUDA(launch_bwd<T>(bm, p->cfg, 3, p->feq2d != 0, s), "backward merged step launch");
+        } else if (p->stage_span > 0 && p->sb_smem > 0) {
             LaunchCfg bc = p->scfg;
             bc.smem = p->sb_smem;
             b.n_chunks = bc.n_chunks;
@@ -652,6 +676,9 @@ static void free_plan(vp_plan* p) {
     cudaFree(p->d_mx);
     cudaFree(p->d_tx);
     cudaFree(p->d_tx64);
+    cudaFree(p->d_mxf);
+    cudaFree(p->d_txf);
+    cudaFree(p->d_txf64);
     cudaFree(p->d_vtab);
     cudaFree(p->d_tw);
     cudaFree(p->d_mult);
@@ -754,6 +781,17 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
         if (mi < 0) mi += nx;
         mx[j] = (int)mi;
     }
+    // full step of the merged-Strang scheme: s_j = v_j*dt/dx (semilag_x_full_kernel, kernels.py:535-556)
+    std::vector<int> mxf(nv);
+    std::vector<double> txf(nv);
+    for (int j = 0; j < nv; ++j) {
+        const double sj = mesh->vs[j] * dt / mesh->dx;
+        const double mf = std::floor(-sj);
+        txf[j] = -sj - mf;
+        long long mi = (long long)mf % nx;
+        if (mi < 0) mi += nx;
+        mxf[j] = (int)mi;
+    }
 
     // Poisson: multiplier of fft_inv_multiplier (poisson.py:34-45): m_k = -1/(i*2*pi*f_k) = i/(2*pi*f_k)
     p->pow2 = (nx & (nx - 1)) == 0;
@@ -828,7 +866,9 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
     if ((rc = upload_bytes((void**)&p->d_feq, f_eq_host, feq_count * sizeof(double))) ||
         (rc = upload_bytes((void**)&p->d_vs, vs.data(), nv * sizeof(double))) ||
         (rc = upload_bytes((void**)&p->d_mx, mx.data(), nv * sizeof(int))) ||
-        (rc = upload_bytes((void**)&p->d_tx64, tx.data(), nv * sizeof(double)))) {
+        (rc = upload_bytes((void**)&p->d_tx64, tx.data(), nv * sizeof(double))) ||
+        (rc = upload_bytes((void**)&p->d_mxf, mxf.data(), nv * sizeof(int))) ||
+        (rc = upload_bytes((void**)&p->d_txf64, txf.data(), nv * sizeof(double)))) {
         free_plan(p);
         return rc;
     }
@@ -851,12 +891,14 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
     if (dtype == VP_F64) {
         if (stage_tables) rc = upload<double>(&p->d_vtab, vtab);
         if (!rc) rc = upload<double>(&p->d_tx, tx);
+        if (!rc) rc = upload<double>(&p->d_txf, txf);
         if (!rc) rc = upload<double>(&p->d_tw, tw);
         if (!rc) rc = upload<double>(&p->d_mult, mult_im);
         if (!rc) rc = upload<double>(&p->d_circ, circ);
     } else {
         if (stage_tables) rc = upload<float>(&p->d_vtab, vtab);
         if (!rc) rc = upload<float>(&p->d_tx, tx);
+        if (!rc) rc = upload<float>(&p->d_txf, txf);
         if (!rc) rc = upload<float>(&p->d_tw, tw);
         if (!rc) rc = upload<float>(&p->d_mult, mult_im);
         if (!rc) rc = upload<float>(&p->d_circ, circ);
@@ -937,6 +979,20 @@ int vp_plan_set_config(vp_plan* plan, const vp_launch_config* cfg) {
     c.n_chunks = (plan->nv + cols - 1) / cols;
     plan->cfg = c;
     plan->cfg.smem = fused_smem(plan, R);
+    return VP_OK;
+}
+
+int vp_plan_set_scheme(vp_plan* plan, int32_t scheme) {
+    if (!plan) return set_err(VP_ERR_ARG, "plan must not be NULL");
+    if (scheme != VP_SCHEME_STRANG && scheme != VP_SCHEME_MERGED)
+        return set_err(VP_ERR_ARG, "scheme must be VP_SCHEME_STRANG (0) or VP_SCHEME_MERGED (1), got %d", scheme);
+    plan->merged = scheme == VP_SCHEME_MERGED ? 1 : 0;
+    return VP_OK;
+}
+
+int vp_plan_get_scheme(const vp_plan* plan, int32_t* scheme) {
+    if (!plan || !scheme) return set_err(VP_ERR_ARG, "plan and scheme must not be NULL");
+    *scheme = plan->merged ? VP_SCHEME_MERGED : VP_SCHEME_STRANG;
     return VP_OK;
 }
 

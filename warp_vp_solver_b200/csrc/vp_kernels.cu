@@ -173,6 +173,8 @@ __device__ void bwd_tail(const BwdArgs<T>& a, PoissonArea<T> w) {
 // Forward
 // PHASE 0 (prologue): h_0 = X(f_iv - f_eq) + Xcorr, rho_0, tail -> E_0.
 // PHASE 1 (step n):   h_n -> o -> d (= f_{n+1} - f_eq) -> [h_{n+1}, rho_{n+1}, tail -> E_{n+1}]
+// PHASE 3 (merged-Strang inner step, warp_vp_solver/solver.py:618-736): h_n -> o -> h_{n+1} =
+//                     X(dt)(o) with the full-step x tables, f_hist[n] = f_eq + h_{n+1}, rho_{n+1}.
 //                     The bracket is skipped when h_out == null (last step). With part == null
 //                     the launch only propagates the state (segment recomputation in the adjoint).
 // ----------------------------------------------------------------------------------------------
@@ -188,6 +190,28 @@ __device__ __forceinline__ void fwd_tile(const FwdArgs<T>& a, int r0, int c_begi
         const T t = __ldg(a.tx + j);
         const double t64 = FEQ2D ? __ldg(a.tx64 + j) : 0.0;
         const T wj = trap_w<T>(j, nv);
+        if (PHASE == 3) {
+            // merged inner step (full-step x tables in mx/tx): h' rows r0 + e from o rows r0 + m + k
+            const int base = wrap1(r0 + m, nx);
+            T o[R + 1];
+#pragma unroll
+            for (int k = 0; k < R + 1; ++k) {
+                const int row = wrap1(base + k, nx);
+                o[k] = v_cell<T, FEQ2D>(a.h_in, a.feq, a.feq_rs, nv, row, j, a.vsh[row]);
+            }
+#pragma unroll
+            for (int e = 0; e < R; ++e) {
+                T hv = lerp(o[e], o[e + 1], t);
+                if (FEQ2D) hv += x_corr<T, FEQ2D>(a.feq, a.feq_rs, nx, r0 + e, m, t64, j);
+                if (a.f_hist_n != nullptr)
+                    a.f_hist_n[(size_t)(r0 + e) * nv + j] = (T)(feq_at<T, FEQ2D>(a.feq, a.feq_rs, r0 + e, j) + (double)hv);
+                if (next) {
+                    a.h_out[(size_t)(r0 + e) * nv + j] = hv;
+                    acc[e] += wj * hv;
+                }
+            }
+            continue;
+        }
         T d[R + 1];
         if (PHASE == 0) {
             const int base = wrap1(r0 + m, nx);
@@ -267,6 +291,8 @@ __global__ void __launch_bounds__(256) vp_fwd_kernel(const FwdArgs<T> a) {
 // PHASE 0 (n = T):   c = g_f_final + g_f_hist[T-1]; w_{T-1} = X^T c; row sums for g_E_total.
 // PHASE 1 (n >= 1):  gh = V^T w_n + rho^T grho_n; c = X^T gh (+ g_f_hist[n-1]); w_{n-1} = X^T c.
 // PHASE 2 (n = 0):   g_f_iv = X^T (V^T w_0 + rho^T grho_0).
+// PHASE 3 (merged inner step, solver.py:1111-1338): c = V^T w_n + rho^T grho_n + g_f_hist[n-1];
+//                    w_{n-1} = X(dt)^T c with the full-step x tables.
 // Tail (phases 0, 1), for step n-1: g_E_total = -dt/dv * sum_j slope*w + g_E_hist; g_H += g_E_total;
 // g_E = g_E_total + ee^T; grho_{n-1} = Poisson^T g_E.
 // ----------------------------------------------------------------------------------------------
@@ -312,6 +338,19 @@ __device__ __forceinline__ void bwd_tile(const BwdArgs<T>& a, int r0, int c_begi
                 if (a.c_src != nullptr) v += __ldg(a.c_src + (size_t)row * nv + j);
                 if (a.c_src2 != nullptr) v += __ldg(a.c_src2 + (size_t)row * nv + j);
                 c[k] = v;
+            }
+        } else if (PHASE == 3) {
+            // merged inner step (full-step x tables): c = V^T w + rho^T grho (+ g_f_hist) on the
+            // rows of the single X^T window
+#pragma unroll
+            for (int k = 0; k < R + 1; ++k) {
+                const int row = wrap1(cbase + k, nx);
+                const VShift<T> vs = a.vsh_n[row];
+                int c0 = wrapneg(j - vs.m, nv);
+                int c1 = wrapneg(c0 - 1, nv);
+                const T* wrow = a.w_in + (size_t)row * nv;
+                c[k] = lerp(__ldg(wrow + c0), __ldg(wrow + c1), vs.t) + wr * __ldg(a.grho + row);
+                if (a.gfh != nullptr) c[k] += __ldg(a.gfh + (size_t)row * nv + j);
             }
         } else {
             // gh rows r0 - 2m - 2 + k, k in [0, R+2)
@@ -851,6 +890,8 @@ static cudaError_t fwd_dispatch_phase(const FwdArgs<T>& a, const LaunchCfg& c, i
     dim3 grid(a.nx / R, c.n_chunks);
     if (phase == 0)
         vp_fwd_kernel<T, R, F2, 0><<<grid, c.threads, c.smem, s>>>(a);
+    else if (phase == 3)
+        vp_fwd_kernel<T, R, F2, 3><<<grid, c.threads, c.smem, s>>>(a);
     else
         vp_fwd_kernel<T, R, F2, 1><<<grid, c.threads, c.smem, s>>>(a);
     count_launch();
@@ -865,6 +906,8 @@ static cudaError_t bwd_dispatch_phase(const BwdArgs<T>& a, const LaunchCfg& c, i
         vp_bwd_kernel<T, R, F2, 0><<<grid, c.threads, c.smem, s>>>(a);
     else if (phase == 1)
         vp_bwd_kernel<T, R, F2, 1><<<grid, c.threads, c.smem, s>>>(a);
+    else if (phase == 3)
+        vp_bwd_kernel<T, R, F2, 3><<<grid, c.threads, c.smem, s>>>(a);
     else
         vp_bwd_kernel<T, R, F2, 2><<<grid, c.threads, c.smem, s>>>(a);
     count_launch();

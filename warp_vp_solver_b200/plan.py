@@ -97,6 +97,18 @@ class Plan:
         _capi.check(self.lib.vp_plan_set_config(self._h, ctypes.byref(c)))
         self._ws = {}   # workspace size depends on n_chunks
 
+    def set_scheme(self, merged: bool) -> None:
+        """Strang splitting (False) or the merged-Strang scheme of the reference's aggressive
+        path (True)."""
+        _capi.check(self.lib.vp_plan_set_scheme(
+            self._h, _capi.VP_SCHEME_MERGED if merged else _capi.VP_SCHEME_STRANG))
+
+    @property
+    def merged(self) -> bool:
+        out = ctypes.c_int32()
+        _capi.check(self.lib.vp_plan_get_scheme(self._h, ctypes.byref(out)))
+        return out.value == _capi.VP_SCHEME_MERGED
+
     def num_steps(self, t_final: float) -> int:
         out = ctypes.c_int32()
         _capi.check(self.lib.vp_num_steps(self._h, float(t_final), ctypes.byref(out)))
