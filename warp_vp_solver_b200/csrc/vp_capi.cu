@@ -1346,6 +1346,7 @@ static void batch_fill(const vp_batch* b, std::vector<BatchInst<T>>& out, const 
         I.tx64 = p->d_tx64;
         I.feq = p->d_feq;
         I.feq_rs = p->feq2d ? p->nv : 0;
+        I.vtab = static_cast<const T*>(p->d_vtab);
         I.P = poisson_tables<T>(p, nullptr, nullptr, true);
         I.dv = (T)p->dv;
         I.dx = (T)p->dx;

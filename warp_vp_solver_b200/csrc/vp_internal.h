@@ -108,6 +108,7 @@ template <typename T> struct BatchInst {
     const int* mx;
     const T* tx;
     const double* tx64;
+    const T* vtab;              // per-shift f_eq correction tables (A, B pairs), or null
     const double* feq;
     int feq_rs;
     PoissonTables<T> P;

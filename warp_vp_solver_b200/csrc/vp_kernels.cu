@@ -63,6 +63,19 @@ __device__ __forceinline__ T v_cell(const T* __restrict__ h, const double* __res
     return o;
 }
 
+// f_eq[d0 + 1] - f_eq[d0] with d0 = j + m (the adjoint's slope term): B_m[j] from the tables, or
+// the float64 difference.
+template <typename T, bool FEQ2D>
+__device__ __forceinline__ T feq_slope(const double* __restrict__ feq, int feq_rs, const T* __restrict__ vtab,
+                                       int nv, int row, int j, int m, int d0, int d1) {
+    if (!FEQ2D && vtab != nullptr) {
+        const int ms = m >= nv / 2 ? m - nv : m;
+        if (ms >= -kStageHalo && ms < kStageHalo)
+            return __ldg(vtab + (size_t)(3 * kStageHalo + ms) * nv + j);   // B_m row
+    }
+    return (T)(feq_at<T, FEQ2D>(feq, feq_rs, row, d1) - feq_at<T, FEQ2D>(feq, feq_rs, row, d0));
+}
+
 // X(f_eq) - f_eq at (row, j) for an x-dependent f_eq (zero otherwise).
 template <typename T, bool FEQ2D>
 __device__ __forceinline__ T x_corr(const double* __restrict__ feq, int feq_rs, int nx, int row,
@@ -384,8 +397,7 @@ __device__ __forceinline__ void bwd_tile(const BwdArgs<T>& a, int r0, int c_begi
             d1 = d1 == nv ? 0 : d1;
             const T* hr = a.h_prev + (size_t)row * nv;
             const T sl = (__ldg(hr + d1) - __ldg(hr + d0)) +
-                         (T)(feq_at<T, FEQ2D>(a.feq, a.feq_rs, row, d1) -
-                             feq_at<T, FEQ2D>(a.feq, a.feq_rs, row, d0));
+                         feq_slope<T, FEQ2D>(a.feq, a.feq_rs, a.vtab, nv, row, j, vp.m, d0, d1);
             acc[e] += sl * wv;
         }
     }
@@ -1009,6 +1021,7 @@ __device__ __forceinline__ FwdArgs<T> batch_fwd_args(const BatchStep<T>& b, cons
     a.tx64 = I.tx64;
     a.feq = I.feq;
     a.feq_rs = I.feq_rs;
+    a.vtab = I.vtab;
     a.P = I.P;
     a.dv = I.dv;
     a.dx = I.dx;
@@ -1041,6 +1054,7 @@ __device__ __forceinline__ BwdArgs<T> batch_bwd_args(const BatchStep<T>& b, cons
     a.tx = I.tx;
     a.feq = I.feq;
     a.feq_rs = I.feq_rs;
+    a.vtab = I.vtab;
     a.P = I.P;
     a.dv = I.dv;
     a.dx = I.dx;
