@@ -243,6 +243,13 @@ int vp_gemm_bf16(const void* A, int64_t lda, const void* B, int64_t ldb, int32_t
 
 /* --- single-stage operators (the reference's helper methods and unit-tested kernels) ------ */
 
+/* KL(f || f_eq) integrated over phase space (warp_vp_solver/utils.py:53-76, the cost of
+ * make_cost_function_kl, utils.py:79-92) and its gradient with respect to f, in float64 on the
+ * device: value (one double) and grad (nx*nv doubles, may be NULL) are device pointers; f is the
+ * float64 final state. The first call on a plan allocates an 8 KiB scratch (do it before any
+ * stream capture). */
+int vp_kl_divergence(vp_plan* plan, const double* f, double eps, double* value, double* grad, void* stream);
+
 /* rho[i] = dv * trapz_j(f_eq[i,j] - f[i,j]). Replaces compute_rho (warp_vp_solver/solver.py:
  * 393-397) and compute_rho_kernel (warp_vp_solver/kernels.py:156-172). f: double[nx*nv],
  * rho: real[nx]. */

@@ -128,6 +128,7 @@ SIGNATURES = {
     "vp_mlp_status": (c_int, [c_vp, ctypes.POINTER(ctypes.c_uint32)]),
     "vp_gemm_bf16": (c_int, [c_vp, c_i64, c_vp, c_i64, c_i32, c_i32, c_i32, c_vp, c_i32, c_vp, c_i64,
                              c_vp, c_i64, c_vp, c_i64, c_vp, c_i64, c_vp, c_vp]),
+    "vp_kl_divergence": (c_int, [c_vp, c_vp, c_dbl, c_vp, c_vp, c_vp]),
     "vp_compute_rho": (c_int, [c_vp, c_vp, c_vp, c_vp]),
     "vp_poisson": (c_int, [c_vp, c_vp, c_vp, c_int, c_vp]),
     "vp_electric_energy": (c_int, [c_vp, c_vp, c_vp, c_vp]),

@@ -77,6 +77,8 @@ struct vp_plan {
     void* d_txf = nullptr;     // merged scheme: full-step x weights               [nv]
     double* d_txf64 = nullptr; // merged scheme: full-step x weights in float64    [nv]
     int merged = 0;            // 1: merged-Strang (aggressive) scheme
+    double feq_integral = 0.0; // trapezoid integral of f_eq over xs and vs (for the KL cost)
+    double* d_kl = nullptr;    // KL cost scratch: 2 * kKlBlocks + 2 doubles
     void* d_vtab = nullptr;    // staged step: [2][2*kStageHalo][nv] reals (x-invariant f_eq only)
     LaunchCfg scfg{};          // staged forward step (R rows x threads columns per CTA)
     int stage_span = 0;        // rows its staging buffer holds (0: staged step not used)
@@ -677,6 +679,7 @@ static void free_plan(vp_plan* p) {
     cudaFree(p->d_tx);
     cudaFree(p->d_tx64);
     cudaFree(p->d_mxf);
+    cudaFree(p->d_kl);
     cudaFree(p->d_txf);
     cudaFree(p->d_txf64);
     cudaFree(p->d_vtab);
@@ -908,6 +911,19 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
         return rc;
     }
     choose_staged(p, n_sms);
+    {   // trapezoid integral of f_eq (kl_divergence's norm_eq without eps, utils.py:59-64)
+        double tot = 0.0;
+        for (int i = 0; i < nx; ++i) {
+            const double wx = (i == 0 || i == nx - 1) ? 0.5 * mesh->dx : mesh->dx;
+            double row = 0.0;
+            for (int j = 0; j < nv; ++j) {
+                const double wv = (j == 0 || j == nv - 1) ? 0.5 * mesh->dv : mesh->dv;
+                row += wv * f_eq_host[(size_t)i * nv + j];
+            }
+            tot += wx * row;
+        }
+        p->feq_integral = tot;
+    }
     *out_plan = p;
     return VP_OK;
 }
@@ -1230,6 +1246,26 @@ int vp_electric_energy(vp_plan* plan, const void* E, void* ee, void* stream) {
                         ? launch_electric_energy<double>(plan->nx, plan->dx, (const double*)E, (double*)ee, s)
                         : launch_electric_energy<float>(plan->nx, plan->dx, (const float*)E, (float*)ee, s);
     return e == cudaSuccess ? VP_OK : cuda_err(e, "electric energy launch");
+}
+
+int vp_kl_divergence(vp_plan* plan, const double* f, double eps, double* value, double* grad, void* stream) {
+    if (!plan) return set_err(VP_ERR_ARG, "plan must not be NULL");
+    if (!std::isfinite(eps) || eps < 0.0) return set_err(VP_ERR_ARG, "eps must be finite and >= 0");
+    int rc;
+    if ((rc = check_dev_ptr(f, "f", plan->device)) || (rc = check_dev_ptr(value, "value", plan->device)) ||
+        (rc = check_opt_ptr(grad, "grad", plan->device)))
+        return rc;
+    if (plan->d_kl == nullptr) {
+        if (stream_capturing(static_cast<cudaStream_t>(stream)))
+            return set_err(VP_ERR_ARG, "the first vp_kl_divergence call on a plan must not be captured "
+                                       "(it allocates the plan's scratch)");
+        VP_CUDA(cudaMalloc(&plan->d_kl, (2 * kKlBlocks + 2) * sizeof(double)), "cudaMalloc(kl scratch)");
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const cudaError_t e = launch_kl_divergence(plan->nx, plan->nv, f, plan->d_feq, plan->feq2d ? plan->nv : 0,
+                                               plan->dx, plan->dv, eps, plan->feq_integral + eps, plan->d_kl,
+                                               value, grad, s);
+    return e == cudaSuccess ? VP_OK : cuda_err(e, "kl divergence launch");
 }
 
 int vp_semilag_x(vp_plan* plan, const void* in, void* out, double dt, int adjoint, void* stream) {

@@ -206,6 +206,11 @@ template <typename T>
 cudaError_t set_tail_smem_limit(size_t bytes);
 template <typename T>
 cudaError_t set_poisson_smem_limit(size_t bytes);
+// KL(f || f_eq) cost and gradient (float64); scratch holds 2 * kKlBlocks + 2 doubles.
+constexpr int kKlBlocks = 512;
+cudaError_t launch_kl_divergence(int nx, int nv, const double* f, const double* feq, int feq_rs, double dx,
+                                 double dv, double eps, double zeq, double* scratch, double* value, double* grad,
+                                 cudaStream_t s);
 
 // Bytes of the Poisson work area (nx complex values plus nx/2+1 complex twiddles).
 inline size_t poisson_area_size(int nx, size_t real_size) {

@@ -5,6 +5,8 @@
 
 #include "vp_device.cuh"
 
+#include <algorithm>
+
 namespace vpb {
 
 // rho[i] = dv * trapz_j(f_eq[i,j] - f[i,j]), accumulated in float64 (one CTA per row).
@@ -151,6 +153,124 @@ cudaError_t launch_semilag_v(int nx, int nv, double dv, double dt, const T* in,
                              cudaStream_t s) {
     semilag_v_kernel<T><<<nx, 256, 0, s>>>(nv, (T)(dt / dv), in, E_total, out, adjoint, f_in, g_E);
     count_launch();
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------
+// KL(f || f_eq) cost, warp_vp_solver/utils.py:53-76, and its gradient with respect to f, in float64:
+//   W_ij = wx_i wv_j (trapezoid weights over xs and vs), Z = sum W f + eps,
+//   Z_eq = sum W f_eq + eps (host), p = f / Z, q = f_eq / Z_eq + eps,
+//   KL = sum W rel_entr(p, q)   (rel_entr: p log(p/q) for p, q > 0; 0 for p = 0, q >= 0; +inf else)
+//   dKL/df_ij = (W_ij / Z) (r_ij - S),  r = log(p/q) + 1 where p, q > 0 (0 elsewhere),
+//   S = sum W r p.
+// Each reduction writes one partial per block and a one-block kernel sums them in block order, so
+// the result is deterministic.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ double kl_w(int i, int n, double d) { return (i == 0 || i == n - 1) ? 0.5 * d : d; }
+
+__device__ __forceinline__ double block_sum_d(double v, double* red) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    __syncthreads();
+    return s;
+}
+
+// MODE 0: partial[b] = sum W f. MODE 1: partial[b] = sum W rel_entr(p, q), partial[B + b] = sum W r p.
+template <int MODE>
+__global__ void __launch_bounds__(256) kl_partial_kernel(int nx, int nv, const double* __restrict__ f,
+                                                         const double* __restrict__ feq, int feq_rs, double dx,
+                                                         double dv, double eps, double zeq,
+                                                         const double* __restrict__ zf, double* partial) {
+    __shared__ double red[8];
+    const long long n = (long long)nx * nv;
+    const double Z = MODE == 1 ? *zf : 1.0;
+    double a = 0.0, b = 0.0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(k / nv), j = (int)(k - (long long)i * nv);
+        const double W = kl_w(i, nx, dx) * kl_w(j, nv, dv);
+        const double fv = f[k];
+        if (MODE == 0) {
+            a += W * fv;
+        } else {
+            const double p = fv / Z;
+            const double q = feq[(size_t)i * feq_rs + j] / zeq + eps;
+            double re;
+            if (p > 0.0 && q > 0.0) {
+                const double l = log(p / q);
+                re = p * l;
+                b += W * (l + 1.0) * p;
+            } else if (p == 0.0 && q >= 0.0) {
+                re = 0.0;
+            } else {
+                re = INFINITY;
+            }
+            a += W * re;
+        }
+    }
+    const double sa = block_sum_d(a, red);
+    if (MODE == 1) {
+        const double sb = block_sum_d(b, red);
+        if (threadIdx.x == 0) partial[gridDim.x + blockIdx.x] = sb;
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = sa;
+}
+
+// out[0] = sum of partial[0..nb) + add0; with two outputs also out[1] = sum partial[nb..2nb).
+__global__ void kl_finish_kernel(const double* partial, int nb, int two, double add0, double* out0, double* out1) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double s = 0.0;
+        for (int b = 0; b < nb; ++b) s += partial[b];
+        *out0 = s + add0;
+        if (two) {
+            double t = 0.0;
+            for (int b = 0; b < nb; ++b) t += partial[nb + b];
+            *out1 = t;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) kl_grad_kernel(int nx, int nv, const double* __restrict__ f,
+                                                      const double* __restrict__ feq, int feq_rs, double dx,
+                                                      double dv, double eps, double zeq,
+                                                      const double* __restrict__ zs, double* grad) {
+    const double Z = zs[0], S = zs[1];
+    const long long n = (long long)nx * nv;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(k / nv), j = (int)(k - (long long)i * nv);
+        const double W = kl_w(i, nx, dx) * kl_w(j, nv, dv);
+        const double p = f[k] / Z;
+        const double q = feq[(size_t)i * feq_rs + j] / zeq + eps;
+        const double r = (p > 0.0 && q > 0.0) ? log(p / q) + 1.0 : 0.0;
+        grad[k] = (W / Z) * (r - S);
+    }
+}
+
+// scratch: [2 * kKlBlocks partials][Z, S]
+cudaError_t launch_kl_divergence(int nx, int nv, const double* f, const double* feq, int feq_rs, double dx,
+                                 double dv, double eps, double zeq, double* scratch, double* value, double* grad,
+                                 cudaStream_t s) {
+    const int nb = kKlBlocks;
+    double* partial = scratch;
+    double* zs = scratch + 2 * nb;
+    kl_partial_kernel<0><<<nb, 256, 0, s>>>(nx, nv, f, feq, feq_rs, dx, dv, eps, zeq, nullptr, partial);
+    count_launch();
+    kl_finish_kernel<<<1, 32, 0, s>>>(partial, nb, 0, eps, zs, nullptr);
+    count_launch();
+    kl_partial_kernel<1><<<nb, 256, 0, s>>>(nx, nv, f, feq, feq_rs, dx, dv, eps, zeq, zs, partial);
+    count_launch();
+    kl_finish_kernel<<<1, 32, 0, s>>>(partial, nb, 1, 0.0, value, zs + 1);
+    count_launch();
+    if (grad != nullptr) {
+        const long long n = (long long)nx * nv;
+        const int blocks = (int)std::min<long long>(4096, (n + 255) / 256);
+        kl_grad_kernel<<<blocks, 256, 0, s>>>(nx, nv, f, feq, feq_rs, dx, dv, eps, zeq, zs, grad);
+        count_launch();
+    }
     return cudaGetLastError();
 }
 

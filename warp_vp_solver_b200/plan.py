@@ -205,6 +205,16 @@ class Plan:
         return g_fiv, g_H
 
     # ---------------------------------------------------------------- single-stage operators
+    def kl_divergence(self, f, eps: float = 1e-12, want_grad: bool = True):
+        """KL(f || f_eq) over phase space and its gradient (float64 device tensors)."""
+        f = self.to_f64(f).reshape(self.nx, self.nv)
+        value = torch.empty(1, dtype=torch.float64, device=self.device)
+        grad = torch.empty_like(f) if want_grad else None
+        with torch.cuda.device(self.device):
+            _capi.check(self.lib.vp_kl_divergence(self._h, _capi.ptr(f), float(eps), _capi.ptr(value),
+                                                  _capi.ptr(grad), _stream_handle(self.device)))
+        return value[0], grad
+
     def compute_rho(self, f) -> torch.Tensor:
         f = self.to_f64(f).reshape(self.nx, self.nv)
         rho = torch.empty(self.nx, dtype=self.dtype, device=self.device)

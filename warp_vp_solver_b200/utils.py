@@ -47,8 +47,28 @@ def _rel_entr(x: torch.Tensor, y: torch.Tensor) -> torch.Tensor:
     return torch.where(bad, torch.full_like(x, float("inf")), val)
 
 
+class _KLFunction(torch.autograd.Function):
+    """KL(f || f_eq) and its gradient from the fused device kernels (vp_kl_divergence)."""
+
+    @staticmethod
+    def forward(ctx, f, plan, eps):
+        value, grad = plan.kl_divergence(f.detach(), eps, want_grad=f.requires_grad)
+        ctx.save_for_backward(grad if grad is not None else torch.empty(0, device=f.device))
+        ctx.f_dtype = f.dtype
+        return value.to(f.dtype)
+
+    @staticmethod
+    def backward(ctx, g):
+        (grad,) = ctx.saved_tensors
+        return (grad * g.to(grad.dtype)).to(ctx.f_dtype), None, None
+
+
 def kl_divergence(f_T, solver, eps: float = 1e-12) -> torch.Tensor:
-    """KL(f_T || f_eq) integrated over phase space (utils.py:53-76)."""
+    """KL(f_T || f_eq) integrated over phase space (utils.py:53-76). A CUDA tensor goes through
+    the fused device kernels of the solver's plan (value and gradient in one pass, float64);
+    other inputs are evaluated with the same expression in torch."""
+    if isinstance(f_T, torch.Tensor) and f_T.is_cuda and hasattr(solver, "plan"):
+        return _KLFunction.apply(f_T, solver.plan, float(eps))
     f_T = _as_tensor(f_T)
     xs = torch.as_tensor(solver.mesh.xs, dtype=f_T.dtype, device=f_T.device)
     vs = torch.as_tensor(solver.mesh.vs, dtype=f_T.dtype, device=f_T.device)
