@@ -127,6 +127,19 @@ int vp_backward(vp_plan* plan, const void* H, int32_t n_steps,
                 const void* g_ee_hist, void* g_f_iv, void* g_H,
                 void* workspace, size_t workspace_bytes, void* stream);
 
+/* vp_forward with f_hist streamed to pinned host memory while the loop runs (the reference
+ * copies f_hist to the host synchronously every step, warp_vp_solver/solver.py:519, 607):
+ * step n's f is written to device slot n % ring_slots of `ring` (ring_slots*nx*nv reals, 2..64
+ * slots) and copied from there to f_hist_host + n*nx*nv (pinned, n_steps*nx*nv reals) on
+ * copy_stream, overlapping the following steps; the compute stream waits for a slot's copy
+ * before reusing it and, at the end, for every copy, so the history is complete once `stream`
+ * is. Other arguments as vp_forward (checkpoint_every as given or 0 for automatic); the
+ * cluster-resident path is not used. */
+int vp_forward_stream_history(vp_plan* plan, const double* f_iv, const void* H, int32_t n_steps, double* f_final,
+                              void* f_hist_host, void* ring, int32_t ring_slots, void* E_hist, void* ee_hist,
+                              void* tape, int32_t checkpoint_every, void* workspace, size_t workspace_bytes,
+                              void* stream, void* copy_stream);
+
 /* Maximum scratch of vp_forward_noalloc: 8 MiB of device memory per GPU that loads the library. */
 #define VP_NOALLOC_SCRATCH_BYTES ((size_t)8 << 20)
 

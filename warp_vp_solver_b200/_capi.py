@@ -103,6 +103,8 @@ SIGNATURES = {
     "vp_backward": (c_int, [c_vp, c_vp, c_i32, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
                             c_vp, c_size, c_vp]),
     "vp_forward_noalloc": (c_int, [c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "vp_forward_stream_history": (c_int, [c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp,
+                                          c_vp, c_i32, c_vp, c_size, c_vp, c_vp]),
     "vp_batch_create": (c_int, [c_i32, ctypes.POINTER(MeshDesc), ctypes.POINTER(c_dbl),
                                 ctypes.POINTER(ctypes.POINTER(c_dbl)), c_int, ctypes.POINTER(c_vp)]),
     "vp_batch_destroy": (c_int, [c_vp]),

@@ -79,6 +79,7 @@ struct vp_plan {
     int merged = 0;            // 1: merged-Strang (aggressive) scheme
     double feq_integral = 0.0; // trapezoid integral of f_eq over xs and vs (for the KL cost)
     double* d_kl = nullptr;    // KL cost scratch: 2 * kKlBlocks + 2 doubles
+    std::vector<cudaEvent_t> ev_written, ev_copied;   // streamed-history slots
     void* d_vtab = nullptr;    // staged step: [2][2*kStageHalo][nv] reals (x-invariant f_eq only)
     LaunchCfg scfg{};          // staged forward step (R rows x threads columns per CTA)
     int stage_span = 0;        // rows its staging buffer holds (0: staged step not used)
@@ -364,10 +365,21 @@ static PoissonTables<T> poisson_tables(const vp_plan* p, unsigned char* ws, cons
 // ---------------------------------------------------------------------------------------------
 // forward orchestration
 // ---------------------------------------------------------------------------------------------
+// f_hist streamed to pinned host memory: step n's f goes to device slot n % slots of f_hist (the
+// ring) and is copied to host + n*nx*nv on `copy`; the compute stream waits for a slot's previous
+// copy before overwriting it, and at the end for every copy.
+struct HistRing {
+    unsigned char* host;
+    int slots;
+    cudaStream_t copy;
+    cudaEvent_t* written;
+    cudaEvent_t* copied;
+};
+
 template <typename T>
 static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps, double* f_final,
                         T* f_hist, T* E_hist, T* ee_hist, unsigned char* tape, int every,
-                        unsigned char* ws, cudaStream_t s) {
+                        unsigned char* ws, cudaStream_t s, const HistRing* ring = nullptr) {
     const int nx = p->nx, nv = p->nv;
     const size_t nxnv = (size_t)nx * nv;
     const WsLayout L = ws_layout(p, T_steps, every);
@@ -382,7 +394,7 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
     T* E_all = tape ? reinterpret_cast<T*>(tape + TL.E) : nullptr;
     VShift<T>* vsh_all = tape ? reinterpret_cast<VShift<T>*>(tape + TL.vsh) : nullptr;
 
-    if (p->res_cn > 0 && !p->merged && (tape == nullptr || K == 1)) {
+    if (p->res_cn > 0 && !p->merged && ring == nullptr && (tape == nullptr || K == 1)) {
         ResFwdArgs<T> r{};
         r.nx = nx;
         r.nv = nv;
@@ -459,7 +471,14 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
         a.h_in = h_slot(n);
         a.h_out = last ? nullptr : h_slot(n + 1);
         a.vsh = vsh_all ? vsh_all + (size_t)n * nx : vsh_ws;
-        a.f_hist_n = f_hist ? f_hist + (size_t)n * nxnv : nullptr;
+        int slot = 0;
+        if (ring != nullptr) {
+            slot = n % ring->slots;
+            if (n >= ring->slots) VP_CUDA(cudaStreamWaitEvent(s, ring->copied[slot], 0), "wait for history slot");
+            a.f_hist_n = f_hist + (size_t)slot * nxnv;
+        } else {
+            a.f_hist_n = f_hist ? f_hist + (size_t)n * nxnv : nullptr;
+        }
         a.f_final = last ? f_final : nullptr;
         a.part = last ? nullptr : part;
         a.E_out = E_all ? E_all + (size_t)(n + 1) * nx : E_ws;
@@ -472,7 +491,6 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
             am.mx = p->d_mxf;
             am.tx = static_cast<const T*>(p->d_txf);
             am.tx64 = p->d_txf64;
-            am.f_hist_n = f_hist ? f_hist + (size_t)n * nxnv : nullptr;
             VP_CUDA(launch_fwd<T>(am, p->cfg, 3, p->feq2d != 0, s), "forward merged step launch");
         } else if (p->stage_span > 0 && !p->merged) {
             a.n_chunks = p->scfg.n_chunks;
@@ -483,7 +501,18 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
         }
         if (!last && !p->tail_inline)
             VP_CUDA(launch_fwd_tail<T>(a, p->tail_threads, p->tail_smem, s), "forward tail launch");
+        if (ring != nullptr) {
+            VP_CUDA(cudaEventRecord(ring->written[slot], s), "record history slot");
+            VP_CUDA(cudaStreamWaitEvent(ring->copy, ring->written[slot], 0), "copy stream wait");
+            VP_CUDA(cudaMemcpyAsync(ring->host + (size_t)n * nxnv * sizeof(T), a.f_hist_n, nxnv * sizeof(T),
+                                    cudaMemcpyDeviceToHost, ring->copy),
+                    "history copy");
+            VP_CUDA(cudaEventRecord(ring->copied[slot], ring->copy), "record history copy");
+        }
     }
+    if (ring != nullptr)
+        for (int q = 0; q < std::min(ring->slots, T_steps); ++q)
+            VP_CUDA(cudaStreamWaitEvent(s, ring->copied[q], 0), "wait for history copies");
     return VP_OK;
 }
 
@@ -680,6 +709,8 @@ static void free_plan(vp_plan* p) {
     cudaFree(p->d_tx64);
     cudaFree(p->d_mxf);
     cudaFree(p->d_kl);
+    for (cudaEvent_t e : p->ev_written) cudaEventDestroy(e);
+    for (cudaEvent_t e : p->ev_copied) cudaEventDestroy(e);
     cudaFree(p->d_txf);
     cudaFree(p->d_txf64);
     cudaFree(p->d_vtab);
@@ -1246,6 +1277,54 @@ int vp_electric_energy(vp_plan* plan, const void* E, void* ee, void* stream) {
                         ? launch_electric_energy<double>(plan->nx, plan->dx, (const double*)E, (double*)ee, s)
                         : launch_electric_energy<float>(plan->nx, plan->dx, (const float*)E, (float*)ee, s);
     return e == cudaSuccess ? VP_OK : cuda_err(e, "electric energy launch");
+}
+
+int vp_forward_stream_history(vp_plan* plan, const double* f_iv, const void* H, int32_t n_steps, double* f_final,
+                              void* f_hist_host, void* ring, int32_t ring_slots, void* E_hist, void* ee_hist,
+                              void* tape, int32_t checkpoint_every, void* workspace, size_t workspace_bytes,
+                              void* stream, void* copy_stream) {
+    if (!plan) return set_err(VP_ERR_ARG, "plan must not be NULL");
+    if (n_steps < 1) return set_err(VP_ERR_ARG, "n_steps must be >= 1 (got %d)", n_steps);
+    if (ring_slots < 2 || ring_slots > 64) return set_err(VP_ERR_ARG, "ring_slots must be in [2, 64] (got %d)", ring_slots);
+    if (copy_stream == nullptr || copy_stream == stream)
+        return set_err(VP_ERR_ARG, "copy_stream must be a stream other than the compute stream");
+    if (f_hist_host == nullptr) return set_err(VP_ERR_ARG, "f_hist_host must not be NULL");
+    {
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, f_hist_host) != cudaSuccess || at.type != cudaMemoryTypeHost) {
+            cudaGetLastError();
+            return set_err(VP_ERR_ARG, "f_hist_host must be pinned host memory (cudaHostAlloc or cudaHostRegister)");
+        }
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    CaptureScope capture_scope(stream_capturing(s));
+    int rc;
+    const int dev = plan->device;
+    if ((rc = check_dev_ptr(f_iv, "f_iv", dev)) || (rc = check_dev_ptr(H, "H", dev)) ||
+        (rc = check_dev_ptr(ring, "ring", dev)) || (rc = check_opt_ptr(f_final, "f_final", dev)) ||
+        (rc = check_opt_ptr(E_hist, "E_hist", dev)) || (rc = check_opt_ptr(ee_hist, "ee_hist", dev)) ||
+        (rc = check_opt_ptr(tape, "tape", dev)))
+        return rc;
+    const int K = resolve_every(plan, n_steps, checkpoint_every);
+    const size_t need = ws_layout(plan, n_steps, K).total;
+    if (workspace_bytes < need) return set_err(VP_ERR_ARG, "workspace has %zu bytes, %zu needed", workspace_bytes, need);
+    if ((rc = check_dev_ptr(workspace, "workspace", dev))) return rc;
+    while ((int)plan->ev_written.size() < ring_slots) {
+        cudaEvent_t a, b;
+        VP_CUDA(cudaEventCreateWithFlags(&a, cudaEventDisableTiming), "cudaEventCreate");
+        VP_CUDA(cudaEventCreateWithFlags(&b, cudaEventDisableTiming), "cudaEventCreate");
+        plan->ev_written.push_back(a);
+        plan->ev_copied.push_back(b);
+    }
+    HistRing hr{static_cast<unsigned char*>(f_hist_host), ring_slots, static_cast<cudaStream_t>(copy_stream),
+                plan->ev_written.data(), plan->ev_copied.data()};
+    unsigned char* w = static_cast<unsigned char*>(workspace);
+    unsigned char* t = static_cast<unsigned char*>(tape);
+    if (plan->dtype == VP_F64)
+        return forward_impl<double>(plan, f_iv, (const double*)H, n_steps, f_final, (double*)ring,
+                                    (double*)E_hist, (double*)ee_hist, t, K, w, s, &hr);
+    return forward_impl<float>(plan, f_iv, (const float*)H, n_steps, f_final, (float*)ring, (float*)E_hist,
+                               (float*)ee_hist, t, K, w, s, &hr);
 }
 
 int vp_kl_divergence(vp_plan* plan, const double* f, double eps, double* value, double* grad, void* stream) {

@@ -179,6 +179,40 @@ class Plan:
         out["H"] = H
         return out
 
+    def forward_stream_history(self, f_iv, H, n_steps: int, slots: int = 4, want_tape: bool = False,
+                               checkpoint_every: int | None = None, want_f_final: bool = True):
+        """Forward with f_hist streamed into a pinned host tensor through a ring of `slots`
+        device buffers (vp_forward_stream_history). The host history is complete once the
+        current stream is; the returned dict keeps the ring and copy stream alive."""
+        nx, nv, dev, dt = self.nx, self.nv, self.device, self.dtype
+        if n_steps < 1:
+            raise ValueError("n_steps must be >= 1")
+        f_iv = self.to_f64(f_iv).reshape(nx, nv)
+        H = self.to_real(H).reshape(nx)
+        every = self.resolve_every(n_steps, checkpoint_every)
+        host = torch.empty((n_steps, nx, nv), dtype=dt, pin_memory=True)
+        ring = torch.empty((slots, nx, nv), dtype=dt, device=dev)
+        out = {
+            "f_final": torch.empty((nx, nv), dtype=torch.float64, device=dev) if want_f_final else None,
+            "f_hist": host,
+            "E_hist": torch.empty((n_steps, nx), dtype=dt, device=dev),
+            "ee_hist": torch.empty((n_steps,), dtype=dt, device=dev),
+            "tape": torch.empty(self.tape_bytes(n_steps, every), dtype=torch.uint8, device=dev)
+            if want_tape else None,
+            "every": every,
+        }
+        ws = self.workspace(n_steps, every)
+        with torch.cuda.device(dev):
+            copy = torch.cuda.Stream(dev)
+            _capi.check(self.lib.vp_forward_stream_history(
+                self._h, _capi.ptr(f_iv), _capi.ptr(H), int(n_steps), _capi.ptr(out["f_final"]),
+                host.data_ptr(), _capi.ptr(ring), int(slots), _capi.ptr(out["E_hist"]),
+                _capi.ptr(out["ee_hist"]), _capi.ptr(out["tape"]), int(every), _capi.ptr(ws), ws.numel(),
+                _stream_handle(dev), int(copy.cuda_stream)))
+        out["H"] = H
+        out["_ring"] = (ring, copy)
+        return out
+
     def backward(self, H: torch.Tensor, n_steps: int, tape: torch.Tensor | None, every: int,
                  g_f_final=None, g_f_hist=None, g_E_hist=None, g_ee_hist=None):
         """Discrete adjoint. Cotangents are device tensors or None (zero)."""

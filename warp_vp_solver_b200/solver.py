@@ -59,6 +59,7 @@ class WarpVlasovPoissonSolver:
         every ceil(sqrt(n_steps)) steps.
         """
         self.mesh = mesh
+        self.history_on_host = None   # None: stream f_hist to pinned host memory when > 256 MiB
         self.dt = float(dt)
         self.f_eq = np.asarray(f_eq, dtype=np.float64)
         if self.f_eq.shape != (mesh.nx, mesh.nv):
@@ -157,7 +158,15 @@ class WarpVlasovPoissonSolver:
             )
         T = self.num_steps(t_final)
         as_torch = isinstance(f_iv, torch.Tensor)
-        out = self.plan.forward(f_iv, H, T, record_history=record_history)
+        itemsize = 8 if self.dtype == torch.float64 else 4
+        host_hist = self.history_on_host
+        if host_hist is None:   # stream large histories to host memory instead of holding them
+            host_hist = T * self.mesh.nx * self.mesh.nv * itemsize > (256 << 20)
+        if record_history and not as_torch and host_hist and T >= 2:
+            out = self.plan.forward_stream_history(f_iv, H, T)
+            torch.cuda.current_stream(self.plan.device).synchronize()
+        else:
+            out = self.plan.forward(f_iv, H, T, record_history=record_history)
         res = (out["f_final"], out["f_hist"], out["E_hist"], out["ee_hist"])
         if as_torch:
             return res
