@@ -245,6 +245,13 @@ int vp_mlp_mse_backward(vp_mlp* mlp, const float* target, int64_t ldt, const int
 /* One Adam step (Kingma and Ba) on the last parameter gradients; the step count lives on the
  * device, so the call can be captured in a CUDA graph. */
 int vp_mlp_adam(vp_mlp* mlp, float lr, float beta1, float beta2, float eps, void* stream);
+/* Adam on one input vector c (length widths[0]) minimising J(c) = sum_n w_n exp(y_mean_n +
+ * y_std_n * net(c * x_scale)_n) for `iters` steps in one single-CTA launch (warp GEMVs on the
+ * network's BF16 weights, FP32 accumulation; widths up to 512); writes the best iterate and its
+ * J (device pointers). The surrogate-warm-started control's search phase. */
+int vp_mlp_search(vp_mlp* mlp, const float* c0, int32_t iters, float lr, float beta1, float beta2, float eps,
+                  float x_scale, const float* y_mean, const float* y_std, const float* weights, float* best_c,
+                  float* best_J, void* stream);
 /* Nonzero bit 0: a tensor-core wait gave up (results of that call are invalid). Synchronous. */
 int vp_mlp_status(vp_mlp* mlp, uint32_t* flags);
 /* One BF16 tile GEMM with the MLP's epilogues: C = act(A[M,K] . B[N,K]^T + bias), act 0 none,

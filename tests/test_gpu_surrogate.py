@@ -23,3 +23,27 @@ def test_surrogate_warm_start_needs_fewer_adjoint_evaluations():
         assert r["warm_reached"], r
         assert r["plain_evals_to_target"] is not None
         assert 3 * r["warm_evals"] <= r["plain_evals_to_target"], r
+
+
+def test_search_kernel_matches_eager_surrogate_descent():
+    """vp_mlp_search (one launch) against Adam driven from the host through the tensor-core MLP's
+    forward and input gradient: same starting point, same lr, the best J within 2%, and the
+    kernel's reported J equals the surrogate evaluated at its best point."""
+    import torch
+
+    from warp_vp_solver_b200.surrogate import (ControlProblem, Surrogate, SurrogateSearch, adam_loop,
+                                               generate_dataset)
+    setup = c5_setup(nx=64, nv=64, n_steps=30, n_modes=4, eps=1e-2)
+    X, Y, _ = generate_dataset(setup, 512, 0.05, seed=0)
+    sur = Surrogate(setup.n_inputs, setup.n_steps, max_batch=512, seed=2)
+    sur.fit(X, Y, steps=300, batch=256)
+    w = ControlProblem(setup).w.float()
+    c0 = torch.tensor([0.05, -0.03, 0.02, 0.04, -0.01, 0.03, 0.0, -0.02], device="cuda")
+    search = SurrogateSearch(sur, w, lr=3e-3)
+    c_k = search.run(c0, 60)
+    J_k = float(search.best_J)
+    J_at, _ = sur.cost_and_grad(c_k, w)
+    assert abs(float(J_at) - J_k) <= 1e-3 * abs(J_k)
+    c_e, J_e, _ = adam_loop(lambda c: sur.cost_and_grad(c, w), c0, 3e-3, 60, lambda h: False)
+    assert abs(J_k - J_e) <= 0.02 * abs(J_e)
+    assert J_k < float(sur.cost_and_grad(c0, w)[0])

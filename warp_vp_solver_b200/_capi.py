@@ -128,6 +128,8 @@ SIGNATURES = {
     "vp_mlp_mse_backward": (c_int, [c_vp, c_vp, c_i64, c_vp, c_i32, c_vp, c_vp]),
     "vp_mlp_adam": (c_int, [c_vp, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, c_vp]),
     "vp_mlp_status": (c_int, [c_vp, ctypes.POINTER(ctypes.c_uint32)]),
+    "vp_mlp_search": (c_int, [c_vp, c_vp, c_i32, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                              ctypes.c_float, ctypes.c_float, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "vp_gemm_bf16": (c_int, [c_vp, c_i64, c_vp, c_i64, c_i32, c_i32, c_i32, c_vp, c_i32, c_vp, c_i64,
                              c_vp, c_i64, c_vp, c_i64, c_vp, c_i64, c_vp, c_vp]),
     "vp_kl_divergence": (c_int, [c_vp, c_vp, c_dbl, c_vp, c_vp, c_vp]),

@@ -446,6 +446,126 @@ __global__ void vp_mlp_step_kernel(int* step) {
     if (threadIdx.x == 0 && blockIdx.x == 0) *step += 1;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Surrogate search: Adam on one input vector c minimising J(c) = sum_n w_n exp(mu_n + sd_n y_n),
+// y = net(c * x_scale), for `iters` steps in one single-CTA launch. The network's products are
+// warp GEMVs on the same BF16 weights (Wb for the forward, WbT for the backward) with the
+// activations and cotangents rounded to BF16 where the tensor-core path rounds them, FP32
+// accumulation, the same GELU; the best iterate (smallest J evaluated) is returned.
+// ---------------------------------------------------------------------------------------------
+constexpr int kSearchMaxWidth = 512;
+
+struct SearchArgs {
+    LayerRefs R;
+    const float* params;   // FP32 master parameters (biases)
+    int w[MAX_LAYERS + 1];
+    const float* c0;
+    int iters;
+    float lr, b1, b2, eps, x_scale;
+    const float* y_mean;
+    const float* y_std;
+    const float* wt;
+    float* best_c;
+    float* best_J;
+};
+
+__device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+
+// out[r] = sum_k M[r * ld + k] * in[k] for r < rows (warp per row, lanes over k, fixed order).
+__device__ __forceinline__ void warp_gemv(const bf16* __restrict__ M, int ld, int rows, int cols,
+                                          const float* __restrict__ in, float* out) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int r = warp; r < rows; r += nw) {
+        const bf16* row = M + (size_t)r * ld;
+        float acc = 0.f;
+        for (int k = lane; k < cols; k += 32) acc = fmaf(__bfloat162float(row[k]), in[k], acc);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) out[r] = acc;
+    }
+}
+
+__global__ void __launch_bounds__(1024) vp_mlp_search_kernel(const SearchArgs A) {
+    __shared__ float act[MAX_LAYERS + 1][kSearchMaxWidth];   // layer inputs (BF16-rounded)
+    __shared__ float pre[MAX_LAYERS][kSearchMaxWidth];       // pre-activations z_l
+    __shared__ float g[2][kSearchMaxWidth];                  // cotangents (ping-pong)
+    __shared__ float c[kSearchMaxWidth], mo[kSearchMaxWidth], ve[kSearchMaxWidth];
+    __shared__ float red[32];
+    __shared__ float sJ, sBest;
+    const int L = A.R.L, n_in = A.w[0], n_out = A.w[L];
+    const int tid = threadIdx.x;
+    for (int k = tid; k < n_in; k += blockDim.x) {
+        c[k] = A.c0[k];
+        mo[k] = 0.f;
+        ve[k] = 0.f;
+        A.best_c[k] = A.c0[k];
+    }
+    if (tid == 0) sBest = INFINITY;
+    __syncthreads();
+    for (int it = 1; it <= A.iters; ++it) {
+        // forward
+        for (int k = tid; k < n_in; k += blockDim.x) act[0][k] = bf16r(c[k] * A.x_scale);
+        __syncthreads();
+        for (int l = 0; l < L; ++l) {
+            const int K = A.w[l], N = A.w[l + 1];
+            warp_gemv(A.R.Wb[l], pad8(K), N, K, act[l], pre[l]);
+            __syncthreads();
+            const float* b = A.params + A.R.off_b[l];
+            for (int r = tid; r < N; r += blockDim.x) {
+                const float z = pre[l][r] + b[r];
+                pre[l][r] = z;
+                if (l < L - 1) act[l + 1][r] = bf16r(gelu(z));
+            }
+            __syncthreads();
+        }
+        // J and the output cotangent
+        float part = 0.f;
+        for (int r = tid; r < n_out; r += blockDim.x) {
+            const float e = A.wt[r] * expf(A.y_mean[r] + A.y_std[r] * pre[L - 1][r]);
+            part += e;
+            g[0][r] = bf16r(e * A.y_std[r]);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        if ((tid & 31) == 0) red[tid >> 5] = part;
+        __syncthreads();
+        if (tid == 0) {
+            float J = 0.f;
+            for (int q = 0; q < (int)(blockDim.x >> 5); ++q) J += red[q];
+            sJ = J;
+        }
+        __syncthreads();
+        if (sJ < sBest) {   // uniform: every thread reads the same shared values
+            for (int k = tid; k < n_in; k += blockDim.x) A.best_c[k] = c[k];
+            __syncthreads();
+            if (tid == 0) sBest = sJ;
+        }
+        // backward to the input
+        int cur = 0;
+        for (int l = L - 1; l >= 0; --l) {
+            const int K = A.w[l], N = A.w[l + 1];
+            warp_gemv(A.R.WbT[l], pad8(N), K, N, g[cur], g[cur ^ 1]);
+            __syncthreads();
+            if (l > 0)
+                for (int k = tid; k < K; k += blockDim.x) g[cur ^ 1][k] = bf16r(g[cur ^ 1][k] * gelu_grad(pre[l - 1][k]));
+            __syncthreads();
+            cur ^= 1;
+        }
+        // Adam on c (gradient = x_scale * dJ/dx)
+        const float c1 = 1.0f - powf(A.b1, (float)it), c2 = 1.0f - powf(A.b2, (float)it);
+        for (int k = tid; k < n_in; k += blockDim.x) {
+            const float gk = g[cur][k] * A.x_scale;
+            const float m = A.b1 * mo[k] + (1.0f - A.b1) * gk;
+            const float v = A.b2 * ve[k] + (1.0f - A.b2) * gk * gk;
+            mo[k] = m;
+            ve[k] = v;
+            c[k] -= A.lr * (m / c1) / (sqrtf(v / c2) + A.eps);
+        }
+        __syncthreads();
+    }
+    if (tid == 0) *A.best_J = sBest;
+}
+
 }  // namespace mlp
 }  // namespace vpb
 
@@ -872,6 +992,36 @@ int vp_mlp_adam(vp_mlp* n, float lr, float beta1, float beta2, float eps, void* 
 int vp_mlp_status(vp_mlp* n, uint32_t* flags) {
     if (!n || !flags) return set_err(VP_ERR_ARG, "mlp and flags must not be NULL");
     MLP_CUDA(cudaMemcpy(flags, n->err, sizeof(unsigned), cudaMemcpyDeviceToHost), "read mlp status");
+    return VP_OK;
+}
+
+int vp_mlp_search(vp_mlp* n, const float* c0, int32_t iters, float lr, float beta1, float beta2, float eps,
+                  float x_scale, const float* y_mean, const float* y_std, const float* weights, float* best_c,
+                  float* best_J, void* stream) {
+    if (!n || !c0 || !y_mean || !y_std || !weights || !best_c || !best_J)
+        return set_err(VP_ERR_ARG, "pointers must not be NULL");
+    if (iters < 1) return set_err(VP_ERR_ARG, "iters must be >= 1");
+    for (int l = 0; l <= n->L; ++l)
+        if (n->w[l] > kSearchMaxWidth) return set_err(VP_ERR_ARG, "layer width %d exceeds %d", n->w[l], kSearchMaxWidth);
+    SearchArgs A{};
+    A.R = n->R;
+    A.params = n->params;
+    for (int l = 0; l <= n->L; ++l) A.w[l] = n->w[l];
+    A.c0 = c0;
+    A.iters = iters;
+    A.lr = lr;
+    A.b1 = beta1;
+    A.b2 = beta2;
+    A.eps = eps;
+    A.x_scale = x_scale;
+    A.y_mean = y_mean;
+    A.y_std = y_std;
+    A.wt = weights;
+    A.best_c = best_c;
+    A.best_J = best_J;
+    vp_mlp_search_kernel<<<1, 1024, 0, static_cast<cudaStream_t>(stream)>>>(A);
+    count_launch();
+    MLP_CUDA(cudaGetLastError(), "mlp search launch");
     return VP_OK;
 }
 

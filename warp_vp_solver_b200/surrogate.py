@@ -12,9 +12,9 @@ Adam from a random initial control (notebooks/01_Two_Stream_Warp.ipynb, cell 12)
   trained by the project's own forward, backward and Adam kernels.
 * :class:`ControlProblem` gives the true J and dJ/d(coefficients) through the fused forward and
   adjoint kernels; :func:`optimize_plain` is Adam on it until J stops improving;
-  :func:`optimize_warm` first minimises the surrogate's J (:class:`SurrogateSearch`, gradient
-  through the MLP's backward to its inputs), then refines with the true gradient until J is
-  within a tolerance of a target.
+  :func:`optimize_warm` first minimises the surrogate's J (:class:`SurrogateSearch`, one
+  single-CTA launch running Adam through the network's forward and input gradient), then refines
+  with the true gradient until J is within a tolerance of a target.
 """
 
 from __future__ import annotations
@@ -209,61 +209,32 @@ def evals_to_reach(history, target: float) -> int | None:
 
 
 class SurrogateSearch:
-    """Adam on the surrogate's J = sum_n w_n exp(y_n(c)) for one coefficient vector, captured
-    once as a CUDA graph (MLP forward, backward to the input, Adam update, best-iterate tracking
-    on the device) and replayed without host synchronisation."""
+    """Adam on the surrogate's J = sum_n w_n exp(y_n(c)) for one coefficient vector, run as one
+    single-CTA launch per search (``vp_mlp_search``: warp GEMVs on the network's BF16 weights,
+    best-iterate tracking on the device, no host synchronisation)."""
 
     def __init__(self, sur: Surrogate, w: torch.Tensor, lr: float, b1: float = 0.9,
                  b2: float = 0.999, eps: float = 1e-8):
+        from . import _capi
         self.sur = sur
+        self.lib = _capi.load()
         dev = sur.net.device
-        n_in, n_out = sur.widths[0], sur.widths[-1]
-        self.w = w.float().to(dev).reshape(1, n_out)
+        self.w = w.float().to(dev).reshape(-1).contiguous()
+        self.y_mean = sur.y_mean.float().to(dev).contiguous()
+        self.y_std = sur.y_std.float().to(dev).contiguous()
         self.lr, self.b1, self.b2, self.eps = lr, b1, b2, eps
-        self.c = torch.zeros(n_in, device=dev)
-        self.m = torch.zeros(n_in, device=dev)
-        self.v = torch.zeros(n_in, device=dev)
-        self.t = torch.zeros((), device=dev)
-        self.best_c = torch.zeros(n_in, device=dev)
-        self.best_J = torch.full((), float("inf"), device=dev)
-        self.x = torch.zeros((1, n_in), device=dev)
-        self.z = torch.zeros((1, n_out), device=dev)
-        self.g_z = torch.zeros((1, n_out), device=dev)
-        self.g_x = torch.zeros((1, n_in), device=dev)
-        self._step()                      # eager once: kernel attributes are set before capture
-        torch.cuda.synchronize(dev)
-        self.graph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(self.graph):
-            self._step()
-
-    def _step(self) -> None:
-        sur, net = self.sur, self.sur.net
-        torch.mul(self.c.reshape(1, -1), sur.x_scale, out=self.x)
-        net.forward_into(self.x, None, 1, self.z)
-        e = torch.exp(self.z * sur.y_std + sur.y_mean) * self.w
-        J = e.sum()
-        better = J < self.best_J
-        self.best_J.copy_(torch.where(better, J, self.best_J))
-        self.best_c.copy_(torch.where(better, self.c, self.best_c))
-        torch.mul(e, sur.y_std, out=self.g_z)
-        net.backward_into(self.g_z, self.g_x, param_grads=False)
-        g = self.g_x.reshape(-1) * sur.x_scale
-        self.t.add_(1.0)
-        self.m.mul_(self.b1).add_((1 - self.b1) * g)
-        self.v.mul_(self.b2).add_((1 - self.b2) * g * g)
-        mh = self.m / (1 - torch.pow(self.b1, self.t))
-        vh = self.v / (1 - torch.pow(self.b2, self.t))
-        self.c.sub_(self.lr * mh / (vh.sqrt() + self.eps))
+        self.best_c = torch.zeros(sur.widths[0], device=dev)
+        self.best_J = torch.zeros(1, device=dev)
 
     def run(self, c0: torch.Tensor, iters: int) -> torch.Tensor:
-        self.c.copy_(c0.float().reshape(-1))
-        self.m.zero_()
-        self.v.zero_()
-        self.t.zero_()
-        self.best_J.fill_(float("inf"))
-        self.best_c.copy_(self.c)
-        for _ in range(iters):
-            self.graph.replay()
+        from . import _capi
+        from .plan import _stream_handle
+        c0 = c0.float().reshape(-1).contiguous().to(self.best_c.device)
+        _capi.check(self.lib.vp_mlp_search(
+            self.sur.net._h, _capi.ptr(c0), int(iters), float(self.lr), float(self.b1), float(self.b2),
+            float(self.eps), float(self.sur.x_scale), _capi.ptr(self.y_mean), _capi.ptr(self.y_std),
+            _capi.ptr(self.w), _capi.ptr(self.best_c), _capi.ptr(self.best_J),
+            _stream_handle(self.best_c.device)))
         return self.best_c.clone()
 
 
