@@ -235,6 +235,36 @@ def test_staged_shapes_agree(rows, cols):
     assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
 
 
+@pytest.mark.parametrize("dtype", DTYPES, ids=_dt_id)
+@pytest.mark.parametrize("layout", ["staged", "percolumn16"])
+def test_separate_tail_large_nx(layout, dtype):
+    """nx = 4096: the Poisson tail is its own one-CTA launch (per-stage twiddles in shared memory
+    for float32, the plain table for float64), and with 16 column chunks the row partials are
+    pre-summed across CTAs before it. Forward and adjoint against the oracle."""
+    m = make_mesh(10.0 * np.pi, 6.0, 4096, 512)
+    f_eq, f_iv = two_stream_state(m, eps=1e-2)
+    H = 0.05 * np.random.default_rng(11).standard_normal(m.nx)
+    T, dt = 4, 0.05
+    s = make_solver(m, dt, f_eq, "stream", dtype=dtype)
+    if layout == "percolumn16":
+        s.plan.set_config(stage_rows=0, rows_per_cta=4, threads=32, n_chunks=16)
+        assert s.plan.get_config()["n_chunks"] == 16
+    cfg = s.plan.get_config()
+    assert cfg["tail_inline"] == 0
+    out = s.run_forward(f_iv, H, T * dt)
+    g = O.grid_from(m)
+    ref = O.delta_forward(g, dt, f_eq, f_iv, H, T)
+    for arr, r, name in zip(out, ref, FIELDS):
+        assert O.rel_err(arr, r) < TOL_FWD[dtype], f"{name}: {O.rel_err(arr, r):.2e}"
+    w = O.trapezoid_time_weights(T, dt)
+    rg = np.random.default_rng(12)
+    gff = rg.standard_normal((m.nx, m.nv))
+    gEh = rg.standard_normal((T, m.nx))
+    gf, gH = s._run_backward(f_iv, H, T * dt, None, gff, None, gEh, w)
+    rf, rH = O.delta_backward(g, dt, f_eq, f_iv, H, T, gff, None, gEh, w)
+    assert O.rel_err(gf, rf) < TOL_BWD[dtype] and O.rel_err(gH, rH) < TOL_BWD[dtype]
+
+
 def test_staged_shape_rejects_unusable_values():
     m = make_mesh(10.0 * np.pi, 6.0, 64, 256)
     f_eq, _ = two_stream_state(m)

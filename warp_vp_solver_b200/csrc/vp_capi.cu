@@ -60,6 +60,7 @@ struct vp_plan {
     int pow2 = 0, log2nx = 0;
     int tail_inline = 0;       // Poisson tail inside the fused launch (small nx)
     size_t tail_smem = 0;      // dynamic shared memory of the separate tail launch (0: global scratch)
+    int tail_tw_stage = 0;     // the separate tail's FFT twiddles are laid out per stage
     int tail_threads = 0;
     LaunchCfg cfg{};
     std::vector<double> host_feq;  // f_eq as given (host), for recognising identical plans
@@ -463,7 +464,7 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
     a.f_hist_n = nullptr;
     a.f_final = nullptr;
     VP_CUDA(launch_fwd<T>(a, p->cfg, 0, p->feq2d != 0, s), "forward prologue launch");
-    if (!p->tail_inline) VP_CUDA(launch_fwd_tail<T>(a, p->tail_threads, p->tail_smem, s), "forward tail launch");
+    if (!p->tail_inline) VP_CUDA(launch_fwd_tail<T>(a, p->tail_threads, p->tail_smem, p->tail_tw_stage != 0, s), "forward tail launch");
 
     for (int n = 0; n < T_steps; ++n) {
         const bool last = (n == T_steps - 1);
@@ -500,7 +501,7 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
             VP_CUDA(launch_fwd<T>(a, p->cfg, 1, p->feq2d != 0, s), "forward step launch");
         }
         if (!last && !p->tail_inline)
-            VP_CUDA(launch_fwd_tail<T>(a, p->tail_threads, p->tail_smem, s), "forward tail launch");
+            VP_CUDA(launch_fwd_tail<T>(a, p->tail_threads, p->tail_smem, p->tail_tw_stage != 0, s), "forward tail launch");
         if (ring != nullptr) {
             VP_CUDA(cudaEventRecord(ring->written[slot], s), "record history slot");
             VP_CUDA(cudaStreamWaitEvent(ring->copy, ring->written[slot], 0), "copy stream wait");
@@ -653,7 +654,7 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
     b.gE_hist = g_Eh ? g_Eh + (size_t)(T_steps - 1) * nx : nullptr;
     b.gee = g_ee ? g_ee + (T_steps - 1) : nullptr;
     VP_CUDA(launch_bwd<T>(b, p->cfg, 0, p->feq2d != 0, s), "backward prologue launch");
-    if (!p->tail_inline) VP_CUDA(launch_bwd_tail<T>(b, p->tail_threads, p->tail_smem, s), "backward tail launch");
+    if (!p->tail_inline) VP_CUDA(launch_bwd_tail<T>(b, p->tail_threads, p->tail_smem, p->tail_tw_stage != 0, s), "backward tail launch");
 
     b.c_src = nullptr;
     b.c_src2 = nullptr;
@@ -684,7 +685,7 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
             VP_CUDA(launch_bwd<T>(b, p->cfg, 1, p->feq2d != 0, s), "backward step launch");
         }
         if (!p->tail_inline)
-            VP_CUDA(launch_bwd_tail<T>(b, p->tail_threads, p->tail_smem, s), "backward tail launch");
+            VP_CUDA(launch_bwd_tail<T>(b, p->tail_threads, p->tail_smem, p->tail_tw_stage != 0, s), "backward tail launch");
     }
     // epilogue (n = 0)
     b.w_in = wbuf[0];
@@ -868,6 +869,10 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
     const size_t area = poisson_area_size(nx, rs);
     p->tail_inline = area <= kInlineTailBytes ? 1 : 0;
     p->tail_smem = (!p->tail_inline && area <= kTailSmemBytes) ? area : 0;
+    if (p->tail_smem > 0 && p->pow2 && poisson_area_size_staged(nx, rs) <= kTailSmemBytes) {
+        p->tail_smem = poisson_area_size_staged(nx, rs);
+        p->tail_tw_stage = 1;
+    }
     p->tail_threads = nx >= 2048 ? 1024 : std::max(32, ((nx / 2 + 31) / 32) * 32);
     p->cfg = choose_cfg(nx, nv, n_sms);
     p->cfg.smem = fused_smem(p, p->cfg.R);

@@ -100,9 +100,12 @@ __device__ __forceinline__ int bitrev(int i, int L) {
     return L == 0 ? 0 : (int)(__brev((unsigned)i) >> (32 - L));
 }
 
+// tw: the nx/2 twiddles exp(-2 pi i q / n), read at q = k * (n >> s) in stage s; or, with
+// `staged`, the same values laid out stage after stage (stage s at [2^(s-1) - 1, 2^s - 1)), so
+// that the lanes of a warp read consecutive entries instead of one shared-memory bank.
 template <typename T>
 __device__ void fft_radix2(typename Cplx<T>::type* z, const typename Cplx<T>::type* tw, int n,
-                           int L) {
+                           int L, bool staged = false) {
     using C = typename Cplx<T>::type;
     for (int s = 1; s <= L; ++s) {
         const int half = 1 << (s - 1);
@@ -111,7 +114,7 @@ __device__ void fft_radix2(typename Cplx<T>::type* z, const typename Cplx<T>::ty
             const int k = b & (half - 1);
             const int i0 = ((b >> (s - 1)) << s) + k;
             const int i1 = i0 + half;
-            const C w = tw[k * stride];
+            const C w = staged ? tw[half - 1 + k] : tw[k * stride];
             const C u = z[i0];
             const C v = z[i1];
             const T vr = v.x * w.x - v.y * w.y;
@@ -150,7 +153,8 @@ __device__ void poisson_core(const PoissonTables<T>& P, typename Cplx<T>::type* 
     __syncthreads();
     if (P.pow2) {
         const int L = P.log2nx;
-        fft_radix2<T>(z, tw_s, nx, L);
+        const bool staged = P.tw_stage != 0 && P.use_smem != 0;
+        fft_radix2<T>(z, tw_s, nx, L, staged);
         const T sgn = adjoint ? T(-1) : T(1);
         for (int i = threadIdx.x; i < nx; i += blockDim.x) {
             const int r = bitrev(i, L);
@@ -165,7 +169,7 @@ __device__ void poisson_core(const PoissonTables<T>& P, typename Cplx<T>::type* 
             }
         }
         __syncthreads();
-        fft_radix2<T>(z, tw_s, nx, L);
+        fft_radix2<T>(z, tw_s, nx, L, staged);
     } else {
         for (int i = threadIdx.x; i < nx; i += blockDim.x) {
             T s = T(0);
@@ -195,7 +199,14 @@ __device__ PoissonArea<T> poisson_area(const PoissonTables<T>& P, unsigned char*
     if (P.use_smem) {
         C* z = reinterpret_cast<C*>(smem);
         C* tw = z + P.nx;
-        if (P.pow2) {
+        if (P.pow2 && P.tw_stage) {
+            // entry e = 2^(s-1) - 1 + k of stage s holds twiddle k * (nx >> s)
+            for (int e = threadIdx.x; e < P.nx - 1; e += blockDim.x) {
+                const int s = 32 - __clz(e + 1);
+                const int k = e + 1 - (1 << (s - 1));
+                tw[e] = P.tw[(size_t)k * (P.nx >> s)];
+            }
+        } else if (P.pow2) {
             for (int i = threadIdx.x; i < (P.nx >> 1); i += blockDim.x) tw[i] = P.tw[i];
         }
         w.z = z;

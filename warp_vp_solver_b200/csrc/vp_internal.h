@@ -30,6 +30,8 @@ template <typename T> struct PoissonTables {
     T* gscratch;                        // nx complex of global scratch, used when the work area
                                         // does not fit in the launch's shared memory
     int use_smem;                       // work area in dynamic shared memory
+    int tw_stage;                       // twiddles in shared memory laid out per FFT stage (pow2,
+                                        // use_smem; the work area is poisson_area_size_staged)
 };
 
 // Arguments of one fused forward launch (see vp_kernels.cu for the phase semantics).
@@ -199,9 +201,9 @@ cudaError_t launch_semilag_v(int nx, int nv, double dv, double dt, const T* in,
                              cudaStream_t s);
 
 template <typename T>
-cudaError_t launch_fwd_tail(const FwdArgs<T>& a, int threads, size_t smem, cudaStream_t s);
+cudaError_t launch_fwd_tail(const FwdArgs<T>& a, int threads, size_t smem, bool tw_stage, cudaStream_t s);
 template <typename T>
-cudaError_t launch_bwd_tail(const BwdArgs<T>& a, int threads, size_t smem, cudaStream_t s);
+cudaError_t launch_bwd_tail(const BwdArgs<T>& a, int threads, size_t smem, bool tw_stage, cudaStream_t s);
 template <typename T>
 cudaError_t set_tail_smem_limit(size_t bytes);
 template <typename T>
@@ -215,6 +217,11 @@ cudaError_t launch_kl_divergence(int nx, int nv, const double* f, const double* 
 // Bytes of the Poisson work area (nx complex values plus nx/2+1 complex twiddles).
 inline size_t poisson_area_size(int nx, size_t real_size) {
     return (size_t)nx * 2 * real_size + (size_t)((nx >> 1) + 1) * 2 * real_size;
+}
+
+// Bytes of the work area with per-stage twiddles (nx complex values plus nx complex twiddles).
+inline size_t poisson_area_size_staged(int nx, size_t real_size) {
+    return (size_t)nx * 4 * real_size;
 }
 
 // Cluster-resident kernels (vp_resident.cu): one cluster runs a whole time loop.

@@ -957,15 +957,54 @@ cudaError_t launch_bwd(const BwdArgs<T>& a, const LaunchCfg& c, int phase, bool 
     return feq2d ? bwd_r<T, true>(a, c, phase, s) : bwd_r<T, false>(a, c, phase, s);
 }
 
+// Sums the column-chunk partials of every row into chunk 0 (part[i] = sum over c of
+// part[c*nx + i], c ascending: the order the tails use), so that the one-CTA tail reads nx values
+// instead of n_chunks*nx. Used before a separate tail launch when there are many partials.
 template <typename T>
-cudaError_t launch_fwd_tail(const FwdArgs<T>& a, int threads, size_t smem, cudaStream_t s) {
+__global__ void __launch_bounds__(256) vp_part_sum_kernel(T* part, int n_chunks, int nx) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nx) return;
+    T s = __ldcg(part + i);
+    int c = 1;
+    for (; c + 8 <= n_chunks; c += 8) {
+        T v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = __ldcg(part + (size_t)(c + u) * nx + i);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) s += v[u];
+    }
+    for (; c < n_chunks; ++c) s += __ldcg(part + (size_t)c * nx + i);
+    part[i] = s;
+}
+
+// Row partials above this count are pre-summed by vp_part_sum_kernel across many CTAs.
+constexpr long long kTailPartialsDirect = 1 << 15;
+
+template <typename T, typename Args>
+static cudaError_t presum_partials(Args& a, cudaStream_t s) {
+    if (a.part == nullptr || a.n_chunks <= 1 || (long long)a.n_chunks * a.nx <= kTailPartialsDirect)
+        return cudaSuccess;
+    vp_part_sum_kernel<T><<<(a.nx + 255) / 256, 256, 0, s>>>(a.part, a.n_chunks, a.nx);
+    count_launch();
+    a.n_chunks = 1;
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_fwd_tail(const FwdArgs<T>& args, int threads, size_t smem, bool tw_stage, cudaStream_t s) {
+    FwdArgs<T> a = args;
+    if (cudaError_t e = presum_partials<T>(a, s)) return e;
+    a.P.tw_stage = tw_stage ? 1 : 0;
     vp_fwd_tail_kernel<T><<<1, threads, smem, s>>>(a);
     count_launch();
     return cudaGetLastError();
 }
 
 template <typename T>
-cudaError_t launch_bwd_tail(const BwdArgs<T>& a, int threads, size_t smem, cudaStream_t s) {
+cudaError_t launch_bwd_tail(const BwdArgs<T>& args, int threads, size_t smem, bool tw_stage, cudaStream_t s) {
+    BwdArgs<T> a = args;
+    if (cudaError_t e = presum_partials<T>(a, s)) return e;
+    a.P.tw_stage = tw_stage ? 1 : 0;
     vp_bwd_tail_kernel<T><<<1, threads, smem, s>>>(a);
     count_launch();
     return cudaGetLastError();
@@ -979,10 +1018,10 @@ cudaError_t set_tail_smem_limit(size_t bytes) {
     return cudaFuncSetAttribute(vp_bwd_tail_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-template cudaError_t launch_fwd_tail<float>(const FwdArgs<float>&, int, size_t, cudaStream_t);
-template cudaError_t launch_fwd_tail<double>(const FwdArgs<double>&, int, size_t, cudaStream_t);
-template cudaError_t launch_bwd_tail<float>(const BwdArgs<float>&, int, size_t, cudaStream_t);
-template cudaError_t launch_bwd_tail<double>(const BwdArgs<double>&, int, size_t, cudaStream_t);
+template cudaError_t launch_fwd_tail<float>(const FwdArgs<float>&, int, size_t, bool, cudaStream_t);
+template cudaError_t launch_fwd_tail<double>(const FwdArgs<double>&, int, size_t, bool, cudaStream_t);
+template cudaError_t launch_bwd_tail<float>(const BwdArgs<float>&, int, size_t, bool, cudaStream_t);
+template cudaError_t launch_bwd_tail<double>(const BwdArgs<double>&, int, size_t, bool, cudaStream_t);
 template cudaError_t set_tail_smem_limit<float>(size_t);
 template cudaError_t set_tail_smem_limit<double>(size_t);
 

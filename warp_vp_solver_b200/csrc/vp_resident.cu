@@ -37,9 +37,9 @@ namespace vpb {
 template <typename T> struct ResSmem {
     T* p0;
     T* p1;
-    T* p2;
-    T* vec0;         // nx: row sums from every CTA, even steps
-    T* vec1;         // nx: row sums from every CTA, odd steps
+    T* p2;           // row partials of the warps: [RC][NVP/32]
+    T* vec0;         // nx: row sums of every CTA, gathered after the step's cluster barrier
+    T* vec1;         // 2 x RC: this CTA's own row sums, step parity (read by the other CTAs)
     T* circ;         // nx: c = real(ifft(m))
     T* fld;          // nx: E (forward) or grho (adjoint), all rows
     T* aux;          // nx: H (forward) or g_E (adjoint)
@@ -47,7 +47,7 @@ template <typename T> struct ResSmem {
     double* feq;     // nv: the f_eq row (x-invariant f_eq)
     T* dfeq;         // nv: f_eq[j+1] - f_eq[j] rounded from float64 (periodic)
     T* red;          // 32
-    double* eep;     // 2 x 16 partial energies (read by CTA 0)
+    double* eep;     // 4 partial energies of the own rows (step s in slot s % 4; read by CTA 0)
     T* own;          // RC: accumulated g_H of the own rows (adjoint)
 };
 
@@ -61,7 +61,7 @@ __host__ __device__ inline size_t res_smem_bytes(int nx, int nv, int RC, size_t 
     b += res_align((size_t)nv * 8);
     b += res_align((size_t)nv * rs);
     b += res_align((size_t)32 * rs);
-    b += res_align((size_t)32 * 8);
+    b += res_align((size_t)64 * 8);
     b += res_align((size_t)RC * rs);
     return b;
 }
@@ -87,7 +87,7 @@ __device__ ResSmem<T> res_carve(unsigned char* smem, int nx, int nv, int RC) {
     s.feq = reinterpret_cast<double*>(take((size_t)nv * sizeof(double)));
     s.dfeq = reinterpret_cast<T*>(take((size_t)nv * sizeof(T)));
     s.red = reinterpret_cast<T*>(take((size_t)32 * sizeof(T)));
-    s.eep = reinterpret_cast<double*>(take((size_t)32 * sizeof(double)));
+    s.eep = reinterpret_cast<double*>(take((size_t)64 * sizeof(double)));
     s.own = reinterpret_cast<T*>(take((size_t)RC * sizeof(T)));
     return s;
 }
@@ -156,20 +156,57 @@ __device__ __forceinline__ void cluster_wait() {
     asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
 }
 
-// Row sums of the plane `vals` (RC x nv, already weighted) for the CTA's own rows, written to
-// vec[gr0 + r] of every CTA of the cluster. Starts with a block barrier; the caller's cluster
-// barrier publishes the stores.
-template <typename T, int RC>
-__device__ __forceinline__ void res_rowsum_broadcast(cg::cluster_group& cluster, const T* vals,
-                                                     T* vec, int nv, int gr0, int CN) {
-    __syncthreads();
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int nw = blockDim.x >> 5;
-    for (int r = wid; r < RC; r += nw) {
+// Row sums in three fixed-order stages. (1) Each warp reduces its RPT rows over its 32 columns
+// with a transposed butterfly (RPT values in log2(RPT) halving exchanges, then a plain xor tree)
+// and writes one partial per row to red[row][column group] (no block barrier). (2) After a block
+// barrier, res_rows_local sums each row's column-group partials in ascending order into the CTA's
+// own row-sum slot. (3) After the cluster barrier that publishes the slots, every CTA gathers all
+// nx row sums from the owners (res_rows_gather). Only local shared-memory stores precede the
+// barrier; the exchange is one distributed-shared-memory load per row after it.
+template <int N> struct ILog2 { static constexpr int value = 1 + ILog2<N / 2>::value; };
+template <> struct ILog2<1> { static constexpr int value = 0; };
+
+template <typename T, int RPT>
+__device__ __forceinline__ void res_warp_rows(T (&v)[RPT], T* red, int rt, int cw, int ncw) {
+    constexpr int LG = ILog2<RPT>::value;
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int st = 0; st < LG; ++st) {
+        const int o = 16 >> st;
+        const int n = RPT >> (st + 1);
+        const bool upper = (lane & o) != 0;
+#pragma unroll
+        for (int i = 0; i < (RPT >> 1); ++i) {
+            if (i < n) {
+                const T send = upper ? v[i] : v[i + n];
+                const T keep = upper ? v[i + n] : v[i];
+                v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+            }
+        }
+    }
+    T r = v[0];
+#pragma unroll
+    for (int o = 16 >> LG; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    // lane L holds the sum of row L >> (5 - LG) of the thread's RPT rows
+    if ((lane & ((32 >> LG) - 1)) == 0) red[(rt + (lane >> (5 - LG))) * ncw + cw] = r;
+}
+
+template <typename T>
+__device__ __forceinline__ void res_rows_local(const T* red, T* slot, int ncw, int RC) {
+    for (int r = threadIdx.x; r < RC; r += blockDim.x) {
         T s = T(0);
-        for (int j = lane; j < nv; j += 32) s += vals[(size_t)r * nv + j];
-        s = warp_sum(s);
-        if (lane < CN) cluster.map_shared_rank(vec, lane)[gr0 + r] = s;
+        for (int w = 0; w < ncw; ++w) s += red[r * ncw + w];
+        slot[r] = s;
+    }
+}
+
+// out[i] = scale * (row sum of row i), read from slot `par` of the owning CTA.
+template <typename T>
+__device__ __forceinline__ void res_rows_gather(cg::cluster_group& cluster, T* own_slots, int par,
+                                                T* out, int nx, int RC, T scale) {
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        const int c = i / RC;
+        out[i] = scale * cluster.map_shared_rank(own_slots, c)[par * RC + (i - c * RC)];
     }
 }
 
@@ -219,41 +256,53 @@ __device__ void res_init_tables(ResSmem<T>& S, const PoissonTables<T>& P, const 
 // Forward
 // ---------------------------------------------------------------------------------------------
 
-// Poisson for step s on the rows this CTA's windows touch, their v shifts, the own rows'
-// outputs and the partial energy of the own rows (summed by CTA 0 one barrier later).
-// `rho_sum` holds the row sums of h_s from every CTA.
+// Poisson for step k on the rows this CTA's windows touch and their v shifts, from the row sums
+// of h_k published in slot `par` of every CTA. CTA 0 also sums the partial energies of step k - 2
+// (published by the barrier before this call) into ee_hist[k - 2]; the remote reads go here, next
+// to the row-sum gather, because the other CTAs are all between the same two barriers. Ends with
+// a block barrier.
 template <typename T>
-__device__ void res_fwd_field(const ResFwdArgs<T>& a, ResSmem<T>& S, cg::cluster_group& cluster,
-                              T* rho_sum, int s, int gr0, int RC, int me, int CN) {
+__device__ void res_fwd_field(const ResFwdArgs<T>& a, ResSmem<T>& S, cg::cluster_group& cluster, int par,
+                              int gr0, int RC, int k, int me, int CN) {
     const int nx = a.nx, nv = a.nv;
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) rho_sum[i] *= -a.dv;   // rho
+    if (me == 0 && k >= 2 && a.ee_hist != nullptr && threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        const double v = lane < CN ? cluster.map_shared_rank(S.eep, lane)[(k - 2) & 3] : 0.0;
+        double tot = 0.0;
+        for (int c = 0; c < CN; ++c) tot += __shfl_sync(0xffffffffu, v, c);
+        if (lane == 0) a.ee_hist[k - 2] = (T)(0.5 * tot * (double)a.dx);
+    }
+    T* rho_sum = S.vec0;
+    res_rows_gather<T>(cluster, S.vec1, par, rho_sum, nx, RC, -a.dv);   // rho
     const int first = ((gr0 + a.win_lo) % nx + nx) % nx;
     res_circ_rows<T>(S.circ, rho_sum, S.fld, nx, first, a.win_n, false);
     for (int r = threadIdx.x; r < a.win_n; r += blockDim.x) {
         const int i = wrap1(first + r, nx);
         S.vsh[i] = res_vshift<T>(S.fld[i] + S.aux[i], a.dtdv, nv);
     }
-    if (threadIdx.x < 32) {
-        double e2 = 0.0;
-        for (int r = threadIdx.x; r < RC; r += 32) {
-            const int i = gr0 + r;
-            const T E = S.fld[i];
-            const T Et = E + S.aux[i];
-            if (a.E_hist != nullptr) a.E_hist[(size_t)s * nx + i] = Et;
-            if (a.E_tape != nullptr) a.E_tape[(size_t)s * nx + i] = E;
-            if (a.vsh_tape != nullptr) a.vsh_tape[(size_t)s * nx + i] = res_vshift<T>(Et, a.dtdv, nv);
-            e2 += (double)(trap_w<T>(i, nx) * E * E);
-        }
-        e2 = warp_sum(e2);
-        if (threadIdx.x == 0) cluster.map_shared_rank(S.eep, 0)[(s & 1) * 16 + me] = e2;
-    }
-    // CTA 0: energy of step s-1, whose partials were published by the last cluster barrier
-    if (me == 0 && threadIdx.x == 0 && s >= 1 && a.ee_hist != nullptr) {
-        double tot = 0.0;
-        for (int c = 0; c < CN; ++c) tot += S.eep[((s - 1) & 1) * 16 + c];
-        a.ee_hist[s - 1] = (T)(0.5 * tot * (double)a.dx);
-    }
     __syncthreads();
+}
+
+// One warp, for step s (the field in S.fld/S.aux is E_s for the own rows): E_hist, E_tape and
+// vsh_tape of the own rows, and the partial energy of the own rows into its slot s % 4 (the next
+// cluster barrier publishes it; CTA 0 sums the partials in the field of step s + 2). Runs between a cluster arrive and wait, off the
+// step's critical path.
+template <typename T>
+__device__ void res_fwd_outputs(const ResFwdArgs<T>& a, ResSmem<T>& S, int s, int gr0, int RC) {
+    const int nx = a.nx, nv = a.nv;
+    const int lane = threadIdx.x & 31;
+    double e2 = 0.0;
+    for (int r = lane; r < RC; r += 32) {
+        const int i = gr0 + r;
+        const T E = S.fld[i];
+        const T Et = E + S.aux[i];
+        if (a.E_hist != nullptr) a.E_hist[(size_t)s * nx + i] = Et;
+        if (a.E_tape != nullptr) a.E_tape[(size_t)s * nx + i] = E;
+        if (a.vsh_tape != nullptr) a.vsh_tape[(size_t)s * nx + i] = res_vshift<T>(Et, a.dtdv, nv);
+        e2 += (double)(trap_w<T>(i, nx) * E * E);
+    }
+    e2 = warp_sum(e2);
+    if (lane == 0) S.eep[s & 3] = e2;
 }
 
 template <typename T, int RC, int RPT, bool FEQ2D>
@@ -270,9 +319,11 @@ __global__ void __launch_bounds__(1024) vp_res_fwd_kernel(const ResFwdArgs<T> a)
     const int rt = (threadIdx.x / NVP) * RPT;   // first own row of this thread (CTA-local)
     const int g = gr0 + rt;                      // first own row of this thread (global)
     const bool colv = j < nv;
+    const int cw = j >> 5, ncw = NVP >> 5;      // warp column group, groups per row
+    const bool out_warp = (int)(threadIdx.x >> 5) == (int)(blockDim.x >> 5) - 1;
     ResSmem<T> S = res_carve<T>(smem, nx, nv, RC);
     T* Hb[2] = {S.p0, S.p1};   // h of even / odd steps, own rows (read remotely)
-    T* Wt = S.p2;              // weighted h' for the row sums
+    T* red = S.p2;             // row partials of the warps
     res_init_tables<T>(S, a.P, a.feq, FEQ2D, nx, nv);
     for (int i = threadIdx.x; i < nx; i += blockDim.x) S.aux[i] = __ldg(a.H + i);
 
@@ -290,7 +341,11 @@ __global__ void __launch_bounds__(1024) vp_res_fwd_kernel(const ResFwdArgs<T> a)
     __syncthreads();
 
     // ---- prologue: h_0 = X(f_iv - f_eq) + corr for the own rows, straight from global memory ----
-    if (colv) {
+    {
+        T wv[RPT];
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) wv[k] = T(0);
+        if (colv) {
         T d[RPT + 1];
         const int base = wrap1(g + m, nx);
 #pragma unroll
@@ -305,13 +360,16 @@ __global__ void __launch_bounds__(1024) vp_res_fwd_kernel(const ResFwdArgs<T> a)
             T h = lerp(d[k], d[k + 1], t);
             if (FEQ2D) h += (T)res_xcorr(a.feq, a.feq_rs, nx, i, m, t64, j);
             Hb[0][(size_t)(rt + k) * nv + j] = h;
-            Wt[(size_t)(rt + k) * nv + j] = wj * h;
+            wv[k] = wj * h;
             if (a.h_tape != nullptr) a.h_tape[(size_t)i * nv + j] = h;
         }
+        }
+        res_warp_rows<T, RPT>(wv, red, rt, cw, ncw);
     }
-    res_rowsum_broadcast<T, RC>(cluster, Wt, S.vec0, nv, gr0, CN);
+    __syncthreads();
+    res_rows_local<T>(red, S.vec1, ncw, RC);
     cluster.sync();
-    res_fwd_field<T>(a, S, cluster, S.vec0, 0, gr0, RC, me, CN);
+    res_fwd_field<T>(a, S, cluster, 0, gr0, RC, 0, me, CN);
 
     for (int n = 0; n < a.n_steps; ++n) {
         const T* cur = Hb[n & 1];
@@ -319,6 +377,9 @@ __global__ void __launch_bounds__(1024) vp_res_fwd_kernel(const ResFwdArgs<T> a)
         const bool last = (n == a.n_steps - 1);
         T d[RPT + 1];
         T hv[RPT];
+        T wv[RPT];
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) wv[k] = T(0);
         int dq = 0;
         if (colv) {
             // o on rows g+2m .. g+2m+RPT+1 (h of those rows, from the owning CTAs)
@@ -360,12 +421,16 @@ __global__ void __launch_bounds__(1024) vp_res_fwd_kernel(const ResFwdArgs<T> a)
                     if (FEQ2D) h += (T)res_xcorr(a.feq, a.feq_rs, nx, g + k, m, t64, j);
                     hv[k] = h;
                     nxt[(rt + k) * nv + j] = h;
-                    Wt[(rt + k) * nv + j] = wj * h;
+                    wv[k] = wj * h;
                 }
             }
         }
-        T* rs = ((n + 1) & 1) ? S.vec1 : S.vec0;
-        if (!last) res_rowsum_broadcast<T, RC>(cluster, Wt, rs, nv, gr0, CN);
+        const int par = (n + 1) & 1;
+        if (!last) {
+            res_warp_rows<T, RPT>(wv, red, rt, cw, ncw);
+            __syncthreads();
+            res_rows_local<T>(red, S.vec1 + par * RC, ncw, RC);
+        }
         cluster_arrive();
         // outputs to global memory, overlapped with the barrier
         if (colv) {
@@ -384,66 +449,132 @@ __global__ void __launch_bounds__(1024) vp_res_fwd_kernel(const ResFwdArgs<T> a)
                 for (int k = 0; k < RPT; ++k) a.h_tape[((size_t)(n + 1) * nx + g + k) * nv + j] = hv[k];
             }
         }
+        if (out_warp) res_fwd_outputs<T>(a, S, n, gr0, RC);
         cluster_wait();
-        if (!last) res_fwd_field<T>(a, S, cluster, rs, n + 1, gr0, RC, me, CN);
+        if (!last) res_fwd_field<T>(a, S, cluster, par, gr0, RC, n + 1, me, CN);
     }
-    // energy of the last step (its partials were stored before the last barrier)
+    // energies of the last two steps (their partials are published by this barrier); the second
+    // barrier keeps every CTA's shared memory alive until CTA 0 has read it
+    cluster.sync();
     if (me == 0 && threadIdx.x == 0 && a.ee_hist != nullptr) {
-        const int s = a.n_steps - 1;
-        double tot = 0.0;
-        for (int c = 0; c < CN; ++c) tot += S.eep[(s & 1) * 16 + c];
-        a.ee_hist[s] = (T)(0.5 * tot * (double)a.dx);
+        for (int s = a.n_steps >= 2 ? a.n_steps - 2 : 0; s < a.n_steps; ++s) {
+            double tot = 0.0;
+            for (int c = 0; c < CN; ++c) tot += cluster.map_shared_rank(S.eep, c)[s & 3];
+            a.ee_hist[s] = (T)(0.5 * tot * (double)a.dx);
+        }
     }
+    cluster.sync();
 }
 
 // ---------------------------------------------------------------------------------------------
 // Adjoint
 // ---------------------------------------------------------------------------------------------
 
+// Tape values that the adjoint field of step s reads, loaded into registers ahead of their use:
+// g_E_hist and E_tape of row threadIdx.x and the v shift of window row threadIdx.x. Rows beyond
+// blockDim.x are read in the field itself.
+template <typename T> struct ResBwdPre {
+    T gEh, Etp, gee;
+    VShift<T> vs;
+};
+
+template <typename T>
+__device__ __forceinline__ ResBwdPre<T> res_bwd_prefetch(const ResBwdArgs<T>& a, int s, int first) {
+    const int nx = a.nx, i = threadIdx.x;
+    ResBwdPre<T> p;
+    p.gee = a.g_ee != nullptr ? __ldg(a.g_ee + s) : T(0);
+    p.gEh = (a.g_Eh != nullptr && i < nx) ? __ldg(a.g_Eh + (size_t)s * nx + i) : T(0);
+    p.Etp = i < nx ? __ldg(a.E_tape + (size_t)s * nx + i) : T(0);
+    p.vs.m = 0;
+    p.vs.t = T(0);
+    if (i < a.win_n) p.vs = a.vsh_tape[(size_t)s * nx + wrap1(first + i, nx)];
+    return p;
+}
+
 // Tail of the adjoint for step s (every CTA, all rows): g_E_total = -dt/dv * rowsum + g_E_hist[s];
 // g_H += g_E_total (own rows); g_E = g_E_total + ee^T; grho = Poisson^T(g_E) (all rows); the v
-// shifts of step s (all rows).
+// shifts of step s (all rows). `pre` holds this thread's tape values of step s.
 template <typename T>
-__device__ void res_bwd_field(const ResBwdArgs<T>& a, ResSmem<T>& S, const T* sums, int s, int gr0,
-                              int RC) {
+__device__ void res_bwd_field(const ResBwdArgs<T>& a, ResSmem<T>& S, cg::cluster_group& cluster, int par,
+                              int s, int gr0, int RC, const ResBwdPre<T>& pre) {
     const int nx = a.nx;
-    const T gee = a.g_ee != nullptr ? __ldg(a.g_ee + s) : T(0);
+    T* sums = S.vec0;
+    res_rows_gather<T>(cluster, S.vec1, par, sums, nx, RC, T(1));
+    const int me_i = threadIdx.x;
+    const T gee = pre.gee;
     for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        const bool own = i == me_i;
         T gEt = a.neg_dt_dv * sums[i];
-        if (a.g_Eh != nullptr) gEt += __ldg(a.g_Eh + (size_t)s * nx + i);
+        if (a.g_Eh != nullptr) gEt += own ? pre.gEh : __ldg(a.g_Eh + (size_t)s * nx + i);
         if (i >= gr0 && i < gr0 + RC) S.own[i - gr0] += gEt;
-        S.aux[i] = gEt + a.dx * trap_w<T>(i, nx) * __ldg(a.E_tape + (size_t)s * nx + i) * gee;
+        const T Et = own ? pre.Etp : __ldg(a.E_tape + (size_t)s * nx + i);
+        S.aux[i] = gEt + a.dx * trap_w<T>(i, nx) * Et * gee;
     }
     const int first = ((gr0 + a.win_lo) % nx + nx) % nx;
     for (int r = threadIdx.x; r < a.win_n; r += blockDim.x) {
         const int i = wrap1(first + r, nx);
-        S.vsh[i] = a.vsh_tape[(size_t)s * nx + i];
+        S.vsh[i] = r == me_i ? pre.vs : a.vsh_tape[(size_t)s * nx + i];
     }
     res_circ_rows<T>(S.circ, S.aux, S.fld, nx, first, a.win_n, true);
 }
 
-// w on the own rows g .. g+RPT-1 from c on rows g-m-1 .. g-m+RPT-1 (held in registers), the
-// slope * w products for the dE row sums (needs h and the v shifts of step np).
+// Slope inputs of step np at the own rows g .. g+RPT-1, column j: the v shifts of those rows
+// (vs, loaded one step ahead) select the two h_tape values (h0, h1) that the slope
+// (h + f_eq)[d1] - (h + f_eq)[d0] needs. The loads are issued a step before their use.
+template <typename T, int RPT>
+__device__ __forceinline__ void res_bwd_load_shifts(const ResBwdArgs<T>& a, int np, int g,
+                                                    VShift<T> (&vs)[RPT]) {
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) {
+        vs[k].m = 0;
+        vs[k].t = T(0);
+    }
+    if (np < 0) return;
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) vs[k] = a.vsh_tape[(size_t)np * a.nx + g + k];
+}
+
+template <typename T, int RPT>
+__device__ __forceinline__ void res_bwd_load_h(const ResBwdArgs<T>& a, int np, int g, int j,
+                                               const VShift<T> (&vs)[RPT], T (&h0)[RPT], T (&h1)[RPT]) {
+    const int nv = a.nv;
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) {
+        h0[k] = T(0);
+        h1[k] = T(0);
+    }
+    if (np < 0) return;
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) {
+        const int d0 = wrap1(j + vs[k].m, nv);
+        const int d1 = d0 + 1 == nv ? 0 : d0 + 1;
+        const T* hr = a.h_tape + ((size_t)np * a.nx + g + k) * nv;
+        h0[k] = __ldg(hr + d0);
+        h1[k] = __ldg(hr + d1);
+    }
+}
+
+// w on the own rows g .. g+RPT-1 from c on rows g-m-1 .. g-m+RPT-1 (held in registers), and the
+// slope * w products for the dE row sums (slope inputs of step np from res_bwd_load_*).
 template <typename T, int RPT, bool FEQ2D>
 __device__ __forceinline__ void res_bwd_w(const ResBwdArgs<T>& a, const ResSmem<T>& S,
-                                          const T (&c)[RPT + 1], T* nxt, T* Wt, int np, int g,
-                                          int rt, int j, T t) {
-    const int nx = a.nx, nv = a.nv;
+                                          const T (&c)[RPT + 1], T* nxt, T (&prod)[RPT],
+                                          const VShift<T> (&vs)[RPT], const T (&h0)[RPT],
+                                          const T (&h1)[RPT], int g, int rt, int j, T t) {
+    const int nv = a.nv;
 #pragma unroll
     for (int k = 0; k < RPT; ++k) {
         const int i = g + k;
         const T wv = lerp(c[k + 1], c[k], t);
         nxt[(size_t)(rt + k) * nv + j] = wv;
-        const VShift<T> vp = a.vsh_tape[(size_t)np * nx + i];
-        const int d0 = wrap1(j + vp.m, nv);
+        const int d0 = wrap1(j + vs[k].m, nv);
         const int d1 = d0 + 1 == nv ? 0 : d0 + 1;
-        const T* hr = a.h_tape + ((size_t)np * nx + i) * nv;
-        T sl = __ldg(hr + d1) - __ldg(hr + d0);
+        T sl = h1[k] - h0[k];
         if (FEQ2D)
             sl += (T)(__ldg(a.feq + (size_t)i * a.feq_rs + d1) - __ldg(a.feq + (size_t)i * a.feq_rs + d0));
         else
             sl += S.dfeq[d0];
-        Wt[(size_t)(rt + k) * nv + j] = sl * wv;
+        prod[k] = sl * wv;
     }
 }
 
@@ -461,9 +592,11 @@ __global__ void __launch_bounds__(1024) vp_res_bwd_kernel(const ResBwdArgs<T> a)
     const int rt = (threadIdx.x / NVP) * RPT;
     const int g = gr0 + rt;
     const bool colv = j < nv;
+    const int cw = j >> 5, ncw = NVP >> 5;
+    const int first = ((gr0 + a.win_lo) % nx + nx) % nx;
     ResSmem<T> S = res_carve<T>(smem, nx, nv, RC);
     T* Wb[2] = {S.p0, S.p1};   // cotangent on the v-step output of even / odd steps, own rows
-    T* Wt = S.p2;              // slope * w for the row sums
+    T* red = S.p2;             // row partials of the warps
     res_init_tables<T>(S, a.P, a.feq, FEQ2D, nx, nv);
     for (int r = threadIdx.x; r < RC; r += blockDim.x) S.own[r] = T(0);
     int m = 0;
@@ -473,11 +606,23 @@ __global__ void __launch_bounds__(1024) vp_res_bwd_kernel(const ResBwdArgs<T> a)
         t = __ldg(a.tx + j);
         wr = -a.dv * trap_w<T>(j, nv);   // rho^T weight (warp_vp_solver/kernels.py:292-299)
     }
+    // slope inputs: vA/hA of the step whose slopes come next, vB the shifts of the step after it
+    VShift<T> vA[RPT], vB[RPT];
+    T hA0[RPT], hA1[RPT];
+    ResBwdPre<T> pre = res_bwd_prefetch<T>(a, T_steps - 1, first);
+    if (colv) {
+        res_bwd_load_shifts<T, RPT>(a, T_steps - 1, g, vA);
+        res_bwd_load_h<T, RPT>(a, T_steps - 1, g, j, vA, hA0, hA1);
+        res_bwd_load_shifts<T, RPT>(a, T_steps - 2, g, vB);
+    }
     __syncthreads();
 
     // ---- prologue (n = T): c = g_f_final + g_f_hist[T-1] on rows g-m-1 .. g-m+RPT-1 ----
     {
         T* nxt = Wb[(T_steps - 1) & 1];
+        T prod[RPT];
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) prod[k] = T(0);
         if (colv) {
             T c[RPT + 1];
             int base = (g - m - 1) % nx;
@@ -490,32 +635,58 @@ __global__ void __launch_bounds__(1024) vp_res_bwd_kernel(const ResBwdArgs<T> a)
                 if (a.g_fh != nullptr) v += __ldg(a.g_fh + ((size_t)(T_steps - 1) * nx + q) * nv + j);
                 c[k] = v;
             }
-            res_bwd_w<T, RPT, FEQ2D>(a, S, c, nxt, Wt, T_steps - 1, g, rt, j, t);
+            res_bwd_w<T, RPT, FEQ2D>(a, S, c, nxt, prod, vA, hA0, hA1, g, rt, j, t);
+            // next: slopes of step T-2
+#pragma unroll
+            for (int k = 0; k < RPT; ++k) vA[k] = vB[k];
+            res_bwd_load_h<T, RPT>(a, T_steps - 2, g, j, vA, hA0, hA1);
+            res_bwd_load_shifts<T, RPT>(a, T_steps - 3, g, vB);
         }
-        T* rs = ((T_steps - 1) & 1) ? S.vec1 : S.vec0;
-        res_rowsum_broadcast<T, RC>(cluster, Wt, rs, nv, gr0, CN);
+        res_warp_rows<T, RPT>(prod, red, rt, cw, ncw);
+        __syncthreads();
+        const int par = (T_steps - 1) & 1;
+        res_rows_local<T>(red, S.vec1 + par * RC, ncw, RC);
         cluster.sync();
-        res_bwd_field<T>(a, S, rs, T_steps - 1, gr0, RC);
+        res_bwd_field<T>(a, S, cluster, par, T_steps - 1, gr0, RC, pre);
     }
 
     for (int n = T_steps - 1; n >= 0; --n) {
         const T* cur = Wb[n & 1];
         T* nxt = Wb[(n + 1) & 1];   // == Wb[(n-1) & 1]
+        if (n > 0) pre = res_bwd_prefetch<T>(a, n - 1, first);
+        T prod[RPT];
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) prod[k] = T(0);
         if (colv) {
             // gh = V^T(w_n) + rho^T(grho_n) on rows g-2m-2 .. g-2m+RPT-1 (w read from the owners)
             const int ng = n == 0 ? RPT + 1 : RPT + 2;   // rows of gh needed
             T gh[RPT + 2];
             int base = (g - (n == 0 ? 1 : 2) * m - (n == 0 ? 1 : 2)) % nx;
             base = wrapneg(base, nx);
+            if (base >= gr0 && base + RPT + 1 < gr0 + RC) {
+                // the whole window lies in this CTA: plain shared-memory loads
 #pragma unroll
-            for (int k = 0; k < RPT + 2; ++k) {
-                if (k < ng) {
-                    const int q = wrap1(base + k, nx);
-                    const VShift<T> v = S.vsh[q];
-                    const T* wrow = res_row<T, RC>(cluster, cur, q, nv, me);
-                    const int c0 = wrapneg(j - v.m, nv);
-                    const int c1 = wrapneg(c0 - 1, nv);
-                    gh[k] = lerp(wrow[c0], wrow[c1], v.t) + wr * S.fld[q];
+                for (int k = 0; k < RPT + 2; ++k) {
+                    if (k < ng) {
+                        const int q = base + k;
+                        const VShift<T> v = S.vsh[q];
+                        const T* wrow = cur + (q - gr0) * nv;
+                        const int c0 = wrapneg(j - v.m, nv);
+                        const int c1 = wrapneg(c0 - 1, nv);
+                        gh[k] = lerp(wrow[c0], wrow[c1], v.t) + wr * S.fld[q];
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < RPT + 2; ++k) {
+                    if (k < ng) {
+                        const int q = wrap1(base + k, nx);
+                        const VShift<T> v = S.vsh[q];
+                        const T* wrow = res_row<T, RC>(cluster, cur, q, nv, me);
+                        const int c0 = wrapneg(j - v.m, nv);
+                        const int c1 = wrapneg(c0 - 1, nv);
+                        gh[k] = lerp(wrow[c0], wrow[c1], v.t) + wr * S.fld[q];
+                    }
                 }
             }
             if (n == 0) {
@@ -533,14 +704,23 @@ __global__ void __launch_bounds__(1024) vp_res_bwd_kernel(const ResBwdArgs<T> a)
                     if (a.g_fh != nullptr)
                         c[k] += __ldg(a.g_fh + ((size_t)(n - 1) * nx + wrap1(cb + k, nx)) * nv + j);
                 }
-                res_bwd_w<T, RPT, FEQ2D>(a, S, c, nxt, Wt, n - 1, g, rt, j, t);
+                res_bwd_w<T, RPT, FEQ2D>(a, S, c, nxt, prod, vA, hA0, hA1, g, rt, j, t);
+                // next: slopes of step n-2 (h loads now, shifts of step n-3 for the one after)
+#pragma unroll
+                for (int k = 0; k < RPT; ++k) vA[k] = vB[k];
+                res_bwd_load_h<T, RPT>(a, n - 2, g, j, vA, hA0, hA1);
+                res_bwd_load_shifts<T, RPT>(a, n - 3, g, vB);
             }
         }
-        T* rs = ((n - 1) & 1) ? S.vec1 : S.vec0;
-        if (n > 0) res_rowsum_broadcast<T, RC>(cluster, Wt, rs, nv, gr0, CN);
+        const int par = (n - 1) & 1;
+        if (n > 0) {
+            res_warp_rows<T, RPT>(prod, red, rt, cw, ncw);
+            __syncthreads();
+            res_rows_local<T>(red, S.vec1 + par * RC, ncw, RC);
+        }
         cluster_arrive();
         cluster_wait();
-        if (n > 0) res_bwd_field<T>(a, S, rs, n - 1, gr0, RC);
+        if (n > 0) res_bwd_field<T>(a, S, cluster, par, n - 1, gr0, RC, pre);
     }
     for (int r = threadIdx.x; r < RC; r += blockDim.x) a.g_H[gr0 + r] = S.own[r];
 }
