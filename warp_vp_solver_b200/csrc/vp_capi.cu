@@ -171,13 +171,27 @@ static LaunchCfg choose_cfg(int nx, int nv, int n_sms) {
 // Largest shared memory a CTA may request on sm_100.
 static const size_t kMaxSmemPerCta = 227 * 1024;
 
+// Halo rows that a resident CTA keeps below and above its own rows: the forward reads rows
+// g + 2m .. g + 2m + RPT + 1 and the adjoint rows g - 2m - 2 .. g - 2m + RPT - 1 of a step's state
+// for x offsets m in [mx_lo, mx_hi] (vp_resident.cu).
+static void res_halo_rows(const vp_plan* p, int* lo, int* hi) {
+    const long long f_lo = -2 * p->mx_lo, f_hi = 2 * p->mx_hi + 2;
+    const long long b_lo = 2 * p->mx_hi + 2, b_hi = -2 * p->mx_lo;
+    *lo = (int)std::max(0LL, std::max(f_lo, b_lo));
+    *hi = (int)std::max(0LL, std::max(f_hi, b_hi));
+}
+
 // Checks that a cluster-resident configuration of cn CTAs can launch; returns its shared memory
 // (0 when it cannot).
 static size_t res_config_ok(const vp_plan* p, int cn) {
     if (cn < 2 || cn > 16 || (cn & (cn - 1)) != 0 || p->nx % cn != 0) return 0;
     const int Rc = p->nx / cn;
     if (!res_rows_supported(Rc)) return 0;
-    const size_t smem = res_smem_size(p->nx, p->nv, Rc, real_size(p));
+    // offsets within one period, with a range short enough to recover them from mx (mod nx)
+    if (p->mx_lo < -p->nx || p->mx_hi > p->nx || p->mx_hi - p->mx_lo >= p->nx / 2) return 0;
+    int hlo = 0, hhi = 0;
+    res_halo_rows(p, &hlo, &hhi);
+    const size_t smem = res_smem_size(p->nx, p->nv, Rc, hlo + hhi, real_size(p));
     if (smem > kMaxSmemPerCta) return 0;
     if (res_threads(Rc, p->nv) > 1024) return 0;
     const int n = p->dtype == VP_F64 ? res_max_clusters<double>(p->feq2d != 0, cn, Rc, p->nv, smem)
@@ -185,19 +199,6 @@ static size_t res_config_ok(const vp_plan* p, int cn) {
     return n > 0 ? smem : 0;
 }
 
-// Rows whose field a resident CTA needs besides its own: 2*max|x offset| + 2 around them
-// (see the window comment in vp_resident.cu); capped at nx.
-static void res_window_rows(const vp_plan* p, int Rc, bool adjoint, int* lo, int* n) {
-    const long long span = (long long)Rc + 2 * (p->mx_hi - p->mx_lo) + 2;
-    if (span >= p->nx) {
-        *lo = 0;
-        *n = p->nx;
-        return;
-    }
-    const long long l = adjoint ? -2 * p->mx_hi - 2 : 2 * p->mx_lo;
-    *lo = (int)(l % p->nx);
-    *n = (int)span;
-}
 
 static size_t fused_smem(const vp_plan* p, int R) {
     const size_t red = ((size_t)32 * R * real_size(p) + 15) & ~(size_t)15;
@@ -419,7 +420,8 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
         r.dv = (T)p->dv;
         r.dx = (T)p->dx;
         r.dtdv = (T)(p->dt / p->dv);
-        res_window_rows(p, r.Rc, false, &r.win_lo, &r.win_n);
+        res_halo_rows(p, &r.h_lo, &r.h_hi);
+        r.mx_lo = (int)p->mx_lo;
         VP_CUDA(launch_res_fwd<T>(r, p->feq2d != 0, p->res_cn, p->res_threads, p->res_smem, s),
                 "cluster-resident forward launch");
         return VP_OK;
@@ -562,7 +564,8 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
         r.dv = (T)p->dv;
         r.dx = (T)p->dx;
         r.neg_dt_dv = (T)(-p->dt / p->dv);
-        res_window_rows(p, r.Rc, true, &r.win_lo, &r.win_n);
+        res_halo_rows(p, &r.h_lo, &r.h_hi);
+        r.mx_lo = (int)p->mx_lo;
         VP_CUDA(launch_res_bwd<T>(r, p->feq2d != 0, p->res_cn, p->res_threads, p->res_smem, s),
                 "cluster-resident backward launch");
         return VP_OK;

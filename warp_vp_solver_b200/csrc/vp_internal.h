@@ -243,7 +243,8 @@ template <typename T> struct ResFwdArgs {
     VShift<T>* vsh_tape;    // v shifts for every step (or null)
     PoissonTables<T> P;
     T dv, dx, dtdv;
-    int win_lo, win_n;      // rows whose field a CTA needs: gr0 + win_lo .. + win_n - 1 (mod nx)
+    int h_lo, h_hi;         // halo rows kept below / above a CTA's own rows
+    int mx_lo;              // smallest unreduced x half-step offset (recovers signed offsets)
 };
 
 template <typename T> struct ResBwdArgs {
@@ -264,7 +265,8 @@ template <typename T> struct ResBwdArgs {
     T* g_H;
     PoissonTables<T> P;
     T dv, dx, neg_dt_dv;
-    int win_lo, win_n;      // rows whose grho a CTA needs: gr0 + win_lo .. + win_n - 1 (mod nx)
+    int h_lo, h_hi;         // halo rows kept below / above a CTA's own rows
+    int mx_lo;              // smallest unreduced x half-step offset (recovers signed offsets)
 };
 
 template <typename T>
@@ -273,7 +275,7 @@ cudaError_t launch_res_fwd(const ResFwdArgs<T>& a, bool feq2d, int cn, int threa
 template <typename T>
 cudaError_t launch_res_bwd(const ResBwdArgs<T>& a, bool feq2d, int cn, int threads, size_t smem,
                            cudaStream_t s);
-size_t res_smem_size(int nx, int nv, int Rc, size_t real_size);
+size_t res_smem_size(int nx, int nv, int Rc, int halo_rows, size_t real_size);
 template <typename T>
 int res_max_clusters(bool feq2d, int cn, int rc, int nv, size_t smem);
 bool res_rows_supported(int rc);

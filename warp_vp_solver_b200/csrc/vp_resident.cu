@@ -6,7 +6,7 @@
 // column j = t % NVP and the RPT consecutive rows g .. g+RPT-1 (g = c*RC + (t / NVP)*RPT) of that
 // column. As in the per-step streaming kernels, a thread computes a whole Strang step for its
 // rows from a window of the previous state: the x shift of column j is one number, so
-//   o = V(h) + [V(f_eq) - f_eq]    on rows g+2m .. g+2m+RPT+1   (h read from the owning CTAs)
+//   o = V(h) + [V(f_eq) - f_eq]    on rows g+2m .. g+2m+RPT+1   (own rows or the halo copy)
 //   d = X(o) + [X(f_eq) - f_eq]    on rows g+m  .. g+m+RPT      (= f_{n+1} - f_eq)
 //   h' = X(d) + [X(f_eq) - f_eq]   on rows g    .. g+RPT-1      (written to the own rows)
 // and the row sums of h' give rho. One hardware cluster barrier per time step (barrier.cluster
@@ -14,7 +14,7 @@
 // are double-buffered so that the next step never overwrites data another CTA may still read.
 // The adjoint mirrors it with gathers (V^T + rho^T, X^T, X^T, dE/dE_total row sums).
 //
-// Poisson is evaluated in every CTA for all rows as the equivalent real circulant product
+// Poisson is evaluated in every CTA, for its own and halo rows, as the equivalent real circulant product
 // E_i = sum_k c[(i-k) mod nx] rho_k with c = real(ifft(m)) built once per plan from the same
 // spectral multiplier as the FFT path (warp_vp_solver/poisson.py:34-69): nx^2 multiply-adds
 // spread over the CTA's threads with no block barrier inside, where an in-block FFT needs
@@ -32,42 +32,53 @@ namespace cg = cooperative_groups;
 
 namespace vpb {
 
-// Shared-memory layout: three RC x nv planes, seven nx vectors, nx v shifts, the f_eq row and
-// its first differences.
+// Halo rows. CTA c keeps, besides its own rows, the rows [gr0 - h_lo, gr0) and
+// [gr0 + RC, gr0 + RC + h_hi) (mod nx) of the state plane it reads in a step: the windows of the
+// forward (rows g + 2m .. g + 2m + RPT + 1) and of the adjoint (rows g - 2m - 2 .. g - 2m + RPT - 1)
+// for every column's x offset m in [mx_lo, mx_hi] lie inside. The halo is filled from the owning
+// CTAs once per step, right after the cluster barrier that publishes the plane (coalesced 16-byte
+// distributed-shared-memory loads), so that the step itself reads shared memory of its own CTA
+// only. Plane row l holds global row gr0 - h_lo + l (mod nx); the own rows are l in
+// [h_lo, h_lo + RC). The per-row field values and v shifts use the same local row index.
+
+// Shared-memory layout: two state planes of W = h_lo + RC + h_hi rows, the row-partial plane,
+// the nx vectors, the per-row field and v shifts of the W rows, the f_eq row and its first
+// differences.
 template <typename T> struct ResSmem {
     T* p0;
     T* p1;
     T* p2;           // row partials of the warps: [RC][NVP/32]
     T* vec0;         // nx: row sums of every CTA, gathered after the step's cluster barrier
     T* vec1;         // 2 x RC: this CTA's own row sums, step parity (read by the other CTAs)
-    T* circ;         // nx: c = real(ifft(m))
-    T* fld;          // nx: E (forward) or grho (adjoint), all rows
-    T* aux;          // nx: H (forward) or g_E (adjoint)
-    VShift<T>* vsh;  // nx: v shifts of the current step, all rows
+    T* circ2;        // 2 nx: c = real(ifft(m)) twice, so that c[(i - k) mod nx] = circ2[i - k + nx]
+    T* fld;          // W: E (forward) or grho (adjoint) of the local rows
+    T* aux;          // nx: H (forward) or g_E (adjoint), global row index
+    VShift<T>* vsh;  // W: v shifts of the current step, local rows
     double* feq;     // nv: the f_eq row (x-invariant f_eq)
     T* dfeq;         // nv: f_eq[j+1] - f_eq[j] rounded from float64 (periodic)
-    T* red;          // 32
     double* eep;     // 4 partial energies of the own rows (step s in slot s % 4; read by CTA 0)
     T* own;          // RC: accumulated g_H of the own rows (adjoint)
 };
 
 __host__ __device__ inline size_t res_align(size_t x) { return (x + 15) & ~(size_t)15; }
 
-__host__ __device__ inline size_t res_smem_bytes(int nx, int nv, int RC, size_t rs) {
+__host__ __device__ inline size_t res_smem_bytes(int nx, int nv, int RC, int W, size_t rs) {
     size_t b = 0;
-    b += res_align((size_t)RC * nv * rs) * 3;
-    b += res_align((size_t)nx * rs) * 5;
-    b += res_align((size_t)nx * (rs == 8 ? 16 : 8));
+    b += res_align((size_t)W * nv * rs) * 2;
+    b += res_align((size_t)RC * nv * rs);
+    b += res_align((size_t)nx * rs) * 3;
+    b += res_align((size_t)2 * nx * rs);
+    b += res_align((size_t)W * rs);
+    b += res_align((size_t)W * (rs == 8 ? 16 : 8));
     b += res_align((size_t)nv * 8);
     b += res_align((size_t)nv * rs);
-    b += res_align((size_t)32 * rs);
-    b += res_align((size_t)64 * 8);
+    b += res_align((size_t)4 * 8);
     b += res_align((size_t)RC * rs);
     return b;
 }
 
 template <typename T>
-__device__ ResSmem<T> res_carve(unsigned char* smem, int nx, int nv, int RC) {
+__device__ ResSmem<T> res_carve(unsigned char* smem, int nx, int nv, int RC, int W) {
     ResSmem<T> s;
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -75,21 +86,34 @@ __device__ ResSmem<T> res_carve(unsigned char* smem, int nx, int nv, int RC) {
         off += res_align(bytes);
         return p;
     };
-    s.p0 = reinterpret_cast<T*>(take((size_t)RC * nv * sizeof(T)));
-    s.p1 = reinterpret_cast<T*>(take((size_t)RC * nv * sizeof(T)));
+    s.p0 = reinterpret_cast<T*>(take((size_t)W * nv * sizeof(T)));
+    s.p1 = reinterpret_cast<T*>(take((size_t)W * nv * sizeof(T)));
     s.p2 = reinterpret_cast<T*>(take((size_t)RC * nv * sizeof(T)));
     s.vec0 = reinterpret_cast<T*>(take((size_t)nx * sizeof(T)));
     s.vec1 = reinterpret_cast<T*>(take((size_t)nx * sizeof(T)));
-    s.circ = reinterpret_cast<T*>(take((size_t)nx * sizeof(T)));
-    s.fld = reinterpret_cast<T*>(take((size_t)nx * sizeof(T)));
     s.aux = reinterpret_cast<T*>(take((size_t)nx * sizeof(T)));
-    s.vsh = reinterpret_cast<VShift<T>*>(take((size_t)nx * sizeof(VShift<T>)));
+    s.circ2 = reinterpret_cast<T*>(take((size_t)2 * nx * sizeof(T)));
+    s.fld = reinterpret_cast<T*>(take((size_t)W * sizeof(T)));
+    s.vsh = reinterpret_cast<VShift<T>*>(take((size_t)W * sizeof(VShift<T>)));
     s.feq = reinterpret_cast<double*>(take((size_t)nv * sizeof(double)));
     s.dfeq = reinterpret_cast<T*>(take((size_t)nv * sizeof(T)));
-    s.red = reinterpret_cast<T*>(take((size_t)32 * sizeof(T)));
-    s.eep = reinterpret_cast<double*>(take((size_t)64 * sizeof(double)));
+    s.eep = reinterpret_cast<double*>(take((size_t)4 * sizeof(double)));
     s.own = reinterpret_cast<T*>(take((size_t)RC * sizeof(T)));
     return s;
+}
+
+// Global row of local row l: gr0 - h_lo + l (mod nx).
+__device__ __forceinline__ int res_grow(int gr0, int h_lo, int l, int nx) {
+    int q = (gr0 - h_lo + l) % nx;
+    return q < 0 ? q + nx : q;
+}
+
+// Unreduced x offset of a column from its table entry m in [0, nx): the offset lies in
+// [mx_lo, mx_hi] with mx_hi - mx_lo < nx, so it is mx_lo + ((m - mx_lo) mod nx).
+__device__ __forceinline__ int res_signed(int m, int mx_lo, int nx) {
+    int r = (m - mx_lo) % nx;
+    r = r < 0 ? r + nx : r;
+    return mx_lo + r;
 }
 
 // v shift from the total field, with a cheap path for the common |shift| < nv case.
@@ -109,7 +133,7 @@ __device__ __forceinline__ VShift<T> res_vshift(T Et, T dtdv, int nv) {
 
 // V(f_eq) - f_eq at column j for a row with shift (m, t). For the usual sub-cell shifts
 // (m = 0, or m = nv-1 i.e. -1) it is t*D[j] or -(1-t)*D[j-1] with D the first differences of
-// f_eq rounded from float64; other shifts use the float64 values.
+// f_eq rounded from float64; other shifts use the float64 values. i: global row (x-dependent f_eq).
 template <typename T, bool FEQ2D>
 __device__ __forceinline__ T res_vcorr(const ResSmem<T>& S, const double* __restrict__ feq, int rs,
                                        int i, int j, int c0, int c1, const VShift<T> v, int nv) {
@@ -136,16 +160,6 @@ __device__ __forceinline__ double res_xcorr(const double* __restrict__ feq, int 
            t64 * (__ldg(feq + (size_t)q1 * rs + j) - fi);
 }
 
-// Row q (0 <= q < nx) of a plane distributed over the cluster with RC rows per CTA.
-template <typename T, int RC>
-__device__ __forceinline__ const T* res_row(cg::cluster_group& cl, const T* plane, int q, int nv,
-                                            int me) {
-    const int cta = q / RC;
-    const int l = q - cta * RC;
-    const T* base = (cta == me) ? plane : cl.map_shared_rank(plane, cta);
-    return base + l * nv;
-}
-
 // Split cluster barrier: arrive (release: this thread's earlier shared/global writes become
 // visible cluster-wide) ... wait (acquire). Work placed between the two overlaps the barrier;
 // the global writes of the outputs go there so the release does not wait for them.
@@ -154,6 +168,42 @@ __device__ __forceinline__ void cluster_arrive() {
 }
 __device__ __forceinline__ void cluster_wait() {
     asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+template <typename T> struct Vec16Of {
+    using type = float4;
+};
+template <> struct Vec16Of<double> {
+    using type = double2;
+};
+
+// Fills the halo rows of `plane` (this CTA's copy) from the owners' own rows of the same plane.
+template <typename T>
+__device__ __forceinline__ void res_fill_halo(cg::cluster_group& cluster, T* plane, int nx, int nv,
+                                              int RC, int gr0, int h_lo, int h_hi) {
+    const int nh = h_lo + h_hi;
+    if (nh == 0) return;
+    using V = typename Vec16Of<T>::type;
+    constexpr int VE = 16 / (int)sizeof(T);
+    if (nv % VE == 0) {
+        const int per = nv / VE;
+        for (int idx = threadIdx.x; idx < nh * per; idx += blockDim.x) {
+            const int h = idx / per, v = idx - h * per;
+            const int l = h < h_lo ? h : h + RC;
+            const int q = res_grow(gr0, h_lo, l, nx);
+            const int c = q / RC;
+            const V* src = reinterpret_cast<const V*>(cluster.map_shared_rank(plane, c) + (size_t)(h_lo + q - c * RC) * nv);
+            reinterpret_cast<V*>(plane + (size_t)l * nv)[v] = src[v];
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < nh * nv; idx += blockDim.x) {
+            const int h = idx / nv, v = idx - h * nv;
+            const int l = h < h_lo ? h : h + RC;
+            const int q = res_grow(gr0, h_lo, l, nx);
+            const int c = q / RC;
+            plane[(size_t)l * nv + v] = cluster.map_shared_rank(plane, c)[(size_t)(h_lo + q - c * RC) * nv + v];
+        }
+    }
 }
 
 // Row sums in three fixed-order stages. (1) Each warp reduces its RPT rows over its 32 columns
@@ -210,11 +260,11 @@ __device__ __forceinline__ void res_rows_gather(cg::cluster_group& cluster, T* o
     }
 }
 
-// out[i] = sum_k c[(i-k) mod nx] x[k] (adjoint: c[(k-i) mod nx]) for the n_rows rows
-// i = (first + r) mod nx, r < n_rows; a power-of-two group of tpr lanes per row. Starts and ends
-// with a block barrier.
+// out[r] = sum_k c[(i-k) mod nx] x[k] (adjoint: c[(k-i) mod nx]) for the n_rows rows
+// i = (first + r) mod nx, r < n_rows; a power-of-two group of tpr lanes per row, lane g summing
+// k = g, g + tpr, ... in order, then an xor tree. Starts and ends with a block barrier.
 template <typename T>
-__device__ __forceinline__ void res_circ_rows(const T* circ, const T* x, T* out, int nx, int first,
+__device__ __forceinline__ void res_circ_rows(const T* circ2, const T* x, T* out, int nx, int first,
                                               int n_rows, bool adjoint) {
     __syncthreads();
     int tpr = 32;
@@ -224,17 +274,22 @@ __device__ __forceinline__ void res_circ_rows(const T* circ, const T* x, T* out,
     const int passes = (n_rows + rows_per_pass - 1) / rows_per_pass;
     for (int p = 0; p < passes; ++p) {
         const int r = p * rows_per_pass + (int)threadIdx.x / tpr;
-        const int i = wrap1(first + (r < n_rows ? r : 0), nx);
+        int i = (first + (r < n_rows ? r : 0)) % nx;
         T s = T(0);
         if (r < n_rows) {
+            // c[(i - k) mod nx] = circ2[nx + i - k]; c[(k - i) mod nx] = circ2[nx - i + k]
+            const T* cp = adjoint ? circ2 + nx - i + g : circ2 + nx + i - g;
+            const int cs = adjoint ? tpr : -tpr;
+            const T* xp = x + g;
+#pragma unroll 8
             for (int k = g; k < nx; k += tpr) {
-                int d = adjoint ? (k - i) : (i - k);
-                d = wrapneg(d, nx);
-                s += circ[d] * x[k];
+                s += *cp * *xp;
+                cp += cs;
+                xp += tpr;
             }
         }
         for (int o = tpr >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (r < n_rows && g == 0) out[i] = s;
+        if (r < n_rows && g == 0) out[r] = s;
     }
     __syncthreads();
 }
@@ -242,7 +297,11 @@ __device__ __forceinline__ void res_circ_rows(const T* circ, const T* x, T* out,
 template <typename T>
 __device__ void res_init_tables(ResSmem<T>& S, const PoissonTables<T>& P, const double* feq,
                                 bool feq2d, int nx, int nv) {
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) S.circ[i] = __ldg(P.circ + i);
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        const T c = __ldg(P.circ + i);
+        S.circ2[i] = c;
+        S.circ2[i + nx] = c;
+    }
     if (!feq2d) {
         for (int j = threadIdx.x; j < nv; j += blockDim.x) {
             const double f = __ldg(feq + j);
@@ -256,15 +315,16 @@ __device__ void res_init_tables(ResSmem<T>& S, const PoissonTables<T>& P, const 
 // Forward
 // ---------------------------------------------------------------------------------------------
 
-// Poisson for step k on the rows this CTA's windows touch and their v shifts, from the row sums
-// of h_k published in slot `par` of every CTA. CTA 0 also sums the partial energies of step k - 2
-// (published by the barrier before this call) into ee_hist[k - 2]; the remote reads go here, next
-// to the row-sum gather, because the other CTAs are all between the same two barriers. Ends with
-// a block barrier.
+// Field of step k: fills the halo of `plane` (holding h_k), gathers the row sums of h_k published
+// in slot `par` of every CTA into rho, evaluates Poisson on the W local rows and their v shifts.
+// CTA 0 also sums the partial energies of step k - 2 (published by the barrier before this call)
+// into ee_hist[k - 2]; the remote reads go here, with the other exchanges of the step, because
+// every CTA is between the same two barriers. Ends with a block barrier.
 template <typename T>
-__device__ void res_fwd_field(const ResFwdArgs<T>& a, ResSmem<T>& S, cg::cluster_group& cluster, int par,
-                              int gr0, int RC, int k, int me, int CN) {
+__device__ void res_fwd_field(const ResFwdArgs<T>& a, ResSmem<T>& S, cg::cluster_group& cluster, T* plane,
+                              int par, int gr0, int RC, int k, int me, int CN) {
     const int nx = a.nx, nv = a.nv;
+    const int W = a.h_lo + RC + a.h_hi;
     if (me == 0 && k >= 2 && a.ee_hist != nullptr && threadIdx.x < 32) {
         const int lane = threadIdx.x;
         const double v = lane < CN ? cluster.map_shared_rank(S.eep, lane)[(k - 2) & 3] : 0.0;
@@ -272,21 +332,18 @@ __device__ void res_fwd_field(const ResFwdArgs<T>& a, ResSmem<T>& S, cg::cluster
         for (int c = 0; c < CN; ++c) tot += __shfl_sync(0xffffffffu, v, c);
         if (lane == 0) a.ee_hist[k - 2] = (T)(0.5 * tot * (double)a.dx);
     }
-    T* rho_sum = S.vec0;
-    res_rows_gather<T>(cluster, S.vec1, par, rho_sum, nx, RC, -a.dv);   // rho
-    const int first = ((gr0 + a.win_lo) % nx + nx) % nx;
-    res_circ_rows<T>(S.circ, rho_sum, S.fld, nx, first, a.win_n, false);
-    for (int r = threadIdx.x; r < a.win_n; r += blockDim.x) {
-        const int i = wrap1(first + r, nx);
-        S.vsh[i] = res_vshift<T>(S.fld[i] + S.aux[i], a.dtdv, nv);
-    }
+    res_fill_halo<T>(cluster, plane, nx, nv, RC, gr0, a.h_lo, a.h_hi);
+    res_rows_gather<T>(cluster, S.vec1, par, S.vec0, nx, RC, -a.dv);   // rho
+    const int first = res_grow(gr0, a.h_lo, 0, nx);
+    res_circ_rows<T>(S.circ2, S.vec0, S.fld, nx, first, W, false);
+    for (int l = threadIdx.x; l < W; l += blockDim.x)
+        S.vsh[l] = res_vshift<T>(S.fld[l] + S.aux[res_grow(gr0, a.h_lo, l, nx)], a.dtdv, nv);
     __syncthreads();
 }
 
-// One warp, for step s (the field in S.fld/S.aux is E_s for the own rows): E_hist, E_tape and
-// vsh_tape of the own rows, and the partial energy of the own rows into its slot s % 4 (the next
-// cluster barrier publishes it; CTA 0 sums the partials in the field of step s + 2). Runs between a cluster arrive and wait, off the
-// step's critical path.
+// One warp, for step s (S.fld holds E_s): E_hist, E_tape and vsh_tape of the own rows, and the
+// partial energy of the own rows into its slot s % 4 (the next cluster barrier publishes it; CTA 0
+// sums the partials in the field of step s + 2). Runs between a cluster arrive and wait.
 template <typename T>
 __device__ void res_fwd_outputs(const ResFwdArgs<T>& a, ResSmem<T>& S, int s, int gr0, int RC) {
     const int nx = a.nx, nv = a.nv;
@@ -294,7 +351,7 @@ __device__ void res_fwd_outputs(const ResFwdArgs<T>& a, ResSmem<T>& S, int s, in
     double e2 = 0.0;
     for (int r = lane; r < RC; r += 32) {
         const int i = gr0 + r;
-        const T E = S.fld[i];
+        const T E = S.fld[a.h_lo + r];
         const T Et = E + S.aux[i];
         if (a.E_hist != nullptr) a.E_hist[(size_t)s * nx + i] = Et;
         if (a.E_tape != nullptr) a.E_tape[(size_t)s * nx + i] = E;
@@ -313,6 +370,7 @@ __global__ void __launch_bounds__(1024) vp_res_fwd_kernel(const ResFwdArgs<T> a)
     const int me = (int)cluster.block_rank();
     const int CN = (int)cluster.num_blocks();
     const int gr0 = me * RC;
+    const int hl = a.h_lo;
     constexpr int G = RC / RPT;
     const int NVP = blockDim.x / G;
     const int j = threadIdx.x % NVP;
@@ -321,18 +379,19 @@ __global__ void __launch_bounds__(1024) vp_res_fwd_kernel(const ResFwdArgs<T> a)
     const bool colv = j < nv;
     const int cw = j >> 5, ncw = NVP >> 5;      // warp column group, groups per row
     const bool out_warp = (int)(threadIdx.x >> 5) == (int)(blockDim.x >> 5) - 1;
-    ResSmem<T> S = res_carve<T>(smem, nx, nv, RC);
-    T* Hb[2] = {S.p0, S.p1};   // h of even / odd steps, own rows (read remotely)
+    ResSmem<T> S = res_carve<T>(smem, nx, nv, RC, hl + RC + a.h_hi);
+    T* Hb[2] = {S.p0, S.p1};   // h of even / odd steps, local rows (own rows read remotely)
     T* red = S.p2;             // row partials of the warps
     res_init_tables<T>(S, a.P, a.feq, FEQ2D, nx, nv);
     for (int i = threadIdx.x; i < nx; i += blockDim.x) S.aux[i] = __ldg(a.H + i);
 
     // per-column constants of the x half-step
-    int m = 0;
+    int m = 0, sm = 0;
     T t = T(0), wj = T(0);
     double t64 = 0.0, feq_j = 0.0;
     if (colv) {
         m = __ldg(a.mx + j);
+        sm = res_signed(m, a.mx_lo, nx);
         t = __ldg(a.tx + j);
         t64 = __ldg(a.tx64 + j);
         wj = trap_w<T>(j, nv);
@@ -346,30 +405,30 @@ __global__ void __launch_bounds__(1024) vp_res_fwd_kernel(const ResFwdArgs<T> a)
 #pragma unroll
         for (int k = 0; k < RPT; ++k) wv[k] = T(0);
         if (colv) {
-        T d[RPT + 1];
-        const int base = wrap1(g + m, nx);
+            T d[RPT + 1];
+            const int base = wrap1(g + m, nx);
 #pragma unroll
-        for (int k = 0; k <= RPT; ++k) {
-            const int q = wrap1(base + k, nx);
-            const double fe = FEQ2D ? __ldg(a.feq + (size_t)q * a.feq_rs + j) : feq_j;
-            d[k] = (T)(__ldg(a.f_iv + (size_t)q * nv + j) - fe);
-        }
+            for (int k = 0; k <= RPT; ++k) {
+                const int q = wrap1(base + k, nx);
+                const double fe = FEQ2D ? __ldg(a.feq + (size_t)q * a.feq_rs + j) : feq_j;
+                d[k] = (T)(__ldg(a.f_iv + (size_t)q * nv + j) - fe);
+            }
 #pragma unroll
-        for (int k = 0; k < RPT; ++k) {
-            const int i = g + k;
-            T h = lerp(d[k], d[k + 1], t);
-            if (FEQ2D) h += (T)res_xcorr(a.feq, a.feq_rs, nx, i, m, t64, j);
-            Hb[0][(size_t)(rt + k) * nv + j] = h;
-            wv[k] = wj * h;
-            if (a.h_tape != nullptr) a.h_tape[(size_t)i * nv + j] = h;
-        }
+            for (int k = 0; k < RPT; ++k) {
+                const int i = g + k;
+                T h = lerp(d[k], d[k + 1], t);
+                if (FEQ2D) h += (T)res_xcorr(a.feq, a.feq_rs, nx, i, m, t64, j);
+                Hb[0][(size_t)(hl + rt + k) * nv + j] = h;
+                wv[k] = wj * h;
+                if (a.h_tape != nullptr) a.h_tape[(size_t)i * nv + j] = h;
+            }
         }
         res_warp_rows<T, RPT>(wv, red, rt, cw, ncw);
     }
     __syncthreads();
     res_rows_local<T>(red, S.vec1, ncw, RC);
     cluster.sync();
-    res_fwd_field<T>(a, S, cluster, 0, gr0, RC, 0, me, CN);
+    res_fwd_field<T>(a, S, cluster, Hb[0], 0, gr0, RC, 0, me, CN);
 
     for (int n = 0; n < a.n_steps; ++n) {
         const T* cur = Hb[n & 1];
@@ -382,30 +441,18 @@ __global__ void __launch_bounds__(1024) vp_res_fwd_kernel(const ResFwdArgs<T> a)
         for (int k = 0; k < RPT; ++k) wv[k] = T(0);
         int dq = 0;
         if (colv) {
-            // o on rows g+2m .. g+2m+RPT+1 (h of those rows, from the owning CTAs)
+            // o on rows g+2m .. g+2m+RPT+1: local rows l0 .. l0+RPT+1 (own or halo)
             T o[RPT + 2];
-            const int q0 = wrap2(g + 2 * m, nx);
-            if (q0 >= gr0 && q0 + RPT + 1 < gr0 + RC) {
-                // the whole window lies in this CTA: plain shared-memory loads
+            const int l0 = hl + rt + 2 * sm;
 #pragma unroll
-                for (int k = 0; k < RPT + 2; ++k) {
-                    const int q = q0 + k;
-                    const VShift<T> v = S.vsh[q];
-                    const T* hr = cur + (q - gr0) * nv;
-                    const int c0 = wrap1(j + v.m, nv);
-                    const int c1 = c0 + 1 == nv ? 0 : c0 + 1;
-                    o[k] = lerp(hr[c0], hr[c1], v.t) + res_vcorr<T, FEQ2D>(S, a.feq, a.feq_rs, q, j, c0, c1, v, nv);
-                }
-            } else {
-#pragma unroll
-                for (int k = 0; k < RPT + 2; ++k) {
-                    const int q = wrap1(q0 + k, nx);
-                    const VShift<T> v = S.vsh[q];
-                    const T* hr = res_row<T, RC>(cluster, cur, q, nv, me);
-                    const int c0 = wrap1(j + v.m, nv);
-                    const int c1 = c0 + 1 == nv ? 0 : c0 + 1;
-                    o[k] = lerp(hr[c0], hr[c1], v.t) + res_vcorr<T, FEQ2D>(S, a.feq, a.feq_rs, q, j, c0, c1, v, nv);
-                }
+            for (int k = 0; k < RPT + 2; ++k) {
+                const int l = l0 + k;
+                const VShift<T> v = S.vsh[l];
+                const T* hr = cur + (size_t)l * nv;
+                const int c0 = wrap1(j + v.m, nv);
+                const int c1 = c0 + 1 == nv ? 0 : c0 + 1;
+                const int q = FEQ2D ? res_grow(gr0, hl, l, nx) : 0;
+                o[k] = lerp(hr[c0], hr[c1], v.t) + res_vcorr<T, FEQ2D>(S, a.feq, a.feq_rs, q, j, c0, c1, v, nv);
             }
             // d on rows g+m .. g+m+RPT (= f_{n+1} - f_eq)
             dq = wrap1(g + m, nx);
@@ -420,7 +467,7 @@ __global__ void __launch_bounds__(1024) vp_res_fwd_kernel(const ResFwdArgs<T> a)
                     T h = lerp(d[k], d[k + 1], t);
                     if (FEQ2D) h += (T)res_xcorr(a.feq, a.feq_rs, nx, g + k, m, t64, j);
                     hv[k] = h;
-                    nxt[(rt + k) * nv + j] = h;
+                    nxt[(size_t)(hl + rt + k) * nv + j] = h;
                     wv[k] = wj * h;
                 }
             }
@@ -451,7 +498,7 @@ __global__ void __launch_bounds__(1024) vp_res_fwd_kernel(const ResFwdArgs<T> a)
         }
         if (out_warp) res_fwd_outputs<T>(a, S, n, gr0, RC);
         cluster_wait();
-        if (!last) res_fwd_field<T>(a, S, cluster, par, gr0, RC, n + 1, me, CN);
+        if (!last) res_fwd_field<T>(a, S, cluster, nxt, par, gr0, RC, n + 1, me, CN);
     }
     // energies of the last two steps (their partials are published by this barrier); the second
     // barrier keeps every CTA's shared memory alive until CTA 0 has read it
@@ -471,7 +518,7 @@ __global__ void __launch_bounds__(1024) vp_res_fwd_kernel(const ResFwdArgs<T> a)
 // ---------------------------------------------------------------------------------------------
 
 // Tape values that the adjoint field of step s reads, loaded into registers ahead of their use:
-// g_E_hist and E_tape of row threadIdx.x and the v shift of window row threadIdx.x. Rows beyond
+// g_E_hist and E_tape of row threadIdx.x and the v shift of local row threadIdx.x. Rows beyond
 // blockDim.x are read in the field itself.
 template <typename T> struct ResBwdPre {
     T gEh, Etp, gee;
@@ -479,7 +526,7 @@ template <typename T> struct ResBwdPre {
 };
 
 template <typename T>
-__device__ __forceinline__ ResBwdPre<T> res_bwd_prefetch(const ResBwdArgs<T>& a, int s, int first) {
+__device__ __forceinline__ ResBwdPre<T> res_bwd_prefetch(const ResBwdArgs<T>& a, int s, int gr0, int W) {
     const int nx = a.nx, i = threadIdx.x;
     ResBwdPre<T> p;
     p.gee = a.g_ee != nullptr ? __ldg(a.g_ee + s) : T(0);
@@ -487,20 +534,23 @@ __device__ __forceinline__ ResBwdPre<T> res_bwd_prefetch(const ResBwdArgs<T>& a,
     p.Etp = i < nx ? __ldg(a.E_tape + (size_t)s * nx + i) : T(0);
     p.vs.m = 0;
     p.vs.t = T(0);
-    if (i < a.win_n) p.vs = a.vsh_tape[(size_t)s * nx + wrap1(first + i, nx)];
+    if (i < W) p.vs = a.vsh_tape[(size_t)s * nx + res_grow(gr0, a.h_lo, i, nx)];
     return p;
 }
 
-// Tail of the adjoint for step s (every CTA, all rows): g_E_total = -dt/dv * rowsum + g_E_hist[s];
-// g_H += g_E_total (own rows); g_E = g_E_total + ee^T; grho = Poisson^T(g_E) (all rows); the v
-// shifts of step s (all rows). `pre` holds this thread's tape values of step s.
+// Tail of the adjoint for step s (every CTA): fills the halo of `plane` (holding w_s), gathers the
+// row sums published in slot `par`; g_E_total = -dt/dv * rowsum + g_E_hist[s]; g_H += g_E_total
+// (own rows); g_E = g_E_total + ee^T; grho = Poisson^T(g_E) and the v shifts of step s on the W
+// local rows. `pre` holds this thread's tape values of step s.
 template <typename T>
-__device__ void res_bwd_field(const ResBwdArgs<T>& a, ResSmem<T>& S, cg::cluster_group& cluster, int par,
-                              int s, int gr0, int RC, const ResBwdPre<T>& pre) {
+__device__ void res_bwd_field(const ResBwdArgs<T>& a, ResSmem<T>& S, cg::cluster_group& cluster, T* plane,
+                              int par, int s, int gr0, int RC, const ResBwdPre<T>& pre) {
     const int nx = a.nx;
+    const int W = a.h_lo + RC + a.h_hi;
+    const int me_i = threadIdx.x;
+    res_fill_halo<T>(cluster, plane, nx, a.nv, RC, gr0, a.h_lo, a.h_hi);
     T* sums = S.vec0;
     res_rows_gather<T>(cluster, S.vec1, par, sums, nx, RC, T(1));
-    const int me_i = threadIdx.x;
     const T gee = pre.gee;
     for (int i = threadIdx.x; i < nx; i += blockDim.x) {
         const bool own = i == me_i;
@@ -510,12 +560,9 @@ __device__ void res_bwd_field(const ResBwdArgs<T>& a, ResSmem<T>& S, cg::cluster
         const T Et = own ? pre.Etp : __ldg(a.E_tape + (size_t)s * nx + i);
         S.aux[i] = gEt + a.dx * trap_w<T>(i, nx) * Et * gee;
     }
-    const int first = ((gr0 + a.win_lo) % nx + nx) % nx;
-    for (int r = threadIdx.x; r < a.win_n; r += blockDim.x) {
-        const int i = wrap1(first + r, nx);
-        S.vsh[i] = r == me_i ? pre.vs : a.vsh_tape[(size_t)s * nx + i];
-    }
-    res_circ_rows<T>(S.circ, S.aux, S.fld, nx, first, a.win_n, true);
+    for (int l = threadIdx.x; l < W; l += blockDim.x)
+        S.vsh[l] = l == me_i ? pre.vs : a.vsh_tape[(size_t)s * nx + res_grow(gr0, a.h_lo, l, nx)];
+    res_circ_rows<T>(S.circ2, S.aux, S.fld, nx, res_grow(gr0, a.h_lo, 0, nx), W, true);
 }
 
 // Slope inputs of step np at the own rows g .. g+RPT-1, column j: the v shifts of those rows
@@ -554,11 +601,12 @@ __device__ __forceinline__ void res_bwd_load_h(const ResBwdArgs<T>& a, int np, i
     }
 }
 
-// w on the own rows g .. g+RPT-1 from c on rows g-m-1 .. g-m+RPT-1 (held in registers), and the
-// slope * w products for the dE row sums (slope inputs of step np from res_bwd_load_*).
+// w on the own rows g .. g+RPT-1 (stored at own_rows, the plane's first own row) from c on rows
+// g-m-1 .. g-m+RPT-1 (held in registers), and the slope * w products for the dE row sums (slope
+// inputs of step np from res_bwd_load_*).
 template <typename T, int RPT, bool FEQ2D>
 __device__ __forceinline__ void res_bwd_w(const ResBwdArgs<T>& a, const ResSmem<T>& S,
-                                          const T (&c)[RPT + 1], T* nxt, T (&prod)[RPT],
+                                          const T (&c)[RPT + 1], T* own_rows, T (&prod)[RPT],
                                           const VShift<T> (&vs)[RPT], const T (&h0)[RPT],
                                           const T (&h1)[RPT], int g, int rt, int j, T t) {
     const int nv = a.nv;
@@ -566,7 +614,7 @@ __device__ __forceinline__ void res_bwd_w(const ResBwdArgs<T>& a, const ResSmem<
     for (int k = 0; k < RPT; ++k) {
         const int i = g + k;
         const T wv = lerp(c[k + 1], c[k], t);
-        nxt[(size_t)(rt + k) * nv + j] = wv;
+        own_rows[(size_t)(rt + k) * nv + j] = wv;
         const int d0 = wrap1(j + vs[k].m, nv);
         const int d1 = d0 + 1 == nv ? 0 : d0 + 1;
         T sl = h1[k] - h0[k];
@@ -586,6 +634,8 @@ __global__ void __launch_bounds__(1024) vp_res_bwd_kernel(const ResBwdArgs<T> a)
     const int me = (int)cluster.block_rank();
     const int CN = (int)cluster.num_blocks();
     const int gr0 = me * RC;
+    const int hl = a.h_lo;
+    const int W = hl + RC + a.h_hi;
     constexpr int G = RC / RPT;
     const int NVP = blockDim.x / G;
     const int j = threadIdx.x % NVP;
@@ -593,23 +643,23 @@ __global__ void __launch_bounds__(1024) vp_res_bwd_kernel(const ResBwdArgs<T> a)
     const int g = gr0 + rt;
     const bool colv = j < nv;
     const int cw = j >> 5, ncw = NVP >> 5;
-    const int first = ((gr0 + a.win_lo) % nx + nx) % nx;
-    ResSmem<T> S = res_carve<T>(smem, nx, nv, RC);
-    T* Wb[2] = {S.p0, S.p1};   // cotangent on the v-step output of even / odd steps, own rows
+    ResSmem<T> S = res_carve<T>(smem, nx, nv, RC, W);
+    T* Wb[2] = {S.p0, S.p1};   // cotangent on the v-step output of even / odd steps, local rows
     T* red = S.p2;             // row partials of the warps
     res_init_tables<T>(S, a.P, a.feq, FEQ2D, nx, nv);
     for (int r = threadIdx.x; r < RC; r += blockDim.x) S.own[r] = T(0);
-    int m = 0;
+    int m = 0, sm = 0;
     T t = T(0), wr = T(0);
     if (colv) {
         m = __ldg(a.mx + j);
+        sm = res_signed(m, a.mx_lo, nx);
         t = __ldg(a.tx + j);
         wr = -a.dv * trap_w<T>(j, nv);   // rho^T weight (warp_vp_solver/kernels.py:292-299)
     }
     // slope inputs: vA/hA of the step whose slopes come next, vB the shifts of the step after it
     VShift<T> vA[RPT], vB[RPT];
     T hA0[RPT], hA1[RPT];
-    ResBwdPre<T> pre = res_bwd_prefetch<T>(a, T_steps - 1, first);
+    ResBwdPre<T> pre = res_bwd_prefetch<T>(a, T_steps - 1, gr0, W);
     if (colv) {
         res_bwd_load_shifts<T, RPT>(a, T_steps - 1, g, vA);
         res_bwd_load_h<T, RPT>(a, T_steps - 1, g, j, vA, hA0, hA1);
@@ -635,7 +685,7 @@ __global__ void __launch_bounds__(1024) vp_res_bwd_kernel(const ResBwdArgs<T> a)
                 if (a.g_fh != nullptr) v += __ldg(a.g_fh + ((size_t)(T_steps - 1) * nx + q) * nv + j);
                 c[k] = v;
             }
-            res_bwd_w<T, RPT, FEQ2D>(a, S, c, nxt, prod, vA, hA0, hA1, g, rt, j, t);
+            res_bwd_w<T, RPT, FEQ2D>(a, S, c, nxt + (size_t)hl * nv, prod, vA, hA0, hA1, g, rt, j, t);
             // next: slopes of step T-2
 #pragma unroll
             for (int k = 0; k < RPT; ++k) vA[k] = vB[k];
@@ -647,46 +697,30 @@ __global__ void __launch_bounds__(1024) vp_res_bwd_kernel(const ResBwdArgs<T> a)
         const int par = (T_steps - 1) & 1;
         res_rows_local<T>(red, S.vec1 + par * RC, ncw, RC);
         cluster.sync();
-        res_bwd_field<T>(a, S, cluster, par, T_steps - 1, gr0, RC, pre);
+        res_bwd_field<T>(a, S, cluster, nxt, par, T_steps - 1, gr0, RC, pre);
     }
 
     for (int n = T_steps - 1; n >= 0; --n) {
         const T* cur = Wb[n & 1];
         T* nxt = Wb[(n + 1) & 1];   // == Wb[(n-1) & 1]
-        if (n > 0) pre = res_bwd_prefetch<T>(a, n - 1, first);
+        if (n > 0) pre = res_bwd_prefetch<T>(a, n - 1, gr0, W);
         T prod[RPT];
 #pragma unroll
         for (int k = 0; k < RPT; ++k) prod[k] = T(0);
         if (colv) {
-            // gh = V^T(w_n) + rho^T(grho_n) on rows g-2m-2 .. g-2m+RPT-1 (w read from the owners)
+            // gh = V^T(w_n) + rho^T(grho_n) on rows g-2m-2 .. g-2m+RPT-1 (n = 0: g-m-1 ..), local rows
             const int ng = n == 0 ? RPT + 1 : RPT + 2;   // rows of gh needed
             T gh[RPT + 2];
-            int base = (g - (n == 0 ? 1 : 2) * m - (n == 0 ? 1 : 2)) % nx;
-            base = wrapneg(base, nx);
-            if (base >= gr0 && base + RPT + 1 < gr0 + RC) {
-                // the whole window lies in this CTA: plain shared-memory loads
+            const int l0 = n == 0 ? hl + rt - sm - 1 : hl + rt - 2 * sm - 2;
 #pragma unroll
-                for (int k = 0; k < RPT + 2; ++k) {
-                    if (k < ng) {
-                        const int q = base + k;
-                        const VShift<T> v = S.vsh[q];
-                        const T* wrow = cur + (q - gr0) * nv;
-                        const int c0 = wrapneg(j - v.m, nv);
-                        const int c1 = wrapneg(c0 - 1, nv);
-                        gh[k] = lerp(wrow[c0], wrow[c1], v.t) + wr * S.fld[q];
-                    }
-                }
-            } else {
-#pragma unroll
-                for (int k = 0; k < RPT + 2; ++k) {
-                    if (k < ng) {
-                        const int q = wrap1(base + k, nx);
-                        const VShift<T> v = S.vsh[q];
-                        const T* wrow = res_row<T, RC>(cluster, cur, q, nv, me);
-                        const int c0 = wrapneg(j - v.m, nv);
-                        const int c1 = wrapneg(c0 - 1, nv);
-                        gh[k] = lerp(wrow[c0], wrow[c1], v.t) + wr * S.fld[q];
-                    }
+            for (int k = 0; k < RPT + 2; ++k) {
+                if (k < ng) {
+                    const int l = l0 + k;
+                    const VShift<T> v = S.vsh[l];
+                    const T* wrow = cur + (size_t)l * nv;
+                    const int c0 = wrapneg(j - v.m, nv);
+                    const int c1 = wrapneg(c0 - 1, nv);
+                    gh[k] = lerp(wrow[c0], wrow[c1], v.t) + wr * S.fld[l];
                 }
             }
             if (n == 0) {
@@ -704,7 +738,7 @@ __global__ void __launch_bounds__(1024) vp_res_bwd_kernel(const ResBwdArgs<T> a)
                     if (a.g_fh != nullptr)
                         c[k] += __ldg(a.g_fh + ((size_t)(n - 1) * nx + wrap1(cb + k, nx)) * nv + j);
                 }
-                res_bwd_w<T, RPT, FEQ2D>(a, S, c, nxt, prod, vA, hA0, hA1, g, rt, j, t);
+                res_bwd_w<T, RPT, FEQ2D>(a, S, c, nxt + (size_t)hl * nv, prod, vA, hA0, hA1, g, rt, j, t);
                 // next: slopes of step n-2 (h loads now, shifts of step n-3 for the one after)
 #pragma unroll
                 for (int k = 0; k < RPT; ++k) vA[k] = vB[k];
@@ -720,9 +754,10 @@ __global__ void __launch_bounds__(1024) vp_res_bwd_kernel(const ResBwdArgs<T> a)
         }
         cluster_arrive();
         cluster_wait();
-        if (n > 0) res_bwd_field<T>(a, S, cluster, par, n - 1, gr0, RC, pre);
+        if (n > 0) res_bwd_field<T>(a, S, cluster, nxt, par, n - 1, gr0, RC, pre);
     }
     for (int r = threadIdx.x; r < RC; r += blockDim.x) a.g_H[gr0 + r] = S.own[r];
+    // no other CTA reads this CTA's shared memory after the last barrier
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -840,8 +875,8 @@ cudaError_t launch_res_bwd(const ResBwdArgs<T>& a, bool feq2d, int cn, int threa
     return cudaErrorInvalidValue;
 }
 
-size_t res_smem_size(int nx, int nv, int Rc, size_t real_size) {
-    return res_smem_bytes(nx, nv, Rc, real_size);
+size_t res_smem_size(int nx, int nv, int Rc, int halo_rows, size_t real_size) {
+    return res_smem_bytes(nx, nv, Rc, Rc + halo_rows, real_size);
 }
 
 template int res_max_clusters<float>(bool, int, int, int, size_t);
