@@ -191,6 +191,7 @@ static size_t res_config_ok(const vp_plan* p, int cn) {
     if (p->mx_lo < -p->nx || p->mx_hi > p->nx || p->mx_hi - p->mx_lo >= p->nx / 2) return 0;
     int hlo = 0, hhi = 0;
     res_halo_rows(p, &hlo, &hhi);
+    if (hlo + hhi >= p->nx) return 0;   // local rows of a CTA span less than two periods
     const size_t smem = res_smem_size(p->nx, p->nv, Rc, hlo + hhi, real_size(p));
     if (smem > kMaxSmemPerCta) return 0;
     if (res_threads(Rc, p->nv) > 1024) return 0;

@@ -102,10 +102,13 @@ __device__ ResSmem<T> res_carve(unsigned char* smem, int nx, int nv, int RC, int
     return s;
 }
 
-// Global row of local row l: gr0 - h_lo + l (mod nx).
+// Global row of local row l: gr0 - h_lo + l (mod nx). The halo is shorter than nx in total, so
+// gr0 - h_lo + l lies in [-nx, 2nx) and one conditional correction suffices (no division: integer
+// division by a runtime value costs tens of instructions, and these helpers run every step).
 __device__ __forceinline__ int res_grow(int gr0, int h_lo, int l, int nx) {
-    int q = (gr0 - h_lo + l) % nx;
-    return q < 0 ? q + nx : q;
+    int q = gr0 - h_lo + l;
+    q += q < 0 ? nx : 0;
+    return q >= nx ? q - nx : q;
 }
 
 // Unreduced x offset of a column from its table entry m in [0, nx): the offset lies in
@@ -177,31 +180,25 @@ template <> struct Vec16Of<double> {
     using type = double2;
 };
 
-// Fills the halo rows of `plane` (this CTA's copy) from the owners' own rows of the same plane.
-template <typename T>
+// Fills the halo rows of `plane` (this CTA's copy) from the owners' own rows of the same plane:
+// one row per warp at a time, 16-byte loads when a row is a whole number of them.
+template <typename T, int RC>
 __device__ __forceinline__ void res_fill_halo(cg::cluster_group& cluster, T* plane, int nx, int nv,
-                                              int RC, int gr0, int h_lo, int h_hi) {
+                                              int gr0, int h_lo, int h_hi) {
     const int nh = h_lo + h_hi;
-    if (nh == 0) return;
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     using V = typename Vec16Of<T>::type;
     constexpr int VE = 16 / (int)sizeof(T);
-    if (nv % VE == 0) {
-        const int per = nv / VE;
-        for (int idx = threadIdx.x; idx < nh * per; idx += blockDim.x) {
-            const int h = idx / per, v = idx - h * per;
-            const int l = h < h_lo ? h : h + RC;
-            const int q = res_grow(gr0, h_lo, l, nx);
-            const int c = q / RC;
-            const V* src = reinterpret_cast<const V*>(cluster.map_shared_rank(plane, c) + (size_t)(h_lo + q - c * RC) * nv);
-            reinterpret_cast<V*>(plane + (size_t)l * nv)[v] = src[v];
-        }
-    } else {
-        for (int idx = threadIdx.x; idx < nh * nv; idx += blockDim.x) {
-            const int h = idx / nv, v = idx - h * nv;
-            const int l = h < h_lo ? h : h + RC;
-            const int q = res_grow(gr0, h_lo, l, nx);
-            const int c = q / RC;
-            plane[(size_t)l * nv + v] = cluster.map_shared_rank(plane, c)[(size_t)(h_lo + q - c * RC) * nv + v];
+    for (int h = (int)(threadIdx.x >> 5); h < nh; h += nw) {
+        const int l = h < h_lo ? h : h + RC;
+        const int q = res_grow(gr0, h_lo, l, nx);
+        const int c = q / RC;   // RC is a power of two known at compile time
+        const T* src = cluster.map_shared_rank(plane, c) + (size_t)(h_lo + q - c * RC) * nv;
+        T* dst = plane + (size_t)l * nv;
+        if (nv % VE == 0) {
+            for (int v = lane; v < nv / VE; v += 32) reinterpret_cast<V*>(dst)[v] = reinterpret_cast<const V*>(src)[v];
+        } else {
+            for (int v = lane; v < nv; v += 32) dst[v] = src[v];
         }
     }
 }
@@ -251,9 +248,9 @@ __device__ __forceinline__ void res_rows_local(const T* red, T* slot, int ncw, i
 }
 
 // out[i] = scale * (row sum of row i), read from slot `par` of the owning CTA.
-template <typename T>
+template <typename T, int RC>
 __device__ __forceinline__ void res_rows_gather(cg::cluster_group& cluster, T* own_slots, int par,
-                                                T* out, int nx, int RC, T scale) {
+                                                T* out, int nx, T scale) {
     for (int i = threadIdx.x; i < nx; i += blockDim.x) {
         const int c = i / RC;
         out[i] = scale * cluster.map_shared_rank(own_slots, c)[par * RC + (i - c * RC)];
@@ -261,20 +258,22 @@ __device__ __forceinline__ void res_rows_gather(cg::cluster_group& cluster, T* o
 }
 
 // out[r] = sum_k c[(i-k) mod nx] x[k] (adjoint: c[(k-i) mod nx]) for the n_rows rows
-// i = (first + r) mod nx, r < n_rows; a power-of-two group of tpr lanes per row, lane g summing
-// k = g, g + tpr, ... in order, then an xor tree. Starts and ends with a block barrier.
+// i = (first + r) mod nx, r < n_rows; a power-of-two group of tpr lanes per row (the largest <= 32
+// with tpr * n_rows <= blockDim.x), lane g summing k = g, g + tpr, ... in order, then an xor tree.
+// Shifts and masks only (no integer division). Starts and ends with a block barrier.
 template <typename T>
 __device__ __forceinline__ void res_circ_rows(const T* circ2, const T* x, T* out, int nx, int first,
                                               int n_rows, bool adjoint) {
     __syncthreads();
-    int tpr = 32;
-    while (tpr > 1 && tpr * n_rows > (int)blockDim.x) tpr >>= 1;
-    const int g = threadIdx.x % tpr;
-    const int rows_per_pass = blockDim.x / tpr;
-    const int passes = (n_rows + rows_per_pass - 1) / rows_per_pass;
-    for (int p = 0; p < passes; ++p) {
-        const int r = p * rows_per_pass + (int)threadIdx.x / tpr;
-        int i = (first + (r < n_rows ? r : 0)) % nx;
+    int lg = 5;
+    while (lg > 0 && (n_rows << lg) > (int)blockDim.x) --lg;
+    const int tpr = 1 << lg;
+    const int g = threadIdx.x & (tpr - 1);
+    const int stride = blockDim.x >> lg;
+    for (int base = 0; base < n_rows; base += stride) {
+        const int r = base + (int)(threadIdx.x >> lg);
+        int i = first + (r < n_rows ? r : 0);
+        while (i >= nx) i -= nx;
         T s = T(0);
         if (r < n_rows) {
             // c[(i - k) mod nx] = circ2[nx + i - k]; c[(k - i) mod nx] = circ2[nx - i + k]
@@ -320,9 +319,9 @@ __device__ void res_init_tables(ResSmem<T>& S, const PoissonTables<T>& P, const 
 // CTA 0 also sums the partial energies of step k - 2 (published by the barrier before this call)
 // into ee_hist[k - 2]; the remote reads go here, with the other exchanges of the step, because
 // every CTA is between the same two barriers. Ends with a block barrier.
-template <typename T>
+template <typename T, int RC>
 __device__ void res_fwd_field(const ResFwdArgs<T>& a, ResSmem<T>& S, cg::cluster_group& cluster, T* plane,
-                              int par, int gr0, int RC, int k, int me, int CN) {
+                              int par, int gr0, int k, int me, int CN) {
     const int nx = a.nx, nv = a.nv;
     const int W = a.h_lo + RC + a.h_hi;
     if (me == 0 && k >= 2 && a.ee_hist != nullptr && threadIdx.x < 32) {
@@ -332,8 +331,8 @@ __device__ void res_fwd_field(const ResFwdArgs<T>& a, ResSmem<T>& S, cg::cluster
         for (int c = 0; c < CN; ++c) tot += __shfl_sync(0xffffffffu, v, c);
         if (lane == 0) a.ee_hist[k - 2] = (T)(0.5 * tot * (double)a.dx);
     }
-    res_fill_halo<T>(cluster, plane, nx, nv, RC, gr0, a.h_lo, a.h_hi);
-    res_rows_gather<T>(cluster, S.vec1, par, S.vec0, nx, RC, -a.dv);   // rho
+    res_fill_halo<T, RC>(cluster, plane, nx, nv, gr0, a.h_lo, a.h_hi);
+    res_rows_gather<T, RC>(cluster, S.vec1, par, S.vec0, nx, -a.dv);   // rho
     const int first = res_grow(gr0, a.h_lo, 0, nx);
     res_circ_rows<T>(S.circ2, S.vec0, S.fld, nx, first, W, false);
     for (int l = threadIdx.x; l < W; l += blockDim.x)
@@ -428,7 +427,7 @@ __global__ void __launch_bounds__(1024) vp_res_fwd_kernel(const ResFwdArgs<T> a)
     __syncthreads();
     res_rows_local<T>(red, S.vec1, ncw, RC);
     cluster.sync();
-    res_fwd_field<T>(a, S, cluster, Hb[0], 0, gr0, RC, 0, me, CN);
+    res_fwd_field<T, RC>(a, S, cluster, Hb[0], 0, gr0, 0, me, CN);
 
     for (int n = 0; n < a.n_steps; ++n) {
         const T* cur = Hb[n & 1];
@@ -498,7 +497,7 @@ __global__ void __launch_bounds__(1024) vp_res_fwd_kernel(const ResFwdArgs<T> a)
         }
         if (out_warp) res_fwd_outputs<T>(a, S, n, gr0, RC);
         cluster_wait();
-        if (!last) res_fwd_field<T>(a, S, cluster, nxt, par, gr0, RC, n + 1, me, CN);
+        if (!last) res_fwd_field<T, RC>(a, S, cluster, nxt, par, gr0, n + 1, me, CN);
     }
     // energies of the last two steps (their partials are published by this barrier); the second
     // barrier keeps every CTA's shared memory alive until CTA 0 has read it
@@ -542,15 +541,15 @@ __device__ __forceinline__ ResBwdPre<T> res_bwd_prefetch(const ResBwdArgs<T>& a,
 // row sums published in slot `par`; g_E_total = -dt/dv * rowsum + g_E_hist[s]; g_H += g_E_total
 // (own rows); g_E = g_E_total + ee^T; grho = Poisson^T(g_E) and the v shifts of step s on the W
 // local rows. `pre` holds this thread's tape values of step s.
-template <typename T>
+template <typename T, int RC>
 __device__ void res_bwd_field(const ResBwdArgs<T>& a, ResSmem<T>& S, cg::cluster_group& cluster, T* plane,
-                              int par, int s, int gr0, int RC, const ResBwdPre<T>& pre) {
+                              int par, int s, int gr0, const ResBwdPre<T>& pre) {
     const int nx = a.nx;
     const int W = a.h_lo + RC + a.h_hi;
     const int me_i = threadIdx.x;
-    res_fill_halo<T>(cluster, plane, nx, a.nv, RC, gr0, a.h_lo, a.h_hi);
+    res_fill_halo<T, RC>(cluster, plane, nx, a.nv, gr0, a.h_lo, a.h_hi);
     T* sums = S.vec0;
-    res_rows_gather<T>(cluster, S.vec1, par, sums, nx, RC, T(1));
+    res_rows_gather<T, RC>(cluster, S.vec1, par, sums, nx, T(1));
     const T gee = pre.gee;
     for (int i = threadIdx.x; i < nx; i += blockDim.x) {
         const bool own = i == me_i;
@@ -675,11 +674,10 @@ __global__ void __launch_bounds__(1024) vp_res_bwd_kernel(const ResBwdArgs<T> a)
         for (int k = 0; k < RPT; ++k) prod[k] = T(0);
         if (colv) {
             T c[RPT + 1];
-            int base = (g - m - 1) % nx;
-            base = wrapneg(base, nx);
+            const int cb = wrapneg(g - m - 1, nx);   // g - m - 1 >= -nx
 #pragma unroll
             for (int k = 0; k <= RPT; ++k) {
-                const int q = wrap1(base + k, nx);
+                const int q = wrap1(cb + k, nx);
                 T v = T(0);
                 if (a.g_ff != nullptr) v += __ldg(a.g_ff + (size_t)q * nv + j);
                 if (a.g_fh != nullptr) v += __ldg(a.g_fh + ((size_t)(T_steps - 1) * nx + q) * nv + j);
@@ -697,7 +695,7 @@ __global__ void __launch_bounds__(1024) vp_res_bwd_kernel(const ResBwdArgs<T> a)
         const int par = (T_steps - 1) & 1;
         res_rows_local<T>(red, S.vec1 + par * RC, ncw, RC);
         cluster.sync();
-        res_bwd_field<T>(a, S, cluster, nxt, par, T_steps - 1, gr0, RC, pre);
+        res_bwd_field<T, RC>(a, S, cluster, nxt, par, T_steps - 1, gr0, pre);
     }
 
     for (int n = T_steps - 1; n >= 0; --n) {
@@ -730,8 +728,7 @@ __global__ void __launch_bounds__(1024) vp_res_bwd_kernel(const ResBwdArgs<T> a)
             } else {
                 // c on rows g-m-1 .. g-m+RPT-1 (+ g_f_hist[n-1]), then w_{n-1} on the own rows
                 T c[RPT + 1];
-                int cb = (g - m - 1) % nx;
-                cb = wrapneg(cb, nx);
+                const int cb = wrapneg(g - m - 1, nx);
 #pragma unroll
                 for (int k = 0; k <= RPT; ++k) {
                     c[k] = lerp(gh[k + 1], gh[k], t);
@@ -754,7 +751,7 @@ __global__ void __launch_bounds__(1024) vp_res_bwd_kernel(const ResBwdArgs<T> a)
         }
         cluster_arrive();
         cluster_wait();
-        if (n > 0) res_bwd_field<T>(a, S, cluster, nxt, par, n - 1, gr0, RC, pre);
+        if (n > 0) res_bwd_field<T, RC>(a, S, cluster, nxt, par, n - 1, gr0, pre);
     }
     for (int r = threadIdx.x; r < RC; r += blockDim.x) a.g_H[gr0 + r] = S.own[r];
     // no other CTA reads this CTA's shared memory after the last barrier
