@@ -25,6 +25,19 @@ __device__ __forceinline__ int wrap2(int x, int n) {
 }
 // x in [-n, n) -> [0, n)
 __device__ __forceinline__ int wrapneg(int x, int n) { return x < 0 ? x + n : x; }
+// x in [-2n, n) -> [0, n)
+__device__ __forceinline__ int wrapneg2(int x, int n) {
+    x = x < 0 ? x + n : x;
+    return x < 0 ? x + n : x;
+}
+// x in [-2n, 2n) -> [0, n)
+__device__ __forceinline__ int wrapboth(int x, int n) {
+    x = x < 0 ? x + n : x;
+    x = x < 0 ? x + n : x;
+    return x >= n ? x - n : x;
+}
+// These replace % n in per-tile index arithmetic: integer division by a runtime value costs
+// tens of instructions.
 
 // Trapezoid weight of index k in [0, n): 0.5 at both ends, 1 inside
 // (warp_vp_solver/kernels.py:167-172 and 192-197).

@@ -321,8 +321,7 @@ __device__ __forceinline__ void bwd_tile(const BwdArgs<T>& a, int r0, int c_begi
         const T wr = -a.dv * trap_w<T>(j, nv);   // rho^T weight (kernels.py:292-299)
         if (PHASE == 2) {
             // gh rows r0 - m - 1 + k, k in [0, R+1); out rows r0 + e
-            int base = (r0 - m - 1) % nx;
-            base = wrapneg(base, nx);
+            const int base = wrapneg(r0 - m - 1, nx);   // r0 - m - 1 >= -nx
             T gh[R + 1];
 #pragma unroll
             for (int k = 0; k < R + 1; ++k) {
@@ -340,8 +339,7 @@ __device__ __forceinline__ void bwd_tile(const BwdArgs<T>& a, int r0, int c_begi
             continue;
         }
         // c rows r0 - m - 1 + k, k in [0, R+1)
-        int cbase = (r0 - m - 1) % nx;
-        cbase = wrapneg(cbase, nx);
+        const int cbase = wrapneg(r0 - m - 1, nx);
         T c[R + 1];
         if (PHASE == 0) {
 #pragma unroll
@@ -367,8 +365,7 @@ __device__ __forceinline__ void bwd_tile(const BwdArgs<T>& a, int r0, int c_begi
             }
         } else {
             // gh rows r0 - 2m - 2 + k, k in [0, R+2)
-            int base = (r0 - 2 * m - 2) % nx;
-            base = wrapneg(base, nx);
+            const int base = wrapneg2(r0 - 2 * m - 2, nx);   // r0 - 2m - 2 >= -2nx
             T gh[R + 2];
 #pragma unroll
             for (int k = 0; k < R + 2; ++k) {
@@ -528,7 +525,7 @@ __global__ void __launch_bounds__(C) vp_fwds_kernel(const FwdArgs<T> a) {
         const int lo = r0 + 2 * s_min;
         const int span = 2 * (s_max - s_min) + R + 2;
         const bool staged = span <= span_max;
-        const int lo_w = ((lo % nx) + nx) % nx;
+        const int lo_w = wrapboth(lo, nx);   // signed offsets in (-nx/2, nx/2]: lo in [-nx-2, 2nx)
         if (staged) {
             for (int idx = tid; idx < span * PER_ROW; idx += C) {
                 const int q = idx / PER_ROW, v = idx - q * PER_ROW;
@@ -717,7 +714,7 @@ __global__ void __launch_bounds__(C) vp_bwds_kernel(const BwdArgs<T> a) {
         const int lo = r0 - 2 * s_max - 2;
         const int span = 2 * (s_max - s_min) + R + 2;
         const bool staged = span <= span_max;
-        const int lo_w = ((lo % nx) + nx) % nx;
+        const int lo_w = wrapboth(lo, nx);   // signed offsets in (-nx/2, nx/2]: lo in [-nx-2, 2nx)
         if (staged) {
             for (int idx = tid; idx < (span + R) * PER_ROW; idx += C) {
                 const int q = idx / PER_ROW, v = idx - q * PER_ROW;
@@ -763,8 +760,8 @@ __global__ void __launch_bounds__(C) vp_bwds_kernel(const BwdArgs<T> a) {
             const T t = __ldg(a.tx + j);
             const T wr = -a.dv * trap_w<T>(j, nv);
             const int sbase = 2 * (s_max - sm);            // staged row of gh[0]
-            const int gbase = wrapneg((r0 - 2 * m - 2) % nx, nx);
-            const int cbase = wrapneg((r0 - m - 1) % nx, nx);
+            const int gbase = wrapneg2(r0 - 2 * m - 2, nx);
+            const int cbase = wrapneg(r0 - m - 1, nx);
             auto ghstep = [&](int k) -> T {
                 if (staged) {
                     const int2 info = iw[sbase + k];
