@@ -194,7 +194,7 @@ static size_t res_config_ok(const vp_plan* p, int cn) {
     if (hlo + hhi >= p->nx) return 0;   // local rows of a CTA span less than two periods
     const size_t smem = res_smem_size(p->nx, p->nv, Rc, hlo + hhi, real_size(p));
     if (smem > kMaxSmemPerCta) return 0;
-    if (res_threads(Rc, p->nv) > 1024) return 0;
+    if (res_threads(Rc, p->nv) == 0) return 0;
     const int n = p->dtype == VP_F64 ? res_max_clusters<double>(p->feq2d != 0, cn, Rc, p->nv, smem)
                                      : res_max_clusters<float>(p->feq2d != 0, cn, Rc, p->nv, smem);
     return n > 0 ? smem : 0;

@@ -62,6 +62,10 @@ template <typename T> struct ResSmem {
 
 __host__ __device__ inline size_t res_align(size_t x) { return (x + 15) & ~(size_t)15; }
 
+// Launch bound of the resident kernels by rows per thread: 1024 threads, or 512 from 8 rows per
+// thread up (their register arrays need more than the 64 registers a 1024-thread CTA allows).
+__host__ __device__ constexpr int res_max_threads(int rpt) { return rpt >= 8 ? 512 : 1024; }
+
 __host__ __device__ inline size_t res_smem_bytes(int nx, int nv, int RC, int W, size_t rs) {
     size_t b = 0;
     b += res_align((size_t)W * nv * rs) * 2;
@@ -362,7 +366,7 @@ __device__ void res_fwd_outputs(const ResFwdArgs<T>& a, ResSmem<T>& S, int s, in
 }
 
 template <typename T, int RC, int RPT, bool FEQ2D>
-__global__ void __launch_bounds__(1024) vp_res_fwd_kernel(const ResFwdArgs<T> a) {
+__global__ void __launch_bounds__(res_max_threads(RPT)) vp_res_fwd_kernel(const ResFwdArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem[];
     cg::cluster_group cluster = cg::this_cluster();
     const int nx = a.nx, nv = a.nv;
@@ -626,7 +630,7 @@ __device__ __forceinline__ void res_bwd_w(const ResBwdArgs<T>& a, const ResSmem<
 }
 
 template <typename T, int RC, int RPT, bool FEQ2D>
-__global__ void __launch_bounds__(1024) vp_res_bwd_kernel(const ResBwdArgs<T> a) {
+__global__ void __launch_bounds__(res_max_threads(RPT)) vp_res_bwd_kernel(const ResBwdArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem[];
     cg::cluster_group cluster = cg::this_cluster();
     const int nx = a.nx, nv = a.nv, T_steps = a.n_steps;
@@ -761,18 +765,27 @@ __global__ void __launch_bounds__(1024) vp_res_bwd_kernel(const ResBwdArgs<T> a)
 // Host-side launch helpers
 // ---------------------------------------------------------------------------------------------
 
-// Rows per thread for RC rows per CTA: the fewest (most threads) that keep the CTA at <= 1024
-// threads, and at least RC/8 (at most 8 row groups).
+// Rows per thread for RC rows per CTA: among the powers of two in [RC/8, RC] whose CTA fits the
+// launch bound, the most rows per thread that still gives at least 512 threads (16 warps), or the
+// largest CTA when none reaches 512; 0 when none fits. More rows per thread means fewer window
+// rows per cell ((RPT+2)/RPT) and fewer per-step overheads; 16 warps keep the latency covered
+// (measured on 128x128 and 256x256 grids: 10-20% faster than the 1024-thread shapes).
 int res_rows_per_thread(int RC, int nv) {
     const int nvp = ((nv + 31) / 32) * 32;
-    int rpt = RC;
-    while (rpt > 1 && rpt > RC / 8 && (RC / (rpt / 2)) * nvp <= 1024) rpt /= 2;
-    return rpt;
+    int best = 0;
+    for (int rpt = RC / 8 > 1 ? RC / 8 : 1; rpt <= RC; rpt *= 2) {
+        const int th = (RC / rpt) * nvp;
+        if (th > res_max_threads(rpt)) continue;
+        if (best == 0 || th >= 512) best = rpt;
+    }
+    return best;
 }
 
+// Threads of the resident CTA for RC rows per CTA (0 when no shape fits).
 int res_threads(int RC, int nv) {
     const int nvp = ((nv + 31) / 32) * 32;
-    return (RC / res_rows_per_thread(RC, nv)) * nvp;
+    const int rpt = res_rows_per_thread(RC, nv);
+    return rpt > 0 ? (RC / rpt) * nvp : 0;
 }
 
 template <typename T, int RC, int RPT, bool F2>
@@ -849,7 +862,7 @@ template <typename T>
 int res_max_clusters(bool feq2d, int cn, int RC, int nv, size_t smem) {
     const int RPT = res_rows_per_thread(RC, nv);
     const int threads = res_threads(RC, nv);
-    if (threads > 1024) return 0;
+    if (RPT == 0 || threads == 0) return 0;
     VP_RES_CASES(res_max_clusters_rc, feq2d, cn, threads, smem)
     return 0;
 }
