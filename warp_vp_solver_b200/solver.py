@@ -234,6 +234,9 @@ class _VPFunction(torch.autograd.Function):
         plan = solver.plan
         out = plan.forward(f_iv.detach(), H.detach(), n_steps, record_history=record_history,
                            want_tape=True, checkpoint_every=solver.checkpoint_every)
+        # outputs the loss does not use arrive as None (no zero-filled cotangents to allocate,
+        # fill and read in the adjoint)
+        ctx.set_materialize_grads(False)
         ctx.plan = plan
         ctx.n_steps = n_steps
         ctx.every = out["every"]
