@@ -1406,6 +1406,7 @@ struct vp_batch {
     int n_tiles = 0, grid_fwd = 0, grid_bwd = 0;
     size_t smem = 0;
     void* d_inst = nullptr;
+    void* d_tiles = nullptr;   // int4 per tile: instance, first row, column chunk (no search on the device)
 };
 
 namespace vpb {
@@ -1488,6 +1489,7 @@ static void free_batch(vp_batch* b) {
         cudaGetDevice(&prev);
         cudaSetDevice(b->device);
         cudaFree(b->d_inst);
+        if (b->d_tiles) cudaFree(b->d_tiles);
         cudaSetDevice(prev);
     }
     delete b;
@@ -1532,27 +1534,44 @@ static int batch_layout(vp_batch* b, int R, int chunk, int threads, int per_sm) 
     size_t bytes = 0;
     int n_tiles = 0;
     std::vector<unsigned char> host;
+    std::vector<int4> tiles;
+    auto tile_map = [&](const auto& v) {
+        for (size_t k = 0; k < v.size(); ++k)
+            for (int lt = 0; lt < v[k].n_tiles; ++lt)
+                tiles.push_back(make_int4((int)k, (lt / v[k].n_chunks) * R, lt % v[k].n_chunks, 0));
+    };
     if (b->dtype == VP_F64) {
         std::vector<BatchInst<double>> v;
         batch_fill<double>(b, v, order, chunk_cols);
         n_tiles = v.back().tile_begin + v.back().n_tiles;
         bytes = v.size() * sizeof(BatchInst<double>);
         host.assign(reinterpret_cast<unsigned char*>(v.data()), reinterpret_cast<unsigned char*>(v.data()) + bytes);
+        tile_map(v);
     } else {
         std::vector<BatchInst<float>> v;
         batch_fill<float>(b, v, order, chunk_cols);
         n_tiles = v.back().tile_begin + v.back().n_tiles;
         bytes = v.size() * sizeof(BatchInst<float>);
         host.assign(reinterpret_cast<unsigned char*>(v.data()), reinterpret_cast<unsigned char*>(v.data()) + bytes);
+        tile_map(v);
     }
     void* d_inst = nullptr;
-    const int rc = upload_bytes(&d_inst, host.data(), bytes);
+    int rc = upload_bytes(&d_inst, host.data(), bytes);
     if (rc != VP_OK) {
         b->R = old_R;
         return rc;
     }
+    void* d_tiles = nullptr;
+    rc = upload_bytes(&d_tiles, tiles.data(), tiles.size() * sizeof(int4));
+    if (rc != VP_OK) {
+        cudaFree(d_inst);
+        b->R = old_R;
+        return rc;
+    }
     if (b->d_inst) cudaFree(b->d_inst);
+    if (b->d_tiles) cudaFree(b->d_tiles);
     b->d_inst = d_inst;
+    b->d_tiles = d_tiles;
     const bool f2 = b->feq2d != 0;
     int n_sms = 148;
     cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, b->device);
@@ -1591,6 +1610,7 @@ static int batch_forward_impl(vp_batch* b, const double* f_iv, const T* H, int T
     VP_CUDA(cudaMemsetAsync(ws + L.counters, 0, (size_t)b->n * sizeof(unsigned), s), "memset(counters)");
     BatchStep<T> st{};
     st.inst = static_cast<const BatchInst<T>*>(b->d_inst);
+    st.tiles = static_cast<const int4*>(b->d_tiles);
     st.n_inst = b->n;
     st.n_tiles = b->n_tiles;
     st.n_steps = Ts;
@@ -1654,6 +1674,7 @@ static int batch_backward_impl(vp_batch* b, const T* H, int Ts, const unsigned c
     VP_CUDA(cudaMemsetAsync(g_H, 0, (size_t)b->total_x * sizeof(T), s), "memset(g_H)");
     BatchStep<T> st{};
     st.inst = static_cast<const BatchInst<T>*>(b->d_inst);
+    st.tiles = static_cast<const int4*>(b->d_tiles);
     st.n_inst = b->n;
     st.n_tiles = b->n_tiles;
     st.n_steps = Ts;

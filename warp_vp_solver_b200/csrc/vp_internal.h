@@ -122,6 +122,7 @@ template <typename T> struct BatchInst {
 // tape slot (n_steps, n).
 template <typename T> struct BatchStep {
     const BatchInst<T>* inst;
+    const int4* tiles;          // per tile: instance (index into inst), first row, column chunk
     int n_inst, n_tiles;
     int last;                   // forward: the last step (no h_out, no tail)
     int n_steps;

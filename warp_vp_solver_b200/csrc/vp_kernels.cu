@@ -1029,20 +1029,10 @@ template cudaError_t launch_bwd<double>(const BwdArgs<double>&, const LaunchCfg&
 
 // ----------------------------------------------------------------------------------------------
 // Ensembles: one persistent launch per time step advances every instance. CTAs stride over the
-// instances' tiles (instances ordered longest first); the CTA that completes an instance's last
-// tile runs that instance's Poisson tail. Per-tile arithmetic is fwd_tile / bwd_tile above.
+// instances' tiles (instances ordered longest first; a host-built map gives each tile's instance,
+// first row and column chunk); the CTA that completes an instance's last tile runs that
+// instance's Poisson tail. Per-tile arithmetic is fwd_tile / bwd_tile above.
 // ----------------------------------------------------------------------------------------------
-
-template <typename T>
-__device__ __forceinline__ int batch_find(const BatchInst<T>* inst, int n, int tile) {
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(&inst[mid].tile_begin) <= tile) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
 
 template <typename T>
 __device__ __forceinline__ FwdArgs<T> batch_fwd_args(const BatchStep<T>& b, const BatchInst<T>& I) {
@@ -1122,11 +1112,10 @@ __global__ void __launch_bounds__(256) vp_batch_fwd_kernel(const BatchStep<T> b)
     __shared__ int s_last;
     const size_t red_bytes = (((size_t)32 * R * sizeof(T)) + 15) & ~(size_t)15;
     for (int tile = blockIdx.x; tile < b.n_tiles; tile += gridDim.x) {
-        const BatchInst<T> I = b.inst[batch_find<T>(b.inst, b.n_inst, tile)];
+        const int4 tm = __ldg(b.tiles + tile);
+        const BatchInst<T> I = b.inst[tm.x];
         const FwdArgs<T> a = batch_fwd_args<T>(b, I);
-        const int lt = tile - I.tile_begin;
-        const int rb = lt / I.n_chunks, ch = lt - rb * I.n_chunks;
-        const int r0 = rb * R, c_begin = ch * I.chunk_cols;
+        const int r0 = tm.y, ch = tm.z, c_begin = ch * I.chunk_cols;
         const int c_end = min(I.nv, c_begin + I.chunk_cols);
         T acc[R];
 #pragma unroll
@@ -1150,11 +1139,10 @@ __global__ void __launch_bounds__(256) vp_batch_bwd_kernel(const BatchStep<T> b)
     __shared__ int s_last;
     const size_t red_bytes = (((size_t)32 * R * sizeof(T)) + 15) & ~(size_t)15;
     for (int tile = blockIdx.x; tile < b.n_tiles; tile += gridDim.x) {
-        const BatchInst<T> I = b.inst[batch_find<T>(b.inst, b.n_inst, tile)];
+        const int4 tm = __ldg(b.tiles + tile);
+        const BatchInst<T> I = b.inst[tm.x];
         const BwdArgs<T> a = batch_bwd_args<T>(b, I);
-        const int lt = tile - I.tile_begin;
-        const int rb = lt / I.n_chunks, ch = lt - rb * I.n_chunks;
-        const int r0 = rb * R, c_begin = ch * I.chunk_cols;
+        const int r0 = tm.y, ch = tm.z, c_begin = ch * I.chunk_cols;
         const int c_end = min(I.nv, c_begin + I.chunk_cols);
         T acc[R];
 #pragma unroll
