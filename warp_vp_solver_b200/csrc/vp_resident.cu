@@ -50,7 +50,7 @@ template <typename T> struct ResSmem {
     T* p2;           // row partials of the warps: [RC][NVP/32]
     T* vec0;         // nx: row sums of every CTA, gathered after the step's cluster barrier
     T* vec1;         // 2 x RC: this CTA's own row sums, step parity (read by the other CTAs)
-    T* circ2;        // 2 nx: c = real(ifft(m)) twice, so that c[(i - k) mod nx] = circ2[i - k + nx]
+    T* ctab;         // 3 nx + 16: ctab[j] = c[(j - nx - 8) mod nx], c = real(ifft(m))
     T* fld;          // W: E (forward) or grho (adjoint) of the local rows
     T* aux;          // nx: H (forward) or g_E (adjoint), global row index
     VShift<T>* vsh;  // W: v shifts of the current step, local rows
@@ -71,7 +71,7 @@ __host__ __device__ inline size_t res_smem_bytes(int nx, int nv, int RC, int W, 
     b += res_align((size_t)W * nv * rs) * 2;
     b += res_align((size_t)RC * nv * rs);
     b += res_align((size_t)nx * rs) * 3;
-    b += res_align((size_t)2 * nx * rs);
+    b += res_align((size_t)(3 * nx + 16) * rs);
     b += res_align((size_t)W * rs);
     b += res_align((size_t)W * (rs == 8 ? 16 : 8));
     b += res_align((size_t)nv * 8);
@@ -96,7 +96,7 @@ __device__ ResSmem<T> res_carve(unsigned char* smem, int nx, int nv, int RC, int
     s.vec0 = reinterpret_cast<T*>(take((size_t)nx * sizeof(T)));
     s.vec1 = reinterpret_cast<T*>(take((size_t)nx * sizeof(T)));
     s.aux = reinterpret_cast<T*>(take((size_t)nx * sizeof(T)));
-    s.circ2 = reinterpret_cast<T*>(take((size_t)2 * nx * sizeof(T)));
+    s.ctab = reinterpret_cast<T*>(take((size_t)(3 * nx + 16) * sizeof(T)));
     s.fld = reinterpret_cast<T*>(take((size_t)W * sizeof(T)));
     s.vsh = reinterpret_cast<VShift<T>*>(take((size_t)W * sizeof(VShift<T>)));
     s.feq = reinterpret_cast<double*>(take((size_t)nv * sizeof(double)));
@@ -262,37 +262,56 @@ __device__ __forceinline__ void res_rows_gather(cg::cluster_group& cluster, T* o
 }
 
 // out[r] = sum_k c[(i-k) mod nx] x[k] (adjoint: c[(k-i) mod nx]) for the n_rows rows
-// i = (first + r) mod nx, r < n_rows; a power-of-two group of tpr lanes per row (the largest <= 32
-// with tpr * n_rows <= blockDim.x), lane g summing k = g, g + tpr, ... in order, then an xor tree.
-// Shifts and masks only (no integer division). Starts and ends with a block barrier.
+// i = (first + r) mod nx, r < n_rows. A warp takes 4 consecutive rows at a time; lane g sums
+// k = g, g + 32, ... in order for the 4 rows at once: the 4 coefficients of one k are
+// consecutive table entries, and consecutive lanes read consecutive entries of x and of the
+// table (no shared-memory bank conflicts). The 4 x 32 partial sums are combined by a transposed
+// butterfly (fixed order). No integer division; starts and ends with a block barrier.
 template <typename T>
-__device__ __forceinline__ void res_circ_rows(const T* circ2, const T* x, T* out, int nx, int first,
+__device__ __forceinline__ void res_circ_rows(const T* ctab, const T* x, T* out, int nx, int first,
                                               int n_rows, bool adjoint) {
     __syncthreads();
-    int lg = 5;
-    while (lg > 0 && (n_rows << lg) > (int)blockDim.x) --lg;
-    const int tpr = 1 << lg;
-    const int g = threadIdx.x & (tpr - 1);
-    const int stride = blockDim.x >> lg;
-    for (int base = 0; base < n_rows; base += stride) {
-        const int r = base + (int)(threadIdx.x >> lg);
-        int i = first + (r < n_rows ? r : 0);
-        while (i >= nx) i -= nx;
-        T s = T(0);
-        if (r < n_rows) {
-            // c[(i - k) mod nx] = circ2[nx + i - k]; c[(k - i) mod nx] = circ2[nx - i + k]
-            const T* cp = adjoint ? circ2 + nx - i + g : circ2 + nx + i - g;
-            const int cs = adjoint ? tpr : -tpr;
-            const T* xp = x + g;
-#pragma unroll 8
-            for (int k = g; k < nx; k += tpr) {
-                s += *cp * *xp;
-                cp += cs;
-                xp += tpr;
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int off = nx + 8;
+    const int ngrp = (n_rows + 3) >> 2;
+    for (int grp = (int)(threadIdx.x >> 5); grp < ngrp; grp += nw) {
+        int i0 = first + 4 * grp;
+        while (i0 >= nx) i0 -= nx;
+        // rows i0 + q (q < 4, not reduced mod nx: the table covers the overhang); coefficient of
+        // row q at k: forward ctab[off + i0 + q - k], adjoint ctab[off + k - i0 - q]
+        T acc[4] = {T(0), T(0), T(0), T(0)};
+        const int sgn = adjoint ? -1 : 1;
+        const T* cp = adjoint ? ctab + off + lane - i0 : ctab + off + i0 - lane;
+        const int cstep = adjoint ? 32 : -32;
+#pragma unroll 4
+        for (int k = lane; k < nx; k += 32) {
+            const T xk = x[k];
+            acc[0] += cp[0] * xk;
+            acc[1] += cp[sgn] * xk;
+            acc[2] += cp[2 * sgn] * xk;
+            acc[3] += cp[3 * sgn] * xk;
+            cp += cstep;
+        }
+        // transposed butterfly: lane l ends with the sum of row l >> 3
+#pragma unroll
+        for (int st = 0; st < 2; ++st) {
+            const int o = 16 >> st;
+            const int n = 2 >> st;
+            const bool upper = (lane & o) != 0;
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                if (q < n) {
+                    const T send = upper ? acc[q] : acc[q + n];
+                    const T keep = upper ? acc[q + n] : acc[q];
+                    acc[q] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+                }
             }
         }
-        for (int o = tpr >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (r < n_rows && g == 0) out[r] = s;
+        T sum = acc[0];
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        const int r = 4 * grp + (lane >> 3);
+        if ((lane & 7) == 0 && r < n_rows) out[r] = sum;
     }
     __syncthreads();
 }
@@ -300,10 +319,10 @@ __device__ __forceinline__ void res_circ_rows(const T* circ2, const T* x, T* out
 template <typename T>
 __device__ void res_init_tables(ResSmem<T>& S, const PoissonTables<T>& P, const double* feq,
                                 bool feq2d, int nx, int nv) {
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-        const T c = __ldg(P.circ + i);
-        S.circ2[i] = c;
-        S.circ2[i + nx] = c;
+    for (int j = threadIdx.x; j < 3 * nx + 16; j += blockDim.x) {
+        int d = (j - nx - 8) % nx;   // once per launch
+        d += d < 0 ? nx : 0;
+        S.ctab[j] = __ldg(P.circ + d);
     }
     if (!feq2d) {
         for (int j = threadIdx.x; j < nv; j += blockDim.x) {
@@ -338,7 +357,7 @@ __device__ void res_fwd_field(const ResFwdArgs<T>& a, ResSmem<T>& S, cg::cluster
     res_fill_halo<T, RC>(cluster, plane, nx, nv, gr0, a.h_lo, a.h_hi);
     res_rows_gather<T, RC>(cluster, S.vec1, par, S.vec0, nx, -a.dv);   // rho
     const int first = res_grow(gr0, a.h_lo, 0, nx);
-    res_circ_rows<T>(S.circ2, S.vec0, S.fld, nx, first, W, false);
+    res_circ_rows<T>(S.ctab, S.vec0, S.fld, nx, first, W, false);
     for (int l = threadIdx.x; l < W; l += blockDim.x)
         S.vsh[l] = res_vshift<T>(S.fld[l] + S.aux[res_grow(gr0, a.h_lo, l, nx)], a.dtdv, nv);
     __syncthreads();
@@ -565,7 +584,7 @@ __device__ void res_bwd_field(const ResBwdArgs<T>& a, ResSmem<T>& S, cg::cluster
     }
     for (int l = threadIdx.x; l < W; l += blockDim.x)
         S.vsh[l] = l == me_i ? pre.vs : a.vsh_tape[(size_t)s * nx + res_grow(gr0, a.h_lo, l, nx)];
-    res_circ_rows<T>(S.circ2, S.aux, S.fld, nx, res_grow(gr0, a.h_lo, 0, nx), W, true);
+    res_circ_rows<T>(S.ctab, S.aux, S.fld, nx, res_grow(gr0, a.h_lo, 0, nx), W, true);
 }
 
 // Slope inputs of step np at the own rows g .. g+RPT-1, column j: the v shifts of those rows
