@@ -145,8 +145,8 @@ template <typename T, bool FEQ2D>
 __device__ __forceinline__ T res_vcorr(const ResSmem<T>& S, const double* __restrict__ feq, int rs,
                                        int i, int j, int c0, int c1, const VShift<T> v, int nv) {
     if (!FEQ2D) {
-        if (v.m == 0) return v.t * S.dfeq[j];
-        if (v.m == nv - 1) return -(T(1) - v.t) * S.dfeq[c0];
+        // m = 0: c0 = j, t*D[j]; m = nv-1: c0 = j-1, (t-1)*D[j-1] (= -(1-t)*D[j-1] exactly)
+        if (v.m == 0 || v.m == nv - 1) return (v.m == 0 ? v.t : v.t - T(1)) * S.dfeq[c0];
         const double fj = S.feq[j];
         const double tt = (double)v.t;
         return (T)((1.0 - tt) * (S.feq[c0] - fj) + tt * (S.feq[c1] - fj));
