@@ -96,11 +96,28 @@ template <typename T, int R>
 __device__ __forceinline__ void store_row_partials(T (&acc)[R], T* red, T* part_row) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int nw = (blockDim.x + 31) >> 5;
+    // transposed butterfly: R sums over the warp in log2(R) halving exchanges plus an xor tree
+    // (R - 1 + 5 - log2(R) shuffles instead of 5 R); lane l ends with row l >> (5 - log2 R)
+    constexpr int LG = R >= 32 ? 5 : R >= 16 ? 4 : R >= 8 ? 3 : R >= 4 ? 2 : R >= 2 ? 1 : 0;
+    static_assert((1 << LG) == R, "rows per CTA must be a power of two <= 32");
 #pragma unroll
-    for (int e = 0; e < R; ++e) {
-        const T v = warp_sum(acc[e]);
-        if (lane == 0) red[wid * R + e] = v;
+    for (int st = 0; st < LG; ++st) {
+        const int o = 16 >> st;
+        const int n = R >> (st + 1);
+        const bool upper = (lane & o) != 0;
+#pragma unroll
+        for (int i = 0; i < (R >> 1); ++i) {
+            if (i < n) {
+                const T send = upper ? acc[i] : acc[i + n];
+                const T keep = upper ? acc[i + n] : acc[i];
+                acc[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+            }
+        }
     }
+    T v = acc[0];
+#pragma unroll
+    for (int o = 16 >> LG; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((lane & ((32 >> LG) - 1)) == 0) red[wid * R + (lane >> (5 - LG))] = v;
     __syncthreads();
     if (threadIdx.x < R) {
         T s = T(0);
