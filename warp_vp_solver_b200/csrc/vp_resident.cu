@@ -266,10 +266,13 @@ __device__ __forceinline__ void res_rows_gather(cg::cluster_group& cluster, T* o
 // k = g, g + 32, ... in order for the 4 rows at once: the 4 coefficients of one k are
 // consecutive table entries, and consecutive lanes read consecutive entries of x and of the
 // table (no shared-memory bank conflicts). The 4 x 32 partial sums are combined by a transposed
-// butterfly (fixed order). No integer division; starts and ends with a block barrier.
+// butterfly (fixed order). With `vsh`, the lane that writes out[r] also writes the v shift of
+// row r from out[r] + aux[global row] (the forward field). No integer division; starts with a
+// block barrier, and the caller places one after it before out or vsh are read.
 template <typename T>
 __device__ __forceinline__ void res_circ_rows(const T* ctab, const T* x, T* out, int nx, int first,
-                                              int n_rows, bool adjoint) {
+                                              int n_rows, bool adjoint, VShift<T>* vsh = nullptr,
+                                              const T* aux = nullptr, T dtdv = T(0), int nv = 0) {
     __syncthreads();
     const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int off = nx + 8;
@@ -311,9 +314,15 @@ __device__ __forceinline__ void res_circ_rows(const T* ctab, const T* x, T* out,
 #pragma unroll
         for (int o = 4; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
         const int r = 4 * grp + (lane >> 3);
-        if ((lane & 7) == 0 && r < n_rows) out[r] = sum;
+        if ((lane & 7) == 0 && r < n_rows) {
+            out[r] = sum;
+            if (vsh != nullptr) {
+                int q = first + r;
+                while (q >= nx) q -= nx;
+                vsh[r] = res_vshift<T>(sum + aux[q], dtdv, nv);
+            }
+        }
     }
-    __syncthreads();
 }
 
 template <typename T>
@@ -357,9 +366,7 @@ __device__ void res_fwd_field(const ResFwdArgs<T>& a, ResSmem<T>& S, cg::cluster
     res_fill_halo<T, RC>(cluster, plane, nx, nv, gr0, a.h_lo, a.h_hi);
     res_rows_gather<T, RC>(cluster, S.vec1, par, S.vec0, nx, -a.dv);   // rho
     const int first = res_grow(gr0, a.h_lo, 0, nx);
-    res_circ_rows<T>(S.ctab, S.vec0, S.fld, nx, first, W, false);
-    for (int l = threadIdx.x; l < W; l += blockDim.x)
-        S.vsh[l] = res_vshift<T>(S.fld[l] + S.aux[res_grow(gr0, a.h_lo, l, nx)], a.dtdv, nv);
+    res_circ_rows<T>(S.ctab, S.vec0, S.fld, nx, first, W, false, S.vsh, S.aux, a.dtdv, nv);
     __syncthreads();
 }
 
@@ -585,6 +592,7 @@ __device__ void res_bwd_field(const ResBwdArgs<T>& a, ResSmem<T>& S, cg::cluster
     for (int l = threadIdx.x; l < W; l += blockDim.x)
         S.vsh[l] = l == me_i ? pre.vs : a.vsh_tape[(size_t)s * nx + res_grow(gr0, a.h_lo, l, nx)];
     res_circ_rows<T>(S.ctab, S.aux, S.fld, nx, res_grow(gr0, a.h_lo, 0, nx), W, true);
+    __syncthreads();
 }
 
 // Slope inputs of step np at the own rows g .. g+RPT-1, column j: the v shifts of those rows
