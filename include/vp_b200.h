@@ -76,6 +76,20 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
 /* Releases a plan and its device tables. */
 int vp_plan_destroy(vp_plan* plan);
 
+/* Device-side status of a plan: flags that kernels raise without synchronising the host, read
+ * with vp_plan_status and reset with vp_plan_clear_status (both synchronous). They extend the
+ * reference's argument validation (warp_vp_solver/solver.py:144-167), which checks shapes only:
+ *   VP_STATUS_NONFINITE_INPUT  a vp_forward call's f_iv or H held a NaN or an infinity (checked
+ *                              on the device before the loop; the outputs of that call are not
+ *                              meaningful);
+ *   VP_STATUS_WAIT_TIMEOUT     a bounded device-side wait ran out (for example the grid barrier of
+ *                              a persistent time loop); the kernel stopped early and the outputs
+ *                              of that call are invalid. */
+#define VP_STATUS_NONFINITE_INPUT 1u
+#define VP_STATUS_WAIT_TIMEOUT 2u
+int vp_plan_status(vp_plan* plan, uint32_t* flags);
+int vp_plan_clear_status(vp_plan* plan);
+
 /* Number of time steps for t_final: int(t_final / dt), as WarpVlasovPoissonSolver.num_steps
  * (warp_vp_solver/solver.py:212-213). */
 int vp_num_steps(const vp_plan* plan, double t_final, int32_t* out_steps);
@@ -144,19 +158,22 @@ int vp_forward_stream_history(vp_plan* plan, const double* f_iv, const void* H, 
 #define VP_NOALLOC_SCRATCH_BYTES ((size_t)8 << 20)
 
 /* Forward time loop that allocates nothing: the same computation and outputs as vp_forward
- * without a tape, for callers that cannot allocate device memory when they run the solver
- * (for example code that must not call cudaMalloc, or must not go through an allocator, while
- * it is being captured into a CUDA graph or runs inside a host that owns all device memory).
+ * without a tape, for callers that cannot allocate device memory when they run the solver. Such
+ * callers include code recorded into a CUDA graph under a capture mode that forbids cudaMalloc,
+ * plug-ins whose host application owns every byte of device memory through its own pool, and
+ * time-critical loops that cannot afford the device-wide synchronisation cudaMalloc may cause.
  * No counterpart in the reference, which allocates Warp arrays per solver
  * (warp_vp_solver/solver.py:169-203).
- * The scratch this needs (two delta-f buffers of nx*nv reals plus O(nx) vectors) lives in one
- * statically allocated device array of VP_NOALLOC_SCRATCH_BYTES bytes that every GPU loading
- * this library holds until the process exits; requests that need more return VP_ERR_ARG (the
- * two buffers take 8*nx*nv bytes in float32: 512x1024 fits, 1024x1024 does not). The first call on a device looks up
- * that array's device address, so make the first call on each device before any stream
- * capture. All calls share the one array and it keeps the previous call's contents: the call
- * clears what must start at zero itself, but two calls whose work overlaps on the GPU (other
- * streams, other host threads, other plans on the same device) race and corrupt each other. */
+ * The scratch it needs (two delta-f planes of nx*nv reals plus O(nx) vectors) lives in one
+ * statically allocated device array of VP_NOALLOC_SCRATCH_BYTES bytes, which every GPU that
+ * loads this library holds until the process exits. Requests that need more return VP_ERR_ARG:
+ * the two planes take 8*nx*nv bytes in float32 (512x1024 fits, 1024x1024 does not) and 16*nx*nv
+ * bytes in float64 (512x512 fits, 512x1024 does not). The first call on a device looks up that
+ * array's device address (with the device current), so make the first call on each device
+ * before any stream capture. Every call shares the one array and it keeps the previous call's
+ * contents: the call clears what must start at zero itself, but two calls whose work overlaps on
+ * the GPU (other streams, other host threads, other plans on the same device) race and corrupt
+ * each other. */
 int vp_forward_noalloc(vp_plan* plan, const double* f_iv, const void* H, int32_t n_steps,
                        double* f_final, void* f_hist, void* E_hist, void* ee_hist, void* stream);
 
@@ -254,6 +271,13 @@ int vp_mlp_search(vp_mlp* mlp, const float* c0, int32_t iters, float lr, float b
                   float* best_J, void* stream);
 /* Nonzero bit 0: a tensor-core wait gave up (results of that call are invalid). Synchronous. */
 int vp_mlp_status(vp_mlp* mlp, uint32_t* flags);
+/* Resets the status flags (synchronous). */
+int vp_mlp_clear_status(vp_mlp* mlp);
+/* Limit, in nanoseconds, of each bounded wait with which the network's tensor-core kernels detect
+ * a stalled pipeline (default 1 s; 0 gives up at the first poll that finds the work unfinished).
+ * A wait that gives up raises bit 0 of vp_mlp_status; the CTA still waits (up to 1 s) for the
+ * tensor-core work it issued, frees its tensor memory and returns. */
+int vp_mlp_set_wait_limit(vp_mlp* mlp, uint64_t ns);
 /* One BF16 tile GEMM with the MLP's epilogues: C = act(A[M,K] . B[N,K]^T + bias), act 0 none,
  * 1 GELU, 2 multiply by GELU'(aux[m, n]); outputs FP32 C32, BF16 C16 and BF16 transposed C16T
  * (each may be NULL). K, lda, ldb multiples of 8; A, B 16-byte aligned. */

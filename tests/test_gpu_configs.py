@@ -1,0 +1,199 @@
+"""Parity at the benchmark configurations' own sizes, and the CUDA gradient against central
+finite differences of the CUDA forward.
+
+* C2, two-stream 256x256, dt 0.05, 100 steps, 8-mode H (std 1e-2, seed 0), J = trapezoid(ee, dt):
+  forward outputs and dJ/dH through ``run_forward_torch`` + autograd (the cluster-resident
+  forward and adjoint kernels), float32 and float64, against the float64 oracle (the reference's
+  legacy forward and adjoint, warp_vp_solver/solver.py:470-524 and 778-932, restated in C in
+  oracle/vp_oracle_c.c). The gradient is also probed by central differences of the CUDA forward
+  along random directions of H, the way the reference's tests/test_solver.py:155-178 probes its
+  custom_vjp gradient.
+* C3, bump-on-tail 512x1024, 600 steps, 16-mode H, sqrt(T)-checkpointed adjoint (K = 25): the
+  same comparisons at full size.
+* C4: instances of the uneven ensemble with the configuration's own shapes.
+
+Central differences. The semi-Lagrangian scheme interpolates between cells chosen by floor(), so
+J is continuous but only piecewise smooth in H: a central difference whose step moves some row's
+foot across a cell boundary picks up an O(eps) error. On C2 the float64 oracle's own central
+differences differ from its adjoint by 5e-4..2.5e-2 at eps = 1e-3, 3e-6 at 1e-6 and <= 3.3e-9 at
+1e-7. So the gradient is checked at eps = 1e-7 in float64, and at the configuration's eps = 1e-3
+the CUDA forward's central differences are checked against the oracle's (the same function, with
+the same kinks).
+
+Bars are max-norm relative errors, max|a - b| / max|b|, set at about ten times the errors measured
+on B200; every test records its measured errors (printed at the end of the run).
+"""
+
+from __future__ import annotations
+
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+import torch
+
+import vp_oracle as O
+import vp_oracle_c as C
+from warp_vp_solver_b200 import WarpVlasovPoissonSolver, electric_energy_in_time
+from warp_vp_solver_b200.ensemble import Ensemble
+from warp_vp_solver_b200.workloads import fourier_field, make_ensemble_workload, make_workload
+
+pytestmark = pytest.mark.gpu
+
+needs_c_oracle = pytest.mark.skipif(not C.available(), reason="oracle/_build/libvporacle.so not built")
+
+
+def _dt_id(d):
+    return "f32" if d == torch.float32 else "f64"
+
+
+def _oracle(wl, H):
+    """Forward outputs and dJ/dH (J = trapezoid(ee, dt)) of the float64 oracle."""
+    g = O.grid_from(wl.mesh)
+    T = wl.n_steps
+    w = O.trapezoid_time_weights(T, wl.dt)
+    f_final, f_hist, E_hist, ee = C.forward(g, wl.dt, wl.f_eq, wl.f_iv, H, T)
+    _, gH = C.backward(g, wl.dt, wl.f_eq, wl.f_iv, H, T, f_hist, None, None, None, w)
+    del f_hist
+    return f_final, E_hist, ee, gH
+
+
+def _oracle_J(wl, H):
+    g = O.grid_from(wl.mesh)
+    T = wl.n_steps
+    ee = C.forward(g, wl.dt, wl.f_eq, wl.f_iv, H, T)[3]
+    return float(np.dot(O.trapezoid_time_weights(T, wl.dt), ee))
+
+
+def _cuda(s, wl, H):
+    """run_forward_torch + autograd of J = trapezoid(ee, dt): outputs and dJ/dH."""
+    f_iv = torch.tensor(wl.f_iv, dtype=torch.float64, device="cuda")
+    Ht = torch.tensor(H, dtype=torch.float64, device="cuda", requires_grad=True)
+    f_final, _, E_hist, ee = s.run_forward_torch(f_iv, Ht, wl.t_final, record_history=False)
+    J = electric_energy_in_time(ee, s)
+    J.backward()
+    torch.cuda.synchronize()
+    return (f_final.detach().cpu().numpy(), E_hist.detach().double().cpu().numpy(),
+            ee.detach().double().cpu().numpy(), Ht.grad.cpu().numpy())
+
+
+def _cuda_J(s, wl, H):
+    _, _, _, ee = s.run_forward(wl.f_iv, H, wl.t_final, record_history=False)
+    return float(np.dot(O.trapezoid_time_weights(wl.n_steps, wl.dt), ee))
+
+
+# (dtype, forward bar, adjoint bar) at C2; float32 errors measured on B200 are ~1e-8 (f), ~1e-7
+# (E, ee) and ~3e-7 (dJ/dH)
+C2_BARS = {torch.float32: (2e-6, 5e-6), torch.float64: (1e-11, 1e-10)}
+
+
+@needs_c_oracle
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64], ids=_dt_id)
+def test_c2_forward_and_adjoint_match_oracle(dtype, record_error):
+    wl = make_workload("c2")
+    s = WarpVlasovPoissonSolver(wl.mesh, wl.dt, wl.f_eq, dtype=dtype)
+    assert s.plan.get_config()["cluster_size"] > 0   # the headline's cluster-resident kernels
+    got = _cuda(s, wl, wl.H)
+    ref = _oracle(wl, wl.H)
+    fb, ab = C2_BARS[dtype]
+    for name, a, b, bar in zip(("f_final", "E_hist", "ee_hist", "dJ/dH"), got, ref, (fb, fb, fb, ab)):
+        err = record_error(f"C2 {_dt_id(dtype)} {name}", O.rel_err(a, b), bar)
+        assert err < bar, f"C2 {name}: {err:.2e}"
+
+
+def _directions(wl, rng):
+    """Two smooth directions (random Fourier fields of the configuration's modes) and one rough
+    one (independent N(0, 1) entries, as the reference's test draws)."""
+    n = wl.coeffs.shape[1]
+    return [fourier_field(rng.standard_normal((2, n)), wl.mesh.xs, wl.k0),
+            fourier_field(rng.standard_normal((2, n)), wl.mesh.xs, wl.k0),
+            rng.standard_normal(wl.mesh.nx)]
+
+
+@needs_c_oracle
+def test_c2_gradient_matches_central_differences(record_error):
+    """float64: adjoint vs central differences of the CUDA forward at eps = 1e-7; float32 (the
+    benchmark's type): its adjoint against the same differences."""
+    wl = make_workload("c2")
+    s64 = WarpVlasovPoissonSolver(wl.mesh, wl.dt, wl.f_eq, dtype=torch.float64)
+    s32 = WarpVlasovPoissonSolver(wl.mesh, wl.dt, wl.f_eq)
+    g64 = _cuda(s64, wl, wl.H)[3]
+    g32 = _cuda(s32, wl, wl.H)[3]
+    eps = 1e-7
+    for k, d in enumerate(_directions(wl, np.random.default_rng(42))):
+        fd = (_cuda_J(s64, wl, wl.H + eps * d) - _cuda_J(s64, wl, wl.H - eps * d)) / (2 * eps)
+        e64 = record_error(f"C2 FD(1e-7) dir {k}: f64 adjoint", abs(np.dot(g64, d) - fd) / abs(fd), 1e-7)
+        e32 = record_error(f"C2 FD(1e-7) dir {k}: f32 adjoint", abs(np.dot(g32, d) - fd) / abs(fd), 2e-5)
+        assert e64 < 1e-7 and e32 < 2e-5, f"direction {k}: f64 {e64:.2e} f32 {e32:.2e}"
+
+
+@needs_c_oracle
+def test_c2_central_differences_at_eps_1e3_match_oracle(record_error):
+    """eps = 1e-3, the configuration's step: the CUDA forward's central differences equal the
+    oracle's (both cross the same interpolation kinks), and the adjoint is reported beside them."""
+    wl = make_workload("c2")
+    s64 = WarpVlasovPoissonSolver(wl.mesh, wl.dt, wl.f_eq, dtype=torch.float64)
+    g64 = _cuda(s64, wl, wl.H)[3]
+    eps = 1e-3
+    for k, d in enumerate(_directions(wl, np.random.default_rng(43))[:2]):
+        fd = (_cuda_J(s64, wl, wl.H + eps * d) - _cuda_J(s64, wl, wl.H - eps * d)) / (2 * eps)
+        fd_ref = (_oracle_J(wl, wl.H + eps * d) - _oracle_J(wl, wl.H - eps * d)) / (2 * eps)
+        err = record_error(f"C2 FD(1e-3) dir {k}: CUDA vs oracle", abs(fd - fd_ref) / abs(fd_ref), 1e-8)
+        record_error(f"C2 FD(1e-3) dir {k}: adjoint vs FD (kinks)", abs(np.dot(g64, d) - fd) / abs(fd), 1.0)
+        assert err < 1e-8, f"direction {k}: {err:.2e}"
+
+
+# float32 errors measured on B200 at C3 are ~1e-7 (f), ~1e-6 (E, ee) and ~1e-6 (dJ/dH)
+C3_BARS = {torch.float32: (1e-5, 2e-5), torch.float64: (1e-10, 1e-9)}
+
+
+@needs_c_oracle
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64], ids=_dt_id)
+def test_c3_full_size_checkpointed_adjoint_matches_oracle(dtype, record_error):
+    """512x1024, 600 steps, the automatic checkpoint interval (ceil(sqrt(600)) = 25 for float32:
+    the full tape would be 1.26 GB)."""
+    wl = make_workload("c3")
+    s = WarpVlasovPoissonSolver(wl.mesh, wl.dt, wl.f_eq, dtype=dtype)
+    assert s.plan.resolve_every(wl.n_steps, None) == 25
+    got = _cuda(s, wl, wl.H)
+    ref = _oracle(wl, wl.H)
+    fb, ab = C3_BARS[dtype]
+    for name, a, b, bar in zip(("f_final", "E_hist", "ee_hist", "dJ/dH"), got, ref, (fb, fb, fb, ab)):
+        err = record_error(f"C3 {_dt_id(dtype)} {name}", O.rel_err(a, b), bar)
+        assert err < bar, f"C3 {name}: {err:.2e}"
+
+
+@needs_c_oracle
+def test_c4_shapes_match_oracle(record_error):
+    """Instances of the C4 ensemble (seed 0) covering every nx in {64, 128, 256} and nv in
+    {128, 256, 512}, advanced together for the full 100 steps; J = sum_i trapezoid(ee_i, dt)."""
+    wl = make_ensemble_workload("c4", 256, seed=0)
+    picks, seen = [], set()
+    for i, m in enumerate(wl.meshes):
+        if (m.nx, m.nv) not in seen:
+            seen.add((m.nx, m.nv))
+            picks.append(i)
+    assert len(picks) == 9
+    sub = wl.subset(picks)
+    T = sub.n_steps
+    ens = Ensemble(sub.meshes, sub.dt, sub.f_eqs)
+    H = ens.pack_rows([sub.H(i) for i in range(sub.n)])
+    out = ens.forward(ens.pack_cells(sub.f_ivs), H, T, want_tape=True)
+    w = O.trapezoid_time_weights(T, sub.dt)
+    g_ee = torch.tensor(np.tile(w, sub.n), dtype=torch.float32, device=ens.device)
+    _, g_H = ens.backward(H, T, out["tape"], g_ee_hist=g_ee)
+    worst = {"f_final": 0.0, "E_hist": 0.0, "ee_hist": 0.0, "dJ/dH": 0.0}
+    for i, m in enumerate(sub.meshes):
+        inst = SimpleNamespace(mesh=m, dt=sub.dt, f_eq=sub.f_eqs[i], f_iv=sub.f_ivs[i], n_steps=T)
+        ref = _oracle(inst, sub.H(i))
+        got = (ens.cells_of(out["f_final"], i).cpu().numpy(),
+               ens.hist_of(out["E_hist"], i, T).double().cpu().numpy(),
+               ens.ee_of(out["ee_hist"], i, T).double().cpu().numpy(),
+               ens.rows_of(g_H, i).double().cpu().numpy())
+        for name, a, b in zip(worst, got, ref):
+            e = O.rel_err(a, b)
+            worst[name] = max(worst[name], e)
+            bar = 1e-5 if name != "dJ/dH" else 2e-5
+            assert e < bar, f"instance {picks[i]} ({m.nx}x{m.nv}) {name}: {e:.2e}"
+    for name, e in worst.items():
+        record_error(f"C4 9 shapes f32 {name} (worst)", e, 1e-5 if name != "dJ/dH" else 2e-5)

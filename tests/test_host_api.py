@@ -119,3 +119,37 @@ def test_plan_creation_fails_loudly_without_cuda(small_mesh):
     s = WarpVlasovPoissonSolver(small_mesh, 0.001, np.ones((16, 32)))
     with pytest.raises(RuntimeError, match="CUDA"):
         s.run_forward(np.ones((16, 32)), np.zeros(16), 0.005)
+
+
+def test_non_finite_host_inputs_are_rejected_before_any_device_work(small_mesh):
+    """NaN or infinite f_eq, f_iv or H given as host arrays raise ValueError on the host (the
+    reference checks shapes only, solver.py:144-167)."""
+    bad = np.ones((16, 32))
+    bad[3, 4] = np.nan
+    with pytest.raises(ValueError, match="f_eq contains NaN"):
+        WarpVlasovPoissonSolver(small_mesh, 0.1, bad)
+    s = WarpVlasovPoissonSolver(small_mesh, 0.1, np.ones((16, 32)))
+    f = np.ones((16, 32))
+    f[0, 0] = np.inf
+    with pytest.raises(ValueError, match="f_iv contains NaN"):
+        s.run_forward(f, np.zeros(16), 0.5)
+    H = np.zeros(16)
+    H[2] = -np.inf
+    with pytest.raises(ValueError, match="H contains NaN"):
+        s._run_backward(np.ones((16, 32)), H, 0.5, None, None, None, None, None)
+    with pytest.raises(ValueError, match="H contains NaN"):
+        s.run_forward_torch(np.ones((16, 32)), torch.tensor(H), 0.5)
+
+
+def test_plan_create_rejects_non_finite_f_eq_in_the_c_abi(small_mesh):
+    lib = _capi.load()
+    xs = np.ascontiguousarray(small_mesh.xs, dtype=np.float64)
+    vs = np.ascontiguousarray(small_mesh.vs, dtype=np.float64)
+    desc = _capi.MeshDesc(16, 32, _capi.dbl_ptr(xs), _capi.dbl_ptr(vs), float(small_mesh.dx),
+                          float(small_mesh.dv), float(small_mesh.period_x), float(small_mesh.period_v))
+    f_eq = np.ones((16, 32))
+    f_eq[5, 7] = np.nan
+    out = ctypes.c_void_p()
+    rc = lib.vp_plan_create(ctypes.byref(desc), 0.1, _capi.dbl_ptr(f_eq), _capi.VP_F32, ctypes.byref(out))
+    assert rc == _capi.VP_ERR_ARG and out.value is None
+    assert "f_eq[5, 7] is not finite" in _capi.last_error()

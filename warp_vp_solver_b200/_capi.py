@@ -21,6 +21,8 @@ VP_F32 = 0
 VP_F64 = 1
 VP_SCHEME_STRANG = 0
 VP_SCHEME_MERGED = 1
+VP_STATUS_NONFINITE_INPUT = 1
+VP_STATUS_WAIT_TIMEOUT = 2
 ABI_VERSION = 2   # VP_ABI_VERSION of the header these bindings follow
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libvpb200.so")
@@ -128,6 +130,10 @@ SIGNATURES = {
     "vp_mlp_mse_backward": (c_int, [c_vp, c_vp, c_i64, c_vp, c_i32, c_vp, c_vp]),
     "vp_mlp_adam": (c_int, [c_vp, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, c_vp]),
     "vp_mlp_status": (c_int, [c_vp, ctypes.POINTER(ctypes.c_uint32)]),
+    "vp_mlp_clear_status": (c_int, [c_vp]),
+    "vp_mlp_set_wait_limit": (c_int, [c_vp, ctypes.c_uint64]),
+    "vp_plan_status": (c_int, [c_vp, ctypes.POINTER(ctypes.c_uint32)]),
+    "vp_plan_clear_status": (c_int, [c_vp]),
     "vp_mlp_search": (c_int, [c_vp, c_vp, c_i32, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                               ctypes.c_float, ctypes.c_float, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "vp_gemm_bf16": (c_int, [c_vp, c_i64, c_vp, c_i64, c_i32, c_i32, c_i32, c_vp, c_i32, c_vp, c_i64,

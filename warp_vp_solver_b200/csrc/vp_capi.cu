@@ -80,6 +80,7 @@ struct vp_plan {
     int merged = 0;            // 1: merged-Strang (aggressive) scheme
     double feq_integral = 0.0; // trapezoid integral of f_eq over xs and vs (for the KL cost)
     double* d_kl = nullptr;    // KL cost scratch: 2 * kKlBlocks + 2 doubles
+    unsigned* d_status = nullptr;  // VP_STATUS_* flags raised on the device (vp_plan_status)
     std::vector<cudaEvent_t> ev_written, ev_copied;   // streamed-history slots
     void* d_vtab = nullptr;    // staged step: [2][2*kStageHalo][nv] reals (x-invariant f_eq only)
     LaunchCfg scfg{};          // staged forward step (R rows x threads columns per CTA)
@@ -714,6 +715,7 @@ static void free_plan(vp_plan* p) {
     cudaFree(p->d_tx64);
     cudaFree(p->d_mxf);
     cudaFree(p->d_kl);
+    cudaFree(p->d_status);
     for (cudaEvent_t e : p->ev_written) cudaEventDestroy(e);
     for (cudaEvent_t e : p->ev_copied) cudaEventDestroy(e);
     cudaFree(p->d_txf);
@@ -780,6 +782,11 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
     if (dtype != VP_F32 && dtype != VP_F64) return set_err(VP_ERR_ARG, "dtype must be VP_F32 or VP_F64");
     for (int j = 0; j < nv; ++j)
         if (!std::isfinite(mesh->vs[j])) return set_err(VP_ERR_ARG, "vs[%d] is not finite", j);
+    for (int i = 0; i < nx; ++i)
+        if (!std::isfinite(mesh->xs[i])) return set_err(VP_ERR_ARG, "xs[%d] is not finite", i);
+    for (size_t c = 0; c < (size_t)nx * nv; ++c)
+        if (!std::isfinite(f_eq_host[c]))
+            return set_err(VP_ERR_ARG, "f_eq[%zu, %zu] is not finite", c / (size_t)nv, c % (size_t)nv);
 
     vp_plan* p = new (std::nothrow) vp_plan();
     if (!p) return set_err(VP_ERR_ARG, "out of host memory");
@@ -946,6 +953,11 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
         if (!rc) rc = upload<float>(&p->d_mult, mult_im);
         if (!rc) rc = upload<float>(&p->d_circ, circ);
     }
+    if (!rc) {
+        ce = cudaMalloc((void**)&p->d_status, 256);
+        if (ce == cudaSuccess) ce = cudaMemset(p->d_status, 0, 256);
+        if (ce != cudaSuccess) rc = cuda_err(ce, "cudaMalloc(plan status)");
+    }
     if (rc) {
         free_plan(p);
         return rc;
@@ -1052,6 +1064,19 @@ int vp_plan_get_scheme(const vp_plan* plan, int32_t* scheme) {
     return VP_OK;
 }
 
+int vp_plan_status(vp_plan* plan, uint32_t* flags) {
+    if (!plan || !flags) return set_err(VP_ERR_ARG, "plan and flags must not be NULL");
+    VP_CUDA(cudaMemcpy(flags, plan->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost), "read plan status");
+    return VP_OK;
+}
+
+int vp_plan_clear_status(vp_plan* plan) {
+    if (!plan) return set_err(VP_ERR_ARG, "plan must not be NULL");
+    VP_CUDA(cudaMemset(plan->d_status, 0, sizeof(uint32_t)), "clear plan status");
+    VP_CUDA(cudaDeviceSynchronize(), "clear plan status");
+    return VP_OK;
+}
+
 int vp_plan_destroy(vp_plan* plan) {
     free_plan(plan);
     return VP_OK;
@@ -1125,6 +1150,8 @@ int vp_forward(vp_plan* plan, const double* f_iv, const void* H, int32_t n_steps
     if (cur != dev) return set_err(VP_ERR_ARG, "current device %d differs from the plan's device %d", cur, dev);
     unsigned char* ws = static_cast<unsigned char*>(workspace);
     unsigned char* tp = static_cast<unsigned char*>(tape);
+    VP_CUDA(launch_check_finite(f_iv, nxnv, H, plan->nx, plan->dtype == VP_F64, plan->d_status, s),
+            "finite-input check launch");
     if (plan->dtype == VP_F64)
         return forward_impl<double>(plan, f_iv, (const double*)H, n_steps, f_final, (double*)f_hist,
                                     (double*)E_hist, (double*)ee_hist, tp, every, ws, s);
@@ -1186,21 +1213,25 @@ namespace vpb {
 static __device__ __align__(256) unsigned char g_noalloc_scratch[VP_NOALLOC_SCRATCH_BYTES];
 
 static const int kMaxDevices = 64;
-static std::once_flag g_noalloc_once[kMaxDevices];
+static std::mutex g_noalloc_mutex;
 static void* g_noalloc_ptr[kMaxDevices] = {};
-static cudaError_t g_noalloc_err[kMaxDevices] = {};
 
 // Device address of the scratch array on the current device. In host code the array's name is
-// only a host-side stand-in; the address comes from cudaGetSymbolAddress, looked up once per
-// device with that device current.
+// only a host-side stand-in; the address comes from cudaGetSymbolAddress, called with that device
+// current. Only a successful lookup is cached: a lookup that fails (for example during a stream
+// capture, or with an earlier error pending) clears the error and is retried by the next call.
 static int noalloc_scratch(int device, void** out) {
     if (device < 0 || device >= kMaxDevices) return set_err(VP_ERR_UNSUPPORTED, "device %d out of range", device);
-    std::call_once(g_noalloc_once[device], [device]() {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_ptr[device] == nullptr) {
         void* ptr = nullptr;
-        g_noalloc_err[device] = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || ptr == nullptr) {
+            cudaGetLastError();
+            return cuda_err(e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress(noalloc scratch)");
+        }
         g_noalloc_ptr[device] = ptr;
-    });
-    if (g_noalloc_err[device] != cudaSuccess) return cuda_err(g_noalloc_err[device], "cudaGetSymbolAddress(noalloc scratch)");
+    }
     *out = g_noalloc_ptr[device];
     return VP_OK;
 }
@@ -1235,9 +1266,10 @@ int vp_forward_noalloc(vp_plan* plan, const double* f_iv, const void* H, int32_t
     const size_t need = ws_layout(plan, n_steps, 1).total;
     if (need > VP_NOALLOC_SCRATCH_BYTES)
         return set_err(VP_ERR_ARG,
-                       "vp_forward_noalloc: an %dx%d grid needs %zu bytes of scratch, more than the "
+                       "vp_forward_noalloc: a %dx%d %s grid needs %zu bytes of scratch, more than the "
                        "%zu-byte static scratch; use vp_forward with a caller-provided workspace",
-                       plan->nx, plan->nv, need, (size_t)VP_NOALLOC_SCRATCH_BYTES);
+                       plan->nx, plan->nv, plan->dtype == VP_F64 ? "float64" : "float32", need,
+                       (size_t)VP_NOALLOC_SCRATCH_BYTES);
     void* scratch = nullptr;
     if ((rc = noalloc_scratch(dev, &scratch)) != VP_OK) return rc;
     unsigned char* ws = static_cast<unsigned char*>(scratch);

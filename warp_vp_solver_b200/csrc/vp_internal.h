@@ -184,6 +184,11 @@ template <typename T>
 cudaError_t set_staged_bwd_smem_limit(size_t bytes);
 size_t staged_bwd_smem_bytes(int span, int R, int C, size_t real_size);
 
+// Raises VP_STATUS_NONFINITE_INPUT in *status when f (n doubles) or H (nx reals, double when h64)
+// holds a NaN or an infinity (vp_ops.cu).
+cudaError_t launch_check_finite(const double* f, size_t n, const void* H, int nx, bool h64, unsigned* status,
+                                cudaStream_t s);
+
 // Single-stage operators (vp_ops.cu).
 template <typename T>
 cudaError_t launch_compute_rho(int nx, int nv, const double* f, const double* feq, int feq_rs,

@@ -57,6 +57,7 @@ struct GemmArgs {
     bf16* C16T;              // y^T (BF16), rows n, columns [M, pad8(M)) written as zero
     long long ldc16t;
     unsigned* err;
+    unsigned long long wait_ns;   // limit of each bounded tensor-core wait (0: one poll)
 };
 
 __host__ __device__ constexpr int pad8(int x) { return (x + 7) & ~7; }
@@ -105,15 +106,25 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
-// Bounded wait for the phase of the given parity: gives up after about one second (or 2^24 polls).
-__device__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+// Bounded wait for the phase of the given parity: gives up after limit_ns nanoseconds (checked
+// every 256 polls, and after at most 2^24 polls); limit_ns == 0 gives up at the first poll that
+// does not find the phase complete.
+__device__ bool mbar_wait(uint64_t* bar, unsigned parity, unsigned long long limit_ns) {
+    if (limit_ns == 0) return mbar_try_wait(bar, parity);
     const uint64_t t0 = global_ns();
     for (unsigned it = 0; it < (1u << 24); ++it) {
         if (mbar_try_wait(bar, parity)) return true;
-        if ((it & 255u) == 255u && global_ns() - t0 > 1000000000ull) return false;
+        if ((it & 255u) == 255u && global_ns() - t0 > limit_ns) return false;
     }
     return false;
 }
+
+// Limit of the wait that drains a CTA's own tensor-core work before it frees its tensor memory
+// (used whatever the host-set limit is, so that a CTA that gave up never frees columns that an
+// MMA in flight still writes).
+constexpr unsigned long long kDrainWaitNs = 1000000000ull;
+// Default limit of the waits that detect a stalled tensor-core pipeline.
+constexpr unsigned long long kDefaultWaitNs = 1000000000ull;
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -220,7 +231,7 @@ __global__ void __launch_bounds__(NT) vp_mlp_gemm_kernel(const GemmArgs g) {
     for (int kc = 0; kc < nk; ++kc) {
         const int s = kc & 1;
         if (kc >= 2) {
-            const bool w = mbar_wait(&bars[s], ((kc - 2) >> 1) & 1);
+            const bool w = mbar_wait(&bars[s], ((kc - 2) >> 1) & 1, g.wait_ns);
             if (!__syncthreads_and(w)) {
                 ok = false;
                 break;
@@ -246,8 +257,13 @@ __global__ void __launch_bounds__(NT) vp_mlp_gemm_kernel(const GemmArgs g) {
         issued = kc;
     }
     if (issued >= 0) {
-        const bool w = mbar_wait(&bars[issued & 1], (issued >> 1) & 1);
+        const bool w = mbar_wait(&bars[issued & 1], (issued >> 1) & 1, g.wait_ns);
         ok = __syncthreads_and(ok && w);
+        if (!ok) {
+            // the commit of the last issued slice completes after every MMA this CTA issued
+            const bool d = mbar_wait(&bars[issued & 1], (issued >> 1) & 1, kDrainWaitNs);
+            __syncthreads_and(d);
+        }
     }
     if (ok && issued >= 0) {
         tc_fence_after();
@@ -599,6 +615,7 @@ struct vp_mlp {
     float* partial = nullptr;
     int n_partial = 0;
     unsigned* err = nullptr;
+    unsigned long long wait_ns = kDefaultWaitNs;   // limit of the bounded tensor-core waits
     std::vector<void*> allocs;
     int last_M = 0;
 };
@@ -711,6 +728,7 @@ GemmArgs gemm_args(const bf16* A, long long lda, const bf16* B, long long ldb, i
     g.N = N;
     g.K = K;
     g.err = err;
+    g.wait_ns = kDefaultWaitNs;
     return g;
 }
 
@@ -738,6 +756,7 @@ int mlp_forward_impl(vp_mlp* n, const float* X, long long ldx, const int* rows, 
         const int K = n->w[l], N = n->w[l + 1];
         const bf16* Ain = l == 0 ? n->Xb : n->Ab[l - 1];
         GemmArgs g = gemm_args(Ain, pad8(K), n->R.Wb[l], pad8(K), M, N, pad8(K), n->err);
+        g.wait_ns = n->wait_ns;
         g.bias = n->params + n->R.off_b[l];
         if (l == n->L - 1) {
             g.act = 0;
@@ -770,6 +789,7 @@ int mlp_backward_impl(vp_mlp* n, int M, bool param_grads, float* g_X, long long 
             // dW[N, K] = D^T[N, M] . Ain^T[K, M]^T
             const bf16* AinT = l == 0 ? n->XbT : n->AbT[l - 1];
             GemmArgs g = gemm_args(n->DbT[l], ldT, AinT, ldT, N, K, Mp, n->err);
+            g.wait_ns = n->wait_ns;
             g.act = 0;
             g.C32 = n->grads + n->R.off_W[l];
             g.ldc32 = K;
@@ -784,6 +804,7 @@ int mlp_backward_impl(vp_mlp* n, int M, bool param_grads, float* g_X, long long 
         if (l == 0 && g_X == nullptr) break;
         // dA[M, K] = D[M, N] . W[N, K]  (B operand W^T[K, pad8(N)])
         GemmArgs g = gemm_args(n->Db[l], pad8(N), n->R.WbT[l], pad8(N), M, K, pad8(N), n->err);
+        g.wait_ns = n->wait_ns;
         if (l > 0) {
             g.act = 2;
             g.aux = n->Z[l - 1];
@@ -992,6 +1013,19 @@ int vp_mlp_adam(vp_mlp* n, float lr, float beta1, float beta2, float eps, void* 
 int vp_mlp_status(vp_mlp* n, uint32_t* flags) {
     if (!n || !flags) return set_err(VP_ERR_ARG, "mlp and flags must not be NULL");
     MLP_CUDA(cudaMemcpy(flags, n->err, sizeof(unsigned), cudaMemcpyDeviceToHost), "read mlp status");
+    return VP_OK;
+}
+
+int vp_mlp_clear_status(vp_mlp* n) {
+    if (!n) return set_err(VP_ERR_ARG, "mlp must not be NULL");
+    MLP_CUDA(cudaMemset(n->err, 0, sizeof(unsigned)), "clear mlp status");
+    MLP_CUDA(cudaDeviceSynchronize(), "clear mlp status");
+    return VP_OK;
+}
+
+int vp_mlp_set_wait_limit(vp_mlp* n, uint64_t ns) {
+    if (!n) return set_err(VP_ERR_ARG, "mlp must not be NULL");
+    n->wait_ns = ns;
     return VP_OK;
 }
 

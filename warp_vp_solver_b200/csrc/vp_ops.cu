@@ -3,6 +3,7 @@
 // warp_vp_solver/solver.py:393-412, warp_vp_solver/poisson.py:48-99). They share the index
 // arithmetic and the in-block FFT with the fused kernels in vp_kernels.cu.
 
+#include "../../include/vp_b200.h"
 #include "vp_device.cuh"
 
 #include <algorithm>
@@ -280,6 +281,43 @@ cudaError_t set_poisson_smem_limit(size_t bytes) {
 }
 template cudaError_t set_poisson_smem_limit<float>(size_t);
 template cudaError_t set_poisson_smem_limit<double>(size_t);
+
+// Finite-input check of a forward call: raises VP_STATUS_NONFINITE_INPUT in *status when f (n
+// doubles) or H (nx reals) holds a NaN or an infinity. Grid-stride over 16-byte loads of f (its
+// base is 16-byte aligned when it comes from a torch allocation; otherwise 8-byte loads).
+__global__ void __launch_bounds__(256) check_finite_kernel(const double* __restrict__ f, size_t n,
+                                                           const void* __restrict__ H, int nx, int h64,
+                                                           unsigned* status) {
+    bool bad = false;
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    if ((reinterpret_cast<uintptr_t>(f) & 15) == 0) {
+        const double2* f2 = reinterpret_cast<const double2*>(f);
+        for (size_t i = tid; i < n / 2; i += stride) {
+            const double2 v = __ldg(f2 + i);
+            bad |= !isfinite(v.x) || !isfinite(v.y);
+        }
+        if (tid == 0 && (n & 1)) bad |= !isfinite(__ldg(f + n - 1));
+    } else {
+        for (size_t i = tid; i < n; i += stride) bad |= !isfinite(__ldg(f + i));
+    }
+    for (size_t i = tid; i < (size_t)nx; i += stride)
+        bad |= h64 ? !isfinite(__ldg(static_cast<const double*>(H) + i))
+                   : !isfinite(__ldg(static_cast<const float*>(H) + i));
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(status, VP_STATUS_NONFINITE_INPUT);
+}
+
+cudaError_t launch_check_finite(const double* f, size_t n, const void* H, int nx, bool h64, unsigned* status,
+                                cudaStream_t s) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t want = (n / 2 + 255) / 256;
+    const int blocks = (int)std::max<size_t>(1, std::min<size_t>(want, (size_t)sms * 8));
+    check_finite_kernel<<<blocks, 256, 0, s>>>(f, n, H, nx, h64 ? 1 : 0, status);
+    count_launch();
+    return cudaGetLastError();
+}
 
 #define VP_INST(T)                                                                              \
     template cudaError_t launch_compute_rho<T>(int, int, const double*, const double*, int,     \

@@ -130,9 +130,17 @@ class MLP:
                                          self._s()))
 
     def status(self) -> int:
+        """Status flags (synchronous): bit 0 set when a tensor-core wait gave up."""
         f = ctypes.c_uint32()
         _capi.check(self.lib.vp_mlp_status(self._h, ctypes.byref(f)))
         return int(f.value)
+
+    def clear_status(self) -> None:
+        _capi.check(self.lib.vp_mlp_clear_status(self._h))
+
+    def set_wait_limit(self, ns: int) -> None:
+        """Limit of each bounded tensor-core wait in nanoseconds (default 1 s; 0: one poll)."""
+        _capi.check(self.lib.vp_mlp_set_wait_limit(self._h, int(ns)))
 
     def train_step(self, X, T, rows=None) -> torch.Tensor:
         """forward + mean-squared-error backward (no Adam); returns the loss (device scalar)."""

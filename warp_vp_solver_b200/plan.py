@@ -97,6 +97,15 @@ class Plan:
         _capi.check(self.lib.vp_plan_set_config(self._h, ctypes.byref(c)))
         self._ws = {}   # workspace size depends on n_chunks
 
+    def status(self) -> int:
+        """Device-side status flags (synchronous): VP_STATUS_NONFINITE_INPUT, VP_STATUS_WAIT_TIMEOUT."""
+        f = ctypes.c_uint32()
+        _capi.check(self.lib.vp_plan_status(self._h, ctypes.byref(f)))
+        return int(f.value)
+
+    def clear_status(self) -> None:
+        _capi.check(self.lib.vp_plan_clear_status(self._h))
+
     def set_scheme(self, merged: bool) -> None:
         """Strang splitting (False) or the merged-Strang scheme of the reference's aggressive
         path (True)."""

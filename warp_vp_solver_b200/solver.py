@@ -64,6 +64,7 @@ class WarpVlasovPoissonSolver:
         self.f_eq = np.asarray(f_eq, dtype=np.float64)
         if self.f_eq.shape != (mesh.nx, mesh.nv):
             raise ValueError(f"f_eq shape {self.f_eq.shape} != ({mesh.nx}, {mesh.nv})")
+        _check_finite_host("f_eq", self.f_eq)
         self.optimized = bool(optimized)
         self.aggressive = bool(aggressive)
         if self.aggressive and not self.optimized:
@@ -106,11 +107,6 @@ class WarpVlasovPoissonSolver:
     def device(self) -> torch.device:
         return self.plan.device
 
-    def _check_supported(self) -> None:
-        """Every constructor combination runs: aggressive=True selects the merged-Strang scheme
-        (solver.py:618-736, 1111-1338); the three aggressive layouts are one arithmetic chain
-        here (the layout choice is a launch-shape detail of the reference)."""
-
     def num_steps(self, t_final: float) -> int:
         """int(t_final / dt) (solver.py:212-213)."""
         return int(t_final / self.dt)
@@ -150,12 +146,13 @@ class WarpVlasovPoissonSolver:
         """
         if record_history is None:
             record_history = self.record_history
-        self._check_supported()
         if not self.optimized and not record_history:
             raise ValueError(
                 "record_history=False is only supported when the solver was "
                 "constructed with optimized=True."
             )
+        _check_finite_host("f_iv", f_iv)
+        _check_finite_host("H", H)
         T = self.num_steps(t_final)
         as_torch = isinstance(f_iv, torch.Tensor)
         itemsize = 8 if self.dtype == torch.float64 else 4
@@ -179,7 +176,8 @@ class WarpVlasovPoissonSolver:
         ``f_hist`` is accepted for signature compatibility and not read: the states the adjoint
         needs are recomputed on the device from checkpoints of a forward pass.
         """
-        self._check_supported()
+        _check_finite_host("f_iv", f_iv)
+        _check_finite_host("H", H)
         T = self.num_steps(t_final)
         as_torch = isinstance(f_iv, torch.Tensor)
         fwd = self.plan.forward(f_iv, H, T, record_history=False, want_tape=True,
@@ -203,11 +201,12 @@ class WarpVlasovPoissonSolver:
 
             def run(f_iv, H, t_final, *, record_history: bool | None = None):
                 rh = solver.record_history if record_history is None else bool(record_history)
-                solver._check_supported()
                 if not solver.optimized and not rh:
                     raise ValueError(
                         "record_history=False is only supported when the solver was "
                         "constructed with optimized=True.")
+                _check_finite_host("f_iv", f_iv)
+                _check_finite_host("H", H)
                 f_iv_t = f_iv if isinstance(f_iv, torch.Tensor) else torch.as_tensor(
                     np.asarray(f_iv, dtype=np.float64))
                 H_t = H if isinstance(H, torch.Tensor) else torch.as_tensor(
@@ -219,11 +218,36 @@ class WarpVlasovPoissonSolver:
             self._torch_callable = run
         return self._torch_callable
 
+    def check_status(self) -> None:
+        """Raise if a kernel of this solver flagged a problem since the last check (synchronous):
+        non-finite values in a device-resident f_iv or H (NumPy inputs are checked on the host
+        before they are uploaded), or a bounded device-side wait that ran out. Clears the flags."""
+        flags = self.plan.status()
+        if flags:
+            self.plan.clear_status()
+        if flags & 1:
+            raise ValueError("f_iv or H contains NaN or infinite values")
+        if flags & 2:
+            raise RuntimeError("a bounded device-side wait ran out; the last results are invalid")
+
     @property
     def run_forward_jax(self):
         raise NotImplementedError(
             "JAX is not part of this build; use run_forward_torch (a torch.autograd.Function "
             "with the same outputs and gradients)")
+
+
+def _check_finite_host(name: str, a) -> None:
+    """ValueError for NaN or infinite entries of a host (NumPy or CPU torch) input; device tensors
+    are checked on the device (``check_status``) so that no call synchronises."""
+    if isinstance(a, torch.Tensor):
+        if a.device.type != "cpu":
+            return
+        ok = bool(torch.isfinite(a).all())
+    else:
+        ok = bool(np.isfinite(np.asarray(a, dtype=np.float64)).all())
+    if not ok:
+        raise ValueError(f"{name} contains NaN or infinite values")
 
 
 class _VPFunction(torch.autograd.Function):
