@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define VP_ABI_VERSION 2
+#define VP_ABI_VERSION 3
 
 /* status codes */
 #define VP_OK 0
@@ -89,6 +89,11 @@ int vp_plan_destroy(vp_plan* plan);
 #define VP_STATUS_WAIT_TIMEOUT 2u
 int vp_plan_status(vp_plan* plan, uint32_t* flags);
 int vp_plan_clear_status(vp_plan* plan);
+/* Limit, in nanoseconds, of each device-side wait of a plan's persistent launches at their grid
+ * barrier (default 1 s; 0: a CTA that is not the last to arrive gives up at once). A wait that
+ * gives up raises VP_STATUS_WAIT_TIMEOUT and its CTA returns; every other CTA then gives up at the
+ * next barrier, so the launch ends and the CUDA context stays usable. */
+int vp_plan_set_wait_limit(vp_plan* plan, uint64_t ns);
 
 /* Number of time steps for t_final: int(t_final / dt), as WarpVlasovPoissonSolver.num_steps
  * (warp_vp_solver/solver.py:212-213). */
@@ -346,12 +351,20 @@ typedef struct vp_launch_config {
     int32_t stage_threads;    /* columns (= threads) per CTA of the staged kernel, dividing nv    */
     int32_t stage_span;       /* rows of its shared-memory staging buffer (derived)               */
     int64_t stage_smem_bytes; /* dynamic shared memory of the staged kernel (derived)             */
+    int32_t persist_rows;     /* > 0: float32 forward loops (and the adjoint's recomputation of   */
+                              /* checkpoint segments) run as one cooperative launch per loop     */
+                              /* whose CTAs own bands of this many rows (4, 8 or 16) and meet at */
+                              /* a bounded grid barrier once per step; 0: off. Needs an          */
+                              /* x-invariant f_eq, nv a multiple of 256 and nx <= 16384; on by   */
+                              /* default where the state is not cluster-resident                */
+    int32_t persist_ctas;     /* CTAs of that launch (derived)                                    */
+    int64_t persist_smem_bytes; /* dynamic shared memory per CTA of that launch (derived)        */
 } vp_launch_config;
 
 /* Reads the plan's current launch shape. */
 int vp_plan_get_config(const vp_plan* plan, vp_launch_config* out);
 
-/* Sets rows_per_cta, threads, n_chunks, cluster_size, stage_rows and stage_threads (the other
+/* Sets rows_per_cta, threads, n_chunks, cluster_size, stage_rows, stage_threads and persist_rows (the other
  * fields are derived and ignored). cluster_size must be 0 or a power of two in [2, 16] that splits nx into 1, 2, 4, 8,
  * 16 or 32 rows per CTA whose state fits in shared memory; the cluster-resident path is used for forward calls without a tape or with
  * checkpoint interval 1, and for backward calls with checkpoint interval 1. Workspace sizes

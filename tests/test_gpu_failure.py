@@ -4,10 +4,10 @@
   return an error for values it has not looked at; a check kernel at the start of the call raises
   VP_STATUS_NONFINITE_INPUT in the plan's status word instead, and ``check_status`` reports it.
 * Bounded waits: the tensor-core MLP kernels wait on mbarriers with a limit. With the limit set
-  to zero every wait gives up at its first unsuccessful poll (the waiting warps poll before the
-  issuing thread has even committed its MMAs), so the status flag must be raised, the call must
-  return normally and the CUDA context must stay usable: with the default limit restored, the same
-  network computes the same outputs as before.
+  to zero a wait is one non-blocking test of the barrier, and the warps that do not issue MMAs
+  reach it before the issuing thread has committed them, so it gives up: the status flag must be
+  raised, the call must return normally (after draining its own MMAs) and the CUDA context must
+  stay usable: with the default limit restored, the same network computes the same outputs.
 """
 
 from __future__ import annotations

@@ -21,7 +21,7 @@ def test_streamed_history_equals_device_history(merged, slots, every):
     f_eq, f_iv = two_stream_state(m, eps=1e-2)
     H = 0.05 * np.random.default_rng(0).standard_normal(m.nx)
     s = WarpVlasovPoissonSolver(m, 0.05, f_eq, aggressive=merged, checkpoint_every=every or None)
-    s.plan.set_config(cluster_size=0)
+    s.plan.set_config(cluster_size=0, persist_rows=0)
     T = 11
     dev = s.plan.forward(f_iv, H, T, record_history=True)
     st = s.plan.forward_stream_history(f_iv, H, T, slots=slots, want_tape=True)

@@ -36,7 +36,7 @@ def make_solver(mesh, dt, f_eq, path="auto", **kw):
     the per-step streaming kernels."""
     s = WarpVlasovPoissonSolver(mesh, dt, f_eq, **kw)
     if path == "stream":
-        s.plan.set_config(cluster_size=0)
+        s.plan.set_config(cluster_size=0, persist_rows=0)
     return s
 
 
@@ -59,12 +59,14 @@ def test_forward_matches_reference_golden(case, dtype, path):
 @pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("dtype", DTYPES, ids=_dt_id)
 @pytest.mark.parametrize("case", BACKWARD_CASES, ids=lambda c: c.name)
-def test_backward_matches_reference_golden(case, dtype, path):
+def test_backward_matches_reference_golden(case, dtype, path, record_error):
     s = make_solver(case.mesh, float(case["dt"]), case["f_eq"], path, dtype=dtype)
     g_f, g_H = s._run_backward(case["f_iv"], case["H"], float(case["t_final"]), None,
                                case["g_f_final"], case["g_f_hist"], case["g_E_hist"],
                                case["g_ee_hist"])
     e1, e2 = O.rel_err(g_f, case["g_f_iv"]), O.rel_err(g_H, case["g_H"])
+    if dtype == torch.float32:
+        record_error(f"golden {case.name} {path} f32 adjoint", max(e1, e2), TOL_BWD[dtype])
     assert e1 < TOL_BWD[dtype] and e2 < TOL_BWD[dtype], f"{case.name}: g_f {e1:.2e} g_H {e2:.2e}"
 
 
@@ -190,7 +192,7 @@ STAGED = [(64, 256, 0.05, 0.02), (128, 128, 0.05, 0.05), (32, 512, 0.1, 0.3), (3
 
 @pytest.mark.parametrize("dtype", DTYPES, ids=_dt_id)
 @pytest.mark.parametrize("shape", STAGED, ids=lambda s: f"{s[0]}x{s[1]}_H{s[3]}")
-def test_staged_step_matches_oracle(shape, dtype):
+def test_staged_step_matches_oracle(shape, dtype, record_error):
     nx, nv, dt, amp = shape
     m = make_mesh(10.0 * np.pi, 6.0, nx, nv)
     f_eq, f_iv = two_stream_state(m, eps=1e-2)
@@ -211,6 +213,9 @@ def test_staged_step_matches_oracle(shape, dtype):
     gEh = rg.standard_normal((T, nx))
     gf, gH = s._run_backward(f_iv, H, T * dt, None, gff, gfh, gEh, w)
     rf, rH = O.delta_backward(g, dt, f_eq, f_iv, H, T, gff, gfh, gEh, w)
+    if dtype == torch.float32:
+        record_error(f"staged {nx}x{nv} H{amp} f32 adjoint", max(O.rel_err(gf, rf), O.rel_err(gH, rH)),
+                     TOL_BWD[dtype])
     assert O.rel_err(gf, rf) < TOL_BWD[dtype] and O.rel_err(gH, rH) < TOL_BWD[dtype]
 
 
@@ -226,7 +231,7 @@ def test_staged_shapes_agree(rows, cols):
     outs = []
     for ce in (1, 4):
         s = make_solver(m, dt, f_eq, "stream", checkpoint_every=ce)
-        s.plan.set_config(stage_rows=rows, stage_threads=cols)
+        s.plan.set_config(stage_rows=rows, stage_threads=cols, persist_rows=0)
         assert s.plan.get_config()["stage_rows"] == rows
         out = s.run_forward(f_iv, H, T * dt)
         assert O.rel_err(out[0], ref[0]) < 1e-5 and O.rel_err(out[3], ref[3]) < 1e-5
@@ -237,7 +242,7 @@ def test_staged_shapes_agree(rows, cols):
 
 @pytest.mark.parametrize("dtype", DTYPES, ids=_dt_id)
 @pytest.mark.parametrize("layout", ["staged", "percolumn16"])
-def test_separate_tail_large_nx(layout, dtype):
+def test_separate_tail_large_nx(layout, dtype, record_error):
     """nx = 4096: the Poisson tail is its own one-CTA launch (per-stage twiddles in shared memory
     for float32, the plain table for float64), and with 16 column chunks the row partials are
     pre-summed across CTAs before it. Forward and adjoint against the oracle."""
@@ -262,6 +267,9 @@ def test_separate_tail_large_nx(layout, dtype):
     gEh = rg.standard_normal((T, m.nx))
     gf, gH = s._run_backward(f_iv, H, T * dt, None, gff, None, gEh, w)
     rf, rH = O.delta_backward(g, dt, f_eq, f_iv, H, T, gff, None, gEh, w)
+    if dtype == torch.float32:
+        record_error(f"tail nx=4096 {layout} f32 adjoint", max(O.rel_err(gf, rf), O.rel_err(gH, rH)),
+                     TOL_BWD[dtype])
     assert O.rel_err(gf, rf) < TOL_BWD[dtype] and O.rel_err(gH, rH) < TOL_BWD[dtype]
 
 

@@ -8,9 +8,10 @@ its scratch is one static device array of ``VP_NOALLOC_SCRATCH_BYTES`` (8 MiB) t
 shares and that keeps the previous call's contents.
 
 The scratch holds the two delta-f state planes, the row partial sums, the completion counter and
-the field vectors of the per-step kernels; the cluster-resident kernels keep their state in
-shared memory and never touch it. So each case here forces a per-step path (per-column kernel,
-staged kernel, and a grid whose Poisson tail is its own launch) and asserts it. Each case makes
+the field vectors of the per-step kernels (or the row sums, field slices, energy partials and grid
+barrier of the persistent loop); the cluster-resident kernels keep their state in shared memory
+and never touch it. So each case here forces a path that uses it (per-column kernel, staged
+kernel, a grid whose Poisson tail is its own launch, the persistent loop) and asserts it. Each case makes
 two calls in a row with different inputs, and a call on a different grid sits between the cases,
 so leftovers in the shared scratch would change a result. Every result must equal, bit for bit,
 the regular ``vp_forward`` on the same inputs with a workspace pre-filled with garbage bytes.
@@ -32,8 +33,9 @@ pytestmark = pytest.mark.gpu
 SCRATCH_BYTES = 8 << 20
 
 # (nx, nv, path): "column" = per-column kernel with the tail inside the step launch, "staged" =
-# staged kernel, "staged_tail" = staged kernel with the Poisson tail as its own launch (nx > 2048)
-CASES = [(128, 128, "column"), (128, 512, "staged"), (4096, 128, "staged_tail")]
+# staged kernel, "staged_tail" = staged kernel with the Poisson tail as its own launch (nx > 2048),
+# "persist" = one cooperative launch for the whole loop
+CASES = [(128, 128, "column"), (128, 512, "staged"), (4096, 128, "staged_tail"), (128, 512, "persist")]
 
 
 def _stream():
@@ -45,11 +47,14 @@ def _solver(nx, nv, path):
     f_eq, _ = two_stream_state(m)
     s = WarpVlasovPoissonSolver(m, 0.05, f_eq)
     if path == "column":
-        s.plan.set_config(cluster_size=0, stage_rows=0)
+        s.plan.set_config(cluster_size=0, stage_rows=0, persist_rows=0)
+    elif path == "persist":
+        s.plan.set_config(cluster_size=0, persist_rows=4)
     else:
-        s.plan.set_config(cluster_size=0)
+        s.plan.set_config(cluster_size=0, persist_rows=0)
     cfg = s.plan.get_config()
     assert cfg["cluster_size"] == 0, "the cluster-resident path would not use the scratch"
+    assert (cfg["persist_rows"] > 0) == (path == "persist")
     assert (cfg["stage_rows"] > 0) == (path != "column")
     assert (cfg["tail_inline"] == 0) == (path == "staged_tail")
     return m, f_eq, s

@@ -23,7 +23,7 @@ VP_SCHEME_STRANG = 0
 VP_SCHEME_MERGED = 1
 VP_STATUS_NONFINITE_INPUT = 1
 VP_STATUS_WAIT_TIMEOUT = 2
-ABI_VERSION = 2   # VP_ABI_VERSION of the header these bindings follow
+ABI_VERSION = 3   # VP_ABI_VERSION of the header these bindings follow
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libvpb200.so")
 
@@ -68,6 +68,9 @@ class LaunchConfig(ctypes.Structure):
         ("stage_threads", c_i32),
         ("stage_span", c_i32),
         ("stage_smem_bytes", c_i64),
+        ("persist_rows", c_i32),
+        ("persist_ctas", c_i32),
+        ("persist_smem_bytes", c_i64),
     ]
 
 
@@ -134,6 +137,7 @@ SIGNATURES = {
     "vp_mlp_set_wait_limit": (c_int, [c_vp, ctypes.c_uint64]),
     "vp_plan_status": (c_int, [c_vp, ctypes.POINTER(ctypes.c_uint32)]),
     "vp_plan_clear_status": (c_int, [c_vp]),
+    "vp_plan_set_wait_limit": (c_int, [c_vp, ctypes.c_uint64]),
     "vp_mlp_search": (c_int, [c_vp, c_vp, c_i32, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                               ctypes.c_float, ctypes.c_float, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "vp_gemm_bf16": (c_int, [c_vp, c_i64, c_vp, c_i64, c_i32, c_i32, c_i32, c_vp, c_i32, c_vp, c_i64,

@@ -4,7 +4,8 @@ fastest per problem signature.
 Tunables (the C ABI's `vp_plan_set_config` / `vp_batch_set_config`):
 
 * single instance: the cluster-resident path (cluster size) for grids whose state fits one
-  cluster, and otherwise the staged step's tile (stage_rows x stage_threads) and the per-column
+  cluster, the persistent loop's band height (persist_rows), otherwise the staged step's tile
+  (stage_rows x stage_threads) and the per-column
   kernel's rows per CTA;
 * ensembles: rows per tile, columns per tile, threads per CTA and persistent CTAs per SM.
 
@@ -118,10 +119,11 @@ def plan_candidates(cfg: dict) -> list[dict]:
     """Candidate single-instance configurations around a plan's current one."""
     cands = []
     if cfg["cluster_size"] > 0:
-        cands += [{"cluster_size": cn} for cn in (16, 8, 4, 2)]
-    cands += [{"cluster_size": 0, "stage_rows": r, "stage_threads": c}
+        cands += [{"cluster_size": cn, "persist_rows": 0} for cn in (16, 8, 4, 2)]
+    cands += [{"cluster_size": 0, "persist_rows": r} for r in (16, 8, 4)]
+    cands += [{"cluster_size": 0, "persist_rows": 0, "stage_rows": r, "stage_threads": c}
               for c in (256, 128) for r in (32, 16, 8, 4)]
-    cands += [{"cluster_size": 0, "stage_rows": 0, "rows_per_cta": r} for r in (16, 8, 4)]
+    cands += [{"cluster_size": 0, "persist_rows": 0, "stage_rows": 0, "rows_per_cta": r} for r in (16, 8, 4)]
     return cands
 
 
@@ -162,7 +164,7 @@ def tune_plan(plan, steps: int = 8, repeats: int = 3, cache: TuneCache | None = 
     best, ms, tried = search(plan_candidates(start), apply, _timer(step, flush), repeats)
     if best is None:
         plan.set_config(**{k: start[k] for k in ("rows_per_cta", "threads", "n_chunks", "cluster_size",
-                                                   "stage_rows", "stage_threads")})
+                                                   "stage_rows", "stage_threads", "persist_rows")})
         return {"config": None, "ms": None, "cached": False}
     plan.set_config(**best)
     cache.put(key, {"config": best, "ms": ms, "tried": tried})

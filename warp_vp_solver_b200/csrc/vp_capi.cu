@@ -91,6 +91,15 @@ struct vp_plan {
     void* d_tw = nullptr;      // nx/2 complex
     void* d_mult = nullptr;    // nx reals (imaginary part)
     void* d_circ = nullptr;    // nx reals
+    // persistent forward path (vp_persist.cu)
+    PersistHost pst;           // launch shape and host tables (pst.R == 0: not eligible)
+    int pst_on = 0;            // forward loops (and the adjoint's recomputation) use it
+    int2* d_pquad = nullptr;   // [nv / 4]
+    float4* d_ptq = nullptr;   // [nv / 4]
+    int2* d_pchunk = nullptr;  // [nv / 256]
+    float* d_dfeq = nullptr;   // [nv]
+    float* d_ctab2 = nullptr;  // [2 nx + 8]
+    unsigned long long wait_ns = 1000000000ull;   // limit of each device-side grid barrier wait
 };
 
 namespace vpb {
@@ -311,7 +320,7 @@ static int resolve_every(const vp_plan* p, int n_steps, int every) {
 }
 
 struct WsLayout {
-    size_t hbuf0, hbuf1, seg, part, counter, vsh, E, grho, gscratch, total;
+    size_t hbuf0, hbuf1, seg, part, counter, vsh, E, grho, gscratch, prho, pvsh, peep, pbar, total;
 };
 
 static WsLayout ws_layout(const vp_plan* p, int n_steps, int every) {
@@ -329,6 +338,12 @@ static WsLayout ws_layout(const vp_plan* p, int n_steps, int every) {
     L.E = off; off += align256((size_t)p->nx * real_size(p));
     L.grho = off; off += align256((size_t)p->nx * real_size(p));
     L.gscratch = off; off += align256((size_t)2 * p->nx * real_size(p));
+    if (p->pst.R > 0) {   // persistent path: rho (two steps), field-slice shifts, energy partials, barrier
+        L.prho = off; off += align256((size_t)2 * p->nx * sizeof(float));
+        L.pvsh = off; off += align256((size_t)p->nx * sizeof(VShift<float>));
+        L.peep = off; off += align256((size_t)4 * p->pst.G * sizeof(double));
+        L.pbar = off; off += 256;
+    }
     L.total = off;
     return L;
 }
@@ -364,6 +379,31 @@ static PoissonTables<T> poisson_tables(const vp_plan* p, unsigned char* ws, cons
     P.gscratch = (ws != nullptr && L != nullptr) ? reinterpret_cast<T*>(ws + L->gscratch) : nullptr;
     P.use_smem = in_smem ? 1 : 0;
     return P;
+}
+
+// Arguments of a persistent launch common to the forward loop and the adjoint's recomputation.
+static PersistArgs persist_args(const vp_plan* p, unsigned char* ws, const WsLayout& L) {
+    PersistArgs a{};
+    a.nx = p->nx;
+    a.nv = p->nv;
+    a.n_chunks = p->nv / 256;
+    a.quad = p->d_pquad;
+    a.tq = p->d_ptq;
+    a.chunk = p->d_pchunk;
+    a.feq = p->d_feq;
+    a.dfeq = p->d_dfeq;
+    a.vtab = static_cast<const float*>(p->d_vtab);
+    a.ctab = p->d_ctab2;
+    a.dv = (float)p->dv;
+    a.dx = (float)p->dx;
+    a.dtdv = (float)(p->dt / p->dv);
+    a.rho = reinterpret_cast<float*>(ws + L.prho);
+    a.vsh_g = reinterpret_cast<VShift<float>*>(ws + L.pvsh);
+    a.eep = reinterpret_cast<double*>(ws + L.peep);
+    a.bar = reinterpret_cast<unsigned*>(ws + L.pbar);
+    a.status = p->d_status;
+    a.wait_ns = p->wait_ns;
+    return a;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -427,6 +467,28 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
         VP_CUDA(launch_res_fwd<T>(r, p->feq2d != 0, p->res_cn, p->res_threads, p->res_smem, s),
                 "cluster-resident forward launch");
         return VP_OK;
+    }
+
+    if constexpr (sizeof(T) == 4) {
+        if (p->pst_on && !p->merged && ring == nullptr) {
+            PersistArgs pa = persist_args(p, ws, L);
+            pa.mode = 0;
+            pa.n_steps = T_steps;
+            pa.K = K;
+            pa.hbuf0 = reinterpret_cast<float*>(hbuf[0]);
+            pa.hbuf1 = reinterpret_cast<float*>(hbuf[1]);
+            pa.ckpt = reinterpret_cast<float*>(ckpt);
+            pa.f_iv = f_iv;
+            pa.H = reinterpret_cast<const float*>(H);
+            pa.f_hist = reinterpret_cast<float*>(f_hist);
+            pa.f_final = f_final;
+            pa.E_hist = reinterpret_cast<float*>(E_hist);
+            pa.ee_hist = reinterpret_cast<float*>(ee_hist);
+            pa.E_tape = reinterpret_cast<float*>(E_all);
+            pa.vsh_tape = reinterpret_cast<VShift<float>*>(vsh_all);
+            VP_CUDA(launch_persist_fwd(pa, p->pst, s), "persistent forward launch");
+            return VP_OK;
+        }
     }
 
     VP_CUDA(cudaMemsetAsync(counter, 0, 256, s), "cudaMemsetAsync(counter)");
@@ -608,6 +670,24 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
         current_seg = sgi;
         const int n0 = sgi * K;
         const int n1 = std::min(n0 + K, T_steps);
+        if constexpr (sizeof(T) == 4) {
+            if (p->pst_on && !p->merged) {
+                // the forward's persistent kernel replays the segment with the tape's shifts:
+                // bitwise the states the forward computed
+                if (n1 - 1 > n0) {
+                    PersistArgs pa = persist_args(p, ws, L);
+                    pa.mode = 1;
+                    pa.first_step = n0;
+                    pa.n_steps = n1 - 1;
+                    pa.K = K;
+                    pa.seg = reinterpret_cast<float*>(seg);
+                    pa.ckpt = const_cast<float*>(reinterpret_cast<const float*>(ckpt));
+                    pa.vsh_tape_in = reinterpret_cast<const VShift<float>*>(vsh_all);
+                    VP_CUDA(launch_persist_fwd(pa, p->pst, s), "persistent recompute launch");
+                }
+                return VP_OK;
+            }
+        }
         for (int n = n0; n < n1 - 1; ++n) {
             fa.h_in = h_ptr(n);
             fa.h_out = h_mut(n + 1);
@@ -724,8 +804,32 @@ static void free_plan(vp_plan* p) {
     cudaFree(p->d_tw);
     cudaFree(p->d_mult);
     cudaFree(p->d_circ);
+    cudaFree(p->d_pquad);
+    cudaFree(p->d_ptq);
+    cudaFree(p->d_pchunk);
+    cudaFree(p->d_dfeq);
+    cudaFree(p->d_ctab2);
     cudaSetDevice(prev);
     delete p;
+}
+
+// c = real(ifft(m)) for the spectral multiplier's imaginary part: c[k] = -(1/nx) * sum_q mult_im[q]
+// * sin(2*pi*((q*k) mod nx)/nx), q ascending, from a table of the nx sines (O(nx^2) multiply-adds).
+static std::vector<double> circulant_of(int nx, const std::vector<double>& mult_im) {
+    std::vector<double> sn(nx);
+    for (int r = 0; r < nx; ++r) sn[r] = std::sin(2.0 * M_PI * (double)r / (double)nx);
+    std::vector<double> c(nx, 0.0);
+    for (int k = 0; k < nx; ++k) {
+        double acc = 0.0;
+        int idx = 0;
+        for (int q = 0; q < nx; ++q) {
+            acc += mult_im[q] * sn[idx];
+            idx += k;
+            idx -= idx >= nx ? nx : 0;
+        }
+        c[k] = -acc / nx;
+    }
+    return c;
 }
 
 template <typename T>
@@ -817,10 +921,12 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
     // x half-step table: s_j = 0.5*v_j*dt/dx, m_j = floor(-s_j) mod nx, t_j = -s_j - floor(-s_j)
     std::vector<int> mx(nv);
     std::vector<double> tx(nv);
+    std::vector<long long> m_signed(nv);
     for (int j = 0; j < nv; ++j) {
         const double sj = 0.5 * mesh->vs[j] * dt / mesh->dx;
         const double mf = std::floor(-sj);
         tx[j] = -sj - mf;
+        m_signed[j] = std::fabs(mf) < 1e15 ? (long long)mf : 0;
         if (j == 0 || (long long)mf < p->mx_lo) p->mx_lo = (long long)mf;
         if (j == 0 || (long long)mf > p->mx_hi) p->mx_hi = (long long)mf;
         long long mi = (long long)mf % nx;
@@ -866,16 +972,7 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
     // circulant kernel c = real(ifft(m)): c[k] = -(1/nx) * sum_q mult_im[q] * sin(2*pi*q*k/nx)
     // (needed by the non-power-of-two FFT fallback and by the cluster-resident path, nx <= 512)
     std::vector<double> circ(nx, 0.0);
-    if (!p->pow2 || nx <= 512) {
-        for (int k = 0; k < nx; ++k) {
-            double s = 0.0;
-            for (int q = 0; q < nx; ++q) {
-                const long long r = ((long long)q * k) % nx;
-                s += mult_im[q] * std::sin(2.0 * M_PI * (double)r / (double)nx);
-            }
-            circ[k] = -s / nx;
-        }
-    }
+    if (!p->pow2 || nx <= 512) circ = circulant_of(nx, mult_im);
     const size_t rs = dtype == VP_F64 ? 8 : 4;
     const size_t area = poisson_area_size(nx, rs);
     p->tail_inline = area <= kInlineTailBytes ? 1 : 0;
@@ -963,6 +1060,29 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
         return rc;
     }
     choose_staged(p, n_sms);
+    // persistent forward path: float32, x-invariant f_eq, nv a multiple of 256, nx <= 16384 (the
+    // circulant table costs O(nx^2) on the host); on by default where the state is not
+    // cluster-resident
+    if (dtype == VP_F32 && inv && p->d_vtab != nullptr && nx <= 16384 &&
+        persist_prepare(p->pst, nx, nv, m_signed, tx, n_sms, 0)) {
+        std::vector<float> dfeq(nv);
+        for (int j = 0; j < nv; ++j) dfeq[j] = (float)(f_eq_host[(j + 1) % nv] - f_eq_host[j]);
+        if (circ.size() != (size_t)nx || (p->pow2 && nx > 512)) circ = circulant_of(nx, mult_im);
+        std::vector<float> ctab2((size_t)2 * nx + 8);
+        for (size_t j = 0; j < ctab2.size(); ++j)
+            ctab2[j] = (float)circ[(size_t)((((long long)j - nx) % nx + nx) % nx)];
+        if ((rc = upload_bytes((void**)&p->d_pquad, p->pst.quad.data(), p->pst.quad.size() * sizeof(int2))) ||
+            (rc = upload_bytes((void**)&p->d_ptq, p->pst.tq.data(), p->pst.tq.size() * sizeof(float))) ||
+            (rc = upload_bytes((void**)&p->d_pchunk, p->pst.chunk.data(), p->pst.chunk.size() * sizeof(int2))) ||
+            (rc = upload_bytes((void**)&p->d_dfeq, dfeq.data(), dfeq.size() * sizeof(float))) ||
+            (rc = upload_bytes((void**)&p->d_ctab2, ctab2.data(), ctab2.size() * sizeof(float)))) {
+            free_plan(p);
+            return rc;
+        }
+        p->pst_on = p->res_cn == 0 ? 1 : 0;
+    } else {
+        p->pst = PersistHost{};
+    }
     {   // trapezoid integral of f_eq (kl_divergence's norm_eq without eps, utils.py:59-64)
         double tot = 0.0;
         for (int i = 0; i < nx; ++i) {
@@ -997,6 +1117,9 @@ int vp_plan_get_config(const vp_plan* plan, vp_launch_config* out) {
     out->stage_threads = plan->stage_span > 0 ? plan->scfg.threads : 0;
     out->stage_span = plan->stage_span;
     out->stage_smem_bytes = plan->stage_span > 0 ? (int64_t)plan->scfg.smem : 0;
+    out->persist_rows = plan->pst_on ? plan->pst.R : 0;
+    out->persist_ctas = plan->pst_on ? plan->pst.G : 0;
+    out->persist_smem_bytes = plan->pst_on ? (int64_t)plan->pst.smem : 0;
     return VP_OK;
 }
 
@@ -1035,6 +1158,31 @@ int vp_plan_set_config(vp_plan* plan, const vp_launch_config* cfg) {
     } else {
         plan->stage_span = 0;
     }
+    if (cfg->persist_rows != 0) {
+        if (plan->d_pquad == nullptr)
+            return set_err(VP_ERR_ARG, "persist_rows=%d: the persistent path needs a float32 plan with an "
+                                       "x-invariant f_eq, nv a multiple of 256 and nx <= 16384", cfg->persist_rows);
+        const PersistHost keep = plan->pst;
+        std::vector<long long> ms(plan->host_mx.size());
+        std::vector<double> tx(plan->host_mx.size());
+        for (size_t q = 0; q < keep.quad.size(); ++q)
+            for (int e = 0; e < 4; ++e) {
+                ms[4 * q + e] = keep.quad[q].x + ((keep.quad[q].y >> e) & 1);
+                tx[4 * q + e] = keep.tq[4 * q + e];
+            }
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (!persist_prepare(plan->pst, plan->nx, plan->nv, ms, tx, sms, cfg->persist_rows)) {
+            plan->pst = keep;
+            return set_err(VP_ERR_ARG, "persist_rows=%d is not usable for a %dx%d grid (4, 8 or 16 dividing nx, "
+                                       "with every CTA resident at once)",
+                           cfg->persist_rows, plan->nx, plan->nv);
+        }
+        plan->pst_on = 1;
+    } else {
+        plan->pst_on = 0;
+    }
     plan->res_cn = cn;
     plan->res_smem = res_smem;
     plan->res_threads = cn ? res_threads(plan->nx / cn, plan->nv) : 0;
@@ -1061,6 +1209,12 @@ int vp_plan_set_scheme(vp_plan* plan, int32_t scheme) {
 int vp_plan_get_scheme(const vp_plan* plan, int32_t* scheme) {
     if (!plan || !scheme) return set_err(VP_ERR_ARG, "plan and scheme must not be NULL");
     *scheme = plan->merged ? VP_SCHEME_MERGED : VP_SCHEME_STRANG;
+    return VP_OK;
+}
+
+int vp_plan_set_wait_limit(vp_plan* plan, uint64_t ns) {
+    if (!plan) return set_err(VP_ERR_ARG, "plan must not be NULL");
+    plan->wait_ns = ns;
     return VP_OK;
 }
 

@@ -6,6 +6,7 @@
 #include <stddef.h>
 
 #include <string>
+#include <vector>
 
 namespace vpb {
 
@@ -183,6 +184,64 @@ cudaError_t launch_bwd_staged(const BwdArgs<T>& a, const LaunchCfg& c, cudaStrea
 template <typename T>
 cudaError_t set_staged_bwd_smem_limit(size_t bytes);
 size_t staged_bwd_smem_bytes(int span, int R, int C, size_t real_size);
+
+// ---- persistent forward time loop (vp_persist.cu): float32, x-invariant f_eq, Strang scheme ----
+// State slot of step n: ckpt + (n / K) * nx * nv when ckpt != null and n % K == 0; otherwise
+// hbuf0/hbuf1 by the parity of n (full mode) or seg + (n % K - 1) * nx * nv (replay mode).
+struct PersistArgs {
+    int nx, nv;
+    int n_steps;                // full mode: T; replay mode: the step after the last one replayed
+    int n_chunks;               // nv / 256
+    int bands_per_cta, span_max, win_lo, win_rows, field_dist;   // launch shape (set by the launcher)
+    int mode;                   // 0: full forward (prologue from f_iv, field, outputs); 1: replay
+                                //    steps first_step .. n_steps - 1 with the tape's v shifts
+    int first_step;
+    int K;
+    float* hbuf0;
+    float* hbuf1;
+    float* seg;
+    float* ckpt;
+    const double* f_iv;
+    const float* H;
+    const int2* quad;           // per 4 columns: smallest x offset bm (signed), bit e set when
+                                // column e's offset is bm + 1                     [nv / 4]
+    const float4* tq;           // per 4 columns: x weights                        [nv / 4]
+    const int2* chunk;          // per 256 columns: (min bm, max bm)               [nv / 256]
+    const double* feq;          // the f_eq row                                     [nv]
+    const float* dfeq;          // f_eq[j+1] - f_eq[j] (periodic), rounded from float64 [nv]
+    const float* vtab;          // A_m, B_m tables of the staged kernels          [2][8][nv]
+    const float* ctab;          // ctab[j] = c[(j - nx) mod nx], c = real(ifft(m)) [2 nx + 8]
+    float dv, dx, dtdv;
+    float* rho;                 // [2][nx]
+    VShift<float>* vsh_g;       // [nx] v shifts of the field slices
+    const VShift<float>* vsh_tape_in;   // replay: the forward's v shifts [n_steps][nx]
+    double* eep;                // [4][G] energy partials
+    unsigned* bar;              // grid barrier counter (zeroed by the launcher)
+    unsigned* status;
+    unsigned long long wait_ns; // limit of each grid barrier wait
+    float* f_hist;
+    double* f_final;
+    float* E_hist;
+    float* ee_hist;
+    float* E_tape;
+    VShift<float>* vsh_tape;
+};
+
+struct PersistHost {
+    int R = 0, G = 0, bands_per_cta = 0, span_max = 0, win_lo = 0, win_rows = 0, field_dist = 0;
+    size_t smem = 0;
+    std::vector<int2> quad;
+    std::vector<float> tq;
+    std::vector<int2> chunk;
+};
+
+// Builds the persistent path's tables and launch shape for a grid (force_rows: 0 = automatic, else
+// the band height 4, 8 or 16); false when the grid is not eligible. m_signed: the unreduced x
+// half-step offsets floor(-s_j); tx their weights.
+bool persist_prepare(PersistHost& ph, int nx, int nv, const std::vector<long long>& m_signed,
+                     const std::vector<double>& tx, int n_sms, int force_rows);
+cudaError_t launch_persist_fwd(const PersistArgs& a, const PersistHost& ph, cudaStream_t s);
+size_t persist_smem_bytes(int span_max, int win_rows, int R);
 
 // Raises VP_STATUS_NONFINITE_INPUT in *status when f (n doubles) or H (nx reals, double when h64)
 // holds a NaN or an infinity (vp_ops.cu).

@@ -100,6 +100,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
     return ok != 0;
 }
 
+// Non-blocking test of the phase (try_wait may suspend the thread for a hardware-defined time).
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
 __device__ __forceinline__ uint64_t global_ns() {
     uint64_t t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -108,9 +121,9 @@ __device__ __forceinline__ uint64_t global_ns() {
 
 // Bounded wait for the phase of the given parity: gives up after limit_ns nanoseconds (checked
 // every 256 polls, and after at most 2^24 polls); limit_ns == 0 gives up at the first poll that
-// does not find the phase complete.
+// does not find the phase complete (a non-blocking test).
 __device__ bool mbar_wait(uint64_t* bar, unsigned parity, unsigned long long limit_ns) {
-    if (limit_ns == 0) return mbar_try_wait(bar, parity);
+    if (limit_ns == 0) return mbar_test_wait(bar, parity);
     const uint64_t t0 = global_ns();
     for (unsigned it = 0; it < (1u << 24); ++it) {
         if (mbar_try_wait(bar, parity)) return true;

@@ -83,9 +83,11 @@ class Plan:
 
     def set_config(self, rows_per_cta: int | None = None, threads: int | None = None,
                    n_chunks: int | None = None, cluster_size: int | None = None,
-                   stage_rows: int | None = None, stage_threads: int | None = None) -> None:
+                   stage_rows: int | None = None, stage_threads: int | None = None,
+                   persist_rows: int | None = None) -> None:
         """Change the launch shape; arguments left as None keep their current values.
-        ``stage_rows=0`` turns the staged forward step off."""
+        ``stage_rows=0`` turns the staged forward step off, ``persist_rows=0`` the persistent
+        (one launch per loop) path."""
         cur = self.get_config()
         c = _capi.LaunchConfig()
         c.rows_per_cta = cur["rows_per_cta"] if rows_per_cta is None else int(rows_per_cta)
@@ -94,8 +96,13 @@ class Plan:
         c.cluster_size = cur["cluster_size"] if cluster_size is None else int(cluster_size)
         c.stage_rows = cur["stage_rows"] if stage_rows is None else int(stage_rows)
         c.stage_threads = cur["stage_threads"] if stage_threads is None else int(stage_threads)
+        c.persist_rows = cur["persist_rows"] if persist_rows is None else int(persist_rows)
         _capi.check(self.lib.vp_plan_set_config(self._h, ctypes.byref(c)))
-        self._ws = {}   # workspace size depends on n_chunks
+        self._ws = {}   # workspace size depends on n_chunks and the persistent launch shape
+
+    def set_wait_limit(self, ns: int) -> None:
+        """Limit of each device-side grid-barrier wait of the persistent launches (ns; 0: no wait)."""
+        _capi.check(self.lib.vp_plan_set_wait_limit(self._h, int(ns)))
 
     def status(self) -> int:
         """Device-side status flags (synchronous): VP_STATUS_NONFINITE_INPUT, VP_STATUS_WAIT_TIMEOUT."""
