@@ -98,7 +98,7 @@ struct vp_plan {
     float4* d_ptq = nullptr;   // [nv / 4]
     int2* d_pchunk = nullptr;  // [nv / 256]
     float* d_dfeq = nullptr;   // [nv]
-    float* d_ctab2 = nullptr;  // [2 nx + 8]
+    float* d_ctab2 = nullptr;  // [3 nx + 8]
     unsigned long long wait_ns = 1000000000ull;   // limit of each device-side grid barrier wait
 };
 
@@ -341,7 +341,7 @@ static WsLayout ws_layout(const vp_plan* p, int n_steps, int every) {
     if (p->pst.R > 0) {   // persistent path: rho (two steps), field-slice shifts, energy partials, barrier
         L.prho = off; off += align256((size_t)2 * p->nx * sizeof(float));
         L.pvsh = off; off += align256((size_t)p->nx * sizeof(VShift<float>));
-        L.peep = off; off += align256((size_t)4 * p->pst.G * sizeof(double));
+        L.peep = off; off += align256((size_t)std::max(1, n_steps) * p->pst.G * sizeof(double));
         L.pbar = off; off += 256;
     }
     L.total = off;
@@ -1061,14 +1061,13 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
     }
     choose_staged(p, n_sms);
     // persistent forward path: float32, x-invariant f_eq, nv a multiple of 256, nx <= 16384 (the
-    // circulant table costs O(nx^2) on the host); on by default where the state is not
-    // cluster-resident
+    // circulant table costs O(nx^2) on the host)
     if (dtype == VP_F32 && inv && p->d_vtab != nullptr && nx <= 16384 &&
         persist_prepare(p->pst, nx, nv, m_signed, tx, n_sms, 0)) {
         std::vector<float> dfeq(nv);
         for (int j = 0; j < nv; ++j) dfeq[j] = (float)(f_eq_host[(j + 1) % nv] - f_eq_host[j]);
         if (circ.size() != (size_t)nx || (p->pow2 && nx > 512)) circ = circulant_of(nx, mult_im);
-        std::vector<float> ctab2((size_t)2 * nx + 8);
+        std::vector<float> ctab2((size_t)3 * nx + 8);
         for (size_t j = 0; j < ctab2.size(); ++j)
             ctab2[j] = (float)circ[(size_t)((((long long)j - nx) % nx + nx) % nx)];
         if ((rc = upload_bytes((void**)&p->d_pquad, p->pst.quad.data(), p->pst.quad.size() * sizeof(int2))) ||
@@ -1079,7 +1078,9 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
             free_plan(p);
             return rc;
         }
-        p->pst_on = p->res_cn == 0 ? 1 : 0;
+        // default: grids that are not cluster-resident and whose field inputs fit beside the stage
+        // buffers (about nx <= 3000); on larger grids the per-step kernels keep more warps busy
+        p->pst_on = (p->res_cn == 0 && !p->pst.fs_alias) ? 1 : 0;
     } else {
         p->pst = PersistHost{};
     }

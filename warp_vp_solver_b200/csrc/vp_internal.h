@@ -193,6 +193,7 @@ struct PersistArgs {
     int n_steps;                // full mode: T; replay mode: the step after the last one replayed
     int n_chunks;               // nv / 256
     int bands_per_cta, span_max, win_lo, win_rows, field_dist;   // launch shape (set by the launcher)
+    int stage_floats, fs_alias, stages, field_rows;
     int mode;                   // 0: full forward (prologue from f_iv, field, outputs); 1: replay
                                 //    steps first_step .. n_steps - 1 with the tape's v shifts
     int first_step;
@@ -210,12 +211,12 @@ struct PersistArgs {
     const double* feq;          // the f_eq row                                     [nv]
     const float* dfeq;          // f_eq[j+1] - f_eq[j] (periodic), rounded from float64 [nv]
     const float* vtab;          // A_m, B_m tables of the staged kernels          [2][8][nv]
-    const float* ctab;          // ctab[j] = c[(j - nx) mod nx], c = real(ifft(m)) [2 nx + 8]
+    const float* ctab;          // ctab[j] = c[(j - nx) mod nx], c = real(ifft(m)) [3 nx + 8]
     float dv, dx, dtdv;
     float* rho;                 // [2][nx]
     VShift<float>* vsh_g;       // [nx] v shifts of the field slices
     const VShift<float>* vsh_tape_in;   // replay: the forward's v shifts [n_steps][nx]
-    double* eep;                // [4][G] energy partials
+    double* eep;                // [n_steps][G] energy partials
     unsigned* bar;              // grid barrier counter (zeroed by the launcher)
     unsigned* status;
     unsigned long long wait_ns; // limit of each grid barrier wait
@@ -229,6 +230,7 @@ struct PersistArgs {
 
 struct PersistHost {
     int R = 0, G = 0, bands_per_cta = 0, span_max = 0, win_lo = 0, win_rows = 0, field_dist = 0;
+    int stage_floats = 0, fs_alias = 0, stages = 2, field_rows = 0;
     size_t smem = 0;
     std::vector<int2> quad;
     std::vector<float> tq;
@@ -241,7 +243,8 @@ struct PersistHost {
 bool persist_prepare(PersistHost& ph, int nx, int nv, const std::vector<long long>& m_signed,
                      const std::vector<double>& tx, int n_sms, int force_rows);
 cudaError_t launch_persist_fwd(const PersistArgs& a, const PersistHost& ph, cudaStream_t s);
-size_t persist_smem_bytes(int span_max, int win_rows, int R);
+size_t persist_smem_bytes(int span_max, int win_rows, int R, int nx, int nv, int field_rows, int stages,
+                          int* stage_floats, int* fs_alias);
 
 // Raises VP_STATUS_NONFINITE_INPUT in *status when f (n doubles) or H (nx reals, double when h64)
 // holds a NaN or an infinity (vp_ops.cu).

@@ -13,9 +13,11 @@
 // m_j of 4 neighbouring columns differ by at most one cell (checked on the host), so the thread
 // walks one window of R + 4 rows of the v-step output o, rows r0 + 2*bm + k (bm = the smallest
 // shift of its quad); a column whose shift is bm + 1 reads the same window two rows lower (a
-// register select). The window rows of a tile are staged into shared memory by bulk-async copies
-// (cp.async.bulk, no multicast) completed on an mbarrier, double-buffered so that the next tile's
-// rows arrive while this one computes. Per window row the v step reads its 5 source cells with one
+// register select). The window rows of a tile are staged into shared memory by asynchronous
+// 16-byte copies of every thread (cp.async.cg through L2, one commit group per tile) into a ring
+// of up to 8 stage buffers, so that later tiles' rows arrive while one computes (one-kilobyte
+// cp.async.bulk copies per row were measured to be limited by the copy engine's per-copy cost:
+// about 80 ns each). Per window row the v step reads its 5 source cells with one
 // 16-byte and one 4-byte shared-memory load and forms V(f_eq) - f_eq for the usual shifts m = 0
 // and m = -1 from the first differences D of f_eq held in registers:
 //   m = 0:  o = h[j] + t*((h[j+1] - h[j]) + D[j])
@@ -31,9 +33,9 @@
 // per-CTA partials that CTA 0 sums in a fixed order one step later, so every result is
 // deterministic.
 //
-// Every wait is bounded: a grid barrier that does not complete within the plan's wait limit
-// raises VP_STATUS_WAIT_TIMEOUT in the plan's status word and the CTA returns (no bulk copy is in
-// flight at a barrier); the bulk-copy waits give up after one second the same way.
+// The grid barrier's wait is bounded: a barrier that does not complete within the plan's wait
+// limit raises VP_STATUS_WAIT_TIMEOUT in the plan's status word and the CTA returns after waiting
+// for its own copies in flight.
 
 #include "../../include/vp_b200.h"
 #include "vp_device.cuh"
@@ -46,10 +48,13 @@ namespace vpb {
 
 namespace {
 
-constexpr int kPstThreads = 64;
-constexpr int kPstC = 4 * kPstThreads;      // columns per tile
+constexpr int kPstGroup = 64;              // threads of a column group: one tile of 256 columns
+constexpr int kPstGroups = 4;              // column groups per CTA (different chunks of a band)
+constexpr int kPstThreads = kPstGroup * kPstGroups;
+constexpr int kPstWarps = kPstThreads / 32;
+constexpr int kPstC = 4 * kPstGroup;       // columns per tile
 constexpr int kPstW = kPstC + 8;            // staged row: 4 halo columns on each side
-constexpr unsigned long long kCopyWaitNs = 1000000000ull;
+constexpr int kPstMaxStages = 8;            // stage buffers: tiles in flight ahead of the compute
 
 __device__ __forceinline__ uint32_t pst_smem(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -61,39 +66,28 @@ __device__ __forceinline__ unsigned long long pst_now() {
     return t;
 }
 
-__device__ __forceinline__ void pst_mbar_init(uint64_t* bar) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(pst_smem(bar)) : "memory");
+// Asynchronous 16-byte (or 4-byte) copies from global to shared memory through L2 (.cg: no L1
+// allocation, so data written earlier in this launch by other CTAs is read coherently), grouped
+// per tile with commit/wait_group.
+__device__ __forceinline__ void pst_cp16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(pst_smem(dst)), "l"(src) : "memory");
 }
-
-__device__ __forceinline__ void pst_expect_tx(uint64_t* bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(pst_smem(bar)), "r"(bytes)
-                 : "memory");
+__device__ __forceinline__ void pst_cp4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(pst_smem(dst)), "l"(src) : "memory");
 }
-
-__device__ __forceinline__ bool pst_try_wait(uint64_t* bar, unsigned parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok)
-        : "r"(pst_smem(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Bulk-async copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from global to
-// this CTA's shared memory, counted on `bar`.
-__device__ __forceinline__ void pst_bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            pst_smem(dst)),
-        "l"(src), "r"(bytes), "r"(pst_smem(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ void pst_fence_async_global() {
-    asm volatile("fence.proxy.async.global;" ::: "memory");
+__device__ __forceinline__ void pst_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Waits until at most n of this thread's copy groups are pending (n < 8).
+__device__ __forceinline__ void pst_cp_wait(int n) {
+    switch (n) {
+        case 0: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
+        case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
+        case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
+        case 3: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
+        case 4: asm volatile("cp.async.wait_group 4;" ::: "memory"); break;
+        case 5: asm volatile("cp.async.wait_group 5;" ::: "memory"); break;
+        case 6: asm volatile("cp.async.wait_group 6;" ::: "memory"); break;
+        default: asm volatile("cp.async.wait_group 7;" ::: "memory"); break;
+    }
 }
 
 __device__ __forceinline__ unsigned pst_ld_acquire(const unsigned* p) {
@@ -113,7 +107,6 @@ __device__ __forceinline__ unsigned pst_add_release(unsigned* p, unsigned v) {
 // (limit 0: only the last CTA to arrive passes), after raising VP_STATUS_WAIT_TIMEOUT.
 __device__ bool pst_grid_barrier(unsigned* ctr, unsigned index, unsigned G, unsigned long long limit_ns,
                                  unsigned* status, int* s_flag) {
-    pst_fence_async_global();   // this thread's state stores are visible to later bulk copies
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
@@ -177,26 +170,45 @@ __device__ __forceinline__ int2 pst_rinfo(const VShift<float> v, int nv) {
 
 }  // namespace
 
-// E_i = sum_k c[(i-k) mod nx] rho_k for n_rows rows i = (first + r) mod nx, r < n_rows; calls
-// out(r, E_i) from one lane per row. A warp takes 4 consecutive rows; lane g sums k = g, g + 32,
-// ... in order (the table ctab[j] = c[(j - nx) mod nx] covers the unreduced row indices), then a
-// fixed-order butterfly combines the 32 partial sums.
+// Stages the inputs of the circulant product for n_rows rows starting at `first` (unreduced) into
+// shared memory: rho (nx floats, 16-byte loads through L2: written by this launch) at fs and the
+// coefficient slice cs[u] = ctab[f0 + 1 + u], u < nx + n_rows + 4 (f0 = first mod nx) after it,
+// where ctab[j] = c[(j - nx) mod nx]; then coefficient (row r, k) = cs[nx - 1 + r - k]. Returns f0.
+// Ends with a block barrier.
+__device__ __forceinline__ int pst_field_inputs(float* fs, const float* rho, const float* __restrict__ ctab,
+                                                int nx, int first, int n_rows) {
+    const int f0 = pst_wrap(first, nx);
+    // asynchronous copies (their latencies overlap), then wait for this group only: tile copies
+    // issued earlier may stay in flight
+    for (int k = (int)threadIdx.x; k < nx / 4; k += blockDim.x) pst_cp16(fs + 4 * k, rho + 4 * k);
+    float* cs = fs + nx;
+    const int len = nx + n_rows + 4;
+    for (int u = threadIdx.x; u < len; u += blockDim.x) pst_cp4(cs + u, ctab + f0 + 1 + u);
+    pst_cp_commit();
+    pst_cp_wait(0);
+    __syncthreads();
+    return f0;
+}
+
+// E_r = sum_k c[(f0 + r - k) mod nx] rho_k for r < n_rows from the staged inputs; calls out(r, E_r)
+// from one lane per row. A warp takes 4 consecutive rows; lane g sums k = g, g + 32, ... in order
+// (consecutive lanes read consecutive words of both arrays), then a fixed-order butterfly combines
+// the 32 partial sums.
 template <typename F>
-__device__ __forceinline__ void pst_circ_rows(const float* __restrict__ ctab, const float* __restrict__ rho,
-                                              int nx, int first, int n_rows, F&& out) {
+__device__ __forceinline__ void pst_circ_rows(const float* fs, int nx, int n_rows, F&& out) {
     const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int ngrp = (n_rows + 3) >> 2;
+    const float* cs = fs + nx;
     for (int grp = (int)(threadIdx.x >> 5); grp < ngrp; grp += nw) {
-        const int i0 = pst_wrap(first + 4 * grp, nx);
         float acc[4] = {0.f, 0.f, 0.f, 0.f};
-        const float* cp = ctab + nx + i0 - lane;
+        const float* cp = cs + nx - 1 + 4 * grp - lane;
 #pragma unroll 4
         for (int k = lane; k < nx; k += 32) {
-            const float xk = __ldcg(rho + k);
-            acc[0] += __ldg(cp) * xk;
-            acc[1] += __ldg(cp + 1) * xk;
-            acc[2] += __ldg(cp + 2) * xk;
-            acc[3] += __ldg(cp + 3) * xk;
+            const float xk = fs[k];
+            acc[0] += cp[0] * xk;
+            acc[1] += cp[1] * xk;
+            acc[2] += cp[2] * xk;
+            acc[3] += cp[3] * xk;
             cp -= 32;
         }
 #pragma unroll
@@ -221,44 +233,91 @@ __device__ __forceinline__ void pst_circ_rows(const float* __restrict__ ctab, co
     }
 }
 
-// Shared memory of a launch: two stage buffers, the row records of the union window, the row-sum
-// scratch.
-size_t persist_smem_bytes(int span_max, int win_rows, int R) {
-    size_t b = (size_t)2 * span_max * kPstW * sizeof(float);
+// Per-quad constants of the tiles (x weights, f_eq differences, smallest shift and its delta bits,
+// the f_eq difference left of the quad), kept in shared memory for the whole launch when the
+// grid's nv/4 records fit in kPstQuadSmemBytes.
+struct __align__(16) PstQuad {
+    float4 t;
+    float4 D;
+    int bm, mask;
+    float Dm1, pad;
+};
+constexpr size_t kPstQuadSmemBytes = 24 * 1024;
+
+// Floats of the field's shared-memory inputs for up to n_rows rows (rho, coefficient slice).
+static size_t pst_field_floats(int nx, int n_rows) { return (size_t)2 * nx + n_rows + 8; }
+
+// Field inputs up to this size get their own shared memory (the first tiles of a step then load
+// while the field is solved); larger ones reuse the stage buffers.
+constexpr size_t kPstOwnFieldBytes = 24 * 1024;
+
+// Shared memory of a launch: the stage area (two stage buffers, or the field inputs when those are
+// larger and share it), the row records of the union window, the row-sum scratch, and the field
+// inputs when they have their own region.
+size_t persist_smem_bytes(int span_max, int win_rows, int R, int nx, int nv, int field_rows, int stages,
+                          int* stage_floats, int* fs_alias) {
+    const int groups = std::min(kPstGroups, nv / kPstC);   // groups that have chunks to stage
+    const size_t st = (size_t)groups * stages * span_max * kPstW;
+    const size_t ff = (pst_field_floats(nx, field_rows) + 3) & ~(size_t)3;
+    const bool alias = ff * sizeof(float) > kPstOwnFieldBytes;
+    const size_t area = alias ? std::max(st, ff) : st;
+    size_t b = area * sizeof(float);
     b += ((size_t)win_rows * sizeof(int2) + 15) & ~(size_t)15;
-    b += (size_t)(kPstThreads / 32) * R * sizeof(float) + 16;
+    b += (size_t)kPstWarps * R * sizeof(float) + 16;
+    if (!alias) b += ff * sizeof(float);
+    const size_t qb = (size_t)(nv / 4) * sizeof(PstQuad);
+    if (qb <= kPstQuadSmemBytes) b += qb;
+    if (stage_floats) *stage_floats = (int)area;
+    if (fs_alias) *fs_alias = alias ? 1 : 0;
     return b;
 }
 
 template <int R>
-__global__ void __launch_bounds__(kPstThreads) vp_persist_fwd_kernel(const PersistArgs a) {
+__global__ void __launch_bounds__(kPstThreads, 1) vp_persist_fwd_kernel(const PersistArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ __align__(8) uint64_t full[2];
     __shared__ int s_flag;
-    __shared__ double s_ee[kPstThreads / 32];
+    __shared__ double s_ee[kPstWarps];
 
     const int nx = a.nx, nv = a.nv, nch = a.n_chunks;
     const size_t nxnv = (size_t)nx * nv;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int gid = tid / kPstGroup, gt = tid - gid * kPstGroup;   // column group and its thread
     const int g = blockIdx.x, G = gridDim.x;
     const int b0 = g * a.bands_per_cta;
     const int r_lo = b0 * R;                          // first own row
     const int own_rows = a.bands_per_cta * R;
-    float* stage0 = reinterpret_cast<float*>(smem);
-    float* stage1 = stage0 + (size_t)a.span_max * kPstW;
-    int2* rinfo = reinterpret_cast<int2*>(stage1 + (size_t)a.span_max * kPstW);
+    const int S = a.stages;                           // stage buffers per group
+    float* stages = reinterpret_cast<float*>(smem);
+    int2* rinfo = reinterpret_cast<int2*>(stages + (size_t)a.stage_floats);
     float* red = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(rinfo) +
                                           (((size_t)a.win_rows * sizeof(int2) + 15) & ~(size_t)15));
+    // field inputs: their own region after the row-sum scratch, or the stage area
+    float* fs = a.fs_alias ? stages : red + kPstWarps * R + 4;
+    const size_t ff = ((size_t)2 * nx + a.field_rows + 8 + 3) & ~(size_t)3;
+    const int nq = nv / 4;
+    PstQuad* sq = ((size_t)nq * sizeof(PstQuad) <= kPstQuadSmemBytes)
+                      ? reinterpret_cast<PstQuad*>(a.fs_alias ? red + kPstWarps * R + 4 : fs + ff)
+                      : nullptr;
     const bool replay = a.mode == 1;
     const int n_first = replay ? a.first_step : 0;
     const int n_end = a.n_steps;                      // steps n_first .. n_end - 1
-    const int ntile = a.bands_per_cta * nch;
+    // chunks of this group: c = gid, gid + 4, ...; its tiles per step: bands x those chunks
+    const int cpg = gid < nch ? (nch - gid + kPstGroups - 1) / kPstGroups : 0;
+    const int ntile = a.bands_per_cta * cpg;
 
-    if (tid == 0) {
-        pst_mbar_init(&full[0]);
-        pst_mbar_init(&full[1]);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
+    auto quad_of = [&](int q) -> PstQuad {
+        PstQuad r;
+        const int2 qi = __ldg(a.quad + q);
+        r.t = __ldg(a.tq + q);
+        r.D = __ldg(reinterpret_cast<const float4*>(a.dfeq) + q);
+        r.bm = qi.x;
+        r.mask = qi.y;
+        r.Dm1 = __ldg(a.dfeq + (q == 0 ? nv - 1 : 4 * q - 1));
+        r.pad = 0.f;
+        return r;
+    };
+    if (sq != nullptr)
+        for (int q = tid; q < nq; q += blockDim.x) sq[q] = quad_of(q);
     __syncthreads();
 
     auto slot = [&](int n) -> float* {
@@ -273,47 +332,41 @@ __global__ void __launch_bounds__(kPstThreads) vp_persist_fwd_kernel(const Persi
         if (!pst_grid_barrier(a.bar, bar_index++, (unsigned)G, a.wait_ns, a.status, &s_flag)) alive = false;
         return alive;
     };
+    auto group_sync = [&]() { asm volatile("bar.sync %0, %1;" ::"r"(1 + gid), "r"(kPstGroup) : "memory"); };
 
-    // ---- staging: tile i of a step (band b0 + i / nch, chunk i % nch) into stage i & 1 ----
-    unsigned long long tiles_issued = 0, tiles_used = 0;   // over the whole launch
-    auto issue = [&](int i, const float* src) {
-        const unsigned long long mine = tiles_issued++;
-        if (wid != 0) return;
-        const int bi = i / nch, c = i - bi * nch;
-        const int r0 = (b0 + bi) * R, c0 = c * kPstC;
+    // ---- staging: the group's tile j of a step (band j / cpg, chunk gid + 4 (j % cpg)) goes to
+    // the group's stage (k % S), k counting the group's tiles over the launch; 16-byte
+    // asynchronous copies of the group's threads, one commit group per tile ----
+    constexpr int kPieces = kPstW / 4;               // 16-byte pieces of a staged row
+    unsigned tiles_issued = 0, tiles_used = 0;
+    auto tile_of = [&](int j, int* r0, int* c) {
+        const int bi = j / cpg;
+        *c = gid + kPstGroups * (j - bi * cpg);
+        *r0 = (b0 + bi) * R;
+    };
+    auto stage_ptr = [&](unsigned k) {
+        return stages + (size_t)(gid * S + (int)(k % (unsigned)S)) * a.span_max * kPstW;
+    };
+    auto issue = [&](int j, const float* src) {
+        const unsigned mine = tiles_issued++;
+        int r0, c;
+        tile_of(j, &r0, &c);
+        const int c0 = c * kPstC;
         const int2 cm = __ldg(a.chunk + c);           // (min bm, max bm) over the chunk
         const int span = 2 * (cm.y - cm.x) + R + 4;
         const int lo = r0 + 2 * cm.x;
-        float* st = (mine & 1) ? stage1 : stage0;
-        uint64_t* fb = &full[mine & 1];
-        if (lane == 0) pst_expect_tx(fb, (unsigned)(span * kPstW * sizeof(float)));
-        __syncwarp();
-        pst_fence_async_global();
-        for (int k = lane; k < span; k += 32) {
-            const float* srow = src + (size_t)pst_wrap(lo + k, nx) * nv;
-            float* drow = st + (size_t)k * kPstW;
-            if (c0 > 0 && c0 + kPstC < nv) {
-                pst_bulk_g2s(drow, srow + c0 - 4, kPstW * sizeof(float), fb);
-            } else {
-                const int lc = c0 == 0 ? nv - 4 : c0 - 4;
-                const int rc = c0 + kPstC == nv ? 0 : c0 + kPstC;
-                pst_bulk_g2s(drow, srow + lc, 16, fb);
-                pst_bulk_g2s(drow + 4, srow + c0, kPstC * sizeof(float), fb);
-                pst_bulk_g2s(drow + 4 + kPstC, srow + rc, 16, fb);
-            }
+        float* st = stage_ptr(mine);
+        for (int p = gt; p < span * kPieces; p += kPstGroup) {
+            const int k = p / kPieces, v = p - k * kPieces;
+            int col = c0 - 4 + 4 * v;
+            col += col < 0 ? nv : 0;
+            col -= col >= nv ? nv : 0;
+            pst_cp16(st + (size_t)k * kPstW + 4 * v, src + (size_t)pst_wrap(lo + k, nx) * nv + col);
         }
+        pst_cp_commit();
     };
-    auto wait_stage = [&]() -> bool {
-        uint64_t* fb = &full[tiles_used & 1];
-        const unsigned parity = (unsigned)((tiles_used >> 1) & 1);
-        bool ok = pst_try_wait(fb, parity);
-        if (!ok) {
-            const unsigned long long t0 = pst_now();
-            while (!(ok = pst_try_wait(fb, parity)))
-                if (pst_now() - t0 > kCopyWaitNs) break;
-        }
-        if (!ok && tid == 0) atomicOr(a.status, VP_STATUS_WAIT_TIMEOUT);
-        return __syncthreads_and(ok) != 0;
+    auto issue_first = [&](const float* src) {
+        for (int j = 0; j < S && j < ntile; ++j) issue(j, src);
     };
 
     // ---- field: v shifts of the union window rows into rinfo ----
@@ -321,9 +374,9 @@ __global__ void __launch_bounds__(kPstThreads) vp_persist_fwd_kernel(const Persi
     auto field_local = [&](int n) {
         // E of every union window row from rho_n; own rows also write E_hist, the tape and the
         // energy partial
-        const float* rho = a.rho + (size_t)(n & 1) * nx;
+        pst_field_inputs(fs, a.rho + (size_t)(n & 1) * nx, a.ctab, nx, win_first, a.win_rows);
         double e2 = 0.0;
-        pst_circ_rows(a.ctab, rho, nx, win_first, a.win_rows, [&](int u, float E) {
+        pst_circ_rows(fs, nx, a.win_rows, [&](int u, float E) {
             const int i = pst_wrap(win_first + u, nx);
             const float Et = E + __ldg(a.H + i);
             const VShift<float> vs = make_vshift<float>(Et, a.dtdv, nv);
@@ -339,12 +392,12 @@ __global__ void __launch_bounds__(kPstThreads) vp_persist_fwd_kernel(const Persi
         return e2;
     };
     auto field_slice = [&](int n) {
-        const float* rho = a.rho + (size_t)(n & 1) * nx;
-        const int S = (nx + G - 1) / G;
-        const int first = g * S;
-        const int cnt = max(0, min(S, nx - first));
+        const int Sl = (nx + G - 1) / G;
+        const int first = g * Sl;
+        const int cnt = max(0, min(Sl, nx - first));
+        pst_field_inputs(fs, a.rho + (size_t)(n & 1) * nx, a.ctab, nx, first, cnt);
         double e2 = 0.0;
-        pst_circ_rows(a.ctab, rho, nx, first, cnt, [&](int u, float E) {
+        pst_circ_rows(fs, nx, cnt, [&](int u, float E) {
             const int i = first + u;
             const float Et = E + __ldg(a.H + i);
             const VShift<float> vs = make_vshift<float>(Et, a.dtdv, nv);
@@ -370,22 +423,19 @@ __global__ void __launch_bounds__(kPstThreads) vp_persist_fwd_kernel(const Persi
         if (lane == 0) s_ee[wid] = e2;
         __syncthreads();
         if (tid == 0) {
-            double s = 0.0;
-            for (int w = 0; w < kPstThreads / 32; ++w) s += s_ee[w];
-            a.eep[(size_t)(n & 3) * G + g] = s;
+            double sum = 0.0;
+            for (int w = 0; w < kPstWarps; ++w) sum += s_ee[w];
+            a.eep[(size_t)n * G + g] = sum;
         }
     };
-    auto sum_energy = [&](int n) {   // CTA 0, after the barrier that published step n's partials
-        if (g != 0 || a.ee_hist == nullptr || wid != 0) return;
-        double s = 0.0;
-        for (int c = lane; c < G; c += 32) s += __ldcg(a.eep + (size_t)(n & 3) * G + c);
-        // fixed order: lane partials, then a fixed butterfly
-        s = warp_sum(s);
-        if (lane == 0) a.ee_hist[n] = (float)(0.5 * s * (double)a.dx);
+    // ee_hist[n] from the G partials of step n (after the barrier that published them): lanes sum
+    // in a fixed order, then a fixed butterfly. The steps are shared out over the CTAs at the end.
+    auto sum_energy = [&](int n) {
+        double sum = 0.0;
+        for (int c = lane; c < G; c += 32) sum += __ldcg(a.eep + (size_t)n * G + c);
+        sum = warp_sum(sum);
+        if (lane == 0) a.ee_hist[n] = (float)(0.5 * sum * (double)a.dx);
     };
-
-    // ---- per-thread column constants ----
-    // (reloaded per chunk: quad record, x weights, f_eq differences, trapezoid weights)
 
     // ---- row sums of a band: acc[R] over the CTA's threads in a fixed order -> rho ----
     auto band_rows = [&](float (&acc)[R], int r0, float* rho_out) {
@@ -410,9 +460,9 @@ __global__ void __launch_bounds__(kPstThreads) vp_persist_fwd_kernel(const Persi
         if ((lane & ((32 >> LG) - 1)) == 0) red[wid * R + (lane >> (5 - LG))] = v;
         __syncthreads();
         if (tid < R) {
-            float s = 0.f;
-            for (int w = 0; w < kPstThreads / 32; ++w) s += red[w * R + tid];
-            rho_out[r0 + tid] = -a.dv * s;
+            float sum = 0.f;
+            for (int w = 0; w < kPstWarps; ++w) sum += red[w * R + tid];
+            rho_out[r0 + tid] = -a.dv * sum;
         }
         __syncthreads();
     };
@@ -425,19 +475,18 @@ __global__ void __launch_bounds__(kPstThreads) vp_persist_fwd_kernel(const Persi
             float acc[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) acc[r] = 0.f;
-            for (int c = 0; c < nch; ++c) {
-                const int q = c * kPstThreads + tid;
+            for (int c = gid; c < nch; c += kPstGroups) {
+                const int q = c * kPstGroup + gt;
                 const int j0 = 4 * q;
-                const int2 qi = __ldg(a.quad + q);
-                const float4 tq = __ldg(a.tq + q);
+                const PstQuad Q = sq != nullptr ? sq[q] : quad_of(q);
                 const double2 fa = __ldg(reinterpret_cast<const double2*>(a.feq + j0));
                 const double2 fb = __ldg(reinterpret_cast<const double2*>(a.feq + j0 + 2));
                 const double fe[4] = {fa.x, fa.y, fb.x, fb.y};
-                const float tt[4] = {tq.x, tq.y, tq.z, tq.w};
+                const float tt[4] = {Q.t.x, Q.t.y, Q.t.z, Q.t.w};
                 float d[R + 2][4];
 #pragma unroll
                 for (int k = 0; k < R + 2; ++k) {
-                    const int row = pst_wrap(r0 + qi.x + k, nx);
+                    const int row = pst_wrap(r0 + Q.bm + k, nx);
                     const double2* fr = reinterpret_cast<const double2*>(a.f_iv + (size_t)row * nv + j0);
                     const double2 u = __ldg(fr), v = __ldg(fr + 1);
                     d[k][0] = (float)(u.x - fe[0]);
@@ -448,7 +497,7 @@ __global__ void __launch_bounds__(kPstThreads) vp_persist_fwd_kernel(const Persi
                 float hv[R][4];
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
-                    const bool dl = (qi.y >> e) & 1;
+                    const bool dl = (Q.mask >> e) & 1;
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         const float p0 = dl ? d[r + 1][e] : d[r][e];
@@ -473,145 +522,143 @@ __global__ void __launch_bounds__(kPstThreads) vp_persist_fwd_kernel(const Persi
         const bool last = !replay && n == a.n_steps - 1;
         const float* src = slot(n);
         float* dst = last ? nullptr : slot(n + 1);
-        // the first two tiles of the step load while the field is solved
-        issue(0, src);
-        if (ntile > 1) issue(1, src);
+        // the first tiles of the step load while the field is solved (after it, when the field's
+        // inputs share the stage buffers)
+        const bool early = replay || !a.fs_alias;
+        if (early) issue_first(src);
         if (replay) {
             rinfo_from(a.vsh_tape_in + (size_t)n * nx);
         } else if (a.field_dist == 0) {
             const double e2 = field_local(n);
             publish_energy(n, e2);
-            if (n >= 1) sum_energy(n - 1);
         } else {
             const double e2 = field_slice(n);
             publish_energy(n, e2);
+            if (!early) issue_first(src);
             if (!barrier()) break;
-            if (n >= 1) sum_energy(n - 1);
             rinfo_from(a.vsh_g);
         }
         __syncthreads();
+        if (!early && a.field_dist == 0) issue_first(src);
 
         float* rho_next = a.rho + (size_t)((n + 1) & 1) * nx;
         float acc[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) acc[r] = 0.f;
-        for (int i = 0; i < ntile; ++i) {
-            const int bi = i / nch, c = i - bi * nch;
-            const int r0 = (b0 + bi) * R, c0 = c * kPstC;
-            const int q = c * kPstThreads + tid;
-            const int j0 = c0 + 4 * tid;
-            const int2 cm = __ldg(a.chunk + c);
-            const int2 qi = __ldg(a.quad + q);
-            const float4 tq = __ldg(a.tq + q);
-            const float tt[4] = {tq.x, tq.y, tq.z, tq.w};
-            const float4 D4 = __ldg(reinterpret_cast<const float4*>(a.dfeq + j0));
-            const float Dm1 = __ldg(a.dfeq + (j0 == 0 ? nv - 1 : j0 - 1));
-            if (!wait_stage()) {
-                alive = false;
-                break;
-            }
-            const float* st = (tiles_used & 1) ? stage1 : stage0;
-            ++tiles_used;
-            // window row k of this thread: stage row 2*(bm - cm.x) + k, global row r0 + 2*bm + k
-            const float* sb = st + (size_t)(2 * (qi.x - cm.x)) * kPstW + 4 + 4 * tid;
-            const int ib = (r0 - r_lo) + 2 * qi.x - a.win_lo;   // rinfo index of window row 0
-            float O[R + 4][4];
+        for (int bi = 0; bi < a.bands_per_cta; ++bi) {
+            const int r0 = (b0 + bi) * R;
+            for (int jj = 0; jj < cpg; ++jj) {
+                const int j = bi * cpg + jj;
+                const int c = gid + kPstGroups * jj;
+                const int c0 = c * kPstC;
+                const int q = c * kPstGroup + gt;
+                const int j0 = c0 + 4 * gt;
+                const int2 cm = __ldg(a.chunk + c);
+                const PstQuad Q = sq != nullptr ? sq[q] : quad_of(q);
+                const int2 qi = make_int2(Q.bm, Q.mask);
+                const float tt[4] = {Q.t.x, Q.t.y, Q.t.z, Q.t.w};
+                const float4 D4 = Q.D;
+                const float Dm1 = Q.Dm1;
+                pst_cp_wait((int)(tiles_issued - tiles_used - 1));   // groups committed after this tile's
+                group_sync();
+                const float* st = stage_ptr(tiles_used);
+                ++tiles_used;
+                // window row k of this thread: stage row 2*(bm - cm.x) + k, global row r0 + 2*bm + k
+                const float* sb = st + (size_t)(2 * (qi.x - cm.x)) * kPstW + 4 + 4 * gt;
+                const int ib = (r0 - r_lo) + 2 * qi.x - a.win_lo;   // rinfo index of window row 0
+                float O[R + 4][4];
 #pragma unroll
-            for (int k = 0; k < R + 4; ++k) {
-                const int2 ri = rinfo[ib + k];
-                const float tv = __int_as_float(ri.y);
-                const float* sr = sb + (size_t)k * kPstW;
-                if (ri.x == 0) {
-                    const float4 h = *reinterpret_cast<const float4*>(sr);
-                    const float h4 = sr[4];
-                    O[k][0] = h.x + tv * ((h.y - h.x) + D4.x);
-                    O[k][1] = h.y + tv * ((h.z - h.y) + D4.y);
-                    O[k][2] = h.z + tv * ((h.w - h.z) + D4.z);
-                    O[k][3] = h.w + tv * ((h4 - h.w) + D4.w);
-                } else if (ri.x == -1) {
-                    const float hm = sr[-1];
-                    const float4 h = *reinterpret_cast<const float4*>(sr);
-                    O[k][0] = (hm - Dm1) + tv * ((h.x - hm) + Dm1);
-                    O[k][1] = (h.x - D4.x) + tv * ((h.y - h.x) + D4.x);
-                    O[k][2] = (h.y - D4.y) + tv * ((h.z - h.y) + D4.y);
-                    O[k][3] = (h.z - D4.z) + tv * ((h.w - h.z) + D4.z);
-                } else if (ri.x >= -kStageHalo && ri.x < kStageHalo) {
-                    const float* p = sr + ri.x;
-                    const float v[5] = {p[0], p[1], p[2], p[3], p[4]};
-                    const float4 A = __ldg(reinterpret_cast<const float4*>(a.vtab + (size_t)(ri.x + kStageHalo) * nv + j0));
-                    const float4 B = __ldg(reinterpret_cast<const float4*>(
-                        a.vtab + (size_t)(2 * kStageHalo + ri.x + kStageHalo) * nv + j0));
-                    O[k][0] = v[0] + tv * (v[1] - v[0]) + (A.x + tv * B.x);
-                    O[k][1] = v[1] + tv * (v[2] - v[1]) + (A.y + tv * B.y);
-                    O[k][2] = v[2] + tv * (v[3] - v[2]) + (A.z + tv * B.z);
-                    O[k][3] = v[3] + tv * (v[4] - v[3]) + (A.w + tv * B.w);
-                } else {
-                    // shift beyond the staged halo: the float64 form from global memory
-                    const int row = pst_wrap(r0 + 2 * qi.x + k, nx);
-                    VShift<float> vs;
-                    vs.m = ri.x < 0 ? ri.x + nv : ri.x;
-                    vs.t = tv;
+                for (int k = 0; k < R + 4; ++k) {
+                    const int2 ri = rinfo[ib + k];
+                    const float tv = __int_as_float(ri.y);
+                    const float* sr = sb + (size_t)k * kPstW;
+                    if (ri.x == 0) {
+                        const float4 h = *reinterpret_cast<const float4*>(sr);
+                        const float h4 = sr[4];
+                        O[k][0] = h.x + tv * ((h.y - h.x) + D4.x);
+                        O[k][1] = h.y + tv * ((h.z - h.y) + D4.y);
+                        O[k][2] = h.z + tv * ((h.w - h.z) + D4.z);
+                        O[k][3] = h.w + tv * ((h4 - h.w) + D4.w);
+                    } else if (ri.x == -1) {
+                        const float hm = sr[-1];
+                        const float4 h = *reinterpret_cast<const float4*>(sr);
+                        O[k][0] = (hm - Dm1) + tv * ((h.x - hm) + Dm1);
+                        O[k][1] = (h.x - D4.x) + tv * ((h.y - h.x) + D4.x);
+                        O[k][2] = (h.y - D4.y) + tv * ((h.z - h.y) + D4.y);
+                        O[k][3] = (h.z - D4.z) + tv * ((h.w - h.z) + D4.z);
+                    } else if (ri.x >= -kStageHalo && ri.x < kStageHalo) {
+                        const float* pp = sr + ri.x;
+                        const float v[5] = {pp[0], pp[1], pp[2], pp[3], pp[4]};
+                        const float4 A = __ldg(reinterpret_cast<const float4*>(a.vtab + (size_t)(ri.x + kStageHalo) * nv + j0));
+                        const float4 B = __ldg(reinterpret_cast<const float4*>(
+                            a.vtab + (size_t)(2 * kStageHalo + ri.x + kStageHalo) * nv + j0));
+                        O[k][0] = v[0] + tv * (v[1] - v[0]) + (A.x + tv * B.x);
+                        O[k][1] = v[1] + tv * (v[2] - v[1]) + (A.y + tv * B.y);
+                        O[k][2] = v[2] + tv * (v[3] - v[2]) + (A.z + tv * B.z);
+                        O[k][3] = v[3] + tv * (v[4] - v[3]) + (A.w + tv * B.w);
+                    } else {
+                        // shift beyond the staged halo: the float64 form from global memory
+                        const int row = pst_wrap(r0 + 2 * qi.x + k, nx);
+                        const int mr = ri.x < 0 ? ri.x + nv : ri.x;
 #pragma unroll
-                    for (int e = 0; e < 4; ++e) O[k][e] = pst_v_cell(src, a.feq, nv, row, j0 + e, vs.m, vs.t);
-                }
-            }
-            // x steps per column: window offset 0 or 2 rows (delta bit), d = X(o), h' = X(d)
-            float dd[R + 1][4];
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const bool dl = (qi.y >> e) & 1;
-                float p0 = dl ? O[2][e] : O[0][e];
-#pragma unroll
-                for (int q2 = 0; q2 <= R; ++q2) {
-                    const float p1 = dl ? O[q2 + 3][e] : O[q2 + 1][e];
-                    dd[q2][e] = pst_lerp(p0, p1, tt[e]);
-                    p0 = p1;
-                }
-            }
-            if (a.f_hist != nullptr || (last && a.f_final != nullptr)) {
-                float* fh = a.f_hist != nullptr ? a.f_hist + (size_t)(n - n_first) * nxnv : nullptr;
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const double fe = __ldg(a.feq + j0 + e);
-                    const int base = r0 + qi.x + ((qi.y >> e) & 1);
-#pragma unroll
-                    for (int r = 0; r < R; ++r) {
-                        const int row = pst_wrap(base + r, nx);
-                        const double f = fe + (double)dd[r][e];
-                        if (fh != nullptr) fh[(size_t)row * nv + j0 + e] = (float)f;
-                        if (last && a.f_final != nullptr) a.f_final[(size_t)row * nv + j0 + e] = f;
+                        for (int e = 0; e < 4; ++e) O[k][e] = pst_v_cell(src, a.feq, nv, row, j0 + e, mr, tv);
                     }
                 }
-            }
-            if (dst != nullptr) {
-                const float w0 = j0 == 0 ? 0.5f : 1.f, w3 = j0 + 3 == nv - 1 ? 0.5f : 1.f;
+                // x steps per column: window offset 0 or 2 rows (delta bit), d = X(o), h' = X(d)
+                float dd[R + 1][4];
 #pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    const float h0v = pst_lerp(dd[r][0], dd[r + 1][0], tt[0]);
-                    const float h1v = pst_lerp(dd[r][1], dd[r + 1][1], tt[1]);
-                    const float h2v = pst_lerp(dd[r][2], dd[r + 1][2], tt[2]);
-                    const float h3v = pst_lerp(dd[r][3], dd[r + 1][3], tt[3]);
-                    *reinterpret_cast<float4*>(dst + (size_t)(r0 + r) * nv + j0) = make_float4(h0v, h1v, h2v, h3v);
-                    acc[r] += w0 * h0v + h1v + h2v + w3 * h3v;
+                for (int e = 0; e < 4; ++e) {
+                    const bool dl = (qi.y >> e) & 1;
+                    float p0 = dl ? O[2][e] : O[0][e];
+#pragma unroll
+                    for (int q2 = 0; q2 <= R; ++q2) {
+                        const float p1 = dl ? O[q2 + 3][e] : O[q2 + 1][e];
+                        dd[q2][e] = pst_lerp(p0, p1, tt[e]);
+                        p0 = p1;
+                    }
                 }
-            }
-            __syncthreads();   // the stage is free
-            if (i + 2 < ntile) issue(i + 2, src);
-            if (c == nch - 1) {
-                if (!replay && !last) band_rows(acc, r0, rho_next);
+                if (a.f_hist != nullptr || (last && a.f_final != nullptr)) {
+                    float* fh = a.f_hist != nullptr ? a.f_hist + (size_t)(n - n_first) * nxnv : nullptr;
 #pragma unroll
-                for (int r = 0; r < R; ++r) acc[r] = 0.f;
+                    for (int e = 0; e < 4; ++e) {
+                        const double fe = __ldg(a.feq + j0 + e);
+                        const int base = r0 + qi.x + ((qi.y >> e) & 1);
+#pragma unroll
+                        for (int r = 0; r < R; ++r) {
+                            const int row = pst_wrap(base + r, nx);
+                            const double f = fe + (double)dd[r][e];
+                            if (fh != nullptr) fh[(size_t)row * nv + j0 + e] = (float)f;
+                            if (last && a.f_final != nullptr) a.f_final[(size_t)row * nv + j0 + e] = f;
+                        }
+                    }
+                }
+                if (dst != nullptr) {
+                    const float w0 = j0 == 0 ? 0.5f : 1.f, w3 = j0 + 3 == nv - 1 ? 0.5f : 1.f;
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const float h0v = pst_lerp(dd[r][0], dd[r + 1][0], tt[0]);
+                        const float h1v = pst_lerp(dd[r][1], dd[r + 1][1], tt[1]);
+                        const float h2v = pst_lerp(dd[r][2], dd[r + 1][2], tt[2]);
+                        const float h3v = pst_lerp(dd[r][3], dd[r + 1][3], tt[3]);
+                        *reinterpret_cast<float4*>(dst + (size_t)(r0 + r) * nv + j0) =
+                            make_float4(h0v, h1v, h2v, h3v);
+                        acc[r] += w0 * h0v + h1v + h2v + w3 * h3v;
+                    }
+                }
+                group_sync();   // the stage is free
+                if (j + S < ntile) issue(j + S, src);
             }
+            // every group has finished the band: its row sums
+            if (!replay && !last) band_rows(acc, r0, rho_next);
+#pragma unroll
+            for (int r = 0; r < R; ++r) acc[r] = 0.f;
         }
-        if (!alive) break;
         if (!barrier()) break;
     }
-    // a CTA that stopped early still owns the bulk copies it issued: wait for them (bounded)
-    while (tiles_used < tiles_issued) {
-        wait_stage();
-        ++tiles_used;
-    }
-    if (alive && !replay) sum_energy(a.n_steps - 1);
+    // a CTA that stopped early still owns the copies it issued: wait for them
+    pst_cp_wait(0);
+    if (alive && !replay && a.ee_hist != nullptr)
+        for (int n = g * kPstWarps + wid; n < a.n_steps; n += G * kPstWarps) sum_energy(n);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -675,7 +722,7 @@ bool persist_prepare(PersistHost& ph, int nx, int nv, const std::vector<long lon
     int dmax = 0;
     for (int c = 0; c < nch; ++c) {
         int lo = 1 << 30, hi = -(1 << 30);
-        for (int q = c * kPstThreads; q < (c + 1) * kPstThreads; ++q) {
+        for (int q = c * kPstGroup; q < (c + 1) * kPstGroup; ++q) {
             lo = std::min(lo, ph.quad[q].x);
             hi = std::max(hi, ph.quad[q].x);
         }
@@ -703,7 +750,18 @@ bool persist_prepare(PersistHost& ph, int nx, int nv, const std::vector<long lon
         const int win_lo = std::min(2 * (int)all_lo, 0);
         const int win_end = std::max(bpc * R + 2 * (int)all_hi + 4, bpc * R);
         const int win_rows = win_end - win_lo;
-        const size_t smem = persist_smem_bytes(span_max, win_rows, R);
+        if (win_rows > nx) return false;   // the coefficient slice of the field covers at most nx rows
+        const int fdist = (long long)win_rows * nx > (1LL << 17) ? 1 : 0;
+        const int field_rows = fdist ? (nx + G - 1) / G : win_rows;
+        // stages per column group: up to all of the group's tiles of a step, within about 160 KB
+        // for the four groups
+        const int ntile = bpc * ((nv / kPstC + kPstGroups - 1) / kPstGroups);
+        const size_t stage_bytes = (size_t)span_max * kPstW * sizeof(float);
+        const int fit = (int)((160 * 1024) / (std::min(kPstGroups, nv / kPstC) * stage_bytes));
+        const int stages = std::max(1, std::min({kPstMaxStages, ntile, fit}));
+        int stage_floats = 0, fs_alias = 0;
+        const size_t smem = persist_smem_bytes(span_max, win_rows, R, nx, nv, field_rows, stages, &stage_floats,
+                                               &fs_alias);
         if (smem > 200 * 1024) continue;
         const int per_sm = pst_max_blocks_r(R, smem);
         if (per_sm <= 0) return false;
@@ -716,7 +774,11 @@ bool persist_prepare(PersistHost& ph, int nx, int nv, const std::vector<long lon
         ph.win_rows = win_rows;
         ph.smem = smem;
         // the field on each CTA's own window when that costs little, else in slices + a barrier
-        ph.field_dist = (long long)win_rows * nx > (1LL << 17) ? 1 : 0;
+        ph.field_dist = fdist;
+        ph.stage_floats = stage_floats;
+        ph.fs_alias = fs_alias;
+        ph.stages = stages;
+        ph.field_rows = field_rows;
         return true;
     }
     return false;
@@ -729,6 +791,10 @@ cudaError_t launch_persist_fwd(const PersistArgs& args, const PersistHost& ph, c
     a.win_lo = ph.win_lo;
     a.win_rows = ph.win_rows;
     a.field_dist = ph.field_dist;
+    a.stage_floats = ph.stage_floats;
+    a.fs_alias = ph.fs_alias;
+    a.stages = ph.stages;
+    a.field_rows = ph.field_rows;
     cudaError_t e = cudaMemsetAsync(a.bar, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
