@@ -56,6 +56,8 @@ def parse_args():
                     help="force the staged step's rows per CTA (0: per-column kernel); skips autotuning")
     ap.add_argument("--stage-threads", type=int, default=None, help="with --stage-rows: threads per CTA")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="c2: skip the 8192^2 roofline and C5 sub-records of the default line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample duration")
     return ap.parse_args()
@@ -346,41 +348,59 @@ def run_ours(args, rank, local_rank, world):
     cell_steps = cells * T * args.steps * world
     value = cell_steps / (total_ms * 1e-3)
 
-    # roofline of the dominant kernel. Streaming path: one fused launch per time step (any
-    # separate Poisson tail launch is charged to it, conservatively). Cluster-resident path: one
-    # launch runs the whole time loop with the state in distributed shared memory, so its
-    # "achieved" figure is an effective bandwidth (the state never travels through HBM).
+    # roofline of the dominant kernel (CUDA events around graph replays of the timed steps):
+    #  * cluster-resident path: one launch per forward (adjoint) loop with the state in distributed
+    #    shared memory, so "achieved" is an effective bandwidth (the state never travels through HBM);
+    #  * persistent path: the forward loop is one cooperative launch (vp_persist_fwd_kernel); the
+    #    adjoint runs one launch per step plus one persistent replay launch per checkpoint segment;
+    #  * per-step path: one fused launch per step (a separate Poisson tail launch is charged to it).
     peak, peak_kind = measured_peaks()
     cfg = plan.get_config()
     resident = cfg["cluster_size"] > 0 and every == 1
+    persistent = (not resident) and cfg["persist_rows"] > 0
+    n_recompute = 0 if every == 1 else sum(max(0, min(s0 + every, T) - s0 - 1) for s0 in range(0, T, every))
+    n_segments = 0 if every == 1 else sum(1 for s0 in range(0, T, every) if min(s0 + every, T) - s0 > 1)
+    tf_loop, tb_loop = tf_ms / args.steps, tb_ms / args.steps
     if resident:
-        n_fused_f, n_fused_b = 1, 1
-        alg_f, alg_b = BYTES_FWD * cells * T, BYTES_BWD * cells * T
         kf, kb = "vp_res_fwd_kernel", "vp_res_bwd_kernel"
+        f_launch, alg_f = tf_loop, BYTES_FWD * cells * T
+        b_launch, alg_b = tb_loop, BYTES_BWD * cells * T
+        b_note = "one launch per adjoint loop"
+    elif persistent:
+        kf = "vp_persist_fwd_kernel"
+        f_launch, alg_f = tf_loop, BYTES_FWD * cells * T
+        kb = "vp_bwds_kernel" if cfg["stage_rows"] > 0 else "vp_bwd_kernel"
+        # the replayed segments cost about the forward's time per step; the rest is the T + 1
+        # per-step adjoint launches
+        replay_ms = tf_loop * n_recompute / max(1, T)
+        b_launch = max(1e-6, (tb_loop - replay_ms) / (T + 1))
+        alg_b = BYTES_BWD * cells
+        b_note = (f"adjoint launch time = (adjoint loop - {n_segments} replay launches estimated at the "
+                  f"forward's time per step) / {T + 1} launches")
     else:
-        n_recompute = 0 if every == 1 else sum(max(0, min(s0 + every, T) - s0 - 1) for s0 in range(0, T, every))
-        n_fused_f, n_fused_b = T + 1, T + 1 + n_recompute
-        alg_f, alg_b = BYTES_FWD * cells, BYTES_BWD * cells
         kf = "vp_fwds_kernel" if cfg["stage_rows"] > 0 else "vp_fwd_kernel"
+        f_launch, alg_f = tf_loop / (T + 1), BYTES_FWD * cells
         kb = "vp_bwd_kernel"
-    f_launch_ms = tf_ms / (args.steps * n_fused_f)
-    b_launch_ms = (tb_ms / (args.steps * n_fused_b)) if wl.adjoint else 0.0
-    if wl.adjoint and tb_ms >= tf_ms and (resident or every == 1):
-        kname, per_ms, alg = kb, b_launch_ms, alg_b
-    else:
-        kname, per_ms, alg = kf, f_launch_ms, alg_f
-    achieved = alg / (per_ms * 1e-3) / 1e9
-    traffic = profile_traffic(kname, wl.name)
-    note = ("one launch per forward (adjoint) time loop, state resident in distributed shared "
-            "memory: achieved is an effective bandwidth over the algorithmic bytes" if resident else
-            "time per fused launch averaged over graph replays of the timed steps, including launch gaps"
-            + ("" if cfg["tail_inline"] else " and the separate Poisson tail launch"))
-    roof = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": peak,
-            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
-            "algorithmic_bytes_per_launch": alg, "avg_launch_us": round(per_ms * 1e3, 3),
-            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
-            else "fallback 6650 GB/s",
-            "note": note}
+        b_launch, alg_b = tb_loop / (T + 1 + n_recompute), BYTES_BWD * cells
+        b_note = "per-step launches, recomputation launches included"
+
+    def roof_of(kname, per_ms, alg, note):
+        achieved = alg / (per_ms * 1e-3) / 1e9
+        return {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": profile_traffic(kname, wl.name),
+                "algorithmic_bytes_per_launch": alg, "avg_launch_us": round(per_ms * 1e3, 3),
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                else "fallback 6650 GB/s",
+                "note": note}
+
+    f_note = ("one launch per forward loop, state resident in distributed shared memory: achieved is an "
+              "effective bandwidth over the algorithmic bytes" if resident else
+              "one cooperative launch per forward loop (grid barrier per step), field solves included"
+              if persistent else "time per fused launch averaged over graph replays, including launch gaps"
+              + ("" if cfg["tail_inline"] else " and the separate Poisson tail launch"))
+    roof_f = roof_of(kf, f_launch, alg_f, f_note)
+    roof_b = roof_of(kb, b_launch, alg_b, b_note) if wl.adjoint else None
+    roof = roof_b if (roof_b is not None and tb_ms >= tf_ms) else roof_f
 
     # end to end through the public API with host buffers (rank 0's replica measured on every rank)
     e2e = None
@@ -407,17 +427,72 @@ def run_ours(args, rank, local_rank, world):
                    "l2": "flushed between timed steps (256 MiB write, untimed)",
                    "cuda_graph": use_graph,
                    "launch": {k: cfg[k] for k in ("rows_per_cta", "threads", "n_chunks", "tail_inline",
-                                                  "cluster_size", "cluster_threads")},
-                   "path": "cluster-resident" if resident else "streaming",
+                                                  "cluster_size", "cluster_threads", "stage_rows",
+                                                  "persist_rows", "persist_ctas")},
+                   "path": "cluster-resident" if resident else ("persistent forward loop" if persistent
+                                                                else "per-step launches"),
                    "autotune": tuned,
                    "fwd_ms_per_step": round(tf_ms / args.steps, 4),
                    "bwd_ms_per_step": round(tb_ms / args.steps, 4)},
         "roofline": roof,
+        "roofline_fwd": roof_f,
+        "roofline_bwd": roof_b,
         "e2e": e2e,
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
     return line, wl
+
+
+def measure_large(args, rank, local_rank, world):
+    """The HBM-bound regime beside the cache-resident headline: a short forward + adjoint on the
+    8192 x 8192 grid (268 MB of float32 state per plane, more than the 126 MB L2), default launch
+    shape, 3 warm-up and 3 timed steps."""
+    sub = argparse.Namespace(**vars(args))
+    sub.workload, sub.steps, sub.warmup = "roofline", 3, 3
+    sub.no_autotune, sub.no_e2e = True, True
+    sub.cluster_size = sub.stage_rows = sub.checkpoint_every = None
+    line, wl = run_ours(sub, rank, local_rank, world)
+    peak, _ = measured_peaks()
+    cfg = line["config"]
+    cell_steps = wl.mesh.nx * wl.mesh.nv * wl.n_steps
+    loop_ms = cfg["fwd_ms_per_step"] + cfg["bwd_ms_per_step"]
+    return {"workload": wl.description, "nx": wl.mesh.nx, "nv": wl.mesh.nv, "n_time_steps": wl.n_steps,
+            "checkpoint_every": cfg["checkpoint_every"], "path": cfg["path"], "launch": cfg["launch"],
+            "value": line["value"], "unit": "cell-steps/s fwd+adjoint",
+            "fwd_ms_per_loop": cfg["fwd_ms_per_step"], "bwd_ms_per_loop": cfg["bwd_ms_per_step"],
+            "loop_hbm_frac": round(cell_steps * (BYTES_FWD + BYTES_BWD) / (loop_ms * 1e-3) / 1e9 / peak, 4),
+            "roofline_fwd": line["roofline_fwd"], "roofline_bwd": line["roofline_bwd"],
+            "clocks": line["clocks"], "steps": 3, "warmup": 3,
+            "l2": "flushed between timed steps (256 MiB write, untimed)"}
+
+
+def measure_c5(args, rank, local_rank, world):
+    """The surrogate-warm-started control against the plain adjoint loop (the C5 workload at
+    its full size), per seed, with the one-off data generation and training reported beside the
+    per-problem times: both the ratio that amortises them over many control problems and the
+    ratio that charges all of it to one."""
+    sub = argparse.Namespace(**vars(args))
+    line, _ = run_surrogate(sub, rank, local_rank, world)
+    sur = line["surrogate"]
+    setup_s = line["ms_per_step"] * 1e-3 + sur["train_seconds"]
+    runs = []
+    for r in sur["runs"]:
+        runs.append({"seed": r["seed"], "plain_seconds": r["plain_seconds"], "warm_seconds": r["warm_seconds"],
+                     "warm_reached": r["warm_reached"], "J_star": r["J_star"], "warm_J": r["warm_J"],
+                     "time_ratio": round(r["time_ratio"], 4),
+                     "time_ratio_with_setup": round((r["warm_seconds"] + setup_s) / r["plain_seconds"], 4)})
+    saved = [r["plain_seconds"] - r["warm_seconds"] for r in runs]
+    return {"workload": line["config"]["workload"], "data_generation_seconds": round(line["ms_per_step"] * 1e-3, 4),
+            "data_cell_steps_per_s": line["value"], "train_seconds": round(sur["train_seconds"], 4),
+            "holdout_mae_log_ee": sur["holdout_mae_log_ee"], "runs": runs,
+            "time_ratio_max": max(r["time_ratio"] for r in runs),
+            "time_ratio_mean": round(float(np.mean([r["time_ratio"] for r in runs])), 4),
+            "problems_to_amortise_setup": (round(setup_s / float(np.mean(saved)), 2)
+                                           if float(np.mean(saved)) > 0 else None),
+            "note": "time_ratio = warm (surrogate search + true-gradient refinement to J <= 1.01 J*) / "
+                    "plain (Adam with the true adjoint gradient until J stops improving); "
+                    "time_ratio_with_setup also charges data generation and training to this one problem"}
 
 
 def e2e_public_api(args, solver, wl, dev, flush):
@@ -822,6 +897,9 @@ def main():
         else:
             line, wl = run_ours(args, rank, local_rank, world)
             base = cpu_baseline
+            if args.workload == "c2" and world == 1 and not args.no_extras:
+                line["roofline_large"] = measure_large(args, rank, local_rank, world)
+                line["c5"] = measure_c5(args, rank, local_rank, world)
         if rank == 0 and world == 1 and not args.no_cpu_baseline and base is not None:
             v, cores, kind, sample = base(wl, args.cpu_seconds)
             line["cpu_baseline"] = {"value": round(v, 1), "unit": "cell-steps/s", "cores": cores,

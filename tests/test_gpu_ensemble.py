@@ -186,3 +186,21 @@ def test_ensemble_rejects_bad_arguments():
         ens.forward(ens.pack_cells(fivs)[:-1], ens.pack_rows(Hs), 3)
     with pytest.raises(ValueError):
         Ensemble(meshes, 0.05, feqs[:1])
+
+
+def test_sharded_ensemble_entry_point_solves_on_the_device():
+    """solve_sharded_ensemble with its default per-shard solve (one Ensemble on this GPU, a
+    single rank here) against the float64 oracle per instance: energy and field histories and
+    dJ/dH of J = trapezoid(ee, dt)."""
+    from warp_vp_solver_b200.sharding import solve_sharded_ensemble
+    T, dt = 10, 0.05
+    meshes, feqs, fivs, Hs = _uneven(6, seed=21)
+    res = solve_sharded_ensemble(meshes, dt, feqs, fivs, Hs, T, want_grad=True)
+    for i, m in enumerate(meshes):
+        g = O.grid_from(m)
+        ref = O.delta_forward(g, dt, feqs[i], fivs[i], Hs[i], T)
+        _, rH = O.delta_backward(g, dt, feqs[i], fivs[i], Hs[i], T, np.zeros((m.nx, m.nv)), None,
+                                 np.zeros((T, m.nx)), O.trapezoid_time_weights(T, dt))
+        assert O.rel_err(res[i]["ee_hist"], ref[3]) < 1e-5
+        assert O.rel_err(res[i]["E_hist"], ref[2]) < 1e-5
+        assert O.rel_err(res[i]["g_H"], rH) < 1e-4

@@ -251,6 +251,32 @@ static size_t pst_field_floats(int nx, int n_rows) { return (size_t)2 * nx + n_r
 // while the field is solved); larger ones reuse the stage buffers.
 constexpr size_t kPstOwnFieldBytes = 24 * 1024;
 
+// V step of one row of a quad for the shifts other than 0 and -1 (kept out of line so that the
+// unrolled tile loop stays small): shifts in [-4, 4) from the staged row and the A_m, B_m tables,
+// larger ones in the float64 form from global memory.
+__device__ __noinline__ float4 pst_v_rare(const PersistArgs& a, const float* sr, const float* src, int ms, float tv,
+                                          int row, int j0) {
+    const int nv = a.nv;
+    float4 o;
+    if (ms >= -kStageHalo && ms < kStageHalo) {
+        const float* pp = sr + ms;
+        const float v[5] = {pp[0], pp[1], pp[2], pp[3], pp[4]};
+        const float4 A = __ldg(reinterpret_cast<const float4*>(a.vtab + (size_t)(ms + kStageHalo) * nv + j0));
+        const float4 B = __ldg(reinterpret_cast<const float4*>(a.vtab + (size_t)(2 * kStageHalo + ms + kStageHalo) * nv + j0));
+        o.x = v[0] + tv * (v[1] - v[0]) + (A.x + tv * B.x);
+        o.y = v[1] + tv * (v[2] - v[1]) + (A.y + tv * B.y);
+        o.z = v[2] + tv * (v[3] - v[2]) + (A.z + tv * B.z);
+        o.w = v[3] + tv * (v[4] - v[3]) + (A.w + tv * B.w);
+    } else {
+        const int mr = ms < 0 ? ms + nv : ms;
+        o.x = pst_v_cell(src, a.feq, nv, row, j0, mr, tv);
+        o.y = pst_v_cell(src, a.feq, nv, row, j0 + 1, mr, tv);
+        o.z = pst_v_cell(src, a.feq, nv, row, j0 + 2, mr, tv);
+        o.w = pst_v_cell(src, a.feq, nv, row, j0 + 3, mr, tv);
+    }
+    return o;
+}
+
 // Shared memory of a launch: the stage area (two stage buffers, or the field inputs when those are
 // larger and share it), the row records of the union window, the row-sum scratch, and the field
 // inputs when they have their own region.
@@ -273,7 +299,7 @@ size_t persist_smem_bytes(int span_max, int win_rows, int R, int nx, int nv, int
 }
 
 template <int R>
-__global__ void __launch_bounds__(kPstThreads, 1) vp_persist_fwd_kernel(const PersistArgs a) {
+__global__ void __launch_bounds__(kPstThreads, 2) vp_persist_fwd_kernel(const PersistArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int s_flag;
     __shared__ double s_ee[kPstWarps];
@@ -283,14 +309,15 @@ __global__ void __launch_bounds__(kPstThreads, 1) vp_persist_fwd_kernel(const Pe
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int gid = tid / kPstGroup, gt = tid - gid * kPstGroup;   // column group and its thread
     const int g = blockIdx.x, G = gridDim.x;
-    const int b0 = g * a.bands_per_cta;
-    const int r_lo = b0 * R;                          // first own row
-    const int own_rows = a.bands_per_cta * R;
+    // bands g, g + G, g + 2G, ...: at any time the CTAs work on neighbouring rows, so the halo rows
+    // a tile reads were just read (or written) by a neighbour and are found in L2
+    const int bpc = a.bands_per_cta;
+    auto band_row = [&](int bi) { return (g + bi * G) * R; };
     const int S = a.stages;                           // stage buffers per group
     float* stages = reinterpret_cast<float*>(smem);
-    int2* rinfo = reinterpret_cast<int2*>(stages + (size_t)a.stage_floats);
+    int2* rinfo = reinterpret_cast<int2*>(stages + (size_t)a.stage_floats);   // [bpc][win_rows]
     float* red = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(rinfo) +
-                                          (((size_t)a.win_rows * sizeof(int2) + 15) & ~(size_t)15));
+                                          (((size_t)bpc * a.win_rows * sizeof(int2) + 15) & ~(size_t)15));
     // field inputs: their own region after the row-sum scratch, or the stage area
     float* fs = a.fs_alias ? stages : red + kPstWarps * R + 4;
     const size_t ff = ((size_t)2 * nx + a.field_rows + 8 + 3) & ~(size_t)3;
@@ -342,7 +369,7 @@ __global__ void __launch_bounds__(kPstThreads, 1) vp_persist_fwd_kernel(const Pe
     auto tile_of = [&](int j, int* r0, int* c) {
         const int bi = j / cpg;
         *c = gid + kPstGroups * (j - bi * cpg);
-        *r0 = (b0 + bi) * R;
+        *r0 = band_row(bi);
     };
     auto stage_ptr = [&](unsigned k) {
         return stages + (size_t)(gid * S + (int)(k % (unsigned)S)) * a.span_max * kPstW;
@@ -369,26 +396,31 @@ __global__ void __launch_bounds__(kPstThreads, 1) vp_persist_fwd_kernel(const Pe
         for (int j = 0; j < S && j < ntile; ++j) issue(j, src);
     };
 
-    // ---- field: v shifts of the union window rows into rinfo ----
-    const int win_first = r_lo + a.win_lo;            // global row of rinfo[0] (unreduced)
+    // ---- field: v shifts of each band's window rows [r0 + win_lo, r0 + win_lo + win_rows) into
+    // rinfo[band][.] ----
     auto field_local = [&](int n) {
-        // E of every union window row from rho_n; own rows also write E_hist, the tape and the
+        // E of every window row from rho_n; the band's own rows also write E_hist, the tape and the
         // energy partial
-        pst_field_inputs(fs, a.rho + (size_t)(n & 1) * nx, a.ctab, nx, win_first, a.win_rows);
         double e2 = 0.0;
-        pst_circ_rows(fs, nx, a.win_rows, [&](int u, float E) {
-            const int i = pst_wrap(win_first + u, nx);
-            const float Et = E + __ldg(a.H + i);
-            const VShift<float> vs = make_vshift<float>(Et, a.dtdv, nv);
-            rinfo[u] = pst_rinfo(vs, nv);
-            const int own = u + a.win_lo;             // row offset from r_lo
-            if (own >= 0 && own < own_rows) {
-                if (a.E_hist != nullptr) a.E_hist[(size_t)n * nx + i] = Et;
-                if (a.E_tape != nullptr) a.E_tape[(size_t)n * nx + i] = E;
-                if (a.vsh_tape != nullptr) a.vsh_tape[(size_t)n * nx + i] = vs;
-                e2 += (double)(trap_w<float>(i, nx) * E * E);
-            }
-        });
+        for (int bi = 0; bi < bpc; ++bi) {
+            const int wf = band_row(bi) + a.win_lo;
+            if (bi > 0) __syncthreads();   // the previous band's circulant has read the inputs
+            pst_field_inputs(fs, a.rho + (size_t)(n & 1) * nx, a.ctab, nx, wf, a.win_rows);
+            int2* ri = rinfo + (size_t)bi * a.win_rows;
+            pst_circ_rows(fs, nx, a.win_rows, [&](int u, float E) {
+                const int i = pst_wrap(wf + u, nx);
+                const float Et = E + __ldg(a.H + i);
+                const VShift<float> vs = make_vshift<float>(Et, a.dtdv, nv);
+                ri[u] = pst_rinfo(vs, nv);
+                const int own = u + a.win_lo;          // row offset from the band's first row
+                if (own >= 0 && own < R) {
+                    if (a.E_hist != nullptr) a.E_hist[(size_t)n * nx + i] = Et;
+                    if (a.E_tape != nullptr) a.E_tape[(size_t)n * nx + i] = E;
+                    if (a.vsh_tape != nullptr) a.vsh_tape[(size_t)n * nx + i] = vs;
+                    e2 += (double)(trap_w<float>(i, nx) * E * E);
+                }
+            });
+        }
         return e2;
     };
     auto field_slice = [&](int n) {
@@ -410,12 +442,13 @@ __global__ void __launch_bounds__(kPstThreads, 1) vp_persist_fwd_kernel(const Pe
         return e2;
     };
     auto rinfo_from = [&](const VShift<float>* vsh) {
-        for (int u = tid; u < a.win_rows; u += blockDim.x) {
-            const VShift<float>* p = vsh + pst_wrap(win_first + u, nx);
+        for (int x = tid; x < bpc * a.win_rows; x += blockDim.x) {
+            const int bi = x / a.win_rows, u = x - bi * a.win_rows;
+            const VShift<float>* p = vsh + pst_wrap(band_row(bi) + a.win_lo + u, nx);
             VShift<float> v;
             v.m = __ldcg(&p->m);
             v.t = __ldcg(&p->t);
-            rinfo[u] = pst_rinfo(v, nv);
+            rinfo[x] = pst_rinfo(v, nv);
         }
     };
     auto publish_energy = [&](int n, double e2) {
@@ -470,8 +503,8 @@ __global__ void __launch_bounds__(kPstThreads, 1) vp_persist_fwd_kernel(const Pe
     // ---- prologue (full mode): h_0 = X(f_iv - f_eq) on the own rows, rho_0 ----
     if (!replay) {
         float* h0 = slot(0);
-        for (int bi = 0; bi < a.bands_per_cta; ++bi) {
-            const int r0 = (b0 + bi) * R;
+        for (int bi = 0; bi < bpc; ++bi) {
+            const int r0 = band_row(bi);
             float acc[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) acc[r] = 0.f;
@@ -483,34 +516,33 @@ __global__ void __launch_bounds__(kPstThreads, 1) vp_persist_fwd_kernel(const Pe
                 const double2 fb = __ldg(reinterpret_cast<const double2*>(a.feq + j0 + 2));
                 const double fe[4] = {fa.x, fa.y, fb.x, fb.y};
                 const float tt[4] = {Q.t.x, Q.t.y, Q.t.z, Q.t.w};
-                float d[R + 2][4];
+                const float w0 = j0 == 0 ? 0.5f : 1.f, w3 = j0 + 3 == nv - 1 ? 0.5f : 1.f;
+                // rolling over the rows of d = f_iv - f_eq: output row r = k - 2 reads d rows
+                // r + delta and r + 1 + delta
+                float d[3][4];
 #pragma unroll
                 for (int k = 0; k < R + 2; ++k) {
                     const int row = pst_wrap(r0 + Q.bm + k, nx);
                     const double2* fr = reinterpret_cast<const double2*>(a.f_iv + (size_t)row * nv + j0);
                     const double2 u = __ldg(fr), v = __ldg(fr + 1);
-                    d[k][0] = (float)(u.x - fe[0]);
-                    d[k][1] = (float)(u.y - fe[1]);
-                    d[k][2] = (float)(v.x - fe[2]);
-                    d[k][3] = (float)(v.y - fe[3]);
-                }
-                float hv[R][4];
+                    d[k % 3][0] = (float)(u.x - fe[0]);
+                    d[k % 3][1] = (float)(u.y - fe[1]);
+                    d[k % 3][2] = (float)(v.x - fe[2]);
+                    d[k % 3][3] = (float)(v.y - fe[3]);
+                    if (k >= 2) {
+                        const int r = k - 2;
+                        float hv[4];
 #pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const bool dl = (Q.mask >> e) & 1;
-#pragma unroll
-                    for (int r = 0; r < R; ++r) {
-                        const float p0 = dl ? d[r + 1][e] : d[r][e];
-                        const float p1 = dl ? d[r + 2][e] : d[r + 1][e];
-                        hv[r][e] = pst_lerp(p0, p1, tt[e]);
+                        for (int e = 0; e < 4; ++e) {
+                            const bool dl = (Q.mask >> e) & 1;
+                            const float p0 = dl ? d[(r + 1) % 3][e] : d[r % 3][e];
+                            const float p1 = dl ? d[(r + 2) % 3][e] : d[(r + 1) % 3][e];
+                            hv[e] = pst_lerp(p0, p1, tt[e]);
+                        }
+                        *reinterpret_cast<float4*>(h0 + (size_t)(r0 + r) * nv + j0) =
+                            make_float4(hv[0], hv[1], hv[2], hv[3]);
+                        acc[r] += w0 * hv[0] + hv[1] + hv[2] + w3 * hv[3];
                     }
-                }
-                const float w0 = j0 == 0 ? 0.5f : 1.f, w3 = j0 + 3 == nv - 1 ? 0.5f : 1.f;
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    *reinterpret_cast<float4*>(h0 + (size_t)(r0 + r) * nv + j0) =
-                        make_float4(hv[r][0], hv[r][1], hv[r][2], hv[r][3]);
-                    acc[r] += w0 * hv[r][0] + hv[r][1] + hv[r][2] + w3 * hv[r][3];
                 }
             }
             band_rows(acc, r0, a.rho);   // rho_0 in buffer 0
@@ -545,8 +577,8 @@ __global__ void __launch_bounds__(kPstThreads, 1) vp_persist_fwd_kernel(const Pe
         float acc[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) acc[r] = 0.f;
-        for (int bi = 0; bi < a.bands_per_cta; ++bi) {
-            const int r0 = (b0 + bi) * R;
+        for (int bi = 0; bi < bpc; ++bi) {
+            const int r0 = band_row(bi);
             for (int jj = 0; jj < cpg; ++jj) {
                 const int j = bi * cpg + jj;
                 const int c = gid + kPstGroups * jj;
@@ -565,84 +597,72 @@ __global__ void __launch_bounds__(kPstThreads, 1) vp_persist_fwd_kernel(const Pe
                 ++tiles_used;
                 // window row k of this thread: stage row 2*(bm - cm.x) + k, global row r0 + 2*bm + k
                 const float* sb = st + (size_t)(2 * (qi.x - cm.x)) * kPstW + 4 + 4 * gt;
-                const int ib = (r0 - r_lo) + 2 * qi.x - a.win_lo;   // rinfo index of window row 0
-                float O[R + 4][4];
+                const int ib = bi * a.win_rows + 2 * qi.x - a.win_lo;   // rinfo index of window row 0
+                // rolling over the window rows: after o row k, d row q = k - 3 (o rows q .. q + 3)
+                // and h' row r = k - 4 (d rows r, r + 1) are complete
+                float O[4][4], dprev[4];
+                float* fh = a.f_hist != nullptr ? a.f_hist + (size_t)(n - n_first) * nxnv : nullptr;
+                const bool fout = fh != nullptr || (last && a.f_final != nullptr);
+                const float w0 = j0 == 0 ? 0.5f : 1.f, w3 = j0 + 3 == nv - 1 ? 0.5f : 1.f;
 #pragma unroll
                 for (int k = 0; k < R + 4; ++k) {
+                    float* o = O[k & 3];
                     const int2 ri = rinfo[ib + k];
                     const float tv = __int_as_float(ri.y);
                     const float* sr = sb + (size_t)k * kPstW;
                     if (ri.x == 0) {
                         const float4 h = *reinterpret_cast<const float4*>(sr);
                         const float h4 = sr[4];
-                        O[k][0] = h.x + tv * ((h.y - h.x) + D4.x);
-                        O[k][1] = h.y + tv * ((h.z - h.y) + D4.y);
-                        O[k][2] = h.z + tv * ((h.w - h.z) + D4.z);
-                        O[k][3] = h.w + tv * ((h4 - h.w) + D4.w);
+                        o[0] = h.x + tv * ((h.y - h.x) + D4.x);
+                        o[1] = h.y + tv * ((h.z - h.y) + D4.y);
+                        o[2] = h.z + tv * ((h.w - h.z) + D4.z);
+                        o[3] = h.w + tv * ((h4 - h.w) + D4.w);
                     } else if (ri.x == -1) {
                         const float hm = sr[-1];
                         const float4 h = *reinterpret_cast<const float4*>(sr);
-                        O[k][0] = (hm - Dm1) + tv * ((h.x - hm) + Dm1);
-                        O[k][1] = (h.x - D4.x) + tv * ((h.y - h.x) + D4.x);
-                        O[k][2] = (h.y - D4.y) + tv * ((h.z - h.y) + D4.y);
-                        O[k][3] = (h.z - D4.z) + tv * ((h.w - h.z) + D4.z);
-                    } else if (ri.x >= -kStageHalo && ri.x < kStageHalo) {
-                        const float* pp = sr + ri.x;
-                        const float v[5] = {pp[0], pp[1], pp[2], pp[3], pp[4]};
-                        const float4 A = __ldg(reinterpret_cast<const float4*>(a.vtab + (size_t)(ri.x + kStageHalo) * nv + j0));
-                        const float4 B = __ldg(reinterpret_cast<const float4*>(
-                            a.vtab + (size_t)(2 * kStageHalo + ri.x + kStageHalo) * nv + j0));
-                        O[k][0] = v[0] + tv * (v[1] - v[0]) + (A.x + tv * B.x);
-                        O[k][1] = v[1] + tv * (v[2] - v[1]) + (A.y + tv * B.y);
-                        O[k][2] = v[2] + tv * (v[3] - v[2]) + (A.z + tv * B.z);
-                        O[k][3] = v[3] + tv * (v[4] - v[3]) + (A.w + tv * B.w);
+                        o[0] = (hm - Dm1) + tv * ((h.x - hm) + Dm1);
+                        o[1] = (h.x - D4.x) + tv * ((h.y - h.x) + D4.x);
+                        o[2] = (h.y - D4.y) + tv * ((h.z - h.y) + D4.y);
+                        o[3] = (h.z - D4.z) + tv * ((h.w - h.z) + D4.z);
                     } else {
-                        // shift beyond the staged halo: the float64 form from global memory
-                        const int row = pst_wrap(r0 + 2 * qi.x + k, nx);
-                        const int mr = ri.x < 0 ? ri.x + nv : ri.x;
-#pragma unroll
-                        for (int e = 0; e < 4; ++e) O[k][e] = pst_v_cell(src, a.feq, nv, row, j0 + e, mr, tv);
+                        const float4 r4 = pst_v_rare(a, sr, src, ri.x, tv, pst_wrap(r0 + 2 * qi.x + k, nx), j0);
+                        o[0] = r4.x;
+                        o[1] = r4.y;
+                        o[2] = r4.z;
+                        o[3] = r4.w;
                     }
-                }
-                // x steps per column: window offset 0 or 2 rows (delta bit), d = X(o), h' = X(d)
-                float dd[R + 1][4];
+                    if (k >= 3) {
+                        // d row q per column: window offset 0 or 2 rows (delta bit)
+                        const int q = k - 3;
+                        float dn[4];
 #pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const bool dl = (qi.y >> e) & 1;
-                    float p0 = dl ? O[2][e] : O[0][e];
-#pragma unroll
-                    for (int q2 = 0; q2 <= R; ++q2) {
-                        const float p1 = dl ? O[q2 + 3][e] : O[q2 + 1][e];
-                        dd[q2][e] = pst_lerp(p0, p1, tt[e]);
-                        p0 = p1;
-                    }
-                }
-                if (a.f_hist != nullptr || (last && a.f_final != nullptr)) {
-                    float* fh = a.f_hist != nullptr ? a.f_hist + (size_t)(n - n_first) * nxnv : nullptr;
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const double fe = __ldg(a.feq + j0 + e);
-                        const int base = r0 + qi.x + ((qi.y >> e) & 1);
-#pragma unroll
-                        for (int r = 0; r < R; ++r) {
-                            const int row = pst_wrap(base + r, nx);
-                            const double f = fe + (double)dd[r][e];
-                            if (fh != nullptr) fh[(size_t)row * nv + j0 + e] = (float)f;
-                            if (last && a.f_final != nullptr) a.f_final[(size_t)row * nv + j0 + e] = f;
+                        for (int e = 0; e < 4; ++e) {
+                            const bool dl = (qi.y >> e) & 1;
+                            const float p0 = dl ? O[(q + 2) & 3][e] : O[q & 3][e];
+                            const float p1 = dl ? O[(q + 3) & 3][e] : O[(q + 1) & 3][e];
+                            dn[e] = pst_lerp(p0, p1, tt[e]);
                         }
-                    }
-                }
-                if (dst != nullptr) {
-                    const float w0 = j0 == 0 ? 0.5f : 1.f, w3 = j0 + 3 == nv - 1 ? 0.5f : 1.f;
+                        if (fout && q < R) {
 #pragma unroll
-                    for (int r = 0; r < R; ++r) {
-                        const float h0v = pst_lerp(dd[r][0], dd[r + 1][0], tt[0]);
-                        const float h1v = pst_lerp(dd[r][1], dd[r + 1][1], tt[1]);
-                        const float h2v = pst_lerp(dd[r][2], dd[r + 1][2], tt[2]);
-                        const float h3v = pst_lerp(dd[r][3], dd[r + 1][3], tt[3]);
-                        *reinterpret_cast<float4*>(dst + (size_t)(r0 + r) * nv + j0) =
-                            make_float4(h0v, h1v, h2v, h3v);
-                        acc[r] += w0 * h0v + h1v + h2v + w3 * h3v;
+                            for (int e = 0; e < 4; ++e) {
+                                const int row = pst_wrap(r0 + qi.x + ((qi.y >> e) & 1) + q, nx);
+                                const double f = __ldg(a.feq + j0 + e) + (double)dn[e];
+                                if (fh != nullptr) fh[(size_t)row * nv + j0 + e] = (float)f;
+                                if (last && a.f_final != nullptr) a.f_final[(size_t)row * nv + j0 + e] = f;
+                            }
+                        }
+                        if (q >= 1 && dst != nullptr) {
+                            const int r = q - 1;
+                            const float h0v = pst_lerp(dprev[0], dn[0], tt[0]);
+                            const float h1v = pst_lerp(dprev[1], dn[1], tt[1]);
+                            const float h2v = pst_lerp(dprev[2], dn[2], tt[2]);
+                            const float h3v = pst_lerp(dprev[3], dn[3], tt[3]);
+                            *reinterpret_cast<float4*>(dst + (size_t)(r0 + r) * nv + j0) =
+                                make_float4(h0v, h1v, h2v, h3v);
+                            acc[r] += w0 * h0v + h1v + h2v + w3 * h3v;
+                        }
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) dprev[e] = dn[e];
                     }
                 }
                 group_sync();   // the stage is free
@@ -745,22 +765,21 @@ bool persist_prepare(PersistHost& ph, int nx, int nv, const std::vector<long lon
     for (int bpc = 1; bpc <= bands; ++bpc) {
         if (bands % bpc != 0) continue;
         const int G = bands / bpc;
-        // the union window of the CTA's tiles (offsets from its first row), widened to cover
-        // its own rows
+        // the window of a band's tiles (offsets from its first row), widened to cover its own rows
         const int win_lo = std::min(2 * (int)all_lo, 0);
-        const int win_end = std::max(bpc * R + 2 * (int)all_hi + 4, bpc * R);
+        const int win_end = std::max(R + 2 * (int)all_hi + 4, R);
         const int win_rows = win_end - win_lo;
         if (win_rows > nx) return false;   // the coefficient slice of the field covers at most nx rows
-        const int fdist = (long long)win_rows * nx > (1LL << 17) ? 1 : 0;
+        const int fdist = (long long)bpc * win_rows * nx > (1LL << 17) ? 1 : 0;
         const int field_rows = fdist ? (nx + G - 1) / G : win_rows;
-        // stages per column group: up to all of the group's tiles of a step, within about 160 KB
+        // stages per column group: up to all of the group's tiles of a step, within about 96 KB
         // for the four groups
         const int ntile = bpc * ((nv / kPstC + kPstGroups - 1) / kPstGroups);
         const size_t stage_bytes = (size_t)span_max * kPstW * sizeof(float);
-        const int fit = (int)((160 * 1024) / (std::min(kPstGroups, nv / kPstC) * stage_bytes));
+        const int fit = (int)((96 * 1024) / (std::min(kPstGroups, nv / kPstC) * stage_bytes));
         const int stages = std::max(1, std::min({kPstMaxStages, ntile, fit}));
         int stage_floats = 0, fs_alias = 0;
-        const size_t smem = persist_smem_bytes(span_max, win_rows, R, nx, nv, field_rows, stages, &stage_floats,
+        const size_t smem = persist_smem_bytes(span_max, bpc * win_rows, R, nx, nv, field_rows, stages, &stage_floats,
                                                &fs_alias);
         if (smem > 200 * 1024) continue;
         const int per_sm = pst_max_blocks_r(R, smem);
