@@ -1078,9 +1078,8 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
             free_plan(p);
             return rc;
         }
-        // default: grids that are not cluster-resident and whose field inputs fit beside the stage
-        // buffers (about nx <= 3000); on larger grids the per-step kernels keep more warps busy
-        p->pst_on = (p->res_cn == 0 && !p->pst.fs_alias) ? 1 : 0;
+        // default: every eligible grid that is not cluster-resident
+        p->pst_on = p->res_cn == 0 ? 1 : 0;
     } else {
         p->pst = PersistHost{};
     }
