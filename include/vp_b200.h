@@ -356,7 +356,8 @@ typedef struct vp_launch_config {
                               /* whose CTAs own bands of this many rows (4, 8 or 16) and meet at */
                               /* a bounded grid barrier once per step; 0: off. Needs an          */
                               /* x-invariant f_eq, nv a multiple of 256 and nx <= 16384; on by   */
-                              /* default where the state is not cluster-resident                */
+                              /* default where the state is not cluster-resident and each CTA  */
+                              /* can solve the field on its own window rows (nx of a few 1000s)  */
     int32_t persist_ctas;     /* CTAs of that launch (derived)                                    */
     int64_t persist_smem_bytes; /* dynamic shared memory per CTA of that launch (derived)        */
 } vp_launch_config;

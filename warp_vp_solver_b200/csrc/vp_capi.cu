@@ -743,7 +743,51 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
 
     b.c_src = nullptr;
     b.c_src2 = nullptr;
-    for (int n = T_steps - 1; n >= 1; --n) {
+    bool adj_persist = false;
+    if constexpr (sizeof(T) == 4) adj_persist = p->pst_on && p->pst.bwd_ok && !p->merged;
+    if (adj_persist) {
+        // one persistent launch per checkpoint segment: adjoint steps n with h_{n-1} in the segment,
+        // after the segment's states are replayed
+        for (int sgi = (T_steps - 2) / K; sgi >= 0 && T_steps >= 2; --sgi) {
+            const int n_lo = sgi * K + 1, n_hi = std::min(sgi * K + K, T_steps - 1);
+            if (n_hi < n_lo) continue;
+            if ((rc = recompute(sgi)) != VP_OK) return rc;
+            PersistBwdArgs pb{};
+            pb.nx = nx;
+            pb.nv = nv;
+            pb.n_chunks = nv / 256;
+            pb.n_hi = n_hi;
+            pb.n_lo = n_lo;
+            pb.K = K;
+            pb.wbuf0 = reinterpret_cast<float*>(wbuf[0]);
+            pb.wbuf1 = reinterpret_cast<float*>(wbuf[1]);
+            pb.ckpt = reinterpret_cast<const float*>(ckpt);
+            pb.seg = reinterpret_cast<const float*>(seg);
+            pb.quad = p->d_pquad;
+            pb.tq = p->d_ptq;
+            pb.chunk = p->d_pchunk;
+            pb.dfeq = p->d_dfeq;
+            pb.vtab = static_cast<const float*>(p->d_vtab);
+            pb.feq = p->d_feq;
+            pb.ctab = p->d_ctab2;
+            pb.dv = (float)p->dv;
+            pb.dx = (float)p->dx;
+            pb.neg_dt_dv = (float)(-p->dt / p->dv);
+            pb.vsh_tape = reinterpret_cast<const VShift<float>*>(vsh_all);
+            pb.E_tape = reinterpret_cast<const float*>(E_all);
+            pb.g_fh = reinterpret_cast<const float*>(g_fh);
+            pb.g_Eh = reinterpret_cast<const float*>(g_Eh);
+            pb.g_ee = reinterpret_cast<const float*>(g_ee);
+            pb.g_H = reinterpret_cast<float*>(g_H);
+            pb.grho = reinterpret_cast<float*>(grho);
+            pb.gE = reinterpret_cast<float*>(ws + L.gscratch);
+            pb.bar = reinterpret_cast<unsigned*>(ws + L.pbar);
+            pb.status = p->d_status;
+            pb.wait_ns = p->wait_ns;
+            VP_CUDA(launch_persist_bwd(pb, p->pst, s), "persistent adjoint launch");
+        }
+    }
+    for (int n = adj_persist ? 0 : T_steps - 1; n >= 1; --n) {
         if ((rc = recompute((n - 1) / K)) != VP_OK) return rc;
         b.w_in = wbuf[n & 1];
         b.grho = grho;
@@ -1078,8 +1122,11 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
             free_plan(p);
             return rc;
         }
-        // default: every eligible grid that is not cluster-resident
-        p->pst_on = p->res_cn == 0 ? 1 : 0;
+        // default: grids that are not cluster-resident and whose CTAs each solve the field on their
+        // own window rows (measured on B200: 512x1024 forward + adjoint 2.0e10 cell-steps/s
+        // against 1.1e10 per step); where the field needs slices and a second barrier per step
+        // (8192x8192) the per-step kernels were faster (7.6e10 against 6.9e10)
+        p->pst_on = (p->res_cn == 0 && p->pst.field_dist == 0) ? 1 : 0;
     } else {
         p->pst = PersistHost{};
     }

@@ -228,10 +228,44 @@ struct PersistArgs {
     VShift<float>* vsh_tape;
 };
 
+// Persistent adjoint steps n_hi .. n_lo (descending, >= 1) of the discrete adjoint (vp_persist.cu).
+struct PersistBwdArgs {
+    int nx, nv, n_chunks;
+    int bands_per_cta, span_max, win_lo, win_rows, field_dist, stage_floats, fs_alias, stages, field_rows;
+    int n_hi, n_lo, K;
+    float* wbuf0;               // cotangent on the v-step output of step n: wbuf[n & 1]
+    float* wbuf1;
+    const float* ckpt;          // h_n: ckpt + (n / K) * nx * nv when n % K == 0, else
+    const float* seg;           //      seg + (n % K - 1) * nx * nv
+    const int2* quad;
+    const float4* tq;
+    const int2* chunk;
+    const float* dfeq;
+    const float* vtab;
+    const double* feq;
+    const float* ctab;
+    float dv, dx, neg_dt_dv;
+    const VShift<float>* vsh_tape;
+    const float* E_tape;
+    const float* g_fh;          // [n_steps][nx][nv] or null
+    const float* g_Eh;          // [n_steps][nx] or null
+    const float* g_ee;          // [n_steps] or null
+    float* g_H;                 // accumulated
+    float* grho;                // [nx] in: cotangent on rho of step n_hi; out: of step n_lo - 1
+    float* gE;                  // [2][nx] scratch
+    unsigned* bar;
+    unsigned* status;
+    unsigned long long wait_ns;
+};
+
 struct PersistHost {
     int R = 0, G = 0, bands_per_cta = 0, span_max = 0, win_lo = 0, win_rows = 0, field_dist = 0;
     int stage_floats = 0, fs_alias = 0, stages = 2, field_rows = 0;
     size_t smem = 0;
+    // adjoint launch shape (same bands, CTAs and column groups): window, stage area, field rows
+    int bwd_ok = 0, bwin_lo = 0, bwin_rows = 0, bstage_floats = 0, bfs_alias = 0, bstages = 1, bfield_rows = 0;
+    int bfield_dist = 0;
+    size_t bsmem = 0;
     std::vector<int2> quad;
     std::vector<float> tq;
     std::vector<int2> chunk;
@@ -243,6 +277,7 @@ struct PersistHost {
 bool persist_prepare(PersistHost& ph, int nx, int nv, const std::vector<long long>& m_signed,
                      const std::vector<double>& tx, int n_sms, int force_rows);
 cudaError_t launch_persist_fwd(const PersistArgs& a, const PersistHost& ph, cudaStream_t s);
+cudaError_t launch_persist_bwd(const PersistBwdArgs& a, const PersistHost& ph, cudaStream_t s);
 size_t persist_smem_bytes(int span_max, int win_rows, int R, int nx, int nv, int field_rows, int stages,
                           int* stage_floats, int* fs_alias);
 

@@ -233,6 +233,62 @@ __device__ __forceinline__ void pst_circ_rows(const float* fs, int nx, int n_row
     }
 }
 
+// The transposed product: E_r = sum_k c[(k - f0 - r) mod nx] x_k (Poisson^T, the adjoint's field),
+// staged as cs[u] = ctab[2 nx - f0 - n_rows - 2 + u], u < nx + n_rows + 6: coefficient (row r, k)
+// = cs[n_rows + 2 - r + k]. Needs n_rows <= nx - 8. Ends with a block barrier.
+__device__ __forceinline__ int pst_field_inputs_t(float* fs, const float* x, const float* __restrict__ ctab,
+                                                  int nx, int first, int n_rows) {
+    const int f0 = pst_wrap(first, nx);
+    for (int k = (int)threadIdx.x; k < nx / 4; k += blockDim.x) pst_cp16(fs + 4 * k, x + 4 * k);
+    float* cs = fs + nx;
+    const int len = nx + n_rows + 6;
+    const float* src = ctab + (2 * nx - f0 - n_rows - 2);
+    for (int u = threadIdx.x; u < len; u += blockDim.x) pst_cp4(cs + u, src + u);
+    pst_cp_commit();
+    pst_cp_wait(0);
+    __syncthreads();
+    return f0;
+}
+
+template <typename F>
+__device__ __forceinline__ void pst_circ_rows_t(const float* fs, int nx, int n_rows, F&& out) {
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int ngrp = (n_rows + 3) >> 2;
+    const float* cs = fs + nx;
+    for (int grp = (int)(threadIdx.x >> 5); grp < ngrp; grp += nw) {
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+        const float* cp = cs + n_rows + 2 - 4 * grp + lane;
+#pragma unroll 4
+        for (int k = lane; k < nx; k += 32) {
+            const float xk = fs[k];
+            acc[0] += cp[0] * xk;
+            acc[1] += cp[-1] * xk;
+            acc[2] += cp[-2] * xk;
+            acc[3] += cp[-3] * xk;
+            cp += 32;
+        }
+#pragma unroll
+        for (int st = 0; st < 2; ++st) {
+            const int o = 16 >> st;
+            const int n = 2 >> st;
+            const bool upper = (lane & o) != 0;
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                if (q < n) {
+                    const float send = upper ? acc[q] : acc[q + n];
+                    const float keep = upper ? acc[q + n] : acc[q];
+                    acc[q] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+                }
+            }
+        }
+        float sum = acc[0];
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        const int r = 4 * grp + (lane >> 3);
+        if ((lane & 7) == 0 && r < n_rows) out(r, sum);
+    }
+}
+
 // Per-quad constants of the tiles (x weights, f_eq differences, smallest shift and its delta bits,
 // the f_eq difference left of the quad), kept in shared memory for the whole launch when the
 // grid's nv/4 records fit in kPstQuadSmemBytes.
@@ -682,6 +738,359 @@ __global__ void __launch_bounds__(kPstThreads, 2) vp_persist_fwd_kernel(const Pe
 }
 
 // ---------------------------------------------------------------------------------------------
+// Persistent adjoint steps (the per-step phase of the discrete adjoint, warp_vp_solver/solver.py:
+// 814-929): for n = n_hi down to n_lo, gh = V^T w_n + rho^T grho_n on a window of R + 4 rows,
+// c = X^T gh (+ the f_hist cotangent), w_{n-1} = X^T c on the own rows, and the slope row sums of
+// h_{n-1}; after the grid barrier g_E and grho_{n-1} = Poisson^T g_E (transposed circulant). Same
+// work split, column groups, staging ring and barrier as the forward loop. The thread of column
+// shift m reads the window rows r0 - 2m - 2 + k; a quad's window is rows r0 - 2 bm - 4 + k',
+// k' < R + 4, and a column with shift bm reads it two rows higher than one with bm + 1.
+// ---------------------------------------------------------------------------------------------
+
+// V^T of one quad row for shifts other than 0 and -1 (out of line): staged for |shift| <= 4,
+// global memory beyond.
+__device__ __noinline__ float4 pst_vt_rare(const float* sr, const float* w_src, int nv, int ms, float tv,
+                                           int row, int j0) {
+    float4 o;
+    if (ms >= -kStageHalo + 1 && ms <= kStageHalo - 1) {
+        const float* pp = sr - ms - 1;
+        const float v[5] = {pp[0], pp[1], pp[2], pp[3], pp[4]};
+        o.x = v[1] + tv * (v[0] - v[1]);
+        o.y = v[2] + tv * (v[1] - v[2]);
+        o.z = v[3] + tv * (v[2] - v[3]);
+        o.w = v[4] + tv * (v[3] - v[4]);
+    } else {
+        const int mr = ms < 0 ? ms + nv : ms;
+        const float* wr = w_src + (size_t)row * nv;
+        float r[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            int c0 = j0 + e - mr;
+            c0 += c0 < 0 ? nv : 0;
+            const int c1 = c0 == 0 ? nv - 1 : c0 - 1;
+            r[e] = (1.f - tv) * __ldcg(wr + c0) + tv * __ldcg(wr + c1);
+        }
+        o = make_float4(r[0], r[1], r[2], r[3]);
+    }
+    return o;
+}
+
+// Slope (h + f_eq)[j + m + 1] - (h + f_eq)[j + m] of one quad row of h_{n-1} for shifts other than
+// 0 and -1 (out of line).
+__device__ __noinline__ float4 pst_slope_rare(const float* hr_s, const float* h_src, const float* vtab,
+                                              const double* feq, int nv, int ms, int row, int j0) {
+    float4 o;
+    if (ms >= -kStageHalo && ms < kStageHalo) {
+        const float* pp = hr_s + ms;
+        const float4 B = __ldg(reinterpret_cast<const float4*>(vtab + (size_t)(2 * kStageHalo + ms + kStageHalo) * nv + j0));
+        o.x = (pp[1] - pp[0]) + B.x;
+        o.y = (pp[2] - pp[1]) + B.y;
+        o.z = (pp[3] - pp[2]) + B.z;
+        o.w = (pp[4] - pp[3]) + B.w;
+    } else {
+        const int mr = ms < 0 ? ms + nv : ms;
+        const float* hr = h_src + (size_t)row * nv;
+        float r[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            int d0 = j0 + e + mr;
+            d0 -= d0 >= nv ? nv : 0;
+            const int d1 = d0 + 1 == nv ? 0 : d0 + 1;
+            r[e] = (__ldcg(hr + d1) - __ldcg(hr + d0)) + (float)(__ldg(feq + d1) - __ldg(feq + d0));
+        }
+        o = make_float4(r[0], r[1], r[2], r[3]);
+    }
+    return o;
+}
+
+template <int R>
+__global__ void __launch_bounds__(kPstThreads, 2) vp_persist_bwd_kernel(const PersistBwdArgs a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ int s_flag;
+
+    const int nx = a.nx, nv = a.nv, nch = a.n_chunks;
+    const size_t nxnv = (size_t)nx * nv;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int gid = tid / kPstGroup, gt = tid - gid * kPstGroup;
+    const int g = blockIdx.x, G = gridDim.x;
+    const int bpc = a.bands_per_cta;
+    auto band_row = [&](int bi) { return (g + bi * G) * R; };
+    const int S = a.stages;
+    const int srows = a.span_max + R;                 // staged rows per stage: w window, then own h rows
+    float* stages = reinterpret_cast<float*>(smem);
+    int4* rinfo = reinterpret_cast<int4*>(stages + (size_t)a.stage_floats);   // [bpc][win_rows]
+    int* hinfo = reinterpret_cast<int*>(rinfo + (size_t)bpc * a.win_rows);   // [bpc][R]
+    float* red = reinterpret_cast<float*>(hinfo + (((size_t)bpc * R + 3) & ~(size_t)3));
+    float* fs = a.fs_alias ? stages : red + kPstWarps * R + 4;
+    const size_t ff = ((size_t)2 * nx + a.field_rows + 8 + 3) & ~(size_t)3;
+    const int nq = nv / 4;
+    PstQuad* sq = ((size_t)nq * sizeof(PstQuad) <= kPstQuadSmemBytes)
+                      ? reinterpret_cast<PstQuad*>(a.fs_alias ? red + kPstWarps * R + 4 : fs + ff)
+                      : nullptr;
+    const int cpg = gid < nch ? (nch - gid + kPstGroups - 1) / kPstGroups : 0;
+    const int ntile = bpc * cpg;
+
+    auto quad_of = [&](int q) -> PstQuad {
+        PstQuad r;
+        const int2 qi = __ldg(a.quad + q);
+        r.t = __ldg(a.tq + q);
+        r.D = __ldg(reinterpret_cast<const float4*>(a.dfeq) + q);
+        r.bm = qi.x;
+        r.mask = qi.y;
+        r.Dm1 = __ldg(a.dfeq + (q == 0 ? nv - 1 : 4 * q - 1));
+        r.pad = 0.f;
+        return r;
+    };
+    if (sq != nullptr)
+        for (int q = tid; q < nq; q += blockDim.x) sq[q] = quad_of(q);
+
+    auto h_slot = [&](int n) -> const float* {
+        if (n % a.K == 0) return a.ckpt + (size_t)(n / a.K) * nxnv;
+        return a.seg + (size_t)(n % a.K - 1) * nxnv;
+    };
+    auto rinfo_row = [&](int n, int row, float gr) {
+        const VShift<float> v = a.vsh_tape[(size_t)n * nx + row];
+        int4 r;
+        r.x = v.m > nv / 2 ? v.m - nv : v.m;
+        r.y = __float_as_int(v.t);
+        r.z = __float_as_int(gr);
+        r.w = 0;
+        return r;
+    };
+    auto load_rinfo = [&](int n) {   // step n's shifts and grho (global) on every band's window rows
+        for (int x = tid; x < bpc * a.win_rows; x += blockDim.x) {
+            const int bi = x / a.win_rows, u = x - bi * a.win_rows;
+            const int row = pst_wrap(band_row(bi) + a.win_lo + u, nx);
+            rinfo[x] = rinfo_row(n, row, __ldcg(a.grho + row));
+        }
+    };
+    auto load_hinfo = [&](int n) {   // step n's signed shifts of the own rows
+        for (int x = tid; x < bpc * R; x += blockDim.x) {
+            const int bi = x / R, r = x - bi * R;
+            const int m = a.vsh_tape[(size_t)n * nx + band_row(bi) + r].m;
+            hinfo[x] = m > nv / 2 ? m - nv : m;
+        }
+    };
+
+    unsigned bar_index = 0;
+    bool alive = true;
+    auto barrier = [&]() -> bool {
+        if (!pst_grid_barrier(a.bar, bar_index++, (unsigned)G, a.wait_ns, a.status, &s_flag)) alive = false;
+        return alive;
+    };
+    auto group_sync = [&]() { asm volatile("bar.sync %0, %1;" ::"r"(1 + gid), "r"(kPstGroup) : "memory"); };
+
+    constexpr int kPieces = kPstW / 4;
+    unsigned tiles_issued = 0, tiles_used = 0;
+    auto stage_ptr = [&](unsigned k) {
+        return stages + (size_t)(gid * S + (int)(k % (unsigned)S)) * srows * kPstW;
+    };
+    auto issue = [&](int j, const float* w_src, const float* h_src) {
+        const unsigned mine = tiles_issued++;
+        const int bi = j / cpg;
+        const int c = gid + kPstGroups * (j - bi * cpg);
+        const int r0 = band_row(bi), c0 = c * kPstC;
+        const int2 cm = __ldg(a.chunk + c);
+        const int span = 2 * (cm.y - cm.x) + R + 4;
+        const int lo = r0 - 2 * cm.y - 4;             // w window of the chunk
+        float* st = stage_ptr(mine);
+        for (int p = gt; p < (span + R) * kPieces; p += kPstGroup) {
+            const int k = p / kPieces, v = p - k * kPieces;
+            int col = c0 - 4 + 4 * v;
+            col += col < 0 ? nv : 0;
+            col -= col >= nv ? nv : 0;
+            const bool wrow = k < span;
+            const float* src = wrow ? w_src + (size_t)pst_wrap(lo + k, nx) * nv + col
+                                    : h_src + (size_t)(r0 + k - span) * nv + col;
+            const int srow = wrow ? k : a.span_max + (k - span);
+            pst_cp16(st + (size_t)srow * kPstW + 4 * v, src);
+        }
+        pst_cp_commit();
+    };
+
+    auto band_rows = [&](float (&acc)[R], int r0, int n) {
+        constexpr int LG = R >= 32 ? 5 : R >= 16 ? 4 : R >= 8 ? 3 : R >= 4 ? 2 : R >= 2 ? 1 : 0;
+#pragma unroll
+        for (int st = 0; st < LG; ++st) {
+            const int o = 16 >> st;
+            const int nn = R >> (st + 1);
+            const bool upper = (lane & o) != 0;
+#pragma unroll
+            for (int i = 0; i < (R >> 1); ++i) {
+                if (i < nn) {
+                    const float send = upper ? acc[i] : acc[i + nn];
+                    const float keep = upper ? acc[i + nn] : acc[i];
+                    acc[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+                }
+            }
+        }
+        float v = acc[0];
+#pragma unroll
+        for (int o = 16 >> LG; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((lane & ((32 >> LG) - 1)) == 0) red[wid * R + (lane >> (5 - LG))] = v;
+        __syncthreads();
+        if (tid < R) {
+            float sum = 0.f;
+            for (int w = 0; w < kPstWarps; ++w) sum += red[w * R + tid];
+            // tail of step n - 1 for this row (warp_vp_solver/solver.py:870-929)
+            const int i = r0 + tid;
+            float gEt = a.neg_dt_dv * sum;
+            if (a.g_Eh != nullptr) gEt += __ldg(a.g_Eh + (size_t)(n - 1) * nx + i);
+            a.g_H[i] += gEt;
+            const float gee = a.g_ee != nullptr ? __ldg(a.g_ee + n - 1) : 0.f;
+            a.gE[(size_t)(n & 1) * nx + i] = gEt + a.dx * trap_w<float>(i, nx) * __ldg(a.E_tape + (size_t)(n - 1) * nx + i) * gee;
+        }
+        __syncthreads();
+    };
+
+    load_rinfo(a.n_hi);
+    load_hinfo(a.n_hi - 1);
+    __syncthreads();
+
+    for (int n = a.n_hi; n >= a.n_lo && alive; --n) {
+        const float* w_src = (n & 1) ? a.wbuf1 : a.wbuf0;
+        float* w_dst = (n & 1) ? a.wbuf0 : a.wbuf1;
+        const float* h_src = h_slot(n - 1);
+        const float* gfh = a.g_fh != nullptr ? a.g_fh + (size_t)(n - 1) * nxnv : nullptr;
+        for (int j = 0; j < S && j < ntile; ++j) issue(j, w_src, h_src);
+
+        float acc[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) acc[r] = 0.f;
+        for (int bi = 0; bi < bpc; ++bi) {
+            const int r0 = band_row(bi);
+            for (int jj = 0; jj < cpg; ++jj) {
+                const int j = bi * cpg + jj;
+                const int c = gid + kPstGroups * jj;
+                const int q = c * kPstGroup + gt;
+                const int j0 = c * kPstC + 4 * gt;
+                const int2 cm = __ldg(a.chunk + c);
+                const PstQuad Q = sq != nullptr ? sq[q] : quad_of(q);
+                const float tt[4] = {Q.t.x, Q.t.y, Q.t.z, Q.t.w};
+                const float4 D4 = Q.D;
+                const float Dm1 = Q.Dm1;
+                const float wr0 = j0 == 0 ? -0.5f * a.dv : -a.dv;          // rho^T weights
+                const float wr3 = j0 + 3 == nv - 1 ? -0.5f * a.dv : -a.dv;
+                pst_cp_wait((int)(tiles_issued - tiles_used - 1));
+                group_sync();
+                const float* st = stage_ptr(tiles_used);
+                ++tiles_used;
+                const float* sb = st + (size_t)(2 * (cm.y - Q.bm)) * kPstW + 4 + 4 * gt;   // window row 0
+                const float* hb = st + (size_t)a.span_max * kPstW + 4 + 4 * gt;            // own row 0
+                const int ib = bi * a.win_rows + (-2 * Q.bm - 4 - a.win_lo);
+                float GH[4][4], cprev[4];
+#pragma unroll
+                for (int k = 0; k < R + 4; ++k) {
+                    float* o = GH[k & 3];
+                    const int4 ri = rinfo[ib + k];
+                    const float tv = __int_as_float(ri.y), gr = __int_as_float(ri.z);
+                    const float* sr = sb + (size_t)k * kPstW;
+                    float4 v4;
+                    if (ri.x == 0) {
+                        const float hm = sr[-1];
+                        const float4 h = *reinterpret_cast<const float4*>(sr);
+                        v4 = make_float4(h.x + tv * (hm - h.x), h.y + tv * (h.x - h.y), h.z + tv * (h.y - h.z),
+                                         h.w + tv * (h.z - h.w));
+                    } else if (ri.x == -1) {
+                        const float4 h = *reinterpret_cast<const float4*>(sr);
+                        const float h4 = sr[4];
+                        v4 = make_float4(h.y + tv * (h.x - h.y), h.z + tv * (h.y - h.z), h.w + tv * (h.z - h.w),
+                                         h4 + tv * (h.w - h4));
+                    } else {
+                        v4 = pst_vt_rare(sr, w_src, nv, ri.x, tv, pst_wrap(r0 - 2 * Q.bm - 4 + k, nx), j0);
+                    }
+                    o[0] = v4.x + wr0 * gr;
+                    o[1] = v4.y - a.dv * gr;
+                    o[2] = v4.z - a.dv * gr;
+                    o[3] = v4.w + wr3 * gr;
+                    if (k >= 3) {
+                        // c row q per column (column shift bm + delta reads window rows q + 2 - 2 delta ..)
+                        const int q2 = k - 3;
+                        float cn[4];
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) {
+                            const bool dl = (Q.mask >> e) & 1;
+                            const float g0 = dl ? GH[q2 & 3][e] : GH[(q2 + 2) & 3][e];
+                            const float g1 = dl ? GH[(q2 + 1) & 3][e] : GH[(q2 + 3) & 3][e];
+                            cn[e] = pst_lerp(g1, g0, tt[e]);
+                            if (gfh != nullptr) {
+                                const int row = pst_wrap(r0 - Q.bm - ((Q.mask >> e) & 1) - 1 + q2, nx);
+                                cn[e] += __ldg(gfh + (size_t)row * nv + j0 + e);
+                            }
+                        }
+                        if (q2 >= 1) {
+                            // w row r = q2 - 1 (own row r0 + r) and its slope products
+                            const int r = q2 - 1;
+                            float wv[4];
+#pragma unroll
+                            for (int e = 0; e < 4; ++e) wv[e] = pst_lerp(cn[e], cprev[e], tt[e]);
+                            *reinterpret_cast<float4*>(w_dst + (size_t)(r0 + r) * nv + j0) =
+                                make_float4(wv[0], wv[1], wv[2], wv[3]);
+                            const int ms = hinfo[bi * R + r];
+                            const float* hr = hb + (size_t)r * kPstW;
+                            float4 sl;
+                            if (ms == 0) {
+                                const float4 h = *reinterpret_cast<const float4*>(hr);
+                                const float h4 = hr[4];
+                                sl = make_float4((h.y - h.x) + D4.x, (h.z - h.y) + D4.y, (h.w - h.z) + D4.z,
+                                                 (h4 - h.w) + D4.w);
+                            } else if (ms == -1) {
+                                const float hm = hr[-1];
+                                const float4 h = *reinterpret_cast<const float4*>(hr);
+                                sl = make_float4((h.x - hm) + Dm1, (h.y - h.x) + D4.x, (h.z - h.y) + D4.y,
+                                                 (h.w - h.z) + D4.z);
+                            } else {
+                                sl = pst_slope_rare(hr, h_src, a.vtab, a.feq, nv, ms, r0 + r, j0);
+                            }
+                            acc[r] += sl.x * wv[0] + sl.y * wv[1] + sl.z * wv[2] + sl.w * wv[3];
+                        }
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) cprev[e] = cn[e];
+                    }
+                }
+                group_sync();   // the stage is free
+                if (j + S < ntile) issue(j + S, w_src, h_src);
+            }
+            band_rows(acc, r0, n);
+#pragma unroll
+            for (int r = 0; r < R; ++r) acc[r] = 0.f;
+        }
+        if (!barrier()) break;
+        // grho_{n-1} = Poisson^T g_E: on every band's window rows (and the own rows to global), or
+        // in slices with a second barrier
+        const float* gE = a.gE + (size_t)(n & 1) * nx;
+        const bool more = n - 1 >= a.n_lo;
+        if (a.field_dist == 0) {
+            for (int bi = 0; bi < bpc; ++bi) {
+                const int wf = band_row(bi) + a.win_lo;
+                if (bi > 0) __syncthreads();
+                pst_field_inputs_t(fs, gE, a.ctab, nx, wf, a.win_rows);
+                int4* ri = rinfo + (size_t)bi * a.win_rows;
+                pst_circ_rows_t(fs, nx, a.win_rows, [&](int u, float v) {
+                    const int row = pst_wrap(wf + u, nx);
+                    if (more) ri[u] = rinfo_row(n - 1, row, v);
+                    const int own = u + a.win_lo;
+                    if (own >= 0 && own < R) a.grho[row] = v;
+                });
+            }
+        } else {
+            const int Sl = (nx + G - 1) / G;
+            const int first = g * Sl;
+            const int cnt = max(0, min(Sl, nx - first));
+            pst_field_inputs_t(fs, gE, a.ctab, nx, first, cnt);
+            pst_circ_rows_t(fs, nx, cnt, [&](int u, float v) { a.grho[first + u] = v; });
+            if (more) {
+                if (!barrier()) break;
+                load_rinfo(n - 1);
+            }
+        }
+        if (more && n - 2 >= 0) load_hinfo(n - 2);
+        __syncthreads();
+    }
+    pst_cp_wait(0);
+}
+
+// ---------------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------------
 
@@ -701,6 +1110,27 @@ static int pst_max_blocks(size_t smem) {
         return 0;
     }
     return n;
+}
+
+template <int R>
+static int pst_bwd_max_blocks(size_t smem) {
+    int n = 0;
+    if (cudaFuncSetAttribute(vp_persist_bwd_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, vp_persist_bwd_kernel<R>, kPstThreads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+static int pst_bwd_max_blocks_r(int R, size_t smem) {
+    switch (R) {
+        case 4: return pst_bwd_max_blocks<4>(smem);
+        case 8: return pst_bwd_max_blocks<8>(smem);
+        case 16: return pst_bwd_max_blocks<16>(smem);
+        default: return 0;
+    }
 }
 
 static int pst_max_blocks_r(int R, size_t smem) {
@@ -769,7 +1199,7 @@ bool persist_prepare(PersistHost& ph, int nx, int nv, const std::vector<long lon
         const int win_lo = std::min(2 * (int)all_lo, 0);
         const int win_end = std::max(R + 2 * (int)all_hi + 4, R);
         const int win_rows = win_end - win_lo;
-        if (win_rows > nx) return false;   // the coefficient slice of the field covers at most nx rows
+        if (win_rows > nx - 8) return false;   // the coefficient slices of the fields cover at most nx - 8 rows
         const int fdist = (long long)bpc * win_rows * nx > (1LL << 17) ? 1 : 0;
         const int field_rows = fdist ? (nx + G - 1) / G : win_rows;
         // stages per column group: up to all of the group's tiles of a step, within about 96 KB
@@ -798,6 +1228,40 @@ bool persist_prepare(PersistHost& ph, int nx, int nv, const std::vector<long lon
         ph.fs_alias = fs_alias;
         ph.stages = stages;
         ph.field_rows = field_rows;
+        // the adjoint: window rows r0 - 2m - 4 .. r0 - 2m + R per column quad, widened to the own
+        // rows; each stage holds the chunk's window of w and the band's own rows of h_{n-1}
+        const int bwin_lo = std::min(-2 * (int)all_hi - 4, 0);
+        const int bwin_end = std::max(R - 2 * (int)all_lo, R);
+        const int bwin_rows = bwin_end - bwin_lo;
+        if (bwin_rows <= nx - 8) {
+            const int bfdist = (long long)bpc * bwin_rows * nx > (1LL << 17) ? 1 : 0;
+            const int bfield_rows = bfdist ? (nx + G - 1) / G : bwin_rows;
+            const int groups = std::min(kPstGroups, nv / kPstC);
+            const size_t bstage_bytes = (size_t)(span_max + R) * kPstW * sizeof(float);
+            const int bfit = (int)((96 * 1024) / (groups * bstage_bytes));
+            const int bstages = std::max(1, std::min({kPstMaxStages, ntile, bfit}));
+            const size_t st = (size_t)groups * bstages * (span_max + R) * kPstW;
+            const size_t ff = (pst_field_floats(nx, bfield_rows) + 3) & ~(size_t)3;
+            const bool alias = ff * sizeof(float) > kPstOwnFieldBytes;
+            const size_t area = alias ? std::max(st, ff) : st;
+            size_t b = area * sizeof(float) + (size_t)bpc * bwin_rows * 16 + (((size_t)bpc * R + 3) & ~(size_t)3) * 4;
+            b += (size_t)kPstWarps * R * sizeof(float) + 16;
+            if (!alias) b += ff * sizeof(float);
+            const size_t qb = (size_t)(nv / 4) * sizeof(PstQuad);
+            if (qb <= kPstQuadSmemBytes) b += qb;
+            const int bper_sm = b <= 200 * 1024 ? pst_bwd_max_blocks_r(R, b) : 0;
+            if (bper_sm > 0 && (long long)bper_sm * n_sms >= G) {
+                ph.bwd_ok = 1;
+                ph.bwin_lo = bwin_lo;
+                ph.bwin_rows = bwin_rows;
+                ph.bstage_floats = (int)area;
+                ph.bfs_alias = alias ? 1 : 0;
+                ph.bstages = bstages;
+                ph.bfield_rows = bfield_rows;
+                ph.bfield_dist = bfdist;
+                ph.bsmem = b;
+            }
+        }
         return true;
     }
     return false;
@@ -830,6 +1294,40 @@ cudaError_t launch_persist_fwd(const PersistArgs& args, const PersistHost& ph, c
         case 4: e = cudaLaunchKernelEx(&cfg, vp_persist_fwd_kernel<4>, a); break;
         case 8: e = cudaLaunchKernelEx(&cfg, vp_persist_fwd_kernel<8>, a); break;
         case 16: e = cudaLaunchKernelEx(&cfg, vp_persist_fwd_kernel<16>, a); break;
+        default: return cudaErrorInvalidValue;
+    }
+    count_launch();
+    return e;
+}
+
+cudaError_t launch_persist_bwd(const PersistBwdArgs& args, const PersistHost& ph, cudaStream_t s) {
+    if (!ph.bwd_ok) return cudaErrorInvalidValue;
+    PersistBwdArgs a = args;
+    a.bands_per_cta = ph.bands_per_cta;
+    a.span_max = ph.span_max;
+    a.win_lo = ph.bwin_lo;
+    a.win_rows = ph.bwin_rows;
+    a.field_dist = ph.bfield_dist;
+    a.stage_floats = ph.bstage_floats;
+    a.fs_alias = ph.bfs_alias;
+    a.stages = ph.bstages;
+    a.field_rows = ph.bfield_rows;
+    cudaError_t e = cudaMemsetAsync(a.bar, 0, sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(ph.G, 1, 1);
+    cfg.blockDim = dim3(kPstThreads, 1, 1);
+    cfg.dynamicSmemBytes = ph.bsmem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    switch (ph.R) {
+        case 4: e = cudaLaunchKernelEx(&cfg, vp_persist_bwd_kernel<4>, a); break;
+        case 8: e = cudaLaunchKernelEx(&cfg, vp_persist_bwd_kernel<8>, a); break;
+        case 16: e = cudaLaunchKernelEx(&cfg, vp_persist_bwd_kernel<16>, a); break;
         default: return cudaErrorInvalidValue;
     }
     count_launch();
