@@ -45,7 +45,7 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "roofline"])
     ap.add_argument("--instances", type=int, default=256, help="c4: instances per GPU")
-    ap.add_argument("--seeds", type=int, default=3, help="c5: random initial controls compared")
+    ap.add_argument("--seeds", type=int, default=8, help="c5: random initial controls compared")
     ap.add_argument("--dtype", default="float32", choices=["float32", "float64"])
     ap.add_argument("--checkpoint-every", type=int, default=None)
     ap.add_argument("--cluster-size", type=int, default=None,
@@ -369,14 +369,17 @@ def run_ours(args, rank, local_rank, world):
     elif persistent:
         kf = "vp_persist_fwd_kernel"
         f_launch, alg_f = tf_loop, BYTES_FWD * cells * T
-        kb = "vp_bwds_kernel" if cfg["stage_rows"] > 0 else "vp_bwd_kernel"
-        # the replayed segments cost about the forward's time per step; the rest is the T + 1
-        # per-step adjoint launches
+        # the adjoint loop: one persistent adjoint launch per checkpoint segment (after the
+        # segment's replay by the forward kernel), plus a prologue and an epilogue launch; the
+        # replays are charged at the forward's time per step, the prologue and epilogue stay in
+        kb = "vp_persist_bwd_kernel"
+        n_adj_launches = len([s0 for s0 in range(0, max(T - 1, 0), every)])
         replay_ms = tf_loop * n_recompute / max(1, T)
-        b_launch = max(1e-6, (tb_loop - replay_ms) / (T + 1))
-        alg_b = BYTES_BWD * cells
-        b_note = (f"adjoint launch time = (adjoint loop - {n_segments} replay launches estimated at the "
-                  f"forward's time per step) / {T + 1} launches")
+        b_launch = max(1e-6, (tb_loop - replay_ms) / max(1, n_adj_launches))
+        alg_b = BYTES_BWD * cells * (T - 1) // max(1, n_adj_launches)
+        b_note = (f"average of {n_adj_launches} persistent adjoint launches (one per checkpoint segment): "
+                  f"(adjoint loop - {n_segments} replays estimated at the forward's time per step) / "
+                  f"{n_adj_launches}; prologue and epilogue launches included")
     else:
         kf = "vp_fwds_kernel" if cfg["stage_rows"] > 0 else "vp_fwd_kernel"
         f_launch, alg_f = tf_loop / (T + 1), BYTES_FWD * cells
@@ -490,9 +493,10 @@ def measure_c5(args, rank, local_rank, world):
             "time_ratio_mean": round(float(np.mean([r["time_ratio"] for r in runs])), 4),
             "problems_to_amortise_setup": (round(setup_s / float(np.mean(saved)), 2)
                                            if float(np.mean(saved)) > 0 else None),
-            "note": "time_ratio = warm (surrogate search + true-gradient refinement to J <= 1.01 J*) / "
-                    "plain (Adam with the true adjoint gradient until J stops improving); "
-                    "time_ratio_with_setup also charges data generation and training to this one problem"}
+            "note": "time_ratio = warm (surrogate search, then Adam with the true adjoint gradient at step "
+                    "size 3e-3 until J <= 1.01 J*) / plain (Adam with the true adjoint gradient at the "
+                    "reference notebook's step size 1e-3 until J stops improving); time_ratio_with_setup "
+                    "also charges data generation and training to this one problem"}
 
 
 def e2e_public_api(args, solver, wl, dev, flush):
@@ -786,7 +790,7 @@ def run_surrogate(args, rank, local_rank, world):
     lib.vp_reset_launch_count()
     with ClockSampler(local_rank) as clk:
         res = run_comparison(setup, n_samples=4096, coeff_std=0.05, train_steps=2000,
-                             seeds=list(range(11, 11 + args.seeds)))
+                             seeds=list(range(11, 11 + args.seeds)), lr=1e-3, lr_refine=3e-3)
     launches = lib.vp_launch_count()
     ratios = [r["time_ratio"] for r in res["runs"]]
     data = res["data"]

@@ -1,8 +1,8 @@
 """Ensembles of uneven instances (one persistent launch per step) against the reference's golden
 vectors, the float64 oracle and the single-instance solver.
 
-Bars as for the single-instance path (max-norm relative error): float32 1e-5 forward, 1e-4
-adjoint; float64 1e-11 forward, 1e-10 adjoint.
+Bars (max-norm relative error): float32 1e-5 forward, 1e-5 adjoint (about ten times the largest
+adjoint error measured on B200); float64 1e-11 forward, 1e-10 adjoint.
 """
 
 from __future__ import annotations
@@ -20,7 +20,8 @@ from warp_vp_solver_b200.workloads import fourier_coefficients, fourier_field
 pytestmark = pytest.mark.gpu
 
 TOL_FWD = {torch.float64: 1e-11, torch.float32: 1e-5}
-TOL_BWD = {torch.float64: 1e-10, torch.float32: 1e-4}
+# float32 adjoint: at most 6.3e-7 measured on B200
+TOL_BWD = {torch.float64: 1e-10, torch.float32: 1e-5}
 DTYPES = [torch.float32, torch.float64]
 
 

@@ -3,7 +3,8 @@
 Bars (max-norm relative error, max|a-b| / max|b|):
   * float64 plan vs reference: 1e-11 forward, 1e-10 adjoint (same scheme, re-associated);
   * float32 plan vs reference: 1e-5 for f, E, ee (the stated requirement); the adjoint, which
-    accumulates cotangents over every step in float32, 1e-4.
+    accumulates cotangents over every step in float32, 2e-5 (about ten times the largest error
+    measured on B200, 1.7e-6).
 """
 
 from __future__ import annotations
@@ -20,7 +21,8 @@ pytestmark = pytest.mark.gpu
 
 FIELDS = ("f_final", "f_hist", "E_hist", "ee_hist")
 TOL_FWD = {torch.float64: 1e-11, torch.float32: 1e-5}
-TOL_BWD = {torch.float64: 1e-10, torch.float32: 1e-4}
+# float32 adjoint: at most 1.7e-6 measured on B200 (staged kernel, fields shifting rows by cells)
+TOL_BWD = {torch.float64: 1e-10, torch.float32: 2e-5}
 DTYPES = [torch.float32, torch.float64]
 
 

@@ -6,8 +6,8 @@ a second grid barrier), band heights 4, 8 and 16 (one or several bands per CTA),
 enough to shift rows by several cells (the table and the far-shift forms of the v step), the
 adjoint's recomputation of checkpoint segments by the same kernel, and the bounded grid barrier.
 
-Bars (max-norm relative error): float32 forward 1e-5 and adjoint 1e-4 against the oracle, as for
-the per-step kernels.
+Bars (max-norm relative error): float32 forward 1e-5 and adjoint 5e-5 against the oracle (the
+largest adjoint error measured on B200 is 3.2e-6, with fields that shift rows by several cells).
 """
 
 from __future__ import annotations
@@ -80,8 +80,8 @@ def test_persistent_forward_and_adjoint_match_oracle(shape, record_error):
     gf, gH = s._run_backward(f_iv, H, T * dt, None, gff, gfh, gEh, w)
     rf, rH = O.delta_backward(g, dt, f_eq, f_iv, H, T, gff, gfh, gEh, w)
     e = max(O.rel_err(gf, rf), O.rel_err(gH, rH))
-    record_error(f"persist {nx}x{nv} {kind} H{amp} R{rows} adj", e, 1e-4)
-    assert e < 1e-4, f"adjoint {e:.2e}"
+    record_error(f"persist {nx}x{nv} {kind} H{amp} R{rows} adj", e, 5e-5)
+    assert e < 5e-5, f"adjoint {e:.2e}"
 
 
 def test_checkpoint_recompute_by_the_persistent_kernel_is_bitwise_neutral():

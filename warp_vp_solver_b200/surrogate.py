@@ -241,8 +241,9 @@ class SurrogateSearch:
 def optimize_warm(problem: ControlProblem, sur: Surrogate, c0, J_target: float,
                   lr_sur: float = 3e-3, lr: float = 1e-3, sur_iters: int = 150,
                   max_iters: int = 4000, search: SurrogateSearch | None = None):
-    """Minimise the surrogate's J from c0, then refine with the true gradient until
-    J <= J_target. ``seconds`` covers both phases (the surrogate's training is separate)."""
+    """Minimise the surrogate's J from c0, then refine with the true gradient (Adam, step size
+    ``lr``) until J <= J_target. ``seconds`` covers both phases (the surrogate's training is
+    separate)."""
     if search is None:
         search = SurrogateSearch(sur, problem.w, lr_sur)
     torch.cuda.synchronize()
@@ -270,9 +271,12 @@ def c5_setup(nx: int = 256, nv: int = 256, n_steps: int = 100, n_modes: int = 16
 
 def run_comparison(setup: ControlSetup, n_samples: int, coeff_std: float, train_steps: int,
                    seeds, batch: int = 1024, sur_iters: int = 150, lr_sur: float = 3e-3,
-                   lr: float = 1e-3, data_seed: int = 0, net_seed: int = 1, tol: float = 0.01):
+                   lr: float = 1e-3, lr_refine: float | None = None, data_seed: int = 0, net_seed: int = 1,
+                   tol: float = 0.01):
     """Data generation, training, then plain vs warm-started control from random initial
-    coefficients (standard deviation ``coeff_std``, one per seed). Returns a summary dict."""
+    coefficients (standard deviation ``coeff_std``, one per seed). The plain loop uses Adam with
+    step size ``lr``; the warm start's true-gradient refinement uses ``lr_refine`` (default
+    ``lr``). Returns a summary dict."""
     X, Y, data = generate_dataset(setup, n_samples, coeff_std, seed=data_seed)
     n_hold = max(1, n_samples // 10)
     sur = Surrogate(setup.n_inputs, setup.n_steps, max_batch=max(256, n_samples), seed=net_seed)
@@ -287,8 +291,8 @@ def run_comparison(setup: ControlSetup, n_samples: int, coeff_std: float, train_
                           dtype=torch.float32, device=prob.plan.device)
         plain = optimize_plain(prob, c0, lr=lr)
         target = (1 + tol) * plain["J"]
-        warm = optimize_warm(prob, sur, c0, target, lr_sur=lr_sur, lr=lr, sur_iters=sur_iters,
-                             search=search)
+        warm = optimize_warm(prob, sur, c0, target, lr_sur=lr_sur, lr=lr if lr_refine is None else lr_refine,
+                             sur_iters=sur_iters, search=search)
         runs.append({"seed": int(seed), "J0": plain["history"][0], "J_star": plain["J"],
                      "plain_evals": plain["evals"], "plain_seconds": plain["seconds"],
                      "plain_evals_to_target": evals_to_reach(plain["history"], target),
