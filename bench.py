@@ -55,6 +55,8 @@ def parse_args():
     ap.add_argument("--stage-rows", type=int, default=None,
                     help="force the staged step's rows per CTA (0: per-column kernel); skips autotuning")
     ap.add_argument("--stage-threads", type=int, default=None, help="with --stage-rows: threads per CTA")
+    ap.add_argument("--strip-rows", type=int, default=None,
+                    help="force the strip path's band height (0: off); skips autotuning")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="c2: skip the 8192^2 roofline and C5 sub-records of the default line")
@@ -248,11 +250,14 @@ def run_ours(args, rank, local_rank, world):
     solver = WarpVlasovPoissonSolver(wl.mesh, wl.dt, wl.f_eq, dtype=dtype, checkpoint_every=ce)
     plan = solver.plan
     tuned = None
-    if args.cluster_size is not None or args.stage_rows is not None:
+    if args.cluster_size is not None or args.stage_rows is not None or args.strip_rows is not None:
         if args.cluster_size is not None:
             plan.set_config(cluster_size=args.cluster_size)
         if args.stage_rows is not None:
-            plan.set_config(cluster_size=0, stage_rows=args.stage_rows, stage_threads=args.stage_threads)
+            plan.set_config(cluster_size=0, persist_rows=0, strip_rows=0, stage_rows=args.stage_rows,
+                            stage_threads=args.stage_threads)
+        if args.strip_rows is not None:
+            plan.set_config(cluster_size=0, persist_rows=0, strip_rows=args.strip_rows)
     elif not args.no_autotune:
         t = solver.autotune(steps=min(8, wl.n_steps))
         tuned = {"config": t["config"], "ms_per_candidate_run": t["ms"], "cached": t["cached"],
@@ -353,11 +358,14 @@ def run_ours(args, rank, local_rank, world):
     #    shared memory, so "achieved" is an effective bandwidth (the state never travels through HBM);
     #  * persistent path: the forward loop is one cooperative launch (vp_persist_fwd_kernel); the
     #    adjoint runs one launch per step plus one persistent replay launch per checkpoint segment;
+    #  * strip path: a strip kernel and a field kernel per step (the field launch and the gap between
+    #    the two are charged to the strip kernel);
     #  * per-step path: one fused launch per step (a separate Poisson tail launch is charged to it).
     peak, peak_kind = measured_peaks()
     cfg = plan.get_config()
     resident = cfg["cluster_size"] > 0 and every == 1
     persistent = (not resident) and cfg["persist_rows"] > 0
+    strip = (not resident) and (not persistent) and cfg.get("strip_rows", 0) > 0
     n_recompute = 0 if every == 1 else sum(max(0, min(s0 + every, T) - s0 - 1) for s0 in range(0, T, every))
     n_segments = 0 if every == 1 else sum(1 for s0 in range(0, T, every) if min(s0 + every, T) - s0 > 1)
     tf_loop, tb_loop = tf_ms / args.steps, tb_ms / args.steps
@@ -380,6 +388,16 @@ def run_ours(args, rank, local_rank, world):
         b_note = (f"average of {n_adj_launches} persistent adjoint launches (one per checkpoint segment): "
                   f"(adjoint loop - {n_segments} replays estimated at the forward's time per step) / "
                   f"{n_adj_launches}; prologue and epilogue launches included")
+    elif strip:
+        kf, kb = "vp_strip_fwd_kernel", "vp_strip_bwd_kernel"
+        f_launch, alg_f = tf_loop / (T + 1), BYTES_FWD * cells
+        # adjoint loop: prologue, T - 1 strip steps, epilogue, and the replays (charged at the
+        # forward's time per step)
+        b_launch = max(1e-6, (tb_loop - n_recompute * f_launch) / (T + 1))
+        alg_b = BYTES_BWD * cells
+        b_note = ("time per adjoint step: strip kernel + Poisson^T field kernel + launch gaps, averaged over "
+                  f"graph replays of the loop; the {n_recompute} replay steps are subtracted at the forward's "
+                  "time per step, the prologue and epilogue counted as steps")
     else:
         kf = "vp_fwds_kernel" if cfg["stage_rows"] > 0 else "vp_fwd_kernel"
         f_launch, alg_f = tf_loop / (T + 1), BYTES_FWD * cells
@@ -399,7 +417,10 @@ def run_ours(args, rank, local_rank, world):
     f_note = ("one launch per forward loop, state resident in distributed shared memory: achieved is an "
               "effective bandwidth over the algorithmic bytes" if resident else
               "one cooperative launch per forward loop (grid barrier per step), field solves included"
-              if persistent else "time per fused launch averaged over graph replays, including launch gaps"
+              if persistent else
+              "time per step: strip kernel + field kernel + launch gaps, averaged over graph replays of the "
+              "loop (prologue counted as a step)" if strip else
+              "time per fused launch averaged over graph replays, including launch gaps"
               + ("" if cfg["tail_inline"] else " and the separate Poisson tail launch"))
     roof_f = roof_of(kf, f_launch, alg_f, f_note)
     roof_b = roof_of(kb, b_launch, alg_b, b_note) if wl.adjoint else None
@@ -431,8 +452,9 @@ def run_ours(args, rank, local_rank, world):
                    "cuda_graph": use_graph,
                    "launch": {k: cfg[k] for k in ("rows_per_cta", "threads", "n_chunks", "tail_inline",
                                                   "cluster_size", "cluster_threads", "stage_rows",
-                                                  "persist_rows", "persist_ctas")},
+                                                  "persist_rows", "persist_ctas", "strip_rows", "strip_ctas")},
                    "path": "cluster-resident" if resident else ("persistent forward loop" if persistent
+                                                                else "strip step kernels" if strip
                                                                 else "per-step launches"),
                    "autotune": tuned,
                    "fwd_ms_per_step": round(tf_ms / args.steps, 4),
@@ -454,7 +476,7 @@ def measure_large(args, rank, local_rank, world):
     sub = argparse.Namespace(**vars(args))
     sub.workload, sub.steps, sub.warmup = "roofline", 3, 3
     sub.no_autotune, sub.no_e2e = True, True
-    sub.cluster_size = sub.stage_rows = sub.checkpoint_every = None
+    sub.cluster_size = sub.stage_rows = sub.strip_rows = sub.checkpoint_every = None
     line, wl = run_ours(sub, rank, local_rank, world)
     peak, _ = measured_peaks()
     cfg = line["config"]

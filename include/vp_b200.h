@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define VP_ABI_VERSION 3
+#define VP_ABI_VERSION 4
 
 /* status codes */
 #define VP_OK 0
@@ -360,16 +360,27 @@ typedef struct vp_launch_config {
                               /* can solve the field on its own window rows (nx of a few 1000s)  */
     int32_t persist_ctas;     /* CTAs of that launch (derived)                                    */
     int64_t persist_smem_bytes; /* dynamic shared memory per CTA of that launch (derived)        */
+    int32_t strip_rows;       /* > 0: float32 Strang steps (forward, recomputation, adjoint) run  */
+                              /* as two launches each: a strip kernel whose 64-thread CTAs walk */
+                              /* runs of bands of this many rows (4, 8 or 16) down one 256-column*/
+                              /* chunk with the window rows in a shared-memory ring, and a field */
+                              /* kernel (circulant product, 32 rows per CTA); 0: off. Same      */
+                              /* conditions as persist_rows; on by default where the persistent  */
+                              /* loop is not (the field would need slices, nx of several 1000s) */
+                              /* and the state is not cluster-resident. persist_rows wins when  */
+                              /* both are set.                                                   */
+    int32_t strip_ctas;       /* CTAs of the forward strip launch (derived)                       */
+    int64_t strip_smem_bytes; /* dynamic shared memory per CTA of the forward strip launch        */
 } vp_launch_config;
 
 /* Reads the plan's current launch shape. */
 int vp_plan_get_config(const vp_plan* plan, vp_launch_config* out);
 
-/* Sets rows_per_cta, threads, n_chunks, cluster_size, stage_rows, stage_threads and persist_rows (the other
+/* Sets rows_per_cta, threads, n_chunks, cluster_size, stage_rows, stage_threads, persist_rows and strip_rows (the other
  * fields are derived and ignored). cluster_size must be 0 or a power of two in [2, 16] that splits nx into 1, 2, 4, 8,
  * 16 or 32 rows per CTA whose state fits in shared memory; the cluster-resident path is used for forward calls without a tape or with
  * checkpoint interval 1, and for backward calls with checkpoint interval 1. Workspace sizes
- * depend on n_chunks: query vp_workspace_bytes() again after changing it. */
+ * depend on n_chunks and strip_rows: query vp_workspace_bytes() again after changing them. */
 int vp_plan_set_config(vp_plan* plan, const vp_launch_config* cfg);
 
 /* Time-splitting scheme of a plan's forward and adjoint loops.

@@ -42,11 +42,14 @@ def test_search_picks_fastest_usable_candidate():
 
 def test_candidate_sets():
     c = plan_candidates({"cluster_size": 8})
-    assert {"cluster_size": 16, "persist_rows": 0} in c and any(x.get("stage_rows") == 16 for x in c)
+    assert {"cluster_size": 16, "persist_rows": 0, "strip_rows": 0} in c and any(x.get("stage_rows") == 16 for x in c)
     c = plan_candidates({"cluster_size": 0})
     assert not any("stage_rows" not in x and x["cluster_size"] > 0 for x in c)
-    assert {"cluster_size": 0, "persist_rows": 16} in c
-    # every non-persistent candidate switches the persistent loop off
-    assert all(x["persist_rows"] == 0 for x in c if "stage_rows" in x or x["cluster_size"] > 0)
+    assert {"cluster_size": 0, "persist_rows": 16, "strip_rows": 0} in c
+    assert {"cluster_size": 0, "persist_rows": 0, "strip_rows": 16} in c
+    # every candidate names both loop paths, and at most one of them is on
+    assert all("persist_rows" in x and "strip_rows" in x for x in c)
+    assert all(x["persist_rows"] == 0 or x["strip_rows"] == 0 for x in c)
+    assert all(x["persist_rows"] == 0 and x["strip_rows"] == 0 for x in c if "stage_rows" in x or x["cluster_size"] > 0)
     e = ensemble_candidates({})
     assert all(x["rows_per_tile"] in (1, 2, 4, 8) for x in e) and len(e) > 10

@@ -116,7 +116,7 @@ def test_persistent_agrees_with_staged_kernels_and_is_deterministic():
 
 def test_plan_default_paths_by_grid_size():
     """Configuration 3's grid runs the persistent loop by default; a cluster-resident grid keeps
-    its one-cluster kernels; a 4096-row grid (field solved in slices) keeps the per-step kernels
+    its one-cluster kernels; a 4096-row grid (field solved in slices) runs the strip step kernels
     unless persist_rows asks for the persistent loop."""
     def plan(lx, lv, nx, nv):
         m = make_mesh(lx, lv, nx, nv)
@@ -125,10 +125,10 @@ def test_plan_default_paths_by_grid_size():
     assert cfg["cluster_size"] == 0 and cfg["persist_rows"] > 0, cfg
     p = plan(10.0 * np.pi, 6.0, 256, 256)
     assert p.get_config()["cluster_size"] > 0 and p.get_config()["persist_rows"] == 0
-    q = plan(10.0 * np.pi, 6.0, 4096, 1024)   # field in slices: per-step kernels by default
-    assert q.get_config()["persist_rows"] == 0 and q.get_config()["stage_rows"] > 0
-    q.set_config(persist_rows=16)
-    assert q.get_config()["persist_rows"] == 16
+    q = plan(10.0 * np.pi, 6.0, 4096, 1024)   # field in slices: strip step kernels by default
+    assert q.get_config()["persist_rows"] == 0 and q.get_config()["strip_rows"] == 4
+    q.set_config(persist_rows=16, strip_rows=0)
+    assert q.get_config()["persist_rows"] == 16 and q.get_config()["strip_rows"] == 0
 
 
 def test_grid_barrier_wait_limit_zero_times_out_cleanly():

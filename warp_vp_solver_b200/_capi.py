@@ -23,7 +23,7 @@ VP_SCHEME_STRANG = 0
 VP_SCHEME_MERGED = 1
 VP_STATUS_NONFINITE_INPUT = 1
 VP_STATUS_WAIT_TIMEOUT = 2
-ABI_VERSION = 3   # VP_ABI_VERSION of the header these bindings follow
+ABI_VERSION = 4   # VP_ABI_VERSION of the header these bindings follow
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libvpb200.so")
 
@@ -71,6 +71,9 @@ class LaunchConfig(ctypes.Structure):
         ("persist_rows", c_i32),
         ("persist_ctas", c_i32),
         ("persist_smem_bytes", c_i64),
+        ("strip_rows", c_i32),
+        ("strip_ctas", c_i32),
+        ("strip_smem_bytes", c_i64),
     ]
 
 

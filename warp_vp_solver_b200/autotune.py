@@ -119,11 +119,13 @@ def plan_candidates(cfg: dict) -> list[dict]:
     """Candidate single-instance configurations around a plan's current one."""
     cands = []
     if cfg["cluster_size"] > 0:
-        cands += [{"cluster_size": cn, "persist_rows": 0} for cn in (16, 8, 4, 2)]
-    cands += [{"cluster_size": 0, "persist_rows": r} for r in (16, 8, 4)]
-    cands += [{"cluster_size": 0, "persist_rows": 0, "stage_rows": r, "stage_threads": c}
+        cands += [{"cluster_size": cn, "persist_rows": 0, "strip_rows": 0} for cn in (16, 8, 4, 2)]
+    cands += [{"cluster_size": 0, "persist_rows": r, "strip_rows": 0} for r in (16, 8, 4)]
+    cands += [{"cluster_size": 0, "persist_rows": 0, "strip_rows": r} for r in (16, 8)]
+    cands += [{"cluster_size": 0, "persist_rows": 0, "strip_rows": 0, "stage_rows": r, "stage_threads": c}
               for c in (256, 128) for r in (32, 16, 8, 4)]
-    cands += [{"cluster_size": 0, "persist_rows": 0, "stage_rows": 0, "rows_per_cta": r} for r in (16, 8, 4)]
+    cands += [{"cluster_size": 0, "persist_rows": 0, "strip_rows": 0, "stage_rows": 0, "rows_per_cta": r}
+              for r in (16, 8, 4)]
     return cands
 
 
@@ -164,7 +166,8 @@ def tune_plan(plan, steps: int = 8, repeats: int = 3, cache: TuneCache | None = 
     best, ms, tried = search(plan_candidates(start), apply, _timer(step, flush), repeats)
     if best is None:
         plan.set_config(**{k: start[k] for k in ("rows_per_cta", "threads", "n_chunks", "cluster_size",
-                                                   "stage_rows", "stage_threads", "persist_rows")})
+                                                   "stage_rows", "stage_threads", "persist_rows",
+                                                   "strip_rows")})
         return {"config": None, "ms": None, "cached": False}
     plan.set_config(**best)
     cache.put(key, {"config": best, "ms": ms, "tried": tried})

@@ -22,8 +22,8 @@ LIB_PATH = os.path.join(PKG_DIR, LIB_NAME)
 INCLUDE_DIR = os.path.join(ROOT_DIR, "include")
 OBJ_DIR = os.path.join(ROOT_DIR, "_build")
 
-SOURCES = ["vp_capi.cu", "vp_kernels.cu", "vp_ops.cu", "vp_resident.cu", "vp_mlp.cu", "vp_persist.cu"]
-HEADERS = ["vp_internal.h", "vp_device.cuh"]
+SOURCES = ["vp_capi.cu", "vp_kernels.cu", "vp_ops.cu", "vp_resident.cu", "vp_mlp.cu", "vp_persist.cu", "vp_strip.cu"]
+HEADERS = ["vp_internal.h", "vp_device.cuh", "vp_pst.cuh"]
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMPILE_FLAGS = [

@@ -99,6 +99,11 @@ struct vp_plan {
     int2* d_pchunk = nullptr;  // [nv / 256]
     float* d_dfeq = nullptr;   // [nv]
     float* d_ctab2 = nullptr;  // [3 nx + 8]
+    // strip step path (vp_strip.cu): per-step kernels for large grids on the same quad tables
+    StripHost strip;           // launch shape (strip.R == 0: not eligible)
+    int strip_on = 0;          // per-step forward and adjoint steps (and recomputation) use it
+    std::vector<long long> host_msigned;   // unreduced x half-step offsets (re-shaping the paths)
+    std::vector<double> host_tx;           // their weights
     unsigned long long wait_ns = 1000000000ull;   // limit of each device-side grid barrier wait
 };
 
@@ -320,7 +325,8 @@ static int resolve_every(const vp_plan* p, int n_steps, int every) {
 }
 
 struct WsLayout {
-    size_t hbuf0, hbuf1, seg, part, counter, vsh, E, grho, gscratch, prho, pvsh, peep, pbar, total;
+    size_t hbuf0, hbuf1, seg, part, counter, vsh, E, grho, gscratch, prho, pvsh, peep, pbar;
+    size_t srho, sgE, seep, sctr, total;
 };
 
 static WsLayout ws_layout(const vp_plan* p, int n_steps, int every) {
@@ -331,7 +337,8 @@ static WsLayout ws_layout(const vp_plan* p, int n_steps, int every) {
     L.hbuf0 = off; off += align256(nxnv);
     L.hbuf1 = off; off += align256(nxnv);
     L.seg = off; off += align256(nxnv * (size_t)std::max(0, K - 1));
-    const int part_chunks = std::max(p->cfg.n_chunks, p->stage_span > 0 ? p->scfg.n_chunks : 0);
+    const int part_chunks = std::max({p->cfg.n_chunks, p->stage_span > 0 ? p->scfg.n_chunks : 0,
+                                      p->strip.R > 0 ? p->strip.n_chunks : 0});
     L.part = off; off += align256((size_t)part_chunks * p->nx * real_size(p));
     L.counter = off; off += 256;
     L.vsh = off; off += align256((size_t)p->nx * vshift_size(p));
@@ -343,6 +350,12 @@ static WsLayout ws_layout(const vp_plan* p, int n_steps, int every) {
         L.pvsh = off; off += align256((size_t)p->nx * sizeof(VShift<float>));
         L.peep = off; off += align256((size_t)std::max(1, n_steps) * p->pst.G * sizeof(double));
         L.pbar = off; off += 256;
+    }
+    if (p->strip.R > 0) {   // strip path: rho, g_E, field energy partials, band and field counters
+        L.srho = off; off += align256((size_t)p->nx * sizeof(float));
+        L.sgE = off; off += align256((size_t)p->nx * sizeof(float));
+        L.seep = off; off += align256((size_t)p->strip.field_ctas * sizeof(double));
+        L.sctr = off; off += align256((size_t)(p->strip.n_bands + 1) * sizeof(unsigned));
     }
     L.total = off;
     return L;
@@ -404,6 +417,44 @@ static PersistArgs persist_args(const vp_plan* p, unsigned char* ws, const WsLay
     a.status = p->d_status;
     a.wait_ns = p->wait_ns;
     return a;
+}
+
+// Table arguments of a strip step launch (forward, replay or adjoint).
+template <typename A>
+static void strip_tables(const vp_plan* p, A& a) {
+    a.nx = p->nx;
+    a.nv = p->nv;
+    a.quad = p->d_pquad;
+    a.tq = p->d_ptq;
+    a.chunk = p->d_pchunk;
+    a.dfeq = p->d_dfeq;
+    a.vtab = static_cast<const float*>(p->d_vtab);
+    a.feq = p->d_feq;
+}
+
+// The strip step kernels run this plan's float32 Strang steps.
+static bool strip_active(const vp_plan* p) { return p->strip_on && p->strip.R > 0 && !p->merged && p->dtype == VP_F32; }
+
+// Field of step n+1 from the strip kernel's rho (forward) into the step's outputs.
+static int strip_field_fwd(const vp_plan* p, unsigned char* ws, const WsLayout& L, const float* H, float* E_out,
+                           float* E_hist_out, VShift<float>* vsh_out, float* ee_out, cudaStream_t s) {
+    StripFieldArgs f{};
+    f.nx = p->nx;
+    f.nv = p->nv;
+    f.adjoint = 0;
+    f.x = reinterpret_cast<const float*>(ws + L.srho);
+    f.ctab = p->d_ctab2;
+    f.H = H;
+    f.dtdv = (float)(p->dt / p->dv);
+    f.dx = (float)p->dx;
+    f.E_out = E_out;
+    f.E_hist_out = E_hist_out;
+    f.vsh_out = vsh_out;
+    f.ee_out = ee_out;
+    f.eep = reinterpret_cast<double*>(ws + L.seep);
+    f.counter = reinterpret_cast<unsigned*>(ws + L.sctr) + p->strip.n_bands;
+    VP_CUDA(launch_strip_field(f, p->strip, s), "strip field launch");
+    return VP_OK;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -492,6 +543,10 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
     }
 
     VP_CUDA(cudaMemsetAsync(counter, 0, 256, s), "cudaMemsetAsync(counter)");
+    const bool strip = sizeof(T) == 4 && strip_active(p);
+    if (strip)
+        VP_CUDA(cudaMemsetAsync(ws + L.sctr, 0, (size_t)(p->strip.n_bands + 1) * sizeof(unsigned), s),
+                "cudaMemsetAsync(strip counters)");
 
     auto h_slot = [&](int n) -> T* {
         if (ckpt != nullptr && n % K == 0) return ckpt + (size_t)(n / K) * nxnv;
@@ -559,6 +614,25 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
             am.tx = static_cast<const T*>(p->d_txf);
             am.tx64 = p->d_txf64;
             VP_CUDA(launch_fwd<T>(am, p->cfg, 3, p->feq2d != 0, s), "forward merged step launch");
+        } else if (strip) {
+            if constexpr (sizeof(T) == 4) {
+                StripFwdArgs sa{};
+                strip_tables(p, sa);
+                sa.h_in = a.h_in;
+                sa.h_out = a.h_out;
+                sa.vsh = a.vsh;
+                sa.f_hist_n = a.f_hist_n;
+                sa.f_final = a.f_final;
+                sa.part = last ? nullptr : part;
+                sa.run_ctr = reinterpret_cast<unsigned*>(ws + L.sctr);
+                sa.rho_out = reinterpret_cast<float*>(ws + L.srho);
+                sa.dv = (float)p->dv;
+                VP_CUDA(launch_strip_fwd(sa, p->strip, s), "strip forward step launch");
+                if (!last) {
+                    const int rc = strip_field_fwd(p, ws, L, H, a.E_out, a.E_hist_out, a.vsh_out, a.ee_out, s);
+                    if (rc != VP_OK) return rc;
+                }
+            }
         } else if (p->stage_span > 0 && !p->merged) {
             a.n_chunks = p->scfg.n_chunks;
             a.chunk_cols = p->scfg.chunk_cols;
@@ -566,7 +640,7 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
         } else {
             VP_CUDA(launch_fwd<T>(a, p->cfg, 1, p->feq2d != 0, s), "forward step launch");
         }
-        if (!last && !p->tail_inline)
+        if (!last && !p->tail_inline && !strip)
             VP_CUDA(launch_fwd_tail<T>(a, p->tail_threads, p->tail_smem, p->tail_tw_stage != 0, s), "forward tail launch");
         if (ring != nullptr) {
             VP_CUDA(cudaEventRecord(ring->written[slot], s), "record history slot");
@@ -637,6 +711,10 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
 
     VP_CUDA(cudaMemsetAsync(counter, 0, 256, s), "cudaMemsetAsync(counter)");
     VP_CUDA(cudaMemsetAsync(g_H, 0, (size_t)nx * sizeof(T), s), "cudaMemsetAsync(g_H)");
+    const bool strip = sizeof(T) == 4 && strip_active(p);
+    if (strip)
+        VP_CUDA(cudaMemsetAsync(ws + L.sctr, 0, (size_t)(p->strip.n_bands + 1) * sizeof(unsigned), s),
+                "cudaMemsetAsync(strip counters)");
 
     auto h_ptr = [&](int n) -> const T* {
         if (n % K == 0) return ckpt + (size_t)(n / K) * nxnv;
@@ -692,7 +770,17 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
             fa.h_in = h_ptr(n);
             fa.h_out = h_mut(n + 1);
             fa.vsh = vsh_all + (size_t)n * nx;
-            if (p->merged) {
+            if (strip) {
+                // the forward's strip kernel, without row sums: bitwise the states it computed
+                if constexpr (sizeof(T) == 4) {
+                    StripFwdArgs sa{};
+                    strip_tables(p, sa);
+                    sa.h_in = fa.h_in;
+                    sa.h_out = fa.h_out;
+                    sa.vsh = fa.vsh;
+                    VP_CUDA(launch_strip_fwd(sa, p->strip, s), "strip recompute launch");
+                }
+            } else if (p->merged) {
                 FwdArgs<T> am = fa;
                 am.mx = p->d_mxf;
                 am.tx = static_cast<const T*>(p->d_txf);
@@ -799,7 +887,38 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
         b.E_prev = E_all + (size_t)(n - 1) * nx;
         b.gE_hist = g_Eh ? g_Eh + (size_t)(n - 1) * nx : nullptr;
         b.gee = g_ee ? g_ee + (n - 1) : nullptr;
-        if (p->merged) {
+        if (strip) {
+            if constexpr (sizeof(T) == 4) {
+                StripBwdArgs sb{};
+                strip_tables(p, sb);
+                sb.w_in = b.w_in;
+                sb.w_out = b.w_out;
+                sb.grho = grho;
+                sb.vsh_n = b.vsh_n;
+                sb.vsh_prev = b.vsh_prev;
+                sb.h_prev = b.h_prev;
+                sb.gfh = b.gfh;
+                sb.part = part;
+                sb.run_ctr = reinterpret_cast<unsigned*>(ws + L.sctr);
+                sb.dv = (float)p->dv;
+                sb.dx = (float)p->dx;
+                sb.neg_dt_dv = (float)(-p->dt / p->dv);
+                sb.gE_hist = b.gE_hist;
+                sb.gee = b.gee;
+                sb.E_prev = b.E_prev;
+                sb.gH = g_H;
+                sb.gE_out = reinterpret_cast<float*>(ws + L.sgE);
+                VP_CUDA(launch_strip_bwd(sb, p->strip, s), "strip adjoint step launch");
+                StripFieldArgs f{};
+                f.nx = nx;
+                f.nv = nv;
+                f.adjoint = 1;
+                f.x = sb.gE_out;
+                f.ctab = p->d_ctab2;
+                f.grho_out = grho;
+                VP_CUDA(launch_strip_field(f, p->strip, s), "strip adjoint field launch");
+            }
+        } else if (p->merged) {
             BwdArgs<T> bm = b;
             bm.mx = p->d_mxf;
             bm.tx = static_cast<const T*>(p->d_txf);
@@ -813,7 +932,7 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
         } else {
             VP_CUDA(launch_bwd<T>(b, p->cfg, 1, p->feq2d != 0, s), "backward step launch");
         }
-        if (!p->tail_inline)
+        if (!p->tail_inline && !strip)
             VP_CUDA(launch_bwd_tail<T>(b, p->tail_threads, p->tail_smem, p->tail_tw_stage != 0, s), "backward tail launch");
     }
     // epilogue (n = 0)
@@ -1104,31 +1223,39 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
         return rc;
     }
     choose_staged(p, n_sms);
-    // persistent forward path: float32, x-invariant f_eq, nv a multiple of 256, nx <= 16384 (the
-    // circulant table costs O(nx^2) on the host)
+    // persistent and strip paths: float32, x-invariant f_eq, nv a multiple of 256, the x shifts of
+    // every 4 neighbouring columns within one cell, nx <= 16384 (the circulant table costs O(nx^2)
+    // on the host)
+    std::vector<int2> quad, chunk;
+    std::vector<float> tq;
     if (dtype == VP_F32 && inv && p->d_vtab != nullptr && nx <= 16384 &&
-        persist_prepare(p->pst, nx, nv, m_signed, tx, n_sms, 0)) {
+        build_quad_tables(nx, nv, m_signed, tx, quad, tq, chunk)) {
+        p->host_msigned = m_signed;
+        p->host_tx = tx;
+        if (!persist_prepare(p->pst, nx, nv, m_signed, tx, n_sms, 0)) p->pst = PersistHost{};
+        if (!strip_prepare(p->strip, nx, nv, chunk, n_sms, 0)) p->strip = StripHost{};
+    }
+    if (p->pst.R > 0 || p->strip.R > 0) {
         std::vector<float> dfeq(nv);
         for (int j = 0; j < nv; ++j) dfeq[j] = (float)(f_eq_host[(j + 1) % nv] - f_eq_host[j]);
         if (circ.size() != (size_t)nx || (p->pow2 && nx > 512)) circ = circulant_of(nx, mult_im);
         std::vector<float> ctab2((size_t)3 * nx + 8);
         for (size_t j = 0; j < ctab2.size(); ++j)
             ctab2[j] = (float)circ[(size_t)((((long long)j - nx) % nx + nx) % nx)];
-        if ((rc = upload_bytes((void**)&p->d_pquad, p->pst.quad.data(), p->pst.quad.size() * sizeof(int2))) ||
-            (rc = upload_bytes((void**)&p->d_ptq, p->pst.tq.data(), p->pst.tq.size() * sizeof(float))) ||
-            (rc = upload_bytes((void**)&p->d_pchunk, p->pst.chunk.data(), p->pst.chunk.size() * sizeof(int2))) ||
+        if ((rc = upload_bytes((void**)&p->d_pquad, quad.data(), quad.size() * sizeof(int2))) ||
+            (rc = upload_bytes((void**)&p->d_ptq, tq.data(), tq.size() * sizeof(float))) ||
+            (rc = upload_bytes((void**)&p->d_pchunk, chunk.data(), chunk.size() * sizeof(int2))) ||
             (rc = upload_bytes((void**)&p->d_dfeq, dfeq.data(), dfeq.size() * sizeof(float))) ||
             (rc = upload_bytes((void**)&p->d_ctab2, ctab2.data(), ctab2.size() * sizeof(float)))) {
             free_plan(p);
             return rc;
         }
-        // default: grids that are not cluster-resident and whose CTAs each solve the field on their
-        // own window rows (measured on B200: 512x1024 forward + adjoint 2.0e10 cell-steps/s
-        // against 1.1e10 per step); where the field needs slices and a second barrier per step
-        // (8192x8192) the per-step kernels were faster (7.6e10 against 6.9e10)
-        p->pst_on = (p->res_cn == 0 && p->pst.field_dist == 0) ? 1 : 0;
-    } else {
-        p->pst = PersistHost{};
+        // defaults, measured on B200: the persistent loop on grids that are not cluster-resident
+        // and whose CTAs each solve the field on their own window rows (512x1024 forward + adjoint
+        // 2.0e10 cell-steps/s against 1.1e10 per step); the strip step kernels where the field
+        // would need slices and a second grid barrier per step (8192x8192)
+        p->pst_on = (p->res_cn == 0 && p->pst.R > 0 && p->pst.field_dist == 0) ? 1 : 0;
+        p->strip_on = (p->res_cn == 0 && !p->pst_on && p->strip.R > 0) ? 1 : 0;
     }
     {   // trapezoid integral of f_eq (kl_divergence's norm_eq without eps, utils.py:59-64)
         double tot = 0.0;
@@ -1167,6 +1294,10 @@ int vp_plan_get_config(const vp_plan* plan, vp_launch_config* out) {
     out->persist_rows = plan->pst_on ? plan->pst.R : 0;
     out->persist_ctas = plan->pst_on ? plan->pst.G : 0;
     out->persist_smem_bytes = plan->pst_on ? (int64_t)plan->pst.smem : 0;
+    const bool strip = plan->strip_on && !plan->pst_on && plan->strip.R > 0;
+    out->strip_rows = strip ? plan->strip.R : 0;
+    out->strip_ctas = strip ? plan->strip.fwd_ctas : 0;
+    out->strip_smem_bytes = strip ? (int64_t)plan->strip.fwd_smem : 0;
     return VP_OK;
 }
 
@@ -1205,31 +1336,38 @@ int vp_plan_set_config(vp_plan* plan, const vp_launch_config* cfg) {
     } else {
         plan->stage_span = 0;
     }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (cfg->persist_rows != 0) {
         if (plan->d_pquad == nullptr)
             return set_err(VP_ERR_ARG, "persist_rows=%d: the persistent path needs a float32 plan with an "
                                        "x-invariant f_eq, nv a multiple of 256 and nx <= 16384", cfg->persist_rows);
         const PersistHost keep = plan->pst;
-        std::vector<long long> ms(plan->host_mx.size());
-        std::vector<double> tx(plan->host_mx.size());
-        for (size_t q = 0; q < keep.quad.size(); ++q)
-            for (int e = 0; e < 4; ++e) {
-                ms[4 * q + e] = keep.quad[q].x + ((keep.quad[q].y >> e) & 1);
-                tx[4 * q + e] = keep.tq[4 * q + e];
-            }
-        int dev = 0, sms = 148;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (!persist_prepare(plan->pst, plan->nx, plan->nv, ms, tx, sms, cfg->persist_rows)) {
+        if (!persist_prepare(plan->pst, plan->nx, plan->nv, plan->host_msigned, plan->host_tx, sms,
+                             cfg->persist_rows)) {
             plan->pst = keep;
             return set_err(VP_ERR_ARG, "persist_rows=%d is not usable for a %dx%d grid (4, 8 or 16 dividing nx, "
                                        "with every CTA resident at once)",
                            cfg->persist_rows, plan->nx, plan->nv);
         }
-        plan->pst_on = 1;
-    } else {
-        plan->pst_on = 0;
     }
+    if (cfg->strip_rows != 0) {
+        if (plan->d_pquad == nullptr)
+            return set_err(VP_ERR_ARG, "strip_rows=%d: the strip path needs a float32 plan with an "
+                                       "x-invariant f_eq, nv a multiple of 256 and nx <= 16384", cfg->strip_rows);
+        std::vector<int2> quad, chunk;
+        std::vector<float> tq;
+        StripHost sh;
+        if (!build_quad_tables(plan->nx, plan->nv, plan->host_msigned, plan->host_tx, quad, tq, chunk) ||
+            !strip_prepare(sh, plan->nx, plan->nv, chunk, sms, cfg->strip_rows))
+            return set_err(VP_ERR_ARG, "strip_rows=%d is not usable for a %dx%d grid (4, 8 or 16 dividing nx, "
+                                       "nx a multiple of 32)",
+                           cfg->strip_rows, plan->nx, plan->nv);
+        plan->strip = sh;
+    }
+    plan->pst_on = cfg->persist_rows != 0 ? 1 : 0;
+    plan->strip_on = cfg->strip_rows != 0 ? 1 : 0;
     plan->res_cn = cn;
     plan->res_smem = res_smem;
     plan->res_threads = cn ? res_threads(plan->nx / cn, plan->nv) : 0;

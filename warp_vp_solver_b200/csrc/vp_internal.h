@@ -280,6 +280,90 @@ cudaError_t launch_persist_fwd(const PersistArgs& a, const PersistHost& ph, cuda
 cudaError_t launch_persist_bwd(const PersistBwdArgs& a, const PersistHost& ph, cudaStream_t s);
 size_t persist_smem_bytes(int span_max, int win_rows, int R, int nx, int nv, int field_rows, int stages,
                           int* stage_floats, int* fs_alias);
+// The column-quad tables of the persistent and strip paths (false: some 4 neighbouring columns'
+// x shifts differ by more than one cell, or a shift reaches half a period).
+bool build_quad_tables(int nx, int nv, const std::vector<long long>& m_signed, const std::vector<double>& tx,
+                       std::vector<int2>& quad, std::vector<float>& tq, std::vector<int2>& chunk);
+
+// Strip step kernels (vp_strip.cu): per-step launches for large grids. A CTA is one column group
+// (64 threads, 256 columns) that walks one run of consecutive bands of R rows of one column chunk,
+// keeping the window rows in a shared-memory ring that the next band's rows load into while the
+// current band computes. Forward step / replay step:
+struct StripFwdArgs {
+    int nx, nv, n_chunks, n_bands, ring_rows, runs;
+    const float* h_in;          // h_n
+    float* h_out;               // h_{n+1}, or null (last step)
+    const VShift<float>* vsh;   // v shifts of step n
+    const int2* quad;
+    const float4* tq;
+    const int2* chunk;
+    const float* dfeq;
+    const float* vtab;
+    const double* feq;
+    float* f_hist_n;            // f after step n (float), or null
+    double* f_final;            // f after the last step, or null
+    float* part;                // row partial sums per chunk [n_chunks][nx], or null (replay)
+    unsigned* run_ctr;          // [runs], zero between launches
+    float* rho_out;             // rho_{n+1}
+    float dv;
+};
+
+// Adjoint step n: w_{n-1} from w_n, the slope row sums of h_{n-1} and, per band once its last chunk
+// is done, g_E of step n-1 (and g_H += g_E_total).
+struct StripBwdArgs {
+    int nx, nv, n_chunks, n_bands, ring_rows, runs;
+    const float* w_in;
+    float* w_out;
+    const float* grho;          // cotangent on rho of step n
+    const VShift<float>* vsh_n;
+    const VShift<float>* vsh_prev;
+    const float* h_prev;        // h_{n-1}
+    const float* gfh;           // cotangent on f_hist[n-1], or null
+    const int2* quad;
+    const float4* tq;
+    const int2* chunk;
+    const float* dfeq;
+    const float* vtab;
+    const double* feq;
+    float* part;
+    unsigned* run_ctr;
+    float dv, dx, neg_dt_dv;
+    const float* gE_hist;       // cotangent on E_hist[n-1], or null
+    const float* gee;           // address of the cotangent on ee_hist[n-1], or null
+    const float* E_prev;        // raw E of step n-1
+    float* gH;
+    float* gE_out;              // g_E of step n-1 (input of Poisson^T)
+};
+
+// Field of all rows by the circulant product, kStripFieldRows rows per CTA: forward E = c * rho
+// with E_hist, the v shifts and ee; adjoint grho = c^T * g_E.
+struct StripFieldArgs {
+    int nx, nv, adjoint;
+    const float* x;             // rho (forward) or g_E (adjoint)
+    const float* ctab;          // [3 nx + 8]: ctab[j] = c[(j - nx) mod nx]
+    const float* H;
+    float dtdv, dx;
+    float* E_out;               // forward: raw E
+    float* E_hist_out;          // forward: E + H, or null
+    VShift<float>* vsh_out;     // forward: v shifts
+    float* ee_out;              // forward: ee, or null
+    double* eep;                // forward: per-CTA energy partials
+    unsigned* counter;          // forward: completion counter, zero between launches
+    float* grho_out;            // adjoint
+};
+
+struct StripHost {
+    int R = 0, n_bands = 0, n_chunks = 0, span_max = 0, ring_rows = 0;
+    int fwd_runs = 0, bwd_runs = 0, fwd_ctas = 0, bwd_ctas = 0, field_ctas = 0;
+    size_t fwd_smem = 0, bwd_smem = 0;
+};
+constexpr int kStripFieldRows = 32;
+
+// Launch shape of the strip path (force_rows 0: automatic, else 4, 8 or 16); false when not eligible.
+bool strip_prepare(StripHost& sh, int nx, int nv, const std::vector<int2>& chunk, int n_sms, int force_rows);
+cudaError_t launch_strip_fwd(const StripFwdArgs& a, const StripHost& sh, cudaStream_t s);
+cudaError_t launch_strip_bwd(const StripBwdArgs& a, const StripHost& sh, cudaStream_t s);
+cudaError_t launch_strip_field(const StripFieldArgs& a, const StripHost& sh, cudaStream_t s);
 
 // Raises VP_STATUS_NONFINITE_INPUT in *status when f (n doubles) or H (nx reals, double when h64)
 // holds a NaN or an infinity (vp_ops.cu).
