@@ -243,19 +243,28 @@ def test_staged_shapes_agree(rows, cols):
 
 
 @pytest.mark.parametrize("dtype", DTYPES, ids=_dt_id)
-@pytest.mark.parametrize("layout", ["staged", "percolumn16"])
+@pytest.mark.parametrize("layout", ["staged", "percolumn16", "strip"])
 def test_separate_tail_large_nx(layout, dtype, record_error):
     """nx = 4096: the Poisson tail is its own one-CTA launch (per-stage twiddles in shared memory
     for float32, the plain table for float64), and with 16 column chunks the row partials are
-    pre-summed across CTAs before it. Forward and adjoint against the oracle."""
+    pre-summed across CTAs before it; the float32 default at this size is the strip path (circulant
+    field kernel). Forward and adjoint against the oracle, the adjoint once with a cotangent on
+    f_final and once with cotangents on E_hist and ee_hist only (the prologue is then two memsets)."""
+    if layout == "strip" and dtype != torch.float32:
+        pytest.skip("the strip path is float32")
     m = make_mesh(10.0 * np.pi, 6.0, 4096, 512)
     f_eq, f_iv = two_stream_state(m, eps=1e-2)
     H = 0.05 * np.random.default_rng(11).standard_normal(m.nx)
     T, dt = 4, 0.05
     s = make_solver(m, dt, f_eq, "stream", dtype=dtype)
     if layout == "percolumn16":
-        s.plan.set_config(stage_rows=0, rows_per_cta=4, threads=32, n_chunks=16)
+        s.plan.set_config(stage_rows=0, strip_rows=0, rows_per_cta=4, threads=32, n_chunks=16)
         assert s.plan.get_config()["n_chunks"] == 16
+    elif layout == "staged":
+        s.plan.set_config(strip_rows=0)
+        assert s.plan.get_config()["stage_rows"] > 0
+    else:
+        assert s.plan.get_config()["strip_rows"] > 0
     cfg = s.plan.get_config()
     assert cfg["tail_inline"] == 0
     out = s.run_forward(f_iv, H, T * dt)
@@ -267,12 +276,14 @@ def test_separate_tail_large_nx(layout, dtype, record_error):
     rg = np.random.default_rng(12)
     gff = rg.standard_normal((m.nx, m.nv))
     gEh = rg.standard_normal((T, m.nx))
-    gf, gH = s._run_backward(f_iv, H, T * dt, None, gff, None, gEh, w)
-    rf, rH = O.delta_backward(g, dt, f_eq, f_iv, H, T, gff, None, gEh, w)
-    if dtype == torch.float32:
-        record_error(f"tail nx=4096 {layout} f32 adjoint", max(O.rel_err(gf, rf), O.rel_err(gH, rH)),
-                     TOL_BWD[dtype])
-    assert O.rel_err(gf, rf) < TOL_BWD[dtype] and O.rel_err(gH, rH) < TOL_BWD[dtype]
+    for name, ff in (("g_f_final", gff), ("E_hist/ee_hist only", None)):
+        gf, gH = s._run_backward(f_iv, H, T * dt, None, ff, None, gEh, w)
+        rf, rH = O.delta_backward(g, dt, f_eq, f_iv, H, T, ff if ff is not None else np.zeros((m.nx, m.nv)),
+                                  None, gEh, w)
+        if dtype == torch.float32:
+            record_error(f"tail nx=4096 {layout} f32 adjoint ({name})",
+                         max(O.rel_err(gf, rf), O.rel_err(gH, rH)), TOL_BWD[dtype])
+        assert O.rel_err(gf, rf) < TOL_BWD[dtype] and O.rel_err(gH, rH) < TOL_BWD[dtype], name
 
 
 def test_staged_shape_rejects_unusable_values():

@@ -826,7 +826,14 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
     b.E_prev = E_all + (size_t)(T_steps - 1) * nx;
     b.gE_hist = g_Eh ? g_Eh + (size_t)(T_steps - 1) * nx : nullptr;
     b.gee = g_ee ? g_ee + (T_steps - 1) : nullptr;
-    VP_CUDA(launch_bwd<T>(b, p->cfg, 0, p->feq2d != 0, s), "backward prologue launch");
+    if (g_ff == nullptr && g_fh == nullptr && !p->tail_inline) {
+        // no cotangent on the final state or the history: w_{T-1} = X^T(0) = 0 and the slope row
+        // sums are 0, so the prologue is two memsets and the tail
+        VP_CUDA(cudaMemsetAsync(b.w_out, 0, nxnv * sizeof(T), s), "cudaMemsetAsync(w)");
+        VP_CUDA(cudaMemsetAsync(part, 0, (size_t)b.n_chunks * nx * sizeof(T), s), "cudaMemsetAsync(part)");
+    } else {
+        VP_CUDA(launch_bwd<T>(b, p->cfg, 0, p->feq2d != 0, s), "backward prologue launch");
+    }
     if (!p->tail_inline) VP_CUDA(launch_bwd_tail<T>(b, p->tail_threads, p->tail_smem, p->tail_tw_stage != 0, s), "backward tail launch");
 
     b.c_src = nullptr;

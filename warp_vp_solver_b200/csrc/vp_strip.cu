@@ -226,6 +226,34 @@ __device__ __forceinline__ void strip_dwin(const float* __restrict__ dfeq, int j
     Dw[8] = c.x; Dw[9] = c.y; Dw[10] = c.z; Dw[11] = c.w;
 }
 
+// a + t (b - a) on two columns at once, each lane rounded exactly as pst_lerp (b - a, then one fma).
+__device__ __forceinline__ float2 strip_lerp2(float2 a, float2 b, float2 t) {
+    return __ffma2_rn(t, __ffma2_rn(a, make_float2(-1.f, -1.f), b), a);
+}
+
+// Stores a quad's 4 values of ring row `slot` into the ring, column e two rows earlier (slot - 2,
+// mod NR) when bit e of smask is set. Phase B then reads one row of 4 values per window row for all
+// of its columns, whichever of the quad's two x shifts each column has.
+__device__ __forceinline__ void strip_put(float* ring, int NR, int slot, int gt, int smask, float v0, float v1,
+                                          float v2, float v3) {
+    float* p = ring + (size_t)slot * kPstW + 4 + 4 * gt;
+    if (smask == 0) {
+        *reinterpret_cast<float4*>(p) = make_float4(v0, v1, v2, v3);
+        return;
+    }
+    int s2 = slot - 2;
+    s2 += s2 < 0 ? NR : 0;
+    float* q = ring + (size_t)s2 * kPstW + 4 + 4 * gt;
+    if (smask == 0xF) {
+        *reinterpret_cast<float4*>(q) = make_float4(v0, v1, v2, v3);
+        return;
+    }
+    (smask & 1 ? q : p)[0] = v0;
+    (smask & 2 ? q : p)[1] = v1;
+    (smask & 4 ? q : p)[2] = v2;
+    (smask & 8 ? q : p)[3] = v3;
+}
+
 // Column index c (in [-4, nv + 4)) reduced mod nv.
 __device__ __forceinline__ int strip_col(int c, int nv) { return c < 0 ? c + nv : (c >= nv ? c - nv : c); }
 
@@ -257,7 +285,6 @@ __global__ void __launch_bounds__(kStripThreads, 8) vp_strip_fwd_kernel(const St
     const int2 cm = __ldg(a.chunk + c);             // smallest / largest quad shift of the chunk
     const int span = 2 * (cm.y - cm.x) + R + 4;      // window rows of a band
     const int L = (span + R - 1) / R;               // slabs of R rows a window spans
-    const int SL = NR / R;                          // slabs the ring holds (>= L + 1)
     const int origin = b0 * R + 2 * cm.x;           // global row of ring row 0 (unreduced)
     const int c0 = c * kPstC;
     const int q = c * kPstGroup + gt, j0 = c0 + 4 * gt;
@@ -272,10 +299,16 @@ __global__ void __launch_bounds__(kStripThreads, 8) vp_strip_fwd_kernel(const St
     const bool two = gt < kStripPieces - kStripThreads;
     const int n_slabs = nb + L - 1;
 
-    // slab g: ring rows g R .. g R + R - 1 (slots (g mod SL) R + r) with their shift records
+    // slab g: ring rows g R .. g R + R - 1 (slots (g R + r) mod NR; NR / R >= L + 1 slabs) with their
+    // shift records
+    // slabs are issued in order: the next one's first slot and global row advance by R
+    int is_slot = 0, is_row = pst_wrap(origin, nx);
     auto issue_slab = [&](int g) {
-        const int s0 = (g % SL) * R;
-        int grow = pst_wrap(origin + g * R, nx);
+        const int s0 = is_slot;
+        int grow = is_row;
+        is_slot = is_slot + R == NR ? 0 : is_slot + R;
+        is_row += R;
+        is_row -= is_row >= nx ? nx : 0;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const float* src = a.h_in + (size_t)grow * nv;
@@ -290,13 +323,15 @@ __global__ void __launch_bounds__(kStripThreads, 8) vp_strip_fwd_kernel(const St
     issue_slab(0);
     if (n_slabs > 1) issue_slab(1);
 
+    int a_slot = 0, b_slot = 0;   // first slots of slab g and of band g - L + 1
     for (int g = 0; g < n_slabs; ++g) {
         if (g + 1 < n_slabs) pst_cp_wait(1);
         else pst_cp_wait(0);
         __syncthreads();
         // phase A: o = V(h) + V(f_eq) - f_eq on the slab's rows, in place; every thread works on the
         // same row at a time, so the row's shift selects one form for the whole CTA
-        const int s0 = (g % SL) * R;
+        const int s0 = a_slot;
+        a_slot = a_slot + R == NR ? 0 : a_slot + R;
         float ov[R][4];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -333,43 +368,36 @@ __global__ void __launch_bounds__(kStripThreads, 8) vp_strip_fwd_kernel(const St
             }
         }
         __syncthreads();   // every thread has read the slab's h (its neighbours' halo cells included)
+        // a column whose x shift is bm + 1 reads its window two rows further: its o goes two rows
+        // earlier, so that window row k of every column of the quad is ring row zb + k below
 #pragma unroll
-        for (int r = 0; r < R; ++r)
-            *reinterpret_cast<float4*>(ring + (size_t)(s0 + r) * kPstW + 4 + 4 * gt) =
-                make_float4(ov[r][0], ov[r][1], ov[r][2], ov[r][3]);
+        for (int r = 0; r < R; ++r) strip_put(ring, NR, s0 + r, gt, qi.y, ov[r][0], ov[r][1], ov[r][2], ov[r][3]);
         __syncthreads();
         // phase B: band i = g - L + 1, whose window (ring rows i R .. i R + span - 1) is complete
         const int i = g - L + 1;
         const int r0 = (b0 + i) * R;
         if (i >= 0) {
             // this thread's window row k is ring row i R + 2 (bm - cm.x) + k, global r0 + 2 bm + k
-            int zb = (i % SL) * R + 2 * (qi.x - cm.x);
+            int zb = b_slot + 2 * (qi.x - cm.x);
+            b_slot = b_slot + R == NR ? 0 : b_slot + R;
             zb -= zb >= NR ? NR : 0;
-            float acc[R];
+            const float2 ta = make_float2(tt[0], tt[1]), tb = make_float2(tt[2], tt[3]);
+            const float2 wa = make_float2(w0, 1.f), wb = make_float2(1.f, w3);
+            float2 acc2[R];
 #pragma unroll
-            for (int r = 0; r < R; ++r) acc[r] = 0.f;
-            float O[4][4], dprev[4];
+            for (int r = 0; r < R; ++r) acc2[r] = make_float2(0.f, 0.f);
+            float2 pa, pb, dpa, dpb;
 #pragma unroll
-            for (int k = 0; k < R + 4; ++k) {
+            for (int k = 0; k < R + 2; ++k) {
                 int sl = zb + k;
                 sl -= sl >= NR ? NR : 0;
                 const float4 o4 = *reinterpret_cast<const float4*>(ring + (size_t)sl * kPstW + 4 + 4 * gt);
-                float* o = O[k & 3];
-                o[0] = o4.x;
-                o[1] = o4.y;
-                o[2] = o4.z;
-                o[3] = o4.w;
-                if (k >= 3) {
-                    // d row q per column: window offset 0 or 2 rows (delta bit)
-                    const int qd = k - 3;
-                    float dn[4];
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const bool dl = (qi.y >> e) & 1;
-                        const float p0 = dl ? O[(qd + 2) & 3][e] : O[qd & 3][e];
-                        const float p1 = dl ? O[(qd + 3) & 3][e] : O[(qd + 1) & 3][e];
-                        dn[e] = pst_lerp(p0, p1, tt[e]);
-                    }
+                const float2 oa = make_float2(o4.x, o4.y), ob = make_float2(o4.z, o4.w);
+                if (k >= 1) {
+                    // d row qd from window rows qd, qd + 1
+                    const int qd = k - 1;
+                    const float2 da = strip_lerp2(pa, oa, ta), db = strip_lerp2(pb, ob, tb);
+                    const float dn[4] = {da.x, da.y, db.x, db.y};
                     if (fout && qd < R) {
 #pragma unroll
                         for (int e = 0; e < 4; ++e) {
@@ -381,19 +409,24 @@ __global__ void __launch_bounds__(kStripThreads, 8) vp_strip_fwd_kernel(const St
                     }
                     if (qd >= 1 && next) {
                         const int r = qd - 1;
-                        const float h0v = pst_lerp(dprev[0], dn[0], tt[0]);
-                        const float h1v = pst_lerp(dprev[1], dn[1], tt[1]);
-                        const float h2v = pst_lerp(dprev[2], dn[2], tt[2]);
-                        const float h3v = pst_lerp(dprev[3], dn[3], tt[3]);
+                        const float2 ha = strip_lerp2(dpa, da, ta), hb = strip_lerp2(dpb, db, tb);
                         *reinterpret_cast<float4*>(a.h_out + (size_t)(r0 + r) * nv + j0) =
-                            make_float4(h0v, h1v, h2v, h3v);
-                        acc[r] += w0 * h0v + h1v + h2v + w3 * h3v;
+                            make_float4(ha.x, ha.y, hb.x, hb.y);
+                        // trapezoid-weighted row sum: (w0 h0 + h2, h1 + w3 h3)
+                        acc2[r] = __fadd2_rn(acc2[r], __ffma2_rn(wb, hb, __fmul2_rn(wa, ha)));
                     }
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) dprev[e] = dn[e];
+                    dpa = da;
+                    dpb = db;
                 }
+                pa = oa;
+                pb = ob;
             }
-            if (sums) strip_rows_stage<R>(acc, red);
+            if (sums) {
+                float acc[R];
+#pragma unroll
+                for (int r = 0; r < R; ++r) acc[r] = acc2[r].x + acc2[r].y;
+                strip_rows_stage<R>(acc, red);
+            }
         }
         __syncthreads();   // band i's first slab is free, the row sums staged
         if (g + 2 < n_slabs) issue_slab(g + 2);
@@ -423,7 +456,6 @@ __global__ void __launch_bounds__(kStripThreads, 6) vp_strip_bwd_kernel(const St
     const int2 cm = __ldg(a.chunk + c);
     const int span = 2 * (cm.y - cm.x) + R + 4;
     const int L = (span + R - 1) / R;
-    const int SL = NR / R;
     const int origin = b0 * R - 2 * cm.y - 4;       // the thread of shift m reads rows r0 - 2m - 4 + k
     const int c0 = c * kPstC;
     const int q = c * kPstGroup + gt, j0 = c0 + 4 * gt;
@@ -441,9 +473,14 @@ __global__ void __launch_bounds__(kStripThreads, 6) vp_strip_bwd_kernel(const St
 
     // slab g of w_n (ring rows g R .. g R + R - 1) with shifts and rho cotangents, and the own rows of
     // h_{n-1} of band g - L + 1 (buffer band & 1) with their shifts: one commit group
+    // slabs are issued in order: the next one's first slot and global row advance by R
+    int is_slot = 0, is_row = pst_wrap(origin, nx);
     auto issue_slab = [&](int g) {
-        const int s0 = (g % SL) * R;
-        int grow = pst_wrap(origin + g * R, nx);
+        const int s0 = is_slot;
+        int grow = is_row;
+        is_slot = is_slot + R == NR ? 0 : is_slot + R;
+        is_row += R;
+        is_row -= is_row >= nx ? nx : 0;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const float* src = a.w_in + (size_t)grow * nv;
@@ -473,11 +510,13 @@ __global__ void __launch_bounds__(kStripThreads, 6) vp_strip_bwd_kernel(const St
     issue_slab(0);
     if (n_slabs > 1) issue_slab(1);
 
+    int a_slot = 0, b_slot = 0;   // first slots of slab g and of band g - L + 1
     for (int g = 0; g < n_slabs; ++g) {
         if (g + 1 < n_slabs) pst_cp_wait(1);
         else pst_cp_wait(0);
         __syncthreads();
-        const int s0 = (g % SL) * R;
+        const int s0 = a_slot;
+        a_slot = a_slot + R == NR ? 0 : a_slot + R;
         const int i = g - L + 1;                    // band whose window completes with this slab
         float* hb = hring + (size_t)(i & 1) * R * kPstW + 4 + 4 * gt;
         // phase A: gh = V^T w + rho^T grho on the slab's rows and, for band i, the slopes
@@ -558,10 +597,11 @@ __global__ void __launch_bounds__(kStripThreads, 6) vp_strip_bwd_kernel(const St
             }
         }
         __syncthreads();   // every thread has read the rows it converts' neighbours
+        // a column whose x shift is bm reads its window two rows further than one of bm + 1: its gh
+        // goes two rows earlier, so that window row k of every column is ring row zb + k below
 #pragma unroll
         for (int r = 0; r < R; ++r)
-            *reinterpret_cast<float4*>(ring + (size_t)(s0 + r) * kPstW + 4 + 4 * gt) =
-                make_float4(gv[r][0], gv[r][1], gv[r][2], gv[r][3]);
+            strip_put(ring, NR, s0 + r, gt, ~qi.y & 0xF, gv[r][0], gv[r][1], gv[r][2], gv[r][3]);
         if (i >= 0) {
 #pragma unroll
             for (int r = 0; r < R; ++r)
@@ -571,53 +611,51 @@ __global__ void __launch_bounds__(kStripThreads, 6) vp_strip_bwd_kernel(const St
         // phase B: band i: c = X^T gh (+ the f_hist cotangent), w_{n-1} = X^T c, slope products
         const int r0 = (b0 + i) * R;
         if (i >= 0) {
-            int zb = (i % SL) * R + 2 * (cm.y - qi.x);
+            int zb = b_slot + 2 * (cm.y - qi.x);
+            b_slot = b_slot + R == NR ? 0 : b_slot + R;
             zb -= zb >= NR ? NR : 0;
-            float acc[R];
+            const float2 ta = make_float2(tt[0], tt[1]), tb = make_float2(tt[2], tt[3]);
+            float2 acc2[R];
 #pragma unroll
-            for (int r = 0; r < R; ++r) acc[r] = 0.f;
-            float GH[4][4], cprev[4];
+            for (int r = 0; r < R; ++r) acc2[r] = make_float2(0.f, 0.f);
+            float2 ga, gb, cpa, cpb;
 #pragma unroll
-            for (int k = 0; k < R + 4; ++k) {
+            for (int k = 0; k < R + 2; ++k) {
                 int sl = zb + k;
                 sl -= sl >= NR ? NR : 0;
                 const float4 g4 = *reinterpret_cast<const float4*>(ring + (size_t)sl * kPstW + 4 + 4 * gt);
-                float* o = GH[k & 3];
-                o[0] = g4.x;
-                o[1] = g4.y;
-                o[2] = g4.z;
-                o[3] = g4.w;
-                if (k >= 3) {
-                    // c row q2 per column (a column of shift bm + delta reads window rows q2 + 2 - 2 delta ..)
-                    const int q2 = k - 3;
-                    float cn[4];
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const bool dl = (qi.y >> e) & 1;
-                        const float g0 = dl ? GH[q2 & 3][e] : GH[(q2 + 2) & 3][e];
-                        const float g1 = dl ? GH[(q2 + 1) & 3][e] : GH[(q2 + 3) & 3][e];
-                        cn[e] = pst_lerp(g1, g0, tt[e]);
-                        if (a.gfh != nullptr) {
-                            const int row = pst_wrap(r0 - qi.x - ((qi.y >> e) & 1) - 1 + q2, nx);
-                            cn[e] += __ldg(a.gfh + (size_t)row * nv + j0 + e);
-                        }
+                const float2 xa = make_float2(g4.x, g4.y), xb = make_float2(g4.z, g4.w);
+                if (k >= 1) {
+                    // c row q2 from window rows q2 (g0) and q2 + 1 (g1): c = g1 + t (g0 - g1)
+                    const int q2 = k - 1;
+                    float2 ca = strip_lerp2(xa, ga, ta), cb = strip_lerp2(xb, gb, tb);
+                    if (a.gfh != nullptr) {
+                        const float* gr = a.gfh + j0;
+                        ca.x += __ldg(gr + (size_t)pst_wrap(r0 - qi.x - (qi.y & 1) - 1 + q2, nx) * nv);
+                        ca.y += __ldg(gr + (size_t)pst_wrap(r0 - qi.x - ((qi.y >> 1) & 1) - 1 + q2, nx) * nv + 1);
+                        cb.x += __ldg(gr + (size_t)pst_wrap(r0 - qi.x - ((qi.y >> 2) & 1) - 1 + q2, nx) * nv + 2);
+                        cb.y += __ldg(gr + (size_t)pst_wrap(r0 - qi.x - ((qi.y >> 3) & 1) - 1 + q2, nx) * nv + 3);
                     }
                     if (q2 >= 1) {
                         // w row r = q2 - 1 (own row r0 + r) and its slope products
                         const int r = q2 - 1;
-                        float wv[4];
-#pragma unroll
-                        for (int e = 0; e < 4; ++e) wv[e] = pst_lerp(cn[e], cprev[e], tt[e]);
+                        const float2 wa = strip_lerp2(ca, cpa, ta), wb = strip_lerp2(cb, cpb, tb);
                         if (a.w_out != nullptr)
                             *reinterpret_cast<float4*>(a.w_out + (size_t)(r0 + r) * nv + j0) =
-                                make_float4(wv[0], wv[1], wv[2], wv[3]);
+                                make_float4(wa.x, wa.y, wb.x, wb.y);
                         const float4 s4 = *reinterpret_cast<const float4*>(hb + (size_t)r * kPstW);
-                        acc[r] += s4.x * wv[0] + s4.y * wv[1] + s4.z * wv[2] + s4.w * wv[3];
+                        acc2[r] = __ffma2_rn(make_float2(s4.z, s4.w), wb,
+                                             __ffma2_rn(make_float2(s4.x, s4.y), wa, acc2[r]));
                     }
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) cprev[e] = cn[e];
+                    cpa = ca;
+                    cpb = cb;
                 }
+                ga = xa;
+                gb = xb;
             }
+            float acc[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) acc[r] = acc2[r].x + acc2[r].y;
             strip_rows_stage<R>(acc, red);
         }
         __syncthreads();   // band i's first slab and its h buffer are free, the row sums staged
