@@ -38,8 +38,7 @@ namespace vpb {
 
 namespace {
 
-constexpr int kStripThreads = kPstGroup;   // one column group per CTA
-constexpr int kStripPieces = kPstW / 4;    // 16-byte pieces of a ring row
+constexpr int kStripThreads = kPstGroup;   // a single-instance CTA: one column group of 256 columns
 constexpr int kFieldThreads = 256;
 constexpr int kFieldWarps = kFieldThreads / 32;
 constexpr int kStripMaxSmem = 200 * 1024;   // dynamic shared memory cap of a strip CTA
@@ -48,20 +47,23 @@ __device__ __forceinline__ void strip_cp8(void* dst, const void* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(pst_smem(dst)), "l"(src) : "memory");
 }
 
+// Ring row of a column group of GT threads: 4 GT columns and 4 halo columns on each side.
+__host__ __device__ constexpr int strip_row(int GT) { return 4 * GT + 8; }
+
 // Shared memory of a forward CTA: NR ring rows, their shift records, the row-sum scratch.
-constexpr size_t strip_fwd_bytes(int NR, int R) {
-    return (size_t)NR * kPstW * 4 + (size_t)NR * 8 + (size_t)2 * R * 4;
+constexpr size_t strip_fwd_bytes(int NR, int R, int GT) {
+    return (size_t)NR * strip_row(GT) * 4 + (size_t)NR * 8 + (size_t)2 * R * 4;
 }
 
 // Adjoint CTA: NR ring rows of w_n with their shift records and rho cotangents, two buffers of the
 // band's R own rows of h_{n-1} with their shifts, the row-sum scratch.
-constexpr size_t strip_bwd_bytes(int NR, int R) {
-    return (size_t)NR * kPstW * 4 + (size_t)2 * R * kPstW * 4 + (size_t)NR * 8 + (size_t)NR * 4 +
+constexpr size_t strip_bwd_bytes(int NR, int R, int GT) {
+    return (size_t)NR * strip_row(GT) * 4 + (size_t)2 * R * strip_row(GT) * 4 + (size_t)NR * 8 + (size_t)NR * 4 +
            (size_t)2 * R * 4 + (size_t)2 * R * 4;
 }
 
 // acc[R] summed over each warp (transposed butterfly) into red[warp][row]; after the next block
-// barrier, thread r < R forms the row's sum red[0][r] + red[1][r] (strip_rows_total).
+// barrier, thread r < R forms the row's sum over the NW warps in order (strip_rows_total).
 template <int R>
 __device__ __forceinline__ void strip_rows_stage(float (&acc)[R], float* red) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -86,9 +88,13 @@ __device__ __forceinline__ void strip_rows_stage(float (&acc)[R], float* red) {
     if ((lane & ((32 >> LG) - 1)) == 0) red[wid * R + (lane >> (5 - LG))] = v;
 }
 
-template <int R>
+template <int R, int NW>
 __device__ __forceinline__ float strip_rows_total(const float* red) {
-    return threadIdx.x < R ? red[threadIdx.x] + red[R + threadIdx.x] : 0.f;
+    if (threadIdx.x >= R) return 0.f;
+    float s = red[threadIdx.x];
+#pragma unroll
+    for (int w = 1; w < NW; ++w) s += red[w * R + threadIdx.x];
+    return s;
 }
 
 // After a CTA has written the row partials of all bands of its run: returns true in every thread
@@ -110,19 +116,13 @@ __device__ __forceinline__ bool strip_run_done(unsigned* run_ctr, int n_chunks, 
     return *s_last != 0;
 }
 
-// Run i of a chunk: bands [i n_bands / runs, (i + 1) n_bands / runs); CTA blockIdx.x takes run
-// blockIdx.x mod runs of chunk blockIdx.x / runs, so the CTAs of one run in neighbouring chunks work
-// on the same rows at the same time and the 4-column halos they read from each other stay in L2.
-struct StripRun {
-    int c, run, b0, nb;
-};
-__device__ __forceinline__ StripRun strip_run(int runs, int n_bands) {
-    StripRun r;
-    r.c = blockIdx.x / runs;
-    r.run = blockIdx.x - r.c * runs;
-    r.b0 = (int)((long long)r.run * n_bands / runs);
-    r.nb = (int)((long long)(r.run + 1) * n_bands / runs) - r.b0;
-    return r;
+// Run i of a chunk: bands [i n_bands / runs, (i + 1) n_bands / runs). A single-instance launch
+// gives CTA blockIdx.x run blockIdx.x mod runs of chunk blockIdx.x / runs, so the CTAs of one run in
+// neighbouring chunks work on the same rows at the same time and the 4-column halos they read from
+// each other stay in L2.
+__device__ __forceinline__ void strip_run_bands(int run, int runs, int n_bands, int* b0, int* nb) {
+    *b0 = (int)((long long)run * n_bands / runs);
+    *nb = (int)((long long)(run + 1) * n_bands / runs) - *b0;
 }
 
 // In-halo shift forms. A thread holds the 8 staged cells w[i] = row[j0 + base + i] (two aligned
@@ -234,16 +234,17 @@ __device__ __forceinline__ float2 strip_lerp2(float2 a, float2 b, float2 t) {
 // Stores a quad's 4 values of ring row `slot` into the ring, column e two rows earlier (slot - 2,
 // mod NR) when bit e of smask is set. Phase B then reads one row of 4 values per window row for all
 // of its columns, whichever of the quad's two x shifts each column has.
+template <int SW>
 __device__ __forceinline__ void strip_put(float* ring, int NR, int slot, int gt, int smask, float v0, float v1,
                                           float v2, float v3) {
-    float* p = ring + (size_t)slot * kPstW + 4 + 4 * gt;
+    float* p = ring + (size_t)slot * SW + 4 + 4 * gt;
     if (smask == 0) {
         *reinterpret_cast<float4*>(p) = make_float4(v0, v1, v2, v3);
         return;
     }
     int s2 = slot - 2;
     s2 += s2 < 0 ? NR : 0;
-    float* q = ring + (size_t)s2 * kPstW + 4 + 4 * gt;
+    float* q = ring + (size_t)s2 * SW + 4 + 4 * gt;
     if (smask == 0xF) {
         *reinterpret_cast<float4*>(q) = make_float4(v0, v1, v2, v3);
         return;
@@ -266,28 +267,26 @@ __device__ __forceinline__ float strip_chunk_sum(const float* part, int nx, int 
 
 }  // namespace
 
-template <int R>
-__global__ void __launch_bounds__(kStripThreads, 8) vp_strip_fwd_kernel(const StripFwdArgs a) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ int s_last;
+template <int R, int GT>
+__device__ __forceinline__ void strip_fwd_body(const StripFwdArgs& a, unsigned char* smem, int* s_last, int c, int run_idx) {
+    constexpr int SW = strip_row(GT);
     const int nx = a.nx, nv = a.nv, NR = a.ring_rows;   // NR = (L + 1) R ring rows
     const int gt = threadIdx.x;
-    float* ring = reinterpret_cast<float*>(smem);                      // [NR][kPstW]
-    int2* rinf = reinterpret_cast<int2*>(ring + (size_t)NR * kPstW);    // [NR] (m mod nv, t)
+    float* ring = reinterpret_cast<float*>(smem);                      // [NR][SW]
+    int2* rinf = reinterpret_cast<int2*>(ring + (size_t)NR * SW);    // [NR] (m mod nv, t)
     float* red = reinterpret_cast<float*>(rinf + NR);                  // [2][R]
     const bool next = a.h_out != nullptr;
     const bool sums = next && a.part != nullptr;
     const bool fout = a.f_hist_n != nullptr || a.f_final != nullptr;
-    const StripRun run = strip_run(a.runs, a.n_bands);
-    if (run.nb <= 0) return;   // (the same run is empty in every chunk: no counter involved)
-    // the run of consecutive bands b0 .. b0 + nb - 1 of chunk c
-    const int c = run.c, b0 = run.b0, nb = run.nb;
+    int b0, nb;
+    strip_run_bands(run_idx, a.runs, a.n_bands, &b0, &nb);
+    if (nb <= 0) return;   // (the same run is empty in every chunk: no counter involved)
     const int2 cm = __ldg(a.chunk + c);             // smallest / largest quad shift of the chunk
     const int span = 2 * (cm.y - cm.x) + R + 4;      // window rows of a band
     const int L = (span + R - 1) / R;               // slabs of R rows a window spans
     const int origin = b0 * R + 2 * cm.x;           // global row of ring row 0 (unreduced)
-    const int c0 = c * kPstC;
-    const int q = c * kPstGroup + gt, j0 = c0 + 4 * gt;
+    const int c0 = c * (4 * GT);
+    const int q = c * GT + gt, j0 = c0 + 4 * gt;
     const int2 qi = __ldg(a.quad + q);
     const float4 t4 = __ldg(a.tq + q);
     float Dw[12];
@@ -295,8 +294,8 @@ __global__ void __launch_bounds__(kStripThreads, 8) vp_strip_fwd_kernel(const St
     const float tt[4] = {t4.x, t4.y, t4.z, t4.w};
     const float w0 = j0 == 0 ? 0.5f : 1.f, w3 = j0 + 3 == nv - 1 ? 0.5f : 1.f;
     const int col0 = strip_col(c0 - 4 + 4 * gt, nv);
-    const int col1 = strip_col(c0 - 4 + 4 * (gt + kStripThreads), nv);
-    const bool two = gt < kStripPieces - kStripThreads;
+    const int col1 = strip_col(c0 - 4 + 4 * (gt + GT), nv);
+    const bool two = gt < (GT + 2) - GT;
     const int n_slabs = nb + L - 1;
 
     // slab g: ring rows g R .. g R + R - 1 (slots (g R + r) mod NR; NR / R >= L + 1 slabs) with their
@@ -312,9 +311,9 @@ __global__ void __launch_bounds__(kStripThreads, 8) vp_strip_fwd_kernel(const St
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const float* src = a.h_in + (size_t)grow * nv;
-            float* dst = ring + (size_t)(s0 + r) * kPstW;
+            float* dst = ring + (size_t)(s0 + r) * SW;
             pst_cp16(dst + 4 * gt, src + col0);
-            if (two) pst_cp16(dst + 4 * (gt + kStripThreads), src + col1);
+            if (two) pst_cp16(dst + 4 * (gt + GT), src + col1);
             if (gt == r) strip_cp8(rinf + s0 + r, a.vsh + grow);
             grow = grow + 1 == nx ? 0 : grow + 1;
         }
@@ -337,7 +336,7 @@ __global__ void __launch_bounds__(kStripThreads, 8) vp_strip_fwd_kernel(const St
         for (int r = 0; r < R; ++r) {
             const int2 ri = rinf[s0 + r];
             const float tv = __int_as_float(ri.y);
-            const float* sr = ring + (size_t)(s0 + r) * kPstW + 4 + 4 * gt;
+            const float* sr = ring + (size_t)(s0 + r) * SW + 4 + 4 * gt;
             float* o = ov[r];
             if (ri.x == 0) {
                 const float4 h = *reinterpret_cast<const float4*>(sr);
@@ -371,7 +370,7 @@ __global__ void __launch_bounds__(kStripThreads, 8) vp_strip_fwd_kernel(const St
         // a column whose x shift is bm + 1 reads its window two rows further: its o goes two rows
         // earlier, so that window row k of every column of the quad is ring row zb + k below
 #pragma unroll
-        for (int r = 0; r < R; ++r) strip_put(ring, NR, s0 + r, gt, qi.y, ov[r][0], ov[r][1], ov[r][2], ov[r][3]);
+        for (int r = 0; r < R; ++r) strip_put<SW>(ring, NR, s0 + r, gt, qi.y, ov[r][0], ov[r][1], ov[r][2], ov[r][3]);
         __syncthreads();
         // phase B: band i = g - L + 1, whose window (ring rows i R .. i R + span - 1) is complete
         const int i = g - L + 1;
@@ -391,7 +390,7 @@ __global__ void __launch_bounds__(kStripThreads, 8) vp_strip_fwd_kernel(const St
             for (int k = 0; k < R + 2; ++k) {
                 int sl = zb + k;
                 sl -= sl >= NR ? NR : 0;
-                const float4 o4 = *reinterpret_cast<const float4*>(ring + (size_t)sl * kPstW + 4 + 4 * gt);
+                const float4 o4 = *reinterpret_cast<const float4*>(ring + (size_t)sl * SW + 4 + 4 * gt);
                 const float2 oa = make_float2(o4.x, o4.y), ob = make_float2(o4.z, o4.w);
                 if (k >= 1) {
                     // d row qd from window rows qd, qd + 1
@@ -430,35 +429,41 @@ __global__ void __launch_bounds__(kStripThreads, 8) vp_strip_fwd_kernel(const St
         }
         __syncthreads();   // band i's first slab is free, the row sums staged
         if (g + 2 < n_slabs) issue_slab(g + 2);
-        if (i >= 0 && sums && gt < R) a.part[(size_t)c * nx + r0 + gt] = strip_rows_total<R>(red);
+        if (i >= 0 && sums && gt < R) a.part[(size_t)c * nx + r0 + gt] = strip_rows_total<R, GT / 32>(red);
     }
     // rho of the run's rows, once every chunk has published them
-    if (sums && strip_run_done(a.run_ctr + run.run, a.n_chunks, &s_last))
-        for (int row = b0 * R + gt; row < (b0 + nb) * R; row += kStripThreads)
+    if (sums && strip_run_done(a.run_ctr + run_idx, a.n_chunks, s_last))
+        for (int row = b0 * R + gt; row < (b0 + nb) * R; row += GT)
             a.rho_out[row] = -a.dv * strip_chunk_sum(a.part, nx, a.n_chunks, row);
 }
 
-template <int R>
-__global__ void __launch_bounds__(kStripThreads, 6) vp_strip_bwd_kernel(const StripBwdArgs a) {
+template <int R, int GT>
+__global__ void __launch_bounds__(GT, 768 / GT) vp_strip_fwd_kernel(const StripFwdArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_last;
+    strip_fwd_body<R, GT>(a, smem, &s_last, blockIdx.x / a.runs, blockIdx.x % a.runs);
+}
+
+template <int R, int GT>
+__device__ __forceinline__ void strip_bwd_body(const StripBwdArgs& a, unsigned char* smem, int* s_last, int c, int run_idx) {
+    constexpr int SW = strip_row(GT);
     const int nx = a.nx, nv = a.nv, NR = a.ring_rows;
     const int gt = threadIdx.x;
-    float* ring = reinterpret_cast<float*>(smem);                       // [NR][kPstW] rows of w_n
-    float* hring = ring + (size_t)NR * kPstW;                           // [2][R][kPstW] rows of h_{n-1}
-    int2* rinf = reinterpret_cast<int2*>(hring + (size_t)2 * R * kPstW);   // [NR] step n shifts
+    float* ring = reinterpret_cast<float*>(smem);                       // [NR][SW] rows of w_n
+    float* hring = ring + (size_t)NR * SW;                           // [2][R][SW] rows of h_{n-1}
+    int2* rinf = reinterpret_cast<int2*>(hring + (size_t)2 * R * SW);   // [NR] step n shifts
     float* rgr = reinterpret_cast<float*>(rinf + NR);                   // [NR] rho cotangents
     int* hinf = reinterpret_cast<int*>(rgr + NR);                       // [2][R] step n-1 shifts
     float* red = reinterpret_cast<float*>(hinf + 2 * R);                // [2][R]
-    const StripRun run = strip_run(a.runs, a.n_bands);
-    if (run.nb <= 0) return;
-    const int c = run.c, b0 = run.b0, nb = run.nb;
+    int b0, nb;
+    strip_run_bands(run_idx, a.runs, a.n_bands, &b0, &nb);
+    if (nb <= 0) return;
     const int2 cm = __ldg(a.chunk + c);
     const int span = 2 * (cm.y - cm.x) + R + 4;
     const int L = (span + R - 1) / R;
     const int origin = b0 * R - 2 * cm.y - 4;       // the thread of shift m reads rows r0 - 2m - 4 + k
-    const int c0 = c * kPstC;
-    const int q = c * kPstGroup + gt, j0 = c0 + 4 * gt;
+    const int c0 = c * (4 * GT);
+    const int q = c * GT + gt, j0 = c0 + 4 * gt;
     const int2 qi = __ldg(a.quad + q);
     const float4 t4 = __ldg(a.tq + q);
     float Dw[12];
@@ -467,8 +472,8 @@ __global__ void __launch_bounds__(kStripThreads, 6) vp_strip_bwd_kernel(const St
     const float wr0 = j0 == 0 ? -0.5f * a.dv : -a.dv;   // rho^T weights (kernels.py:276-299)
     const float wr3 = j0 + 3 == nv - 1 ? -0.5f * a.dv : -a.dv;
     const int col0 = strip_col(c0 - 4 + 4 * gt, nv);
-    const int col1 = strip_col(c0 - 4 + 4 * (gt + kStripThreads), nv);
-    const bool two = gt < kStripPieces - kStripThreads;
+    const int col1 = strip_col(c0 - 4 + 4 * (gt + GT), nv);
+    const bool two = gt < (GT + 2) - GT;
     const int n_slabs = nb + L - 1;
 
     // slab g of w_n (ring rows g R .. g R + R - 1) with shifts and rho cotangents, and the own rows of
@@ -484,9 +489,9 @@ __global__ void __launch_bounds__(kStripThreads, 6) vp_strip_bwd_kernel(const St
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const float* src = a.w_in + (size_t)grow * nv;
-            float* dst = ring + (size_t)(s0 + r) * kPstW;
+            float* dst = ring + (size_t)(s0 + r) * SW;
             pst_cp16(dst + 4 * gt, src + col0);
-            if (two) pst_cp16(dst + 4 * (gt + kStripThreads), src + col1);
+            if (two) pst_cp16(dst + 4 * (gt + GT), src + col1);
             if (gt == r) {
                 strip_cp8(rinf + s0 + r, a.vsh_n + grow);
                 pst_cp4(rgr + s0 + r, a.grho + grow);
@@ -496,12 +501,12 @@ __global__ void __launch_bounds__(kStripThreads, 6) vp_strip_bwd_kernel(const St
         const int band = g - L + 1;
         if (band >= 0 && band < nb) {
             const int hr0 = (b0 + band) * R;
-            float* hb = hring + (size_t)(band & 1) * R * kPstW;
+            float* hb = hring + (size_t)(band & 1) * R * SW;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const float* src = a.h_prev + (size_t)(hr0 + r) * nv;
-                pst_cp16(hb + (size_t)r * kPstW + 4 * gt, src + col0);
-                if (two) pst_cp16(hb + (size_t)r * kPstW + 4 * (gt + kStripThreads), src + col1);
+                pst_cp16(hb + (size_t)r * SW + 4 * gt, src + col0);
+                if (two) pst_cp16(hb + (size_t)r * SW + 4 * (gt + GT), src + col1);
             }
             if (gt < R) pst_cp4(hinf + (band & 1) * R + gt, &a.vsh_prev[hr0 + gt].m);
         }
@@ -518,7 +523,7 @@ __global__ void __launch_bounds__(kStripThreads, 6) vp_strip_bwd_kernel(const St
         const int s0 = a_slot;
         a_slot = a_slot + R == NR ? 0 : a_slot + R;
         const int i = g - L + 1;                    // band whose window completes with this slab
-        float* hb = hring + (size_t)(i & 1) * R * kPstW + 4 + 4 * gt;
+        float* hb = hring + (size_t)(i & 1) * R * SW + 4 + 4 * gt;
         // phase A: gh = V^T w + rho^T grho on the slab's rows and, for band i, the slopes
         // (h + f_eq)[j + m + 1] - (h + f_eq)[j + m] of its own rows of h_{n-1}; in place, one row
         // (one shift) at a time for the whole CTA
@@ -527,7 +532,7 @@ __global__ void __launch_bounds__(kStripThreads, 6) vp_strip_bwd_kernel(const St
         for (int r = 0; r < R; ++r) {
             const int2 ri = rinf[s0 + r];
             const float tv = __int_as_float(ri.y), gr = rgr[s0 + r];
-            const float* sr = ring + (size_t)(s0 + r) * kPstW + 4 + 4 * gt;
+            const float* sr = ring + (size_t)(s0 + r) * SW + 4 + 4 * gt;
             float* o = gv[r];
             if (ri.x == 0) {
                 const float hm = sr[-1];
@@ -565,7 +570,7 @@ __global__ void __launch_bounds__(kStripThreads, 6) vp_strip_bwd_kernel(const St
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const int mh = hi[r];
-                const float* hr = hb + (size_t)r * kPstW;
+                const float* hr = hb + (size_t)r * SW;
                 float* o = sv[r];
                 if (mh == 0) {
                     const float4 h = *reinterpret_cast<const float4*>(hr);
@@ -601,11 +606,11 @@ __global__ void __launch_bounds__(kStripThreads, 6) vp_strip_bwd_kernel(const St
         // goes two rows earlier, so that window row k of every column is ring row zb + k below
 #pragma unroll
         for (int r = 0; r < R; ++r)
-            strip_put(ring, NR, s0 + r, gt, ~qi.y & 0xF, gv[r][0], gv[r][1], gv[r][2], gv[r][3]);
+            strip_put<SW>(ring, NR, s0 + r, gt, ~qi.y & 0xF, gv[r][0], gv[r][1], gv[r][2], gv[r][3]);
         if (i >= 0) {
 #pragma unroll
             for (int r = 0; r < R; ++r)
-                *reinterpret_cast<float4*>(hb + (size_t)r * kPstW) = make_float4(sv[r][0], sv[r][1], sv[r][2], sv[r][3]);
+                *reinterpret_cast<float4*>(hb + (size_t)r * SW) = make_float4(sv[r][0], sv[r][1], sv[r][2], sv[r][3]);
         }
         __syncthreads();
         // phase B: band i: c = X^T gh (+ the f_hist cotangent), w_{n-1} = X^T c, slope products
@@ -623,7 +628,7 @@ __global__ void __launch_bounds__(kStripThreads, 6) vp_strip_bwd_kernel(const St
             for (int k = 0; k < R + 2; ++k) {
                 int sl = zb + k;
                 sl -= sl >= NR ? NR : 0;
-                const float4 g4 = *reinterpret_cast<const float4*>(ring + (size_t)sl * kPstW + 4 + 4 * gt);
+                const float4 g4 = *reinterpret_cast<const float4*>(ring + (size_t)sl * SW + 4 + 4 * gt);
                 const float2 xa = make_float2(g4.x, g4.y), xb = make_float2(g4.z, g4.w);
                 if (k >= 1) {
                     // c row q2 from window rows q2 (g0) and q2 + 1 (g1): c = g1 + t (g0 - g1)
@@ -643,7 +648,7 @@ __global__ void __launch_bounds__(kStripThreads, 6) vp_strip_bwd_kernel(const St
                         if (a.w_out != nullptr)
                             *reinterpret_cast<float4*>(a.w_out + (size_t)(r0 + r) * nv + j0) =
                                 make_float4(wa.x, wa.y, wb.x, wb.y);
-                        const float4 s4 = *reinterpret_cast<const float4*>(hb + (size_t)r * kPstW);
+                        const float4 s4 = *reinterpret_cast<const float4*>(hb + (size_t)r * SW);
                         acc2[r] = __ffma2_rn(make_float2(s4.z, s4.w), wb,
                                              __ffma2_rn(make_float2(s4.x, s4.y), wa, acc2[r]));
                     }
@@ -660,18 +665,25 @@ __global__ void __launch_bounds__(kStripThreads, 6) vp_strip_bwd_kernel(const St
         }
         __syncthreads();   // band i's first slab and its h buffer are free, the row sums staged
         if (g + 2 < n_slabs) issue_slab(g + 2);
-        if (i >= 0 && gt < R) a.part[(size_t)c * nx + r0 + gt] = strip_rows_total<R>(red);
+        if (i >= 0 && gt < R) a.part[(size_t)c * nx + r0 + gt] = strip_rows_total<R, GT / 32>(red);
     }
-    if (strip_run_done(a.run_ctr + run.run, a.n_chunks, &s_last)) {
+    if (strip_run_done(a.run_ctr + run_idx, a.n_chunks, s_last)) {
         // tail of step n - 1 for the run's rows (warp_vp_solver/solver.py:870-929)
         const float gee = a.gee != nullptr ? __ldg(a.gee) : 0.f;
-        for (int row = b0 * R + gt; row < (b0 + nb) * R; row += kStripThreads) {
+        for (int row = b0 * R + gt; row < (b0 + nb) * R; row += GT) {
             float gEt = a.neg_dt_dv * strip_chunk_sum(a.part, nx, a.n_chunks, row);
             if (a.gE_hist != nullptr) gEt += __ldg(a.gE_hist + row);
             a.gH[row] += gEt;
             a.gE_out[row] = gEt + a.dx * trap_w<float>(row, nx) * __ldg(a.E_prev + row) * gee;
         }
     }
+}
+
+template <int R, int GT>
+__global__ void __launch_bounds__(GT, 512 / GT) vp_strip_bwd_kernel(const StripBwdArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_last;
+    strip_bwd_body<R, GT>(a, smem, &s_last, blockIdx.x / a.runs, blockIdx.x % a.runs);
 }
 
 __global__ void __launch_bounds__(kFieldThreads) vp_strip_field_kernel(const StripFieldArgs a) {
@@ -773,19 +785,19 @@ __global__ void __launch_bounds__(kFieldThreads) vp_strip_field_kernel(const Str
 // host side
 // ---------------------------------------------------------------------------------------------
 
-template <int R>
+template <int R, int GT>
 static int strip_occupancy(bool fwd, size_t smem) {
     int n = 0;
     cudaError_t e;
     // the attribute is the largest size any plan uses, so that plans of other grids stay launchable
     if (fwd) {
-        e = cudaFuncSetAttribute(vp_strip_fwd_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStripMaxSmem);
+        e = cudaFuncSetAttribute(vp_strip_fwd_kernel<R, GT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStripMaxSmem);
         if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, vp_strip_fwd_kernel<R>, kStripThreads, smem);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, vp_strip_fwd_kernel<R, GT>, GT, smem);
     } else {
-        e = cudaFuncSetAttribute(vp_strip_bwd_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStripMaxSmem);
+        e = cudaFuncSetAttribute(vp_strip_bwd_kernel<R, GT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStripMaxSmem);
         if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, vp_strip_bwd_kernel<R>, kStripThreads, smem);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, vp_strip_bwd_kernel<R, GT>, GT, smem);
     }
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -805,12 +817,12 @@ bool strip_prepare(StripHost& sh, int nx, int nv, const std::vector<int2>& chunk
         const int span_max = 2 * dmax + R + 4;
         // ring: a band's window (span rows, at most L slabs of R rows) plus the slab in flight
         const int NR = ((span_max + R - 1) / R + 1) * R;
-        const size_t fb = strip_fwd_bytes(NR, R), bb = strip_bwd_bytes(NR, R);
+        const size_t fb = strip_fwd_bytes(NR, R, kStripThreads), bb = strip_bwd_bytes(NR, R, kStripThreads);
         if (fb > (size_t)kStripMaxSmem || bb > (size_t)kStripMaxSmem) continue;
-        const int pf = R == 16 ? strip_occupancy<16>(true, fb) : R == 8 ? strip_occupancy<8>(true, fb)
-                                                                        : strip_occupancy<4>(true, fb);
-        const int pb = R == 16 ? strip_occupancy<16>(false, bb) : R == 8 ? strip_occupancy<8>(false, bb)
-                                                                         : strip_occupancy<4>(false, bb);
+        const int pf = R == 16 ? strip_occupancy<16, kStripThreads>(true, fb) : R == 8 ? strip_occupancy<8, kStripThreads>(true, fb)
+                                                                        : strip_occupancy<4, kStripThreads>(true, fb);
+        const int pb = R == 16 ? strip_occupancy<16, kStripThreads>(false, bb) : R == 8 ? strip_occupancy<8, kStripThreads>(false, bb)
+                                                                         : strip_occupancy<4, kStripThreads>(false, bb);
         if (pf <= 0 || pb <= 0) continue;
         sh.R = R;
         sh.n_bands = nx / R;
@@ -838,9 +850,9 @@ cudaError_t launch_strip_fwd(const StripFwdArgs& args, const StripHost& sh, cuda
     a.ring_rows = sh.ring_rows;
     a.runs = sh.fwd_runs;
     switch (sh.R) {
-        case 4: vp_strip_fwd_kernel<4><<<sh.fwd_ctas, kStripThreads, sh.fwd_smem, s>>>(a); break;
-        case 8: vp_strip_fwd_kernel<8><<<sh.fwd_ctas, kStripThreads, sh.fwd_smem, s>>>(a); break;
-        case 16: vp_strip_fwd_kernel<16><<<sh.fwd_ctas, kStripThreads, sh.fwd_smem, s>>>(a); break;
+        case 4: vp_strip_fwd_kernel<4, kStripThreads><<<sh.fwd_ctas, kStripThreads, sh.fwd_smem, s>>>(a); break;
+        case 8: vp_strip_fwd_kernel<8, kStripThreads><<<sh.fwd_ctas, kStripThreads, sh.fwd_smem, s>>>(a); break;
+        case 16: vp_strip_fwd_kernel<16, kStripThreads><<<sh.fwd_ctas, kStripThreads, sh.fwd_smem, s>>>(a); break;
         default: return cudaErrorInvalidValue;
     }
     count_launch();
@@ -854,9 +866,9 @@ cudaError_t launch_strip_bwd(const StripBwdArgs& args, const StripHost& sh, cuda
     a.ring_rows = sh.ring_rows;
     a.runs = sh.bwd_runs;
     switch (sh.R) {
-        case 4: vp_strip_bwd_kernel<4><<<sh.bwd_ctas, kStripThreads, sh.bwd_smem, s>>>(a); break;
-        case 8: vp_strip_bwd_kernel<8><<<sh.bwd_ctas, kStripThreads, sh.bwd_smem, s>>>(a); break;
-        case 16: vp_strip_bwd_kernel<16><<<sh.bwd_ctas, kStripThreads, sh.bwd_smem, s>>>(a); break;
+        case 4: vp_strip_bwd_kernel<4, kStripThreads><<<sh.bwd_ctas, kStripThreads, sh.bwd_smem, s>>>(a); break;
+        case 8: vp_strip_bwd_kernel<8, kStripThreads><<<sh.bwd_ctas, kStripThreads, sh.bwd_smem, s>>>(a); break;
+        case 16: vp_strip_bwd_kernel<16, kStripThreads><<<sh.bwd_ctas, kStripThreads, sh.bwd_smem, s>>>(a); break;
         default: return cudaErrorInvalidValue;
     }
     count_launch();
