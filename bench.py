@@ -699,18 +699,23 @@ def run_ensemble(args, rank, local_rank, world):
     peak, peak_kind = measured_peaks()
     n_launch = T + 1   # prologue + T steps (forward); prologue + T-1 steps + epilogue (adjoint)
     f_launch_ms, b_launch_ms = tf_ms / (args.steps * n_launch), tb_ms / (args.steps * n_launch)
+    strip = bool(ens.get_config().get("strip", 0))
+    kb_name, kf_name = (("vp_strip_ens_bwd_kernel", "vp_strip_ens_fwd_kernel") if strip
+                        else ("vp_batch_bwd_kernel", "vp_batch_fwd_kernel"))
     if b_launch_ms >= f_launch_ms:
-        kname, per_ms, alg = "vp_batch_bwd_kernel", b_launch_ms, BYTES_BWD * cells
+        kname, per_ms, alg = kb_name, b_launch_ms, BYTES_BWD * cells
     else:
-        kname, per_ms, alg = "vp_batch_fwd_kernel", f_launch_ms, BYTES_FWD * cells
+        kname, per_ms, alg = kf_name, f_launch_ms, BYTES_FWD * cells
     achieved = alg / (per_ms * 1e-3) / 1e9
     roof = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": peak,
             "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": profile_traffic(kname, "c4"),
             "algorithmic_bytes_per_launch": alg, "avg_launch_us": round(per_ms * 1e3, 3),
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
             else "fallback 6650 GB/s",
-            "note": "time per persistent ensemble launch averaged over graph replays of the timed "
-                    "steps; the packed state of all instances is read and written once per launch"}
+            "note": ("time per step (strip launch + field launch + gap) averaged over graph replays of the "
+                     "timed loops" if strip else
+                     "time per persistent ensemble launch averaged over graph replays of the timed steps")
+                    + "; the packed state of all instances is read and written once per step"}
     e2e = None if args.no_e2e else e2e_ensemble(args, ens, ew, dev, flush)
     shapes = {}
     for m in ew.meshes:
@@ -733,7 +738,9 @@ def run_ensemble(args, rank, local_rank, world):
                    "instances": ew.n, "cells_per_step": cells, "n_time_steps": T,
                    "shapes": shapes, "parallelism": f"ensemble shards x{world}" if world > 1 else "single",
                    "l2": "flushed between timed steps (256 MiB write, untimed)",
-                   "cuda_graph": use_graph, "path": "ensemble persistent launch per time step",
+                   "cuda_graph": use_graph,
+                   "path": ("ensemble strip kernels: one launch over all instances + a field launch per step"
+                            if strip else "ensemble persistent launch per time step"),
                    "autotune": tuned, "tile": ens.get_config(),
                    "fwd_ms_per_step": round(tf_ms / args.steps, 4),
                    "bwd_ms_per_step": round(tb_ms / args.steps, 4)},

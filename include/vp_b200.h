@@ -227,6 +227,12 @@ typedef struct vp_batch_config {
     int32_t n_tiles;          /* derived: tiles per step over all instances                       */
     int32_t grid_fwd;         /* derived: persistent grid of the forward launches                 */
     int32_t grid_bwd;         /* derived: persistent grid of the adjoint launches                 */
+    int32_t strip;            /* 1: the steps run on the strip kernels (one launch over all       */
+                              /* instances' 128-column groups and runs of bands, then a field     */
+                              /* launch); on by default where every instance qualifies (float32,  */
+                              /* x-invariant f_eq, nv a multiple of 128, nx of 32); 0: the tile  */
+                              /* kernels above                                                    */
+    int32_t strip_ctas;       /* derived: CTAs of a strip launch                                  */
 } vp_batch_config;
 
 int vp_batch_get_config(const vp_batch* batch, vp_batch_config* out);

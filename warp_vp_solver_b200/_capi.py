@@ -86,6 +86,8 @@ class BatchConfig(ctypes.Structure):
         ("n_tiles", c_i32),
         ("grid_fwd", c_i32),
         ("grid_bwd", c_i32),
+        ("strip", c_i32),
+        ("strip_ctas", c_i32),
     ]
 
 

@@ -121,7 +121,7 @@ def plan_candidates(cfg: dict) -> list[dict]:
     if cfg["cluster_size"] > 0:
         cands += [{"cluster_size": cn, "persist_rows": 0, "strip_rows": 0} for cn in (16, 8, 4, 2)]
     cands += [{"cluster_size": 0, "persist_rows": r, "strip_rows": 0} for r in (16, 8, 4)]
-    cands += [{"cluster_size": 0, "persist_rows": 0, "strip_rows": r} for r in (16, 8)]
+    cands += [{"cluster_size": 0, "persist_rows": 0, "strip_rows": r} for r in (4, 8, 16)]
     cands += [{"cluster_size": 0, "persist_rows": 0, "strip_rows": 0, "stage_rows": r, "stage_threads": c}
               for c in (256, 128) for r in (32, 16, 8, 4)]
     cands += [{"cluster_size": 0, "persist_rows": 0, "strip_rows": 0, "stage_rows": 0, "rows_per_cta": r}
@@ -180,13 +180,16 @@ def plan_feq(plan) -> np.ndarray:
 
 
 def ensemble_candidates(cfg: dict) -> list[dict]:
+    """The strip kernels first (where the ensemble qualifies for them), then tile shapes."""
     cands = []
+    if cfg.get("strip", 0):
+        cands.append({"strip": 1})
     for r in (8, 4, 2, 1):
         for chunk in (128, 256, 64):
             for th in (128, 256, 64):
                 if th > chunk * 2:
                     continue
-                cands.append({"rows_per_tile": r, "chunk_cols": chunk, "threads": th, "ctas_per_sm": 0})
+                cands.append({"rows_per_tile": r, "chunk_cols": chunk, "threads": th, "ctas_per_sm": 0, "strip": 0})
     return cands
 
 

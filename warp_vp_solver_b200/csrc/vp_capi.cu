@@ -102,6 +102,7 @@ struct vp_plan {
     // strip step path (vp_strip.cu): per-step kernels for large grids on the same quad tables
     StripHost strip;           // launch shape (strip.R == 0: not eligible)
     int strip_on = 0;          // per-step forward and adjoint steps (and recomputation) use it
+    int2* d_echunk = nullptr;  // ensembles on the strip kernels: quad shift range per 128 columns
     std::vector<long long> host_msigned;   // unreduced x half-step offsets (re-shaping the paths)
     std::vector<double> host_tx;           // their weights
     unsigned long long wait_ns = 1000000000ull;   // limit of each device-side grid barrier wait
@@ -979,8 +980,24 @@ static void free_plan(vp_plan* p) {
     cudaFree(p->d_pchunk);
     cudaFree(p->d_dfeq);
     cudaFree(p->d_ctab2);
+    cudaFree(p->d_echunk);
     cudaSetDevice(prev);
     delete p;
+}
+
+// Imaginary part of the multiplier of fft_inv_multiplier (poisson.py:34-45): m_k = -1/(i*2*pi*f_k)
+// = i/(2*pi*f_k), f_k the FFT frequencies of nx points over the period (m_0 = 0).
+static std::vector<double> poisson_mult_im(int nx, double period_x) {
+    std::vector<double> mult_im(nx, 0.0);
+    const double d = period_x / nx;
+    const double val = 1.0 / (nx * d);
+    const int npos = (nx - 1) / 2 + 1;
+    for (int k = 1; k < nx; ++k) {
+        const double kk = k < npos ? (double)k : (double)(k - nx);
+        const double f = kk * val;
+        mult_im[k] = 1.0 / ((2.0 * M_PI) * f);
+    }
+    return mult_im;
 }
 
 // c = real(ifft(m)) for the spectral multiplier's imaginary part: c[k] = -(1/nx) * sum_q mult_im[q]
@@ -1017,6 +1034,47 @@ static int upload_bytes(void** dst, const void* src, size_t bytes) {
     VP_CUDA(cudaMalloc(dst, std::max<size_t>(1, bytes)), "cudaMalloc(plan table)");
     if (bytes) VP_CUDA(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice), "cudaMemcpy(plan table)");
     return VP_OK;
+}
+
+// Tables of a plan for ensembles on the strip kernels (128-column groups): the quads, their x
+// weights, the f_eq differences, the circulant table (built here when the plan's own paths did not
+// need them) and the quad shift range per 128 columns. Returns false when the plan is not eligible:
+// float32, x-invariant f_eq, nv a multiple of 128, nx a multiple of 32 and at most 16384, the x
+// shifts of every 4 neighbouring columns within one cell.
+static bool plan_ens_tables(vp_plan* p, int* rc) {
+    *rc = VP_OK;
+    if (p->d_echunk != nullptr) return true;
+    const int nx = p->nx, nv = p->nv;
+    if (p->dtype != VP_F32 || p->feq2d || p->d_vtab == nullptr || nv % 128 != 0 || nx % kStripFieldRows != 0 ||
+        nx > 16384 || nx % kStripEnsRows != 0)
+        return false;
+    std::vector<long long> m_signed(nv);
+    std::vector<double> tx(nv);
+    for (int j = 0; j < nv; ++j) {
+        const double sj = 0.5 * p->host_vs[j] * p->dt / p->dx;
+        const double mf = std::floor(-sj);
+        tx[j] = -sj - mf;
+        m_signed[j] = std::fabs(mf) < 1e15 ? (long long)mf : 0;
+    }
+    std::vector<int2> quad, chunk;
+    std::vector<float> tq;
+    if (!build_quad_tables(nx, nv, m_signed, tx, quad, tq, chunk, 128)) return false;
+    if (p->d_pquad == nullptr) {
+        const double* fe = p->host_feq.data();
+        std::vector<float> dfeq(nv);
+        for (int j = 0; j < nv; ++j) dfeq[j] = (float)(fe[(j + 1) % nv] - fe[j]);
+        const std::vector<double> circ = circulant_of(nx, poisson_mult_im(nx, p->period_x));
+        std::vector<float> ctab2((size_t)3 * nx + 8);
+        for (size_t j = 0; j < ctab2.size(); ++j)
+            ctab2[j] = (float)circ[(size_t)((((long long)j - nx) % nx + nx) % nx)];
+        if ((*rc = upload_bytes((void**)&p->d_pquad, quad.data(), quad.size() * sizeof(int2))) ||
+            (*rc = upload_bytes((void**)&p->d_ptq, tq.data(), tq.size() * sizeof(float))) ||
+            (*rc = upload_bytes((void**)&p->d_dfeq, dfeq.data(), dfeq.size() * sizeof(float))) ||
+            (*rc = upload_bytes((void**)&p->d_ctab2, ctab2.data(), ctab2.size() * sizeof(float))))
+            return false;
+    }
+    if ((*rc = upload_bytes((void**)&p->d_echunk, chunk.data(), chunk.size() * sizeof(int2)))) return false;
+    return true;
 }
 
 }  // namespace vpb
@@ -1119,17 +1177,7 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
     p->pow2 = (nx & (nx - 1)) == 0;
     p->log2nx = 0;
     while ((1 << p->log2nx) < nx) ++p->log2nx;
-    std::vector<double> mult_im(nx, 0.0);
-    {
-        const double d = mesh->period_x / nx;
-        const double val = 1.0 / (nx * d);
-        const int npos = (nx - 1) / 2 + 1;
-        for (int k = 1; k < nx; ++k) {
-            const double kk = k < npos ? (double)k : (double)(k - nx);
-            const double f = kk * val;
-            mult_im[k] = 1.0 / ((2.0 * M_PI) * f);
-        }
-    }
+    const std::vector<double> mult_im = poisson_mult_im(nx, mesh->period_x);
     std::vector<double> tw;  // interleaved (re, im)
     if (p->pow2) {
         tw.resize((size_t)std::max(1, nx / 2) * 2);
@@ -1785,12 +1833,23 @@ struct vp_batch {
     size_t smem = 0;
     void* d_inst = nullptr;
     void* d_tiles = nullptr;   // int4 per tile: instance, first row, column chunk (no search on the device)
+    // strip step kernels (float32 ensembles whose instances all qualify): instance table, CTA maps,
+    // launch shapes and the sizes of their workspace regions
+    int strip_ok = 0, strip_on = 0;
+    void* d_sinst = nullptr;   // StripInst per instance (caller order)
+    void* d_smap = nullptr;    // int4 per strip CTA: instance, chunk, run
+    void* d_sfmap = nullptr;   // int2 per field CTA: instance, 32-row block
+    int s_ctas = 0, s_fctas = 0, s_small = 0;   // s_small: every nx <= kStripSmallField
+    size_t s_fsmem = 0, s_bsmem = 0;
+    long long s_part = 0, s_ctr = 0, s_eep = 0;
 };
 
 namespace vpb {
 
 struct BatchWs {
-    size_t h0, h1, part, counters, vsh, E, grho, total;
+    size_t h0, h1, part, counters, vsh, E, grho;
+    size_t spart, sctr, srho, sgE, seep;   // strip kernels: row partials, counters, rho, g_E, energies
+    size_t total;
 };
 
 static BatchWs batch_ws(const vp_batch* b) {
@@ -1804,6 +1863,13 @@ static BatchWs batch_ws(const vp_batch* b) {
     L.vsh = off; off += align256((size_t)b->total_x * vs);
     L.E = off; off += align256((size_t)b->total_x * rs);
     L.grho = off; off += align256((size_t)b->total_x * rs);
+    if (b->strip_ok) {
+        L.spart = off; off += align256((size_t)b->s_part * sizeof(float));
+        L.sctr = off; off += align256((size_t)(b->s_ctr + b->n) * sizeof(unsigned));
+        L.srho = off; off += align256((size_t)b->total_x * sizeof(float));
+        L.sgE = off; off += align256((size_t)b->total_x * sizeof(float));
+        L.seep = off; off += align256((size_t)b->s_eep * sizeof(double));
+    }
     L.total = off;
     return L;
 }
@@ -1868,6 +1934,9 @@ static void free_batch(vp_batch* b) {
         cudaSetDevice(b->device);
         cudaFree(b->d_inst);
         if (b->d_tiles) cudaFree(b->d_tiles);
+        cudaFree(b->d_sinst);
+        cudaFree(b->d_smap);
+        cudaFree(b->d_sfmap);
         cudaSetDevice(prev);
     }
     delete b;
@@ -1974,6 +2043,103 @@ static int batch_layout(vp_batch* b, int R, int chunk, int threads, int per_sm) 
     return VP_OK;
 }
 
+// Instance table and CTA maps of an ensemble on the strip kernels (128-column groups, bands of
+// kStripEnsRows rows, runs of about 8 bands). Sets b->strip_ok when every instance qualifies; the
+// strip kernels are then used by default.
+static int batch_strip_layout(vp_batch* b) {
+    b->strip_ok = b->strip_on = 0;
+    if (b->dtype != VP_F32) return VP_OK;
+    for (vp_plan* p : b->owned) {
+        int rc = VP_OK;
+        if (!plan_ens_tables(p, &rc)) return rc;   // not eligible (rc VP_OK) or an upload error
+    }
+    constexpr int RR = kStripEnsRows;
+    const int n = b->n;
+    std::vector<StripInst> inst(n);
+    long long part = 0, ctr = 0, eep = 0;
+    int max_nr = 0;
+    for (int k = 0; k < n; ++k) {
+        vp_plan* p = b->plan_of[k];
+        StripInst& I = inst[k];
+        I.nx = p->nx;
+        I.nv = p->nv;
+        I.n_chunks = p->nv / 128;
+        I.n_bands = p->nx / RR;
+        std::vector<int2> chunk(I.n_chunks);
+        VP_CUDA(cudaMemcpy(chunk.data(), p->d_echunk, chunk.size() * sizeof(int2), cudaMemcpyDeviceToHost),
+                "cudaMemcpy(chunk table)");
+        int dmax = 0;
+        for (const int2& c : chunk) dmax = std::max(dmax, c.y - c.x);
+        const int span_max = 2 * dmax + RR + 4;
+        I.ring_rows = ((span_max + RR - 1) / RR + 1) * RR;
+        max_nr = std::max(max_nr, I.ring_rows);
+        I.runs = std::max(1, std::min(I.n_bands, (I.n_bands + 7) / 8));
+        I.index = k;
+        I.off_x = (int)b->off_x[k];
+        I.off_f = b->off_f[k];
+        I.off_part = (int)part;
+        part += (long long)I.n_chunks * p->nx;
+        I.off_ctr = (int)ctr;
+        ctr += I.runs;
+        I.field_ctas = p->nx / kStripFieldRows;
+        I.off_eep = (int)eep;
+        eep += I.field_ctas;
+        I.quad = p->d_pquad;
+        I.tq = p->d_ptq;
+        I.chunk = p->d_echunk;
+        I.dfeq = p->d_dfeq;
+        I.vtab = static_cast<const float*>(p->d_vtab);
+        I.feq = p->d_feq;
+        I.ctab = p->d_ctab2;
+        I.dv = (float)p->dv;
+        I.dx = (float)p->dx;
+        I.dtdv = (float)(p->dt / p->dv);
+        I.neg_dt_dv = (float)(-p->dt / p->dv);
+    }
+    const size_t fsmem = strip_ens_fwd_bytes(max_nr), bsmem = strip_ens_bwd_bytes(max_nr);
+    if (strip_ens_occupancy(true, fsmem) <= 0 || strip_ens_occupancy(false, bsmem) <= 0) return VP_OK;
+    // CTA maps, largest instances first
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+        return (long long)inst[a].nx * inst[a].nv > (long long)inst[c].nx * inst[c].nv;
+    });
+    std::vector<int4> map;
+    std::vector<int2> fmap;
+    for (int k : order) {
+        for (int c = 0; c < inst[k].n_chunks; ++c)
+            for (int r = 0; r < inst[k].runs; ++r) map.push_back(make_int4(k, c, r, 0));
+        for (int rb = 0; rb < inst[k].field_ctas; ++rb) fmap.push_back(make_int2(k, rb));
+    }
+    void *d_inst = nullptr, *d_map = nullptr, *d_fmap = nullptr;
+    int rc = upload_bytes(&d_inst, inst.data(), inst.size() * sizeof(StripInst));
+    if (!rc) rc = upload_bytes(&d_map, map.data(), map.size() * sizeof(int4));
+    if (!rc) rc = upload_bytes(&d_fmap, fmap.data(), fmap.size() * sizeof(int2));
+    if (rc) {
+        cudaFree(d_inst);
+        cudaFree(d_map);
+        cudaFree(d_fmap);
+        return rc;
+    }
+    cudaFree(b->d_sinst);
+    cudaFree(b->d_smap);
+    cudaFree(b->d_sfmap);
+    b->d_sinst = d_inst;
+    b->d_smap = d_map;
+    b->d_sfmap = d_fmap;
+    b->s_ctas = (int)map.size();
+    b->s_small = 1;
+    for (const StripInst& I : inst) b->s_small = b->s_small && I.nx <= kStripSmallField;
+    b->s_fctas = (int)fmap.size();
+    b->s_fsmem = fsmem;
+    b->s_bsmem = bsmem;
+    b->s_part = part;
+    b->s_ctr = ctr;
+    b->s_eep = eep;
+    b->strip_ok = b->strip_on = 1;
+    return VP_OK;
+}
+
 template <typename T>
 static int batch_forward_impl(vp_batch* b, const double* f_iv, const T* H, int Ts, double* f_final,
                               T* E_hist, T* ee_hist, unsigned char* tape, unsigned char* ws, cudaStream_t s) {
@@ -2015,6 +2181,42 @@ static int batch_forward_impl(vp_batch* b, const double* f_iv, const T* H, int T
     set_out(0);
     VP_CUDA(launch_batch_fwd<T>(st, b->R, 0, b->feq2d != 0, b->grid_fwd, b->threads, b->smem, s), "batch prologue");
     st.f_iv = nullptr;
+    if constexpr (sizeof(T) == 4) {
+        if (b->strip_on) {
+            // the steps on the strip kernels: a strip launch and a field launch per step
+            VP_CUDA(cudaMemsetAsync(ws + L.sctr, 0, (size_t)(b->s_ctr + b->n) * sizeof(unsigned), s),
+                    "memset(strip counters)");
+            st.part = reinterpret_cast<T*>(ws + L.spart);
+            st.counters = reinterpret_cast<unsigned*>(ws + L.sctr);
+            st.rho = reinterpret_cast<T*>(ws + L.srho);
+            st.eep = reinterpret_cast<double*>(ws + L.seep);
+            st.fctr = reinterpret_cast<unsigned*>(ws + L.sctr) + b->s_ctr;
+            const StripInst* si = static_cast<const StripInst*>(b->d_sinst);
+            for (int n = 0; n < Ts; ++n) {
+                const bool last = (n == Ts - 1);
+                if (tape) {
+                    st.c_in = th; st.c_in_mul = Ts; st.c_in_step = n;
+                    st.vsh_in = tv; st.vsh_in_mul = Ts; st.vsh_in_step = n;
+                } else {
+                    st.c_in = hb[n & 1]; st.c_in_mul = 1; st.c_in_step = 0;
+                    st.vsh_in = vsh_ws; st.vsh_in_mul = 1; st.vsh_in_step = 0;
+                }
+                if (last) st.c_out = nullptr;
+                else set_out(n + 1);
+                st.last = last ? 1 : 0;
+                st.hist_step = n + 1;
+                st.f_final = last ? f_final : nullptr;
+                VP_CUDA(launch_strip_ens_fwd(si, static_cast<const int4*>(b->d_smap), b->s_ctas, b->s_fsmem, st, s),
+                        "ensemble strip step");
+                if (!last)
+                    VP_CUDA(b->s_small ? launch_strip_ens_field_small(si, b->n, st, 0, s)
+                                       : launch_strip_ens_field(si, static_cast<const int2*>(b->d_sfmap), b->s_fctas,
+                                                                st, 0, s),
+                            "ensemble field");
+            }
+            return VP_OK;
+        }
+    }
     for (int n = 0; n < Ts; ++n) {
         const bool last = (n == Ts - 1);
         if (tape) {
@@ -2073,7 +2275,36 @@ static int batch_backward_impl(vp_batch* b, const T* H, int Ts, const unsigned c
     VP_CUDA(launch_batch_bwd<T>(st, b->R, 0, b->feq2d != 0, b->grid_bwd, b->threads, b->smem, s), "batch bwd prologue");
     st.g_ff = nullptr;
     st.grho = grho;
-    for (int n = Ts - 1; n >= 1; --n) {
+    bool strip = false;
+    if constexpr (sizeof(T) == 4) strip = b->strip_on != 0;
+    if (strip) {
+        if constexpr (sizeof(T) == 4) {
+            // adjoint steps n = T-1 .. 1 on the strip kernels (strip launch, Poisson^T field launch)
+            VP_CUDA(cudaMemsetAsync(ws + L.sctr, 0, (size_t)(b->s_ctr + b->n) * sizeof(unsigned), s),
+                    "memset(strip counters)");
+            BatchStep<T> ss = st;
+            ss.part = reinterpret_cast<T*>(ws + L.spart);
+            ss.counters = reinterpret_cast<unsigned*>(ws + L.sctr);
+            ss.gE = reinterpret_cast<T*>(ws + L.sgE);
+            const StripInst* si = static_cast<const StripInst*>(b->d_sinst);
+            for (int n = Ts - 1; n >= 1; --n) {
+                ss.c_in = wb[n & 1]; ss.c_in_mul = 1; ss.c_in_step = 0;
+                ss.c_out = wb[(n - 1) & 1];
+                ss.vsh_in = tv; ss.vsh_in_mul = Ts; ss.vsh_in_step = n;
+                ss.h_prev_step = n - 1;
+                ss.vsh_prev_step = n - 1;
+                ss.E_prev_step = n - 1;
+                ss.g_step = n - 1;
+                VP_CUDA(launch_strip_ens_bwd(si, static_cast<const int4*>(b->d_smap), b->s_ctas, b->s_bsmem, ss, s),
+                        "ensemble strip adjoint step");
+                VP_CUDA(b->s_small ? launch_strip_ens_field_small(si, b->n, ss, 1, s)
+                                   : launch_strip_ens_field(si, static_cast<const int2*>(b->d_sfmap), b->s_fctas, ss,
+                                                            1, s),
+                        "ensemble adjoint field");
+            }
+        }
+    }
+    for (int n = strip ? 0 : Ts - 1; n >= 1; --n) {
         st.c_in = wb[n & 1]; st.c_in_mul = 1; st.c_in_step = 0;
         st.c_out = wb[(n - 1) & 1];
         st.vsh_in = tv; st.vsh_in_mul = Ts; st.vsh_in_step = n;
@@ -2150,7 +2381,8 @@ int vp_batch_create(int32_t n, const vp_mesh_desc* meshes, const double* dts,
         return set_err(VP_ERR_ARG, "ensemble has more than 2^31 rows");
     }
     b->feq2d = feq2d ? 1 : 0;
-    const int rc = batch_layout(b, R, 128, 128, 0);
+    int rc = batch_layout(b, R, 128, 128, 0);
+    if (rc == VP_OK) rc = batch_strip_layout(b);
     if (rc != VP_OK) {
         free_batch(b);
         return rc;
@@ -2168,12 +2400,19 @@ int vp_batch_get_config(const vp_batch* b, vp_batch_config* out) {
     out->n_tiles = b->n_tiles;
     out->grid_fwd = b->grid_fwd;
     out->grid_bwd = b->grid_bwd;
+    out->strip = b->strip_on;
+    out->strip_ctas = b->strip_on ? b->s_ctas : 0;
     return VP_OK;
 }
 
 int vp_batch_set_config(vp_batch* b, const vp_batch_config* cfg) {
     if (!b || !cfg) return set_err(VP_ERR_ARG, "batch and cfg must not be NULL");
-    return batch_layout(b, cfg->rows_per_tile, cfg->chunk_cols, cfg->threads, cfg->ctas_per_sm);
+    if (cfg->strip != 0 && !b->strip_ok)
+        return set_err(VP_ERR_ARG, "strip=1: the strip kernels need a float32 ensemble whose instances all have an "
+                                   "x-invariant f_eq, nv a multiple of 128 and nx a multiple of 32");
+    const int rc = batch_layout(b, cfg->rows_per_tile, cfg->chunk_cols, cfg->threads, cfg->ctas_per_sm);
+    if (rc == VP_OK) b->strip_on = cfg->strip != 0 ? 1 : 0;
+    return rc;
 }
 
 int vp_batch_destroy(vp_batch* b) {

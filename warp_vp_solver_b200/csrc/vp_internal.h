@@ -147,6 +147,12 @@ template <typename T> struct BatchStep {
     const VShift<T>* vsh_prev; int vsh_prev_step; // tape shifts of step n-1
     const T* E_prev; int E_prev_step;            // tape E of step n-1
     const double* unused_;
+    // strip step kernels of an ensemble: packed rho and g_E rows, per-instance field energy
+    // partials and field completion counters
+    T* rho;
+    T* gE;
+    double* eep;
+    unsigned* fctr;
     const T* g_ff;              // prologue: cotangent on f_final (packed cells)
     const T* g_Eh;              // [inst][n_steps][nx], row n-1
     const T* g_ee;              // [inst][n_steps], entry n-1
@@ -283,7 +289,8 @@ size_t persist_smem_bytes(int span_max, int win_rows, int R, int nx, int nv, int
 // The column-quad tables of the persistent and strip paths (false: some 4 neighbouring columns'
 // x shifts differ by more than one cell, or a shift reaches half a period).
 bool build_quad_tables(int nx, int nv, const std::vector<long long>& m_signed, const std::vector<double>& tx,
-                       std::vector<int2>& quad, std::vector<float>& tq, std::vector<int2>& chunk);
+                       std::vector<int2>& quad, std::vector<float>& tq, std::vector<int2>& chunk,
+                       int chunk_cols = 256);
 
 // Strip step kernels (vp_strip.cu): per-step launches for large grids. A CTA is one column group
 // (64 threads, 256 columns) that walks one run of consecutive bands of R rows of one column chunk,
@@ -352,6 +359,22 @@ struct StripFieldArgs {
     float* grho_out;            // adjoint
 };
 
+// One instance of an ensemble on the strip kernels: its tables, launch shape and offsets in the
+// ensemble's packed buffers.
+struct StripInst {
+    int nx, nv, n_chunks, n_bands, ring_rows, runs, index;
+    int off_x, off_part, off_ctr, off_eep, field_ctas;
+    long long off_f;
+    const int2* quad;
+    const float4* tq;
+    const int2* chunk;
+    const float* dfeq;
+    const float* vtab;
+    const double* feq;
+    const float* ctab;
+    float dv, dx, dtdv, neg_dt_dv;
+};
+
 struct StripHost {
     int R = 0, n_bands = 0, n_chunks = 0, span_max = 0, ring_rows = 0;
     int fwd_runs = 0, bwd_runs = 0, fwd_ctas = 0, bwd_ctas = 0, field_ctas = 0;
@@ -364,6 +387,23 @@ bool strip_prepare(StripHost& sh, int nx, int nv, const std::vector<int2>& chunk
 cudaError_t launch_strip_fwd(const StripFwdArgs& a, const StripHost& sh, cudaStream_t s);
 cudaError_t launch_strip_bwd(const StripBwdArgs& a, const StripHost& sh, cudaStream_t s);
 cudaError_t launch_strip_field(const StripFieldArgs& a, const StripHost& sh, cudaStream_t s);
+// Ensembles: one launch over the CTA map (instance, chunk, run) of all instances, 128-column groups
+// and bands of kStripEnsRows rows; field launches over (instance, 32-row block).
+constexpr int kStripEnsRows = 4;
+constexpr int kStripEnsThreads = 32;
+size_t strip_ens_fwd_bytes(int ring_rows);
+size_t strip_ens_bwd_bytes(int ring_rows);
+int strip_ens_occupancy(bool fwd, size_t smem);
+cudaError_t launch_strip_ens_fwd(const StripInst* insts, const int4* map, int n_ctas, size_t smem,
+                                 const BatchStep<float>& b, cudaStream_t s);
+cudaError_t launch_strip_ens_bwd(const StripInst* insts, const int4* map, int n_ctas, size_t smem,
+                                 const BatchStep<float>& b, cudaStream_t s);
+cudaError_t launch_strip_ens_field(const StripInst* insts, const int2* fmap, int n_ctas, const BatchStep<float>& b,
+                                   int adjoint, cudaStream_t s);
+// Ensembles whose instances all have nx <= kStripSmallField: the field of each instance in one CTA.
+constexpr int kStripSmallField = 256;
+cudaError_t launch_strip_ens_field_small(const StripInst* insts, int n_inst, const BatchStep<float>& b, int adjoint,
+                                         cudaStream_t s);
 
 // Raises VP_STATUS_NONFINITE_INPUT in *status when f (n doubles) or H (nx reals, double when h64)
 // holds a NaN or an infinity (vp_ops.cu).

@@ -832,8 +832,8 @@ static int pst_max_blocks_r(int R, size_t smem) {
 // is not eligible: nv a multiple of 256, the x shifts of every 4 neighbouring columns within one
 // cell of each other, windows shorter than a period.
 bool build_quad_tables(int nx, int nv, const std::vector<long long>& m_signed, const std::vector<double>& tx,
-                       std::vector<int2>& quad, std::vector<float>& tq, std::vector<int2>& chunk) {
-    if (nv % kPstC != 0 || nx < 8) return false;
+                       std::vector<int2>& quad, std::vector<float>& tq, std::vector<int2>& chunk, int chunk_cols) {
+    if (chunk_cols % 4 != 0 || nv % chunk_cols != 0 || nx < 8) return false;
     const int nq = nv / 4;
     quad.assign(nq, make_int2(0, 0));
     tq.assign((size_t)4 * nq, 0.f);
@@ -849,11 +849,11 @@ bool build_quad_tables(int nx, int nv, const std::vector<long long>& m_signed, c
         quad[q] = make_int2((int)lo, mask);
         for (int e = 0; e < 4; ++e) tq[(size_t)4 * q + e] = (float)tx[4 * q + e];
     }
-    const int nch = nv / kPstC;
+    const int nch = nv / chunk_cols, qpc = chunk_cols / 4;
     chunk.assign(nch, make_int2(0, 0));
     for (int c = 0; c < nch; ++c) {
         int lo = 1 << 30, hi = -(1 << 30);
-        for (int q = c * kPstGroup; q < (c + 1) * kPstGroup; ++q) {
+        for (int q = c * qpc; q < (c + 1) * qpc; ++q) {
             lo = std::min(lo, quad[q].x);
             hi = std::max(hi, quad[q].x);
         }

@@ -686,13 +686,15 @@ __global__ void __launch_bounds__(GT, 512 / GT) vp_strip_bwd_kernel(const StripB
     strip_bwd_body<R, GT>(a, smem, &s_last, blockIdx.x / a.runs, blockIdx.x % a.runs);
 }
 
-__global__ void __launch_bounds__(kFieldThreads) vp_strip_field_kernel(const StripFieldArgs a) {
+// Rows blk * 32 .. blk * 32 + 31 of the field; nblk CTAs solve the whole field (their energy
+// partials are summed by the last of them).
+__device__ __forceinline__ void strip_field_body(const StripFieldArgs& a, int blk, int nblk) {
     constexpr int FR = kStripFieldRows;
     __shared__ float red[kFieldWarps][FR];
     __shared__ double s_e[FR];
     __shared__ int s_last;
     const int nx = a.nx;
-    const int i0 = blockIdx.x * FR;
+    const int i0 = blk * FR;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     float acc[FR];
 #pragma unroll
@@ -764,20 +766,177 @@ __global__ void __launch_bounds__(kFieldThreads) vp_strip_field_kernel(const Str
         double e = s_e[lane];
         e = warp_sum(e);
         if (lane == 0) {
-            a.eep[blockIdx.x] = e;
+            a.eep[blk] = e;
             __threadfence();
-            s_last = atomicAdd(a.counter, 1u) == gridDim.x - 1 ? 1 : 0;
+            s_last = atomicAdd(a.counter, 1u) == (unsigned)(nblk - 1) ? 1 : 0;
         }
         e = 0.0;
         if (__shfl_sync(0xffffffffu, s_last, 0)) {
             __threadfence();
-            for (int g = lane; g < (int)gridDim.x; g += 32) e += __ldcg(a.eep + g);
+            for (int g = lane; g < nblk; g += 32) e += __ldcg(a.eep + g);
             e = warp_sum(e);
             if (lane == 0) {
                 *a.ee_out = (float)(0.5 * e * (double)a.dx);
                 *a.counter = 0u;
             }
         }
+    }
+}
+
+__global__ void __launch_bounds__(kFieldThreads) vp_strip_field_kernel(const StripFieldArgs a) {
+    strip_field_body(a, blockIdx.x, gridDim.x);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Ensembles: the same bodies over all instances of an ensemble in one launch. CTA blockIdx.x works
+// on map[blockIdx.x] = (instance, chunk, run) with 128-column groups; the per-step buffers are the
+// ensemble's packed ones (BatchStep), the tables and offsets each instance's (StripInst).
+// ---------------------------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kStripEnsThreads, 24)
+    vp_strip_ens_fwd_kernel(const StripInst* __restrict__ insts, const int4* __restrict__ map,
+                            const BatchStep<float> b) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_last;
+    const int4 m = __ldg(map + blockIdx.x);
+    const StripInst& I = insts[m.x];
+    const long long nn = (long long)I.nx * I.nv;
+    StripFwdArgs a{};
+    a.nx = I.nx;
+    a.nv = I.nv;
+    a.n_chunks = I.n_chunks;
+    a.n_bands = I.n_bands;
+    a.ring_rows = I.ring_rows;
+    a.runs = I.runs;
+    a.quad = I.quad;
+    a.tq = I.tq;
+    a.chunk = I.chunk;
+    a.dfeq = I.dfeq;
+    a.vtab = I.vtab;
+    a.feq = I.feq;
+    a.h_in = b.c_in + b.c_in_mul * I.off_f + (long long)b.c_in_step * nn;
+    a.h_out = b.c_out ? b.c_out + b.c_out_mul * I.off_f + (long long)b.c_out_step * nn : nullptr;
+    a.vsh = b.vsh_in + (long long)b.vsh_in_mul * I.off_x + (long long)b.vsh_in_step * I.nx;
+    a.f_hist_n = nullptr;
+    a.f_final = b.f_final ? b.f_final + I.off_f : nullptr;
+    a.part = b.part ? b.part + I.off_part : nullptr;
+    a.run_ctr = b.counters + I.off_ctr;
+    a.rho_out = b.rho + I.off_x;
+    a.dv = I.dv;
+    strip_fwd_body<kStripEnsRows, kStripEnsThreads>(a, smem, &s_last, m.y, m.z);
+}
+
+__global__ void __launch_bounds__(kStripEnsThreads, 16)
+    vp_strip_ens_bwd_kernel(const StripInst* __restrict__ insts, const int4* __restrict__ map,
+                            const BatchStep<float> b) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_last;
+    const int4 m = __ldg(map + blockIdx.x);
+    const StripInst& I = insts[m.x];
+    const long long nn = (long long)I.nx * I.nv;
+    StripBwdArgs a{};
+    a.nx = I.nx;
+    a.nv = I.nv;
+    a.n_chunks = I.n_chunks;
+    a.n_bands = I.n_bands;
+    a.ring_rows = I.ring_rows;
+    a.runs = I.runs;
+    a.quad = I.quad;
+    a.tq = I.tq;
+    a.chunk = I.chunk;
+    a.dfeq = I.dfeq;
+    a.vtab = I.vtab;
+    a.feq = I.feq;
+    a.w_in = b.c_in + b.c_in_mul * I.off_f + (long long)b.c_in_step * nn;
+    a.w_out = b.c_out ? b.c_out + b.c_out_mul * I.off_f + (long long)b.c_out_step * nn : nullptr;
+    a.grho = b.grho + I.off_x;
+    a.vsh_n = b.vsh_in + (long long)b.vsh_in_mul * I.off_x + (long long)b.vsh_in_step * I.nx;
+    a.vsh_prev = b.vsh_prev + (long long)b.n_steps * I.off_x + (long long)b.vsh_prev_step * I.nx;
+    a.h_prev = b.h_prev + (long long)b.n_steps * I.off_f + (long long)b.h_prev_step * nn;
+    a.gfh = nullptr;
+    a.part = b.part + I.off_part;
+    a.run_ctr = b.counters + I.off_ctr;
+    a.dv = I.dv;
+    a.dx = I.dx;
+    a.neg_dt_dv = I.neg_dt_dv;
+    a.gE_hist = b.g_Eh ? b.g_Eh + (long long)b.n_steps * I.off_x + (long long)b.g_step * I.nx : nullptr;
+    a.gee = b.g_ee ? b.g_ee + (long long)I.index * b.n_steps + b.g_step : nullptr;
+    a.E_prev = b.E_prev + (long long)b.n_steps * I.off_x + (long long)b.E_prev_step * I.nx;
+    a.gH = b.g_H + I.off_x;
+    a.gE_out = b.gE + I.off_x;
+    strip_bwd_body<kStripEnsRows, kStripEnsThreads>(a, smem, &s_last, m.y, m.z);
+}
+
+__global__ void __launch_bounds__(kFieldThreads)
+    vp_strip_ens_field_kernel(const StripInst* __restrict__ insts, const int2* __restrict__ fmap,
+                              const BatchStep<float> b, int adjoint) {
+    const int2 m = __ldg(fmap + blockIdx.x);   // (instance, 32-row block)
+    const StripInst& I = insts[m.x];
+    StripFieldArgs f{};
+    f.nx = I.nx;
+    f.nv = I.nv;
+    f.adjoint = adjoint;
+    f.ctab = I.ctab;
+    f.dx = I.dx;
+    if (adjoint) {
+        f.x = b.gE + I.off_x;
+        f.grho_out = b.grho_out + I.off_x;
+    } else {
+        f.x = b.rho + I.off_x;
+        f.H = b.H + I.off_x;
+        f.dtdv = I.dtdv;
+        f.E_out = b.E_out + (long long)b.E_out_mul * I.off_x + (long long)b.E_out_step * I.nx;
+        f.E_hist_out = b.E_hist ? b.E_hist + (long long)b.n_steps * I.off_x + (long long)b.hist_step * I.nx : nullptr;
+        f.vsh_out = b.vsh_out + (long long)b.vsh_out_mul * I.off_x + (long long)b.vsh_out_step * I.nx;
+        f.ee_out = b.ee_hist ? b.ee_hist + (long long)I.index * b.n_steps + b.hist_step : nullptr;
+        f.eep = b.eep + I.off_eep;
+        f.counter = b.fctr + I.index;
+    }
+    strip_field_body(f, m.y, I.field_ctas);
+}
+
+// The field of a whole small instance (nx <= kStripSmallField) in one CTA: thread i sums row i,
+// E_i = sum_k c[(i - k) mod nx] x_k (adjoint: c[(k - i) mod nx]), from x and the coefficient table
+// ctab[1 .. 2 nx) staged in shared memory, in four interleaved partial sums (k mod 4) added in a
+// fixed order; the energy is a fixed-order block sum. blockIdx.x is the instance.
+__global__ void __launch_bounds__(kStripSmallField)
+    vp_strip_ens_field_small_kernel(const StripInst* __restrict__ insts, const BatchStep<float> b, int adjoint) {
+    __shared__ float xs[kStripSmallField];
+    __shared__ float cs[2 * kStripSmallField];
+    __shared__ double red[kStripSmallField / 32];
+    const StripInst& I = insts[blockIdx.x];
+    const int nx = I.nx, t = threadIdx.x;
+    const float* x = adjoint ? b.gE + I.off_x : b.rho + I.off_x;
+    for (int k = t; k < nx; k += blockDim.x) xs[k] = __ldcg(x + k);
+    for (int u = t; u < 2 * nx - 1; u += blockDim.x) cs[u] = __ldg(I.ctab + 1 + u);   // cs[u] = c[(u + 1 - nx) mod nx]
+    __syncthreads();
+    double e2 = 0.0;
+    if (t < nx) {
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+        // forward: coefficient (t, k) = cs[nx - 1 + t - k]; adjoint: cs[nx - 1 + k - t]
+        const int base = nx - 1 + (adjoint ? -t : t), step = adjoint ? 1 : -1;
+#pragma unroll 4
+        for (int k = 0; k < nx; ++k) acc[k & 3] += cs[base + step * k] * xs[k];
+        const float E = (acc[0] + acc[1]) + (acc[2] + acc[3]);
+        if (adjoint) {
+            b.grho_out[I.off_x + t] = E;
+        } else {
+            const float Et = E + __ldg(b.H + I.off_x + t);
+            b.E_out[(long long)b.E_out_mul * I.off_x + (long long)b.E_out_step * nx + t] = E;
+            if (b.E_hist) b.E_hist[(long long)b.n_steps * I.off_x + (long long)b.hist_step * nx + t] = Et;
+            b.vsh_out[(long long)b.vsh_out_mul * I.off_x + (long long)b.vsh_out_step * nx + t] =
+                make_vshift<float>(Et, I.dtdv, I.nv);
+            e2 = (double)(trap_w<float>(t, nx) * E * E);
+        }
+    }
+    if (adjoint || b.ee_hist == nullptr) return;
+    e2 = warp_sum(e2);
+    if ((t & 31) == 0) red[t >> 5] = e2;
+    __syncthreads();
+    if (t == 0) {
+        double sum = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) sum += red[w];
+        b.ee_hist[(long long)I.index * b.n_steps + b.hist_step] = (float)(0.5 * sum * (double)I.dx);
     }
 }
 
@@ -878,6 +1037,56 @@ cudaError_t launch_strip_bwd(const StripBwdArgs& args, const StripHost& sh, cuda
 cudaError_t launch_strip_field(const StripFieldArgs& a, const StripHost& sh, cudaStream_t s) {
     if (a.nx % kStripFieldRows != 0 || a.nx % 8 != 0) return cudaErrorInvalidValue;
     vp_strip_field_kernel<<<sh.field_ctas, kFieldThreads, 0, s>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+size_t strip_ens_fwd_bytes(int ring_rows) { return strip_fwd_bytes(ring_rows, kStripEnsRows, kStripEnsThreads); }
+size_t strip_ens_bwd_bytes(int ring_rows) { return strip_bwd_bytes(ring_rows, kStripEnsRows, kStripEnsThreads); }
+
+int strip_ens_occupancy(bool fwd, size_t smem) {
+    int n = 0;
+    cudaError_t e;
+    if (fwd) {
+        e = cudaFuncSetAttribute(vp_strip_ens_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kStripMaxSmem);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, vp_strip_ens_fwd_kernel, kStripEnsThreads, smem);
+    } else {
+        e = cudaFuncSetAttribute(vp_strip_ens_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kStripMaxSmem);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, vp_strip_ens_bwd_kernel, kStripEnsThreads, smem);
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+cudaError_t launch_strip_ens_fwd(const StripInst* insts, const int4* map, int n_ctas, size_t smem,
+                                 const BatchStep<float>& b, cudaStream_t s) {
+    vp_strip_ens_fwd_kernel<<<n_ctas, kStripEnsThreads, smem, s>>>(insts, map, b);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_strip_ens_bwd(const StripInst* insts, const int4* map, int n_ctas, size_t smem,
+                                 const BatchStep<float>& b, cudaStream_t s) {
+    vp_strip_ens_bwd_kernel<<<n_ctas, kStripEnsThreads, smem, s>>>(insts, map, b);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_strip_ens_field(const StripInst* insts, const int2* fmap, int n_ctas, const BatchStep<float>& b,
+                                   int adjoint, cudaStream_t s) {
+    vp_strip_ens_field_kernel<<<n_ctas, kFieldThreads, 0, s>>>(insts, fmap, b, adjoint);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_strip_ens_field_small(const StripInst* insts, int n_inst, const BatchStep<float>& b, int adjoint,
+                                         cudaStream_t s) {
+    vp_strip_ens_field_small_kernel<<<n_inst, kStripSmallField, 0, s>>>(insts, b, adjoint);
     count_launch();
     return cudaGetLastError();
 }

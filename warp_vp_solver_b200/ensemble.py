@@ -108,14 +108,18 @@ class Ensemble:
         return {f: getattr(c, f) for f, _ in _capi.BatchConfig._fields_}
 
     def set_config(self, rows_per_tile: int | None = None, chunk_cols: int | None = None,
-                   threads: int | None = None, ctas_per_sm: int | None = None) -> None:
-        """Change the tile shape (None keeps the current value). Invalidates captured graphs."""
+                   threads: int | None = None, ctas_per_sm: int | None = None,
+                   strip: int | None = None) -> None:
+        """Change the tile shape (None keeps the current value); ``strip=1`` runs the steps on the
+        strip kernels (where every instance qualifies), ``strip=0`` on the tile kernels.
+        Invalidates captured graphs."""
         cur = self.get_config()
         c = _capi.BatchConfig()
         c.rows_per_tile = cur["rows_per_tile"] if rows_per_tile is None else int(rows_per_tile)
         c.chunk_cols = cur["chunk_cols"] if chunk_cols is None else int(chunk_cols)
         c.threads = cur["threads"] if threads is None else int(threads)
         c.ctas_per_sm = cur["ctas_per_sm"] if ctas_per_sm is None else int(ctas_per_sm)
+        c.strip = cur["strip"] if strip is None else int(strip)
         with torch.cuda.device(self.device):
             _capi.check(self.lib.vp_batch_set_config(self._h, ctypes.byref(c)))
         self._ws = {}
