@@ -69,6 +69,7 @@ struct vp_plan {
     long long mx_lo = 0, mx_hi = 0;  // extremes of the unreduced x half-step offsets floor(-s_j)
     int res_threads = 0;
     size_t res_smem = 0;
+    int res_vrows = 0;      // the resident forward computes the v step once per (row, column)
     // device tables (owned)
     double* d_feq = nullptr;   // nv (x-invariant) or nx*nv
     double* d_vs = nullptr;    // nv
@@ -198,8 +199,11 @@ static void res_halo_rows(const vp_plan* p, int* lo, int* hi) {
 }
 
 // Checks that a cluster-resident configuration of cn CTAs can launch; returns its shared memory
-// (0 when it cannot).
-static size_t res_config_ok(const vp_plan* p, int cn) {
+// (0 when it cannot). *vrows is set when the forward's phase-A plane (the v step of the local rows,
+// float32 with an x-invariant f_eq, 4-column quads tiling the block) fits as well; the shared
+// memory returned then includes it.
+static size_t res_config_ok(const vp_plan* p, int cn, int* vrows) {
+    *vrows = 0;
     if (cn < 2 || cn > 16 || (cn & (cn - 1)) != 0 || p->nx % cn != 0) return 0;
     const int Rc = p->nx / cn;
     if (!res_rows_supported(Rc)) return 0;
@@ -208,12 +212,21 @@ static size_t res_config_ok(const vp_plan* p, int cn) {
     int hlo = 0, hhi = 0;
     res_halo_rows(p, &hlo, &hhi);
     if (hlo + hhi >= p->nx) return 0;   // local rows of a CTA span less than two periods
-    const size_t smem = res_smem_size(p->nx, p->nv, Rc, hlo + hhi, real_size(p));
+    const size_t smem = res_smem_size(p->nx, p->nv, Rc, hlo + hhi, real_size(p), false);
     if (smem > kMaxSmemPerCta) return 0;
-    if (res_threads(Rc, p->nv) == 0) return 0;
+    const int threads = res_threads(Rc, p->nv);
+    if (threads == 0) return 0;
     const int n = p->dtype == VP_F64 ? res_max_clusters<double>(p->feq2d != 0, cn, Rc, p->nv, smem)
                                      : res_max_clusters<float>(p->feq2d != 0, cn, Rc, p->nv, smem);
-    return n > 0 ? smem : 0;
+    if (n <= 0) return 0;
+    if (p->dtype == VP_F32 && !p->feq2d && p->nv % 4 == 0 && threads % (p->nv / 4) == 0) {
+        const size_t smem_v = res_smem_size(p->nx, p->nv, Rc, hlo + hhi, real_size(p), true);
+        if (smem_v <= kMaxSmemPerCta && res_max_clusters<float>(false, cn, Rc, p->nv, smem_v) > 0) {
+            *vrows = 1;
+            return smem_v;
+        }
+    }
+    return smem;
 }
 
 
@@ -516,6 +529,7 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
         r.dtdv = (T)(p->dt / p->dv);
         res_halo_rows(p, &r.h_lo, &r.h_hi);
         r.mx_lo = (int)p->mx_lo;
+        r.vrows = p->res_vrows;
         VP_CUDA(launch_res_fwd<T>(r, p->feq2d != 0, p->res_cn, p->res_threads, p->res_smem, s),
                 "cluster-resident forward launch");
         return VP_OK;
@@ -1206,11 +1220,13 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
     // cluster-resident path: the largest cluster (16, 8, 4, 2 CTAs) whose per-CTA share of the
     // state fits in shared memory and that the occupancy calculator accepts
     for (int cn : {16, 8, 4, 2}) {
-        const size_t smem = res_config_ok(p, cn);
+        int vrows = 0;
+        const size_t smem = res_config_ok(p, cn, &vrows);
         if (smem > 0) {
             p->res_cn = cn;
             p->res_threads = res_threads(nx / cn, nv);
             p->res_smem = smem;
+            p->res_vrows = vrows;
             break;
         }
     }
@@ -1368,8 +1384,9 @@ int vp_plan_set_config(vp_plan* plan, const vp_launch_config* cfg) {
     if (ch < 1 || ch > plan->nv) return set_err(VP_ERR_ARG, "n_chunks must be in [1, nv] (got %d)", ch);
     const int cn = cfg->cluster_size;
     size_t res_smem = 0;
+    int res_vrows = 0;
     if (cn != 0) {
-        res_smem = res_config_ok(plan, cn);
+        res_smem = res_config_ok(plan, cn, &res_vrows);
         if (res_smem == 0)
             return set_err(VP_ERR_ARG, "cluster_size=%d is not usable for a %dx%d grid (must be a power of two "
                                        "in [2,16] dividing nx into 1, 2, 4, 8, 16 or 32 rows per CTA whose "
@@ -1425,6 +1442,7 @@ int vp_plan_set_config(vp_plan* plan, const vp_launch_config* cfg) {
     plan->strip_on = cfg->strip_rows != 0 ? 1 : 0;
     plan->res_cn = cn;
     plan->res_smem = res_smem;
+    plan->res_vrows = res_vrows;
     plan->res_threads = cn ? res_threads(plan->nx / cn, plan->nv) : 0;
     LaunchCfg c{};
     c.R = R;

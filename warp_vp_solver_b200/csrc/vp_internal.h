@@ -472,6 +472,7 @@ template <typename T> struct ResFwdArgs {
     T dv, dx, dtdv;
     int h_lo, h_hi;         // halo rows kept below / above a CTA's own rows
     int mx_lo;              // smallest unreduced x half-step offset (recovers signed offsets)
+    int vrows;              // 1: v step once per (row, column) into a shared plane (phase A)
 };
 
 template <typename T> struct ResBwdArgs {
@@ -502,7 +503,7 @@ cudaError_t launch_res_fwd(const ResFwdArgs<T>& a, bool feq2d, int cn, int threa
 template <typename T>
 cudaError_t launch_res_bwd(const ResBwdArgs<T>& a, bool feq2d, int cn, int threads, size_t smem,
                            cudaStream_t s);
-size_t res_smem_size(int nx, int nv, int Rc, int halo_rows, size_t real_size);
+size_t res_smem_size(int nx, int nv, int Rc, int halo_rows, size_t real_size, bool vrows);
 template <typename T>
 int res_max_clusters(bool feq2d, int cn, int rc, int nv, size_t smem);
 bool res_rows_supported(int rc);

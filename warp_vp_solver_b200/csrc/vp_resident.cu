@@ -58,6 +58,7 @@ template <typename T> struct ResSmem {
     T* dfeq;         // nv: f_eq[j+1] - f_eq[j] rounded from float64 (periodic)
     double* eep;     // 4 partial energies of the own rows (step s in slot s % 4; read by CTA 0)
     T* own;          // RC: accumulated g_H of the own rows (adjoint)
+    T* po;           // W rows: the v step of the current plane (forward: o), computed once per row
 };
 
 __host__ __device__ inline size_t res_align(size_t x) { return (x + 15) & ~(size_t)15; }
@@ -66,7 +67,8 @@ __host__ __device__ inline size_t res_align(size_t x) { return (x + 15) & ~(size
 // thread up (their register arrays need more than the 64 registers a 1024-thread CTA allows).
 __host__ __device__ constexpr int res_max_threads(int rpt) { return rpt >= 8 ? 512 : 1024; }
 
-__host__ __device__ inline size_t res_smem_bytes(int nx, int nv, int RC, int W, size_t rs) {
+// po: with the plane of phase-A results (forward float32 with an x-invariant f_eq).
+__host__ __device__ inline size_t res_smem_bytes(int nx, int nv, int RC, int W, size_t rs, bool po) {
     size_t b = 0;
     b += res_align((size_t)W * nv * rs) * 2;
     b += res_align((size_t)RC * nv * rs);
@@ -78,11 +80,12 @@ __host__ __device__ inline size_t res_smem_bytes(int nx, int nv, int RC, int W, 
     b += res_align((size_t)nv * rs);
     b += res_align((size_t)4 * 8);
     b += res_align((size_t)RC * rs);
+    if (po) b += res_align((size_t)W * nv * rs);
     return b;
 }
 
 template <typename T>
-__device__ ResSmem<T> res_carve(unsigned char* smem, int nx, int nv, int RC, int W) {
+__device__ ResSmem<T> res_carve(unsigned char* smem, int nx, int nv, int RC, int W, bool po) {
     ResSmem<T> s;
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -103,6 +106,7 @@ __device__ ResSmem<T> res_carve(unsigned char* smem, int nx, int nv, int RC, int
     s.dfeq = reinterpret_cast<T*>(take((size_t)nv * sizeof(T)));
     s.eep = reinterpret_cast<double*>(take((size_t)4 * sizeof(double)));
     s.own = reinterpret_cast<T*>(take((size_t)RC * sizeof(T)));
+    s.po = po ? reinterpret_cast<T*>(take((size_t)W * nv * sizeof(T))) : nullptr;
     return s;
 }
 
@@ -342,6 +346,53 @@ __device__ void res_init_tables(ResSmem<T>& S, const PoissonTables<T>& P, const 
     }
 }
 
+// Phase A of a float32 step with an x-invariant f_eq: o = V(h) + [V(f_eq) - f_eq] of every local
+// row of `cur` into S.po, computed once per (row, column) instead of once per thread window. Thread
+// t takes the 4 columns j0 = 4 (t mod nv/4) .. j0 + 3 and rows t / (nv/4), + blockDim / (nv/4), ...,
+// so a warp works on one row (one shift) at a time. The arithmetic is the per-cell form of the
+// thread-window code (lerp of the two source cells plus res_vcorr), so the results are the same
+// bits. Needs nv % 4 == 0 and blockDim.x a multiple of nv / 4.
+__device__ __forceinline__ void res_v_rows(const ResSmem<float>& S, const float* cur, int nv, int W) {
+    const int nq = nv >> 2;
+    const int q = threadIdx.x % nq, j0 = 4 * q;
+    const int lstep = blockDim.x / nq;
+    const int jm = j0 == 0 ? nv - 1 : j0 - 1, jp = j0 + 4 == nv ? 0 : j0 + 4;
+#pragma unroll 1
+    for (int l = threadIdx.x / nq; l < W; l += lstep) {
+        const VShift<float> v = S.vsh[l];
+        const float* hr = cur + (size_t)l * nv;
+        float4 o;
+        if (v.m == 0) {
+            const float4 h = *reinterpret_cast<const float4*>(hr + j0);
+            const float4 dd = *reinterpret_cast<const float4*>(S.dfeq + j0);
+            const float t = v.t;
+            o.x = lerp(h.x, h.y, t) + t * dd.x;
+            o.y = lerp(h.y, h.z, t) + t * dd.y;
+            o.z = lerp(h.z, h.w, t) + t * dd.z;
+            o.w = lerp(h.w, hr[jp], t) + t * dd.w;
+        } else if (v.m == nv - 1) {
+            const float4 h = *reinterpret_cast<const float4*>(hr + j0);
+            const float4 dd = *reinterpret_cast<const float4*>(S.dfeq + j0);
+            const float t = v.t, tm = v.t - 1.f;
+            o.x = lerp(hr[jm], h.x, t) + tm * S.dfeq[jm];
+            o.y = lerp(h.x, h.y, t) + tm * dd.x;
+            o.z = lerp(h.y, h.z, t) + tm * dd.y;
+            o.w = lerp(h.z, h.w, t) + tm * dd.z;
+        } else {
+            float r[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int j = j0 + e;
+                const int c0 = wrap1(j + v.m, nv);
+                const int c1 = c0 + 1 == nv ? 0 : c0 + 1;
+                r[e] = lerp(hr[c0], hr[c1], v.t) + res_vcorr<float, false>(S, nullptr, 0, 0, j, c0, c1, v, nv);
+            }
+            o = make_float4(r[0], r[1], r[2], r[3]);
+        }
+        *reinterpret_cast<float4*>(S.po + (size_t)l * nv + j0) = o;
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // Forward
 // ---------------------------------------------------------------------------------------------
@@ -408,7 +459,10 @@ __global__ void __launch_bounds__(res_max_threads(RPT)) vp_res_fwd_kernel(const 
     const bool colv = j < nv;
     const int cw = j >> 5, ncw = NVP >> 5;      // warp column group, groups per row
     const bool out_warp = (int)(threadIdx.x >> 5) == (int)(blockDim.x >> 5) - 1;
-    ResSmem<T> S = res_carve<T>(smem, nx, nv, RC, hl + RC + a.h_hi);
+    const int W = hl + RC + a.h_hi;
+    // the v step by rows (phase A) when the host gave the block the plane for it
+    const bool vrows = a.vrows != 0;
+    ResSmem<T> S = res_carve<T>(smem, nx, nv, RC, W, vrows);
     T* Hb[2] = {S.p0, S.p1};   // h of even / odd steps, local rows (own rows read remotely)
     T* red = S.p2;             // row partials of the warps
     res_init_tables<T>(S, a.P, a.feq, FEQ2D, nx, nv);
@@ -469,19 +523,33 @@ __global__ void __launch_bounds__(res_max_threads(RPT)) vp_res_fwd_kernel(const 
 #pragma unroll
         for (int k = 0; k < RPT; ++k) wv[k] = T(0);
         int dq = 0;
+        if constexpr (sizeof(T) == 4 && !FEQ2D) {
+            if (vrows) {
+                res_v_rows(S, cur, nv, W);   // phase A: the v step once per (row, column)
+                __syncthreads();
+            }
+        }
         if (colv) {
             // o on rows g+2m .. g+2m+RPT+1: local rows l0 .. l0+RPT+1 (own or halo)
             T o[RPT + 2];
             const int l0 = hl + rt + 2 * sm;
+            bool from_plane = false;
+            if constexpr (sizeof(T) == 4 && !FEQ2D) from_plane = vrows;
+            if (from_plane) {
+                const T* op = S.po + (size_t)l0 * nv + j;
 #pragma unroll
-            for (int k = 0; k < RPT + 2; ++k) {
-                const int l = l0 + k;
-                const VShift<T> v = S.vsh[l];
-                const T* hr = cur + (size_t)l * nv;
-                const int c0 = wrap1(j + v.m, nv);
-                const int c1 = c0 + 1 == nv ? 0 : c0 + 1;
-                const int q = FEQ2D ? res_grow(gr0, hl, l, nx) : 0;
-                o[k] = lerp(hr[c0], hr[c1], v.t) + res_vcorr<T, FEQ2D>(S, a.feq, a.feq_rs, q, j, c0, c1, v, nv);
+                for (int k = 0; k < RPT + 2; ++k) o[k] = op[(size_t)k * nv];
+            } else {
+#pragma unroll
+                for (int k = 0; k < RPT + 2; ++k) {
+                    const int l = l0 + k;
+                    const VShift<T> v = S.vsh[l];
+                    const T* hr = cur + (size_t)l * nv;
+                    const int c0 = wrap1(j + v.m, nv);
+                    const int c1 = c0 + 1 == nv ? 0 : c0 + 1;
+                    const int q = FEQ2D ? res_grow(gr0, hl, l, nx) : 0;
+                    o[k] = lerp(hr[c0], hr[c1], v.t) + res_vcorr<T, FEQ2D>(S, a.feq, a.feq_rs, q, j, c0, c1, v, nv);
+                }
             }
             // d on rows g+m .. g+m+RPT (= f_{n+1} - f_eq)
             dq = wrap1(g + m, nx);
@@ -673,7 +741,7 @@ __global__ void __launch_bounds__(res_max_threads(RPT)) vp_res_bwd_kernel(const 
     const int g = gr0 + rt;
     const bool colv = j < nv;
     const int cw = j >> 5, ncw = NVP >> 5;
-    ResSmem<T> S = res_carve<T>(smem, nx, nv, RC, W);
+    ResSmem<T> S = res_carve<T>(smem, nx, nv, RC, W, false);
     T* Wb[2] = {S.p0, S.p1};   // cotangent on the v-step output of even / odd steps, local rows
     T* red = S.p2;             // row partials of the warps
     res_init_tables<T>(S, a.P, a.feq, FEQ2D, nx, nv);
@@ -912,8 +980,8 @@ cudaError_t launch_res_bwd(const ResBwdArgs<T>& a, bool feq2d, int cn, int threa
     return cudaErrorInvalidValue;
 }
 
-size_t res_smem_size(int nx, int nv, int Rc, int halo_rows, size_t real_size) {
-    return res_smem_bytes(nx, nv, Rc, Rc + halo_rows, real_size);
+size_t res_smem_size(int nx, int nv, int Rc, int halo_rows, size_t real_size, bool vrows) {
+    return res_smem_bytes(nx, nv, Rc, Rc + halo_rows, real_size, vrows);
 }
 
 template int res_max_clusters<float>(bool, int, int, int, size_t);

@@ -895,29 +895,41 @@ __global__ void __launch_bounds__(kFieldThreads)
     strip_field_body(f, m.y, I.field_ctas);
 }
 
-// The field of a whole small instance (nx <= kStripSmallField) in one CTA: thread i sums row i,
-// E_i = sum_k c[(i - k) mod nx] x_k (adjoint: c[(k - i) mod nx]), from x and the coefficient table
-// ctab[1 .. 2 nx) staged in shared memory, in four interleaved partial sums (k mod 4) added in a
-// fixed order; the energy is a fixed-order block sum. blockIdx.x is the instance.
-__global__ void __launch_bounds__(kStripSmallField)
+// The field of a whole small instance (nx <= kStripSmallField) in one CTA of 4 x kStripSmallField
+// threads: part p = threadIdx.x / kStripSmallField of row i sums k in [p nx / 4, (p + 1) nx / 4) of
+// E_i = sum_k c[(i - k) mod nx] x_k (adjoint: c[(k - i) mod nx]) from x and the coefficient table
+// ctab[1 .. 2 nx) staged in shared memory, in two interleaved partial sums; the four parts are
+// added in a fixed order and the energy is a fixed-order block sum. blockIdx.x is the instance.
+__global__ void __launch_bounds__(4 * kStripSmallField)
     vp_strip_ens_field_small_kernel(const StripInst* __restrict__ insts, const BatchStep<float> b, int adjoint) {
-    __shared__ float xs[kStripSmallField];
-    __shared__ float cs[2 * kStripSmallField];
-    __shared__ double red[kStripSmallField / 32];
+    constexpr int NF = kStripSmallField;
+    __shared__ float xs[NF];
+    __shared__ float cs[2 * NF];
+    __shared__ float ps[4][NF];
+    __shared__ double red[NF / 32];
     const StripInst& I = insts[blockIdx.x];
-    const int nx = I.nx, t = threadIdx.x;
+    const int nx = I.nx, t = threadIdx.x % NF, part = threadIdx.x / NF;
     const float* x = adjoint ? b.gE + I.off_x : b.rho + I.off_x;
-    for (int k = t; k < nx; k += blockDim.x) xs[k] = __ldcg(x + k);
-    for (int u = t; u < 2 * nx - 1; u += blockDim.x) cs[u] = __ldg(I.ctab + 1 + u);   // cs[u] = c[(u + 1 - nx) mod nx]
+    for (int k = threadIdx.x; k < nx; k += blockDim.x) xs[k] = __ldcg(x + k);
+    for (int u = threadIdx.x; u < 2 * nx - 1; u += blockDim.x) cs[u] = __ldg(I.ctab + 1 + u);   // c[(u + 1 - nx) mod nx]
     __syncthreads();
-    double e2 = 0.0;
     if (t < nx) {
-        float acc[4] = {0.f, 0.f, 0.f, 0.f};
         // forward: coefficient (t, k) = cs[nx - 1 + t - k]; adjoint: cs[nx - 1 + k - t]
         const int base = nx - 1 + (adjoint ? -t : t), step = adjoint ? 1 : -1;
+        const int k0 = part * (nx / 4), k1 = k0 + nx / 4;
+        float a0 = 0.f, a1 = 0.f;
 #pragma unroll 4
-        for (int k = 0; k < nx; ++k) acc[k & 3] += cs[base + step * k] * xs[k];
-        const float E = (acc[0] + acc[1]) + (acc[2] + acc[3]);
+        for (int k = k0; k < k1; k += 2) {
+            a0 += cs[base + step * k] * xs[k];
+            a1 += cs[base + step * (k + 1)] * xs[k + 1];
+        }
+        ps[part][t] = a0 + a1;
+    }
+    __syncthreads();
+    if (part != 0) return;
+    double e2 = 0.0;
+    if (t < nx) {
+        const float E = (ps[0][t] + ps[1][t]) + (ps[2][t] + ps[3][t]);
         if (adjoint) {
             b.grho_out[I.off_x + t] = E;
         } else {
@@ -932,10 +944,10 @@ __global__ void __launch_bounds__(kStripSmallField)
     if (adjoint || b.ee_hist == nullptr) return;
     e2 = warp_sum(e2);
     if ((t & 31) == 0) red[t >> 5] = e2;
-    __syncthreads();
+    asm volatile("bar.sync 1, %0;" ::"r"(NF) : "memory");   // the part-0 warps only
     if (t == 0) {
         double sum = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) sum += red[w];
+        for (int w = 0; w < NF / 32; ++w) sum += red[w];
         b.ee_hist[(long long)I.index * b.n_steps + b.hist_step] = (float)(0.5 * sum * (double)I.dx);
     }
 }
@@ -1086,7 +1098,7 @@ cudaError_t launch_strip_ens_field(const StripInst* insts, const int2* fmap, int
 
 cudaError_t launch_strip_ens_field_small(const StripInst* insts, int n_inst, const BatchStep<float>& b, int adjoint,
                                          cudaStream_t s) {
-    vp_strip_ens_field_small_kernel<<<n_inst, kStripSmallField, 0, s>>>(insts, b, adjoint);
+    vp_strip_ens_field_small_kernel<<<n_inst, 4 * kStripSmallField, 0, s>>>(insts, b, adjoint);
     count_launch();
     return cudaGetLastError();
 }
