@@ -492,6 +492,30 @@ def measure_large(args, rank, local_rank, world):
             "l2": "flushed between timed steps (256 MiB write, untimed)"}
 
 
+def measure_config(args, rank, local_rank, world, workload):
+    """Another benchmark configuration at its full size beside the headline (C1 forward, C3
+    checkpointed forward + adjoint, C4 uneven ensemble forward + adjoint): default launch shape,
+    3 warm-up and 3 timed steps, device-timed, end to end through the public API included."""
+    sub = argparse.Namespace(**vars(args))
+    sub.workload, sub.steps, sub.warmup = workload, 3, 3
+    sub.no_autotune = True
+    sub.cluster_size = sub.stage_rows = sub.strip_rows = sub.checkpoint_every = None
+    if workload == "c4":
+        line, wl = run_ensemble(sub, rank, local_rank, world)
+    else:
+        line, wl = run_ours(sub, rank, local_rank, world)
+    cfg = line["config"]
+    keep = ("workload", "path", "checkpoint_every", "fwd_ms_per_step", "bwd_ms_per_step", "instances")
+    out = {"metric": line["metric"], "value": line["value"], "unit": line["unit"], "ms_per_step": line["ms_per_step"],
+           "e2e": line.get("e2e"), "config": {k: cfg[k] for k in keep if k in cfg},
+           "clocks": line["clocks"], "steps": 3, "warmup": 3}
+    for k in ("roofline", "roofline_fwd", "roofline_bwd"):
+        if line.get(k) is not None:
+            out[k] = {q: line[k][q] for q in ("kernel", "achieved", "peak", "unit", "frac", "avg_launch_us")
+                      if q in line[k]}
+    return out
+
+
 def measure_c5(args, rank, local_rank, world):
     """The surrogate-warm-started control against the plain adjoint loop (the C5 workload at
     its full size), per seed, with the one-off data generation and training reported beside the
@@ -932,6 +956,7 @@ def main():
             base = cpu_baseline
             if args.workload == "c2" and world == 1 and not args.no_extras:
                 line["roofline_large"] = measure_large(args, rank, local_rank, world)
+                line["configs"] = {w: measure_config(args, rank, local_rank, world, w) for w in ("c1", "c3", "c4")}
                 line["c5"] = measure_c5(args, rank, local_rank, world)
         if rank == 0 and world == 1 and not args.no_cpu_baseline and base is not None:
             v, cores, kind, sample = base(wl, args.cpu_seconds)

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define VP_ABI_VERSION 4
+#define VP_ABI_VERSION 5
 
 /* status codes */
 #define VP_OK 0
@@ -332,6 +332,68 @@ int vp_semilag_x(vp_plan* plan, const void* in, void* out, double dt, int adjoin
  * semilag_v_fused_adjoint_kernel, warp_vp_solver/kernels.py:244-273, 396-429). */
 int vp_semilag_v(vp_plan* plan, const void* in, const void* E_total, void* out, double dt,
                  int adjoint, const void* f_in, void* g_E, void* stream);
+
+/* --- x-slab decomposition ---------------------------------------------------------------- */
+
+/* One grid split into slabs of consecutive x rows, one slab per device (rank), for grids whose
+ * state does not fit one GPU. No counterpart in the reference, which keeps every array of a solve
+ * on one Warp device (warp_vp_solver/solver.py:170-203); each call below runs one piece of the
+ * reference's forward step (solver.py:573-609) or adjoint step (solver.py:814-929) on a slab.
+ *
+ * A slab owns grid rows [row0, row0 + n_rows). Its state arrays ("_ext", real[ext_rows * nv])
+ * hold `ghost` rows copied from the neighbour below, then the owned rows, then `ghost` rows
+ * copied from the neighbour above (periodic in x), then pad rows the calls never read for the
+ * owned rows: array row k is grid row (row0 - ghost + k) mod nx. Between calls the caller
+ * fills the ghost rows of the next call's input state from the neighbours' owned rows (the
+ * rows next to the boundary), and gathers every slab's row sums (real[n_rows] each) into one
+ * real[nx] array in grid-row order. The field of a step (E, E + H, ee, v shifts) is then solved
+ * by every rank on the same gathered sums, into a caller-held "field record" of field_bytes
+ * (256-byte aligned); records of past steps feed the adjoint. A slab belongs to its plan: destroy
+ * the slab first. Needs an x-invariant f_eq and the Strang scheme; the slab's per-column launch
+ * shape is the plan's at vp_slab_create. The calls allocate device memory for the slab's row
+ * buffers at vp_slab_create, and for one cell buffer on the first call that returns cells
+ * (f_rows, f_final_rows, g_f_iv_rows). */
+typedef struct vp_slab vp_slab;
+/* n_rows must be at least the ghost width 2 * (largest x half-step offset in cells) + 2. */
+int vp_slab_create(vp_plan* plan, int32_t row0, int32_t n_rows, vp_slab** out_slab);
+int vp_slab_destroy(vp_slab* slab);
+int vp_slab_geometry(const vp_slab* slab, int32_t* ghost_rows, int32_t* ext_rows, size_t* field_bytes);
+
+/* Forward prologue: h_0 = X(f_iv - f_eq) on the owned rows of h_ext and their trapezoid row
+ * sums. f_iv_ext: double[ext_rows * nv] with its ghost rows filled. */
+int vp_slab_forward_start(vp_slab* slab, const double* f_iv_ext, void* h_ext, void* row_sums, void* stream);
+/* Field of step n from the gathered row sums (real[nx]) and H (real[nx]): into field; E + H into
+ * E_hist_row (real[nx]) and ee into ee (real[1]) when not NULL. */
+int vp_slab_field(vp_slab* slab, const void* row_sums_all, const void* H, void* field, void* E_hist_row, void* ee,
+                  void* stream);
+/* Step n: from h_ext (h_n, ghost rows filled) and the field record of step n, h_{n+1} on the
+ * owned rows of h_out_ext (NULL on the last step) and its row sums (NULL: not needed, e.g. when
+ * replaying a checkpoint segment); f_{n+1} of the owned rows into f_rows (real[n_rows * nv]) and
+ * f_final_rows (double[n_rows * nv]) when not NULL. */
+int vp_slab_forward_step(vp_slab* slab, const void* h_ext, const void* field, void* h_out_ext, void* row_sums,
+                         void* f_rows, double* f_final_rows, void* stream);
+
+/* Adjoint prologue (n = T): w_{T-1} = X^T g on the owned rows of w_out_ext from the
+ * cotangent on f_final (g_f_ext, ghost rows filled; NULL = zero), and the slope row sums of
+ * the v step with h_{T-1} (h_prev_ext) and the field record of step T-1. */
+int vp_slab_backward_start(vp_slab* slab, const void* g_f_ext, const void* h_prev_ext, const void* field_prev,
+                           void* w_out_ext, void* slope_sums, void* stream);
+/* Adjoint field of step n-1 from the gathered slope sums (real[nx]): g_E_total = -dt/dv * sums
+ * + gE_hist_row, g_H += g_E_total, and grho (real[nx]) = Poisson^T(g_E_total + ee^T(gee)).
+ * gE_hist_row (real[nx]) and gee (real[1], the cotangent on ee of step n-1) may be NULL. */
+int vp_slab_backward_field(vp_slab* slab, const void* slope_sums_all, const void* field_prev, const void* gE_hist_row,
+                           const void* gee, void* g_H, void* grho, void* stream);
+/* Adjoint step n (1 <= n < T): w_{n-1} on the owned rows of w_out_ext and its slope row sums,
+ * from w_ext (w_n, ghost rows filled), the cotangent on f_hist[n-1] (g_f_ext, ghost rows
+ * filled; NULL = zero), grho of step n (real[nx]), the field records of steps n and n-1 and
+ * h_{n-1} (h_prev_ext). */
+int vp_slab_backward_step(vp_slab* slab, const void* w_ext, const void* g_f_ext, const void* grho,
+                          const void* field_n, const void* field_prev, const void* h_prev_ext, void* w_out_ext,
+                          void* slope_sums, void* stream);
+/* Adjoint epilogue (n = 0): the cotangent on f_iv's owned rows (real[n_rows * nv]) from w_0
+ * (ghost rows filled), grho of step 0 and the field record of step 0. */
+int vp_slab_backward_finish(vp_slab* slab, const void* w_ext, const void* grho, const void* field0, void* g_f_iv_rows,
+                            void* stream);
 
 /* --- launch configuration (autotuning) ---------------------------------------------------- */
 

@@ -23,7 +23,7 @@ VP_SCHEME_STRANG = 0
 VP_SCHEME_MERGED = 1
 VP_STATUS_NONFINITE_INPUT = 1
 VP_STATUS_WAIT_TIMEOUT = 2
-ABI_VERSION = 4   # VP_ABI_VERSION of the header these bindings follow
+ABI_VERSION = 5   # VP_ABI_VERSION of the header these bindings follow
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libvpb200.so")
 
@@ -112,6 +112,16 @@ SIGNATURES = {
                            c_size, c_vp]),
     "vp_backward": (c_int, [c_vp, c_vp, c_i32, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
                             c_vp, c_size, c_vp]),
+    "vp_slab_create": (c_int, [c_vp, c_i32, c_i32, ctypes.POINTER(c_vp)]),
+    "vp_slab_destroy": (c_int, [c_vp]),
+    "vp_slab_geometry": (c_int, [c_vp, ctypes.POINTER(c_i32), ctypes.POINTER(c_i32), ctypes.POINTER(c_size)]),
+    "vp_slab_forward_start": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "vp_slab_field": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "vp_slab_forward_step": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "vp_slab_backward_start": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "vp_slab_backward_field": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "vp_slab_backward_step": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "vp_slab_backward_finish": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "vp_forward_noalloc": (c_int, [c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "vp_forward_stream_history": (c_int, [c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp,
                                           c_vp, c_i32, c_vp, c_size, c_vp, c_vp]),

@@ -106,6 +106,7 @@ struct vp_plan {
     int2* d_echunk = nullptr;  // ensembles on the strip kernels: quad shift range per 128 columns
     std::vector<long long> host_msigned;   // unreduced x half-step offsets (re-shaping the paths)
     std::vector<double> host_tx;           // their weights
+    std::vector<long long> host_mxs;       // unreduced x half-step offsets of every plan (x slabs)
     unsigned long long wait_ns = 1000000000ull;   // limit of each device-side grid barrier wait
 };
 
@@ -1175,6 +1176,7 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
         if (mi < 0) mi += nx;
         mx[j] = (int)mi;
     }
+    p->host_mxs = m_signed;
     // full step of the merged-Strang scheme: s_j = v_j*dt/dx (semilag_x_full_kernel, kernels.py:535-556)
     std::vector<int> mxf(nv);
     std::vector<double> txf(nv);
@@ -2524,6 +2526,467 @@ int vp_batch_backward(vp_batch* b, const void* H, int32_t n_steps, const void* t
     return batch_backward_impl<float>(b, (const float*)H, n_steps, t, (const float*)g_f_final,
                                       (const float*)g_E_hist, (const float*)g_ee_hist, (float*)g_f_iv,
                                       (float*)g_H, w, s);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// x-slab decomposition: one grid split into slabs of rows, one per device. A slab's state arrays
+// hold its own rows plus `ghost` copied rows of each neighbour (and pad rows up to a multiple of
+// the per-column kernels' rows per CTA). The step kernels are the per-column ones, launched over
+// the slab's array as if it were a periodic grid of ext_rows rows with the x offsets reduced mod
+// ext_rows: the owned rows read only owned and ghost rows, so they see exactly what the one-grid
+// step sees; the ghost and pad rows' results are discarded. The caller exchanges ghost rows and
+// gathers the rows' sums between the calls; the field (Poisson, E, ee, v shifts) is solved on the
+// whole x grid by every rank on the same gathered sums.
+// ---------------------------------------------------------------------------------------------
+struct vp_slab {
+    vp_plan* plan = nullptr;
+    int row0 = 0, n_rows = 0, ghost = 0, ext_rows = 0, row_first = 0;
+    LaunchCfg cfg{};            // launch shape of the slab's per-column launches (rows per CTA fixed)
+    int tail_threads = 0;
+    size_t tail_smem = 0;
+    int tail_tw_stage = 0;
+    int* d_mx = nullptr;        // x half-step offsets reduced mod ext_rows      [nv]
+    void* d_part = nullptr;     // column-chunk partial sums                    [n_chunks][ext_rows]
+    void* d_vsh = nullptr;      // v shifts of step n in slab row order          [ext_rows]
+    void* d_vsh2 = nullptr;     // v shifts of step n-1 (adjoint)                [ext_rows]
+    void* d_grho = nullptr;     // cotangent on rho of step n                    [ext_rows]
+    void* d_gscratch = nullptr; // Poisson work area when the tail's is not in shared memory
+    void* d_cells = nullptr;    // f_{n+1} or g_f_iv over the slab's rows (allocated on first use)
+    double* d_cells64 = nullptr;// f_final over the slab's rows (allocated on first use)
+};
+
+namespace vpb {
+
+static size_t slab_field_vsh_bytes(const vp_plan* p) { return align256((size_t)p->nx * vshift_size(p)); }
+static size_t slab_field_bytes(const vp_plan* p) {
+    return slab_field_vsh_bytes(p) + align256((size_t)p->nx * real_size(p));
+}
+
+static void free_slab(vp_slab* sl) {
+    if (!sl) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(sl->plan->device);
+    for (void* q : {(void*)sl->d_mx, sl->d_part, sl->d_vsh, sl->d_vsh2, sl->d_grho, sl->d_gscratch, sl->d_cells,
+                    (void*)sl->d_cells64})
+        if (q) cudaFree(q);
+    cudaSetDevice(prev);
+    delete sl;
+}
+
+static int slab_check(vp_slab* sl, cudaStream_t s) {
+    if (!sl) return set_err(VP_ERR_ARG, "slab must not be NULL");
+    if (sl->plan->merged)
+        return set_err(VP_ERR_UNSUPPORTED, "x slabs run the Strang scheme only (the plan is set to the merged scheme)");
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != sl->plan->device)
+        return set_err(VP_ERR_ARG, "current device %d differs from the slab's device %d", cur, sl->plan->device);
+    (void)s;
+    return VP_OK;
+}
+
+template <typename T>
+static VShift<T>* field_vsh(const vp_plan* p, const void* field) {
+    return reinterpret_cast<VShift<T>*>(const_cast<void*>(field));
+}
+template <typename T>
+static T* field_E(const vp_plan* p, const void* field) {
+    return reinterpret_cast<T*>(static_cast<unsigned char*>(const_cast<void*>(field)) + slab_field_vsh_bytes(p));
+}
+
+template <typename T>
+static PoissonTables<T> slab_poisson(const vp_slab* sl) {
+    PoissonTables<T> P = poisson_tables<T>(sl->plan, nullptr, nullptr, sl->tail_smem > 0);
+    P.gscratch = static_cast<T*>(sl->d_gscratch);
+    return P;
+}
+
+// FwdArgs of a per-column launch over the slab's rows.
+template <typename T>
+static FwdArgs<T> slab_fwd_args(const vp_slab* sl) {
+    const vp_plan* p = sl->plan;
+    FwdArgs<T> a{};
+    a.nx = sl->ext_rows;
+    a.nv = p->nv;
+    a.n_chunks = sl->cfg.n_chunks;
+    a.chunk_cols = sl->cfg.chunk_cols;
+    a.mx = sl->d_mx;
+    a.tx = static_cast<const T*>(p->d_tx);
+    a.tx64 = p->d_tx64;
+    a.feq = p->d_feq;
+    a.feq_rs = 0;
+    a.counter = nullptr;   // no tail inside the launch: the field is solved on the gathered sums
+    a.dv = (T)p->dv;
+    a.dx = (T)p->dx;
+    a.dtdv = (T)(p->dt / p->dv);
+    return a;
+}
+
+template <typename T>
+static int slab_lazy_cells(vp_slab* sl, bool f64) {
+    const size_t n = (size_t)sl->ext_rows * sl->plan->nv;
+    if (f64 && sl->d_cells64 == nullptr)
+        VP_CUDA(cudaMalloc((void**)&sl->d_cells64, n * sizeof(double)), "cudaMalloc(slab f_final rows)");
+    if (!f64 && sl->d_cells == nullptr) VP_CUDA(cudaMalloc(&sl->d_cells, n * sizeof(T)), "cudaMalloc(slab cells)");
+    return VP_OK;
+}
+
+// Owned rows of a slab-ordered cell array into a caller's (n_rows, nv) array.
+static int slab_copy_owned(const vp_slab* sl, const void* ext, void* out, size_t elem, cudaStream_t s) {
+    const size_t row = (size_t)sl->plan->nv * elem;
+    VP_CUDA(cudaMemcpyAsync(out, static_cast<const unsigned char*>(ext) + (size_t)sl->ghost * row,
+                            (size_t)sl->n_rows * row, cudaMemcpyDeviceToDevice, s),
+            "slab owned-row copy");
+    return VP_OK;
+}
+
+template <typename T>
+static int slab_forward_impl(vp_slab* sl, int phase, const void* in_ext, const void* field, void* out_ext,
+                             void* row_sums, void* f_rows, double* f_final_rows, cudaStream_t s) {
+    const vp_plan* p = sl->plan;
+    FwdArgs<T> a = slab_fwd_args<T>(sl);
+    int rc;
+    if (phase == 0) {
+        a.f_iv = static_cast<const double*>(in_ext);
+        a.h_out = static_cast<T*>(out_ext);
+    } else {
+        VP_CUDA(launch_slab_gather_rows<T>(p->nx, sl->row_first, sl->ext_rows, field_vsh<T>(p, field),
+                                           static_cast<VShift<T>*>(sl->d_vsh), nullptr, nullptr, nullptr, nullptr, s),
+                "slab row gather launch");
+        a.h_in = static_cast<const T*>(in_ext);
+        a.h_out = static_cast<T*>(out_ext);
+        a.vsh = static_cast<const VShift<T>*>(sl->d_vsh);
+        if (f_rows != nullptr) {
+            if ((rc = slab_lazy_cells<T>(sl, false)) != VP_OK) return rc;
+            a.f_hist_n = static_cast<T*>(sl->d_cells);
+        }
+        if (f_final_rows != nullptr) {
+            if ((rc = slab_lazy_cells<T>(sl, true)) != VP_OK) return rc;
+            a.f_final = sl->d_cells64;
+        }
+    }
+    a.part = row_sums != nullptr ? static_cast<T*>(sl->d_part) : nullptr;
+    VP_CUDA(launch_fwd<T>(a, sl->cfg, phase, false, s), phase == 0 ? "slab forward start launch" : "slab forward step launch");
+    if (row_sums != nullptr && (phase == 0 || out_ext != nullptr))
+        VP_CUDA(launch_slab_row_sums<T>(static_cast<const T*>(sl->d_part), sl->cfg.n_chunks, sl->ext_rows, sl->ghost,
+                                        sl->n_rows, static_cast<T*>(row_sums), s),
+                "slab row sums launch");
+    if (f_rows != nullptr && (rc = slab_copy_owned(sl, sl->d_cells, f_rows, sizeof(T), s)) != VP_OK) return rc;
+    if (f_final_rows != nullptr && (rc = slab_copy_owned(sl, sl->d_cells64, f_final_rows, sizeof(double), s)) != VP_OK)
+        return rc;
+    return VP_OK;
+}
+
+template <typename T>
+static int slab_field_impl(vp_slab* sl, const T* sums, const T* H, void* field, T* E_hist_row, T* ee,
+                           cudaStream_t s) {
+    const vp_plan* p = sl->plan;
+    FwdArgs<T> a{};
+    a.nx = p->nx;
+    a.nv = p->nv;
+    a.n_chunks = 1;
+    a.part = const_cast<T*>(sums);
+    a.P = slab_poisson<T>(sl);
+    a.dv = (T)p->dv;
+    a.dx = (T)p->dx;
+    a.dtdv = (T)(p->dt / p->dv);
+    a.H = H;
+    a.E_out = field_E<T>(p, field);
+    a.E_hist_out = E_hist_row;
+    a.ee_out = ee;
+    a.vsh_out = field_vsh<T>(p, field);
+    VP_CUDA(launch_fwd_tail<T>(a, sl->tail_threads, sl->tail_smem, sl->tail_tw_stage != 0, s), "slab field launch");
+    return VP_OK;
+}
+
+template <typename T>
+static BwdArgs<T> slab_bwd_args(const vp_slab* sl) {
+    const vp_plan* p = sl->plan;
+    BwdArgs<T> b{};
+    b.nx = sl->ext_rows;
+    b.nv = p->nv;
+    b.n_chunks = sl->cfg.n_chunks;
+    b.chunk_cols = sl->cfg.chunk_cols;
+    b.mx = sl->d_mx;
+    b.tx = static_cast<const T*>(p->d_tx);
+    b.feq = p->d_feq;
+    b.feq_rs = 0;
+    b.part = static_cast<T*>(sl->d_part);
+    b.counter = nullptr;
+    b.dv = (T)p->dv;
+    b.dx = (T)p->dx;
+    b.neg_dt_dv = (T)(-p->dt / p->dv);
+    b.vtab = static_cast<const T*>(p->d_vtab);
+    return b;
+}
+
+// phase 0: prologue (n = T), 1: step n, 2: epilogue (n = 0); see vp_bwd_kernel.
+template <typename T>
+static int slab_backward_impl(vp_slab* sl, int phase, const void* w_ext, const void* g_ext, const T* grho,
+                              const void* field_n, const void* field_prev, const void* h_prev_ext, void* w_out_ext,
+                              void* slope_sums, void* g_f_iv_rows, cudaStream_t s) {
+    const vp_plan* p = sl->plan;
+    BwdArgs<T> b = slab_bwd_args<T>(sl);
+    int rc;
+    VP_CUDA(launch_slab_gather_rows<T>(
+                p->nx, sl->row_first, sl->ext_rows, phase != 0 ? field_vsh<T>(p, field_n) : nullptr,
+                static_cast<VShift<T>*>(sl->d_vsh), phase != 2 ? field_vsh<T>(p, field_prev) : nullptr,
+                static_cast<VShift<T>*>(sl->d_vsh2), phase != 0 ? grho : nullptr, static_cast<T*>(sl->d_grho), s),
+            "slab row gather launch");
+    b.vsh_n = static_cast<const VShift<T>*>(sl->d_vsh);
+    b.vsh_prev = static_cast<const VShift<T>*>(sl->d_vsh2);
+    b.grho = static_cast<const T*>(sl->d_grho);
+    b.w_in = static_cast<const T*>(w_ext);
+    b.h_prev = static_cast<const T*>(h_prev_ext);
+    b.w_out = static_cast<T*>(w_out_ext);
+    if (phase == 0) {
+        b.c_src = static_cast<const T*>(g_ext);
+    } else if (phase == 1) {
+        b.gfh = static_cast<const T*>(g_ext);
+    } else {
+        if ((rc = slab_lazy_cells<T>(sl, false)) != VP_OK) return rc;
+        b.gfiv_out = static_cast<T*>(sl->d_cells);
+    }
+    if (phase == 0 && g_ext == nullptr) {
+        // no cotangent on the final state: w_{T-1} = X^T(0) = 0 and the slope sums are 0
+        VP_CUDA(cudaMemsetAsync(w_out_ext, 0, (size_t)sl->ext_rows * p->nv * sizeof(T), s), "cudaMemsetAsync(w)");
+        VP_CUDA(cudaMemsetAsync(slope_sums, 0, (size_t)sl->n_rows * sizeof(T), s), "cudaMemsetAsync(slope sums)");
+        return VP_OK;
+    }
+    VP_CUDA(launch_bwd<T>(b, sl->cfg, phase, false, s), "slab adjoint launch");
+    if (phase == 2) return slab_copy_owned(sl, sl->d_cells, g_f_iv_rows, sizeof(T), s);
+    VP_CUDA(launch_slab_row_sums<T>(static_cast<const T*>(sl->d_part), sl->cfg.n_chunks, sl->ext_rows, sl->ghost,
+                                    sl->n_rows, static_cast<T*>(slope_sums), s),
+            "slab row sums launch");
+    return VP_OK;
+}
+
+template <typename T>
+static int slab_backward_field_impl(vp_slab* sl, const T* sums, const void* field_prev, const T* gE_hist_row,
+                                    const T* gee, T* g_H, T* grho, cudaStream_t s) {
+    const vp_plan* p = sl->plan;
+    BwdArgs<T> b{};
+    b.nx = p->nx;
+    b.nv = p->nv;
+    b.n_chunks = 1;
+    b.part = const_cast<T*>(sums);
+    b.P = slab_poisson<T>(sl);
+    b.dv = (T)p->dv;
+    b.dx = (T)p->dx;
+    b.neg_dt_dv = (T)(-p->dt / p->dv);
+    b.E_prev = field_E<T>(p, field_prev);
+    b.gE_hist = gE_hist_row;
+    b.gee = gee;
+    b.gH = g_H;
+    b.grho_out = grho;
+    VP_CUDA(launch_bwd_tail<T>(b, sl->tail_threads, sl->tail_smem, sl->tail_tw_stage != 0, s), "slab adjoint field launch");
+    return VP_OK;
+}
+
+}  // namespace vpb
+
+extern "C" {
+
+int vp_slab_create(vp_plan* plan, int32_t row0, int32_t n_rows, vp_slab** out) {
+    if (!plan || !out) return set_err(VP_ERR_ARG, "plan and out must not be NULL");
+    *out = nullptr;
+    if (plan->feq2d)
+        return set_err(VP_ERR_UNSUPPORTED, "x slabs need an x-invariant f_eq (one row of nv values)");
+    if (n_rows < 1 || row0 < 0 || row0 + (int64_t)n_rows > plan->nx)
+        return set_err(VP_ERR_ARG, "slab rows [%d, %d) do not lie in [0, %d)", row0, row0 + n_rows, plan->nx);
+    // rows a step reads around its own: x offsets m in [mx_lo, mx_hi]; the forward reads rows r + 2m
+    // .. r + 2m + 2 (v-step inputs of the two x half-steps), the adjoint rows r - 2m - 2 .. r - 2m
+    const long long g = std::max({-2 * plan->mx_lo, 2 * plan->mx_hi + 2, 1LL});
+    if (g > n_rows)
+        return set_err(VP_ERR_ARG,
+                       "a slab of %d rows is thinner than the %lld ghost rows a step reads from each neighbour "
+                       "(x shifts of up to %lld cells); use fewer, thicker slabs",
+                       n_rows, g, std::max(-plan->mx_lo, plan->mx_hi + 1));
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(plan->device);
+    vp_slab* sl = new (std::nothrow) vp_slab();
+    if (!sl) {
+        cudaSetDevice(prev);
+        return set_err(VP_ERR_ARG, "out of host memory");
+    }
+    sl->plan = plan;
+    sl->row0 = row0;
+    sl->n_rows = n_rows;
+    sl->ghost = (int)g;
+    sl->cfg = plan->cfg;
+    const int R = std::max(1, sl->cfg.R);
+    sl->ext_rows = (n_rows + 2 * sl->ghost + R - 1) / R * R;
+    sl->row_first = (int)(((long long)row0 - sl->ghost) % plan->nx + plan->nx) % plan->nx;
+    const size_t rs = real_size(plan);
+    if (plan->tail_inline) {
+        // the one-grid path solves the field inside the step launch, with the step's block size
+        sl->tail_threads = plan->cfg.threads;
+        sl->tail_smem = poisson_area_size(plan->nx, rs);
+    } else {
+        sl->tail_threads = plan->tail_threads;
+        sl->tail_smem = plan->tail_smem;
+        sl->tail_tw_stage = plan->tail_tw_stage;
+    }
+    std::vector<int> mx(plan->nv);
+    for (int j = 0; j < plan->nv; ++j) {
+        const long long m = plan->host_mxs[j];
+        mx[j] = (int)(((m % sl->ext_rows) + sl->ext_rows) % sl->ext_rows);
+    }
+    cudaError_t e = cudaSuccess;
+    auto alloc = [&](void** q, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(q, bytes);
+    };
+    alloc((void**)&sl->d_mx, (size_t)plan->nv * sizeof(int));
+    alloc(&sl->d_part, (size_t)sl->cfg.n_chunks * sl->ext_rows * rs);
+    alloc(&sl->d_vsh, (size_t)sl->ext_rows * vshift_size(plan));
+    alloc(&sl->d_vsh2, (size_t)sl->ext_rows * vshift_size(plan));
+    alloc(&sl->d_grho, (size_t)sl->ext_rows * rs);
+    if (sl->tail_smem == 0) alloc(&sl->d_gscratch, (size_t)2 * plan->nx * rs);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(sl->d_mx, mx.data(), mx.size() * sizeof(int), cudaMemcpyHostToDevice);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) {
+        free_slab(sl);
+        return cuda_err(e, "vp_slab_create");
+    }
+    *out = sl;
+    return VP_OK;
+}
+
+int vp_slab_destroy(vp_slab* slab) {
+    free_slab(slab);
+    return VP_OK;
+}
+
+int vp_slab_geometry(const vp_slab* slab, int32_t* ghost_rows, int32_t* ext_rows, size_t* field_bytes) {
+    if (!slab) return set_err(VP_ERR_ARG, "slab must not be NULL");
+    if (ghost_rows) *ghost_rows = slab->ghost;
+    if (ext_rows) *ext_rows = slab->ext_rows;
+    if (field_bytes) *field_bytes = slab_field_bytes(slab->plan);
+    return VP_OK;
+}
+
+int vp_slab_forward_start(vp_slab* slab, const double* f_iv_ext, void* h_ext, void* row_sums, void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int rc;
+    if ((rc = slab_check(slab, s)) != VP_OK) return rc;
+    const int dev = slab->plan->device;
+    if ((rc = check_dev_ptr(f_iv_ext, "f_iv_ext", dev)) || (rc = check_dev_ptr(h_ext, "h_ext", dev)) ||
+        (rc = check_dev_ptr(row_sums, "row_sums", dev)))
+        return rc;
+    if (slab->plan->dtype == VP_F64)
+        return slab_forward_impl<double>(slab, 0, f_iv_ext, nullptr, h_ext, row_sums, nullptr, nullptr, s);
+    return slab_forward_impl<float>(slab, 0, f_iv_ext, nullptr, h_ext, row_sums, nullptr, nullptr, s);
+}
+
+int vp_slab_field(vp_slab* slab, const void* row_sums_all, const void* H, void* field, void* E_hist_row, void* ee,
+                  void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int rc;
+    if ((rc = slab_check(slab, s)) != VP_OK) return rc;
+    const int dev = slab->plan->device;
+    if ((rc = check_dev_ptr(row_sums_all, "row_sums_all", dev)) || (rc = check_dev_ptr(H, "H", dev)) ||
+        (rc = check_dev_ptr(field, "field", dev)) || (rc = check_opt_ptr(E_hist_row, "E_hist_row", dev)) ||
+        (rc = check_opt_ptr(ee, "ee", dev)))
+        return rc;
+    if (((uintptr_t)field & 255) != 0) return set_err(VP_ERR_ARG, "field must be 256-byte aligned");
+    if (slab->plan->dtype == VP_F64)
+        return slab_field_impl<double>(slab, (const double*)row_sums_all, (const double*)H, field, (double*)E_hist_row,
+                                       (double*)ee, s);
+    return slab_field_impl<float>(slab, (const float*)row_sums_all, (const float*)H, field, (float*)E_hist_row,
+                                  (float*)ee, s);
+}
+
+int vp_slab_forward_step(vp_slab* slab, const void* h_ext, const void* field, void* h_out_ext, void* row_sums,
+                         void* f_rows, double* f_final_rows, void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int rc;
+    if ((rc = slab_check(slab, s)) != VP_OK) return rc;
+    const int dev = slab->plan->device;
+    if ((rc = check_dev_ptr(h_ext, "h_ext", dev)) || (rc = check_dev_ptr(field, "field", dev)) ||
+        (rc = check_opt_ptr(h_out_ext, "h_out_ext", dev)) || (rc = check_opt_ptr(row_sums, "row_sums", dev)) ||
+        (rc = check_opt_ptr(f_rows, "f_rows", dev)) || (rc = check_opt_ptr(f_final_rows, "f_final_rows", dev)))
+        return rc;
+    if (h_ext == h_out_ext) return set_err(VP_ERR_ARG, "h_ext and h_out_ext must be different arrays");
+    if (slab->plan->dtype == VP_F64)
+        return slab_forward_impl<double>(slab, 1, h_ext, field, h_out_ext, row_sums, f_rows, f_final_rows, s);
+    return slab_forward_impl<float>(slab, 1, h_ext, field, h_out_ext, row_sums, f_rows, f_final_rows, s);
+}
+
+int vp_slab_backward_start(vp_slab* slab, const void* g_f_ext, const void* h_prev_ext, const void* field_prev,
+                           void* w_out_ext, void* slope_sums, void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int rc;
+    if ((rc = slab_check(slab, s)) != VP_OK) return rc;
+    const int dev = slab->plan->device;
+    if ((rc = check_opt_ptr(g_f_ext, "g_f_ext", dev)) || (rc = check_dev_ptr(h_prev_ext, "h_prev_ext", dev)) ||
+        (rc = check_dev_ptr(field_prev, "field_prev", dev)) || (rc = check_dev_ptr(w_out_ext, "w_out_ext", dev)) ||
+        (rc = check_dev_ptr(slope_sums, "slope_sums", dev)))
+        return rc;
+    if (slab->plan->dtype == VP_F64)
+        return slab_backward_impl<double>(slab, 0, nullptr, g_f_ext, nullptr, nullptr, field_prev, h_prev_ext,
+                                          w_out_ext, slope_sums, nullptr, s);
+    return slab_backward_impl<float>(slab, 0, nullptr, g_f_ext, nullptr, nullptr, field_prev, h_prev_ext, w_out_ext,
+                                     slope_sums, nullptr, s);
+}
+
+int vp_slab_backward_field(vp_slab* slab, const void* slope_sums_all, const void* field_prev, const void* gE_hist_row,
+                           const void* gee, void* g_H, void* grho, void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int rc;
+    if ((rc = slab_check(slab, s)) != VP_OK) return rc;
+    const int dev = slab->plan->device;
+    if ((rc = check_dev_ptr(slope_sums_all, "slope_sums_all", dev)) ||
+        (rc = check_dev_ptr(field_prev, "field_prev", dev)) || (rc = check_opt_ptr(gE_hist_row, "gE_hist_row", dev)) ||
+        (rc = check_opt_ptr(gee, "gee", dev)) || (rc = check_dev_ptr(g_H, "g_H", dev)) ||
+        (rc = check_dev_ptr(grho, "grho", dev)))
+        return rc;
+    if (slab->plan->dtype == VP_F64)
+        return slab_backward_field_impl<double>(slab, (const double*)slope_sums_all, field_prev,
+                                                (const double*)gE_hist_row, (const double*)gee, (double*)g_H,
+                                                (double*)grho, s);
+    return slab_backward_field_impl<float>(slab, (const float*)slope_sums_all, field_prev, (const float*)gE_hist_row,
+                                           (const float*)gee, (float*)g_H, (float*)grho, s);
+}
+
+int vp_slab_backward_step(vp_slab* slab, const void* w_ext, const void* g_f_ext, const void* grho,
+                          const void* field_n, const void* field_prev, const void* h_prev_ext, void* w_out_ext,
+                          void* slope_sums, void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int rc;
+    if ((rc = slab_check(slab, s)) != VP_OK) return rc;
+    const int dev = slab->plan->device;
+    if ((rc = check_dev_ptr(w_ext, "w_ext", dev)) || (rc = check_opt_ptr(g_f_ext, "g_f_ext", dev)) ||
+        (rc = check_dev_ptr(grho, "grho", dev)) || (rc = check_dev_ptr(field_n, "field_n", dev)) ||
+        (rc = check_dev_ptr(field_prev, "field_prev", dev)) || (rc = check_dev_ptr(h_prev_ext, "h_prev_ext", dev)) ||
+        (rc = check_dev_ptr(w_out_ext, "w_out_ext", dev)) || (rc = check_dev_ptr(slope_sums, "slope_sums", dev)))
+        return rc;
+    if (w_ext == w_out_ext) return set_err(VP_ERR_ARG, "w_ext and w_out_ext must be different arrays");
+    if (slab->plan->dtype == VP_F64)
+        return slab_backward_impl<double>(slab, 1, w_ext, g_f_ext, (const double*)grho, field_n, field_prev,
+                                          h_prev_ext, w_out_ext, slope_sums, nullptr, s);
+    return slab_backward_impl<float>(slab, 1, w_ext, g_f_ext, (const float*)grho, field_n, field_prev, h_prev_ext,
+                                     w_out_ext, slope_sums, nullptr, s);
+}
+
+int vp_slab_backward_finish(vp_slab* slab, const void* w_ext, const void* grho, const void* field0, void* g_f_iv_rows,
+                            void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int rc;
+    if ((rc = slab_check(slab, s)) != VP_OK) return rc;
+    const int dev = slab->plan->device;
+    if ((rc = check_dev_ptr(w_ext, "w_ext", dev)) || (rc = check_dev_ptr(grho, "grho", dev)) ||
+        (rc = check_dev_ptr(field0, "field0", dev)) || (rc = check_dev_ptr(g_f_iv_rows, "g_f_iv_rows", dev)))
+        return rc;
+    if (slab->plan->dtype == VP_F64)
+        return slab_backward_impl<double>(slab, 2, w_ext, nullptr, (const double*)grho, field0, nullptr, nullptr,
+                                          nullptr, nullptr, g_f_iv_rows, s);
+    return slab_backward_impl<float>(slab, 2, w_ext, nullptr, (const float*)grho, field0, nullptr, nullptr, nullptr,
+                                     nullptr, g_f_iv_rows, s);
 }
 
 }  // extern "C"

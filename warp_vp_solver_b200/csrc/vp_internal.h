@@ -441,6 +441,16 @@ cudaError_t launch_kl_divergence(int nx, int nv, const double* f, const double* 
                                  double dv, double eps, double zeq, double* scratch, double* value, double* grad,
                                  cudaStream_t s);
 
+// x-slab decomposition (vp_ops.cu): per-row records in a slab's row order (array row k = grid row
+// (row_first + k) mod nx), and the owned rows' sums over the column-chunk partials.
+template <typename T>
+cudaError_t launch_slab_gather_rows(int nx, int row_first, int ext_rows, const VShift<T>* vsh, VShift<T>* vsh_out,
+                                    const VShift<T>* vsh2, VShift<T>* vsh2_out, const T* grho, T* grho_out,
+                                    cudaStream_t s);
+template <typename T>
+cudaError_t launch_slab_row_sums(const T* part, int n_chunks, int ext_rows, int ghost, int n_rows, T* out,
+                                 cudaStream_t s);
+
 // Bytes of the Poisson work area (nx complex values plus nx/2+1 complex twiddles).
 inline size_t poisson_area_size(int nx, size_t real_size) {
     return (size_t)nx * 2 * real_size + (size_t)((nx >> 1) + 1) * 2 * real_size;

@@ -319,7 +319,63 @@ cudaError_t launch_check_finite(const double* f, size_t n, const void* H, int nx
     return cudaGetLastError();
 }
 
+// ---- x-slab decomposition: per-row records of a slab's rows, and its owned rows' sums --------
+// A slab's arrays hold ext_rows rows; array row k is grid row (row_first + k) mod nx. This copies
+// the per-row records the step kernels read (v shifts of step n and n-1, cotangent on rho) from
+// the full-grid arrays every rank holds into the slab's own row order. Null pairs are skipped.
+template <typename T>
+__global__ void __launch_bounds__(256) slab_gather_rows_kernel(int nx, int row_first, int ext_rows,
+                                                               const VShift<T>* __restrict__ vsh,
+                                                               VShift<T>* __restrict__ vsh_out,
+                                                               const VShift<T>* __restrict__ vsh2,
+                                                               VShift<T>* __restrict__ vsh2_out,
+                                                               const T* __restrict__ grho,
+                                                               T* __restrict__ grho_out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ext_rows) return;
+    const int r = (row_first + k) % nx;   // row_first in [0, nx)
+    if (vsh != nullptr) vsh_out[k] = vsh[r];
+    if (vsh2 != nullptr) vsh2_out[k] = vsh2[r];
+    if (grho != nullptr) grho_out[k] = grho[r];
+}
+
+// out[i] = sum over column chunks c (ascending) of part[c][ghost + i], i < n_rows: the owned rows'
+// trapezoid sums, added in the order the single-grid tails add the same partials.
+template <typename T>
+__global__ void __launch_bounds__(256) slab_row_sums_kernel(const T* __restrict__ part, int n_chunks,
+                                                            int ext_rows, int ghost, int n_rows,
+                                                            T* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_rows) return;
+    const T* p = part + ghost + i;
+    T s = p[0];
+    for (int c = 1; c < n_chunks; ++c) s += p[(size_t)c * ext_rows];
+    out[i] = s;
+}
+
+template <typename T>
+cudaError_t launch_slab_gather_rows(int nx, int row_first, int ext_rows, const VShift<T>* vsh, VShift<T>* vsh_out,
+                                    const VShift<T>* vsh2, VShift<T>* vsh2_out, const T* grho, T* grho_out,
+                                    cudaStream_t s) {
+    slab_gather_rows_kernel<T><<<(ext_rows + 255) / 256, 256, 0, s>>>(nx, row_first, ext_rows, vsh, vsh_out,
+                                                                      vsh2, vsh2_out, grho, grho_out);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_slab_row_sums(const T* part, int n_chunks, int ext_rows, int ghost, int n_rows, T* out,
+                                 cudaStream_t s) {
+    slab_row_sums_kernel<T><<<(n_rows + 255) / 256, 256, 0, s>>>(part, n_chunks, ext_rows, ghost, n_rows, out);
+    count_launch();
+    return cudaGetLastError();
+}
+
 #define VP_INST(T)                                                                              \
+    template cudaError_t launch_slab_gather_rows<T>(int, int, int, const VShift<T>*, VShift<T>*, \
+                                                    const VShift<T>*, VShift<T>*, const T*, T*, \
+                                                    cudaStream_t);                              \
+    template cudaError_t launch_slab_row_sums<T>(const T*, int, int, int, int, T*, cudaStream_t); \
     template cudaError_t launch_compute_rho<T>(int, int, const double*, const double*, int,     \
                                                double, T*, cudaStream_t);                       \
     template cudaError_t launch_poisson<T>(const PoissonTables<T>&, const T*, T*, int,          \
