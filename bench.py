@@ -55,6 +55,10 @@ def parse_args():
     ap.add_argument("--stage-rows", type=int, default=None,
                     help="force the staged step's rows per CTA (0: per-column kernel); skips autotuning")
     ap.add_argument("--stage-threads", type=int, default=None, help="with --stage-rows: threads per CTA")
+    ap.add_argument("--strip-cols", type=int, default=None,
+                    help="with --strip-rows: 128 or 256 columns per forward strip CTA")
+    ap.add_argument("--strip-adj-cols", type=int, default=None,
+                    help="with --strip-rows: 128 or 256 columns per adjoint strip CTA")
     ap.add_argument("--strip-rows", type=int, default=None,
                     help="force the strip path's band height (0: off); skips autotuning")
     ap.add_argument("--no-e2e", action="store_true")
@@ -257,7 +261,8 @@ def run_ours(args, rank, local_rank, world):
             plan.set_config(cluster_size=0, persist_rows=0, strip_rows=0, stage_rows=args.stage_rows,
                             stage_threads=args.stage_threads)
         if args.strip_rows is not None:
-            plan.set_config(cluster_size=0, persist_rows=0, strip_rows=args.strip_rows)
+            plan.set_config(cluster_size=0, persist_rows=0, strip_rows=args.strip_rows, strip_cols=args.strip_cols,
+                            strip_adj_cols=args.strip_adj_cols)
     elif not args.no_autotune:
         t = solver.autotune(steps=min(8, wl.n_steps))
         tuned = {"config": t["config"], "ms_per_candidate_run": t["ms"], "cached": t["cached"],
@@ -452,7 +457,8 @@ def run_ours(args, rank, local_rank, world):
                    "cuda_graph": use_graph,
                    "launch": {k: cfg[k] for k in ("rows_per_cta", "threads", "n_chunks", "tail_inline",
                                                   "cluster_size", "cluster_threads", "stage_rows",
-                                                  "persist_rows", "persist_ctas", "strip_rows", "strip_ctas")},
+                                                  "persist_rows", "persist_ctas", "strip_rows", "strip_ctas", "strip_cols",
+                                                  "strip_adj_cols")},
                    "path": "cluster-resident" if resident else ("persistent forward loop" if persistent
                                                                 else "strip step kernels" if strip
                                                                 else "per-step launches"),

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define VP_ABI_VERSION 5
+#define VP_ABI_VERSION 6
 
 /* status codes */
 #define VP_OK 0
@@ -439,12 +439,15 @@ typedef struct vp_launch_config {
                               /* both are set.                                                   */
     int32_t strip_ctas;       /* CTAs of the forward strip launch (derived)                       */
     int64_t strip_smem_bytes; /* dynamic shared memory per CTA of the forward strip launch        */
+    int32_t strip_cols;       /* columns a forward strip CTA walks: 256 (two warps) or 128 (one   */
+                              /* warp); 0 in vp_plan_set_config keeps the current width          */
+    int32_t strip_adj_cols;   /* the same for the adjoint strip CTAs                              */
 } vp_launch_config;
 
 /* Reads the plan's current launch shape. */
 int vp_plan_get_config(const vp_plan* plan, vp_launch_config* out);
 
-/* Sets rows_per_cta, threads, n_chunks, cluster_size, stage_rows, stage_threads, persist_rows and strip_rows (the other
+/* Sets rows_per_cta, threads, n_chunks, cluster_size, stage_rows, stage_threads, persist_rows, strip_rows, strip_cols and strip_adj_cols (the other
  * fields are derived and ignored). cluster_size must be 0 or a power of two in [2, 16] that splits nx into 1, 2, 4, 8,
  * 16 or 32 rows per CTA whose state fits in shared memory; the cluster-resident path is used for forward calls without a tape or with
  * checkpoint interval 1, and for backward calls with checkpoint interval 1. Workspace sizes

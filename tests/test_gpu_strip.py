@@ -26,22 +26,26 @@ pytestmark = pytest.mark.gpu
 FIELDS = ("f_final", "f_hist", "E_hist", "ee_hist")
 
 
-def _solver(m, dt, f_eq, rows, **kw):
+def _solver(m, dt, f_eq, rows, cols=256, **kw):
     s = WarpVlasovPoissonSolver(m, dt, f_eq, **kw)
-    s.plan.set_config(cluster_size=0, persist_rows=0, strip_rows=rows)
+    s.plan.set_config(cluster_size=0, persist_rows=0, strip_rows=rows, strip_cols=cols)
     cfg = s.plan.get_config()
     assert cfg["strip_rows"] == rows and cfg["strip_ctas"] > 0 and cfg["persist_rows"] == 0
+    assert cfg["strip_cols"] == cols
     return s
 
 
-# (nx, nv, set-up, field amplitude, band rows)
+# (nx, nv, set-up, field amplitude, band rows, columns per CTA)
 SHAPES = [
-    (64, 256, "two_stream", 0.02, 8),
-    (128, 512, "two_stream", 0.3, 16),
-    (128, 512, "two_stream", 2.0, 8),     # shifts beyond the 4-cell halo
-    (96, 512, "bump_on_tail", 0.05, 16),  # 6 bands x 2 chunks over the CTAs: runs cross chunks
-    (2048, 512, "two_stream", 0.05, 16),  # x shifts of many cells: windows far from the band
-    (64, 512, "two_stream", 0.5, 4),      # a window of four slabs of 4 rows
+    (64, 256, "two_stream", 0.02, 8, 256),
+    (128, 512, "two_stream", 0.3, 16, 256),
+    (128, 512, "two_stream", 2.0, 8, 256),     # shifts beyond the 4-cell halo
+    (96, 512, "bump_on_tail", 0.05, 16, 256),  # 6 bands x 2 chunks over the CTAs: runs cross chunks
+    (2048, 512, "two_stream", 0.05, 16, 256),  # x shifts of many cells: windows far from the band
+    (64, 512, "two_stream", 0.5, 4, 256),      # a window of four slabs of 4 rows
+    (128, 512, "two_stream", 2.0, 8, 128),     # one-warp CTAs over 128 columns
+    (96, 512, "bump_on_tail", 0.05, 4, 128),
+    (2048, 256, "two_stream", 0.05, 4, 128),
 ]
 
 
@@ -56,12 +60,12 @@ def _setup(nx, nv, kind, amp):
     return m, f_eq, f_iv, H
 
 
-@pytest.mark.parametrize("shape", SHAPES, ids=lambda s: f"{s[0]}x{s[1]}_{s[2]}_H{s[3]}_R{s[4]}")
+@pytest.mark.parametrize("shape", SHAPES, ids=lambda s: f"{s[0]}x{s[1]}_{s[2]}_H{s[3]}_R{s[4]}_C{s[5]}")
 def test_strip_forward_and_adjoint_match_oracle(shape, record_error):
-    nx, nv, kind, amp, rows = shape
+    nx, nv, kind, amp, rows, cols = shape
     m, f_eq, f_iv, H = _setup(nx, nv, kind, amp)
     T, dt = 6, 0.05
-    s = _solver(m, dt, f_eq, rows, checkpoint_every=3)
+    s = _solver(m, dt, f_eq, rows, cols, checkpoint_every=3)
     out = s.run_forward(f_iv, H, T * dt)
     g = O.grid_from(m)
     ref = O.delta_forward(g, dt, f_eq, f_iv, H, T)
@@ -70,7 +74,7 @@ def test_strip_forward_and_adjoint_match_oracle(shape, record_error):
         err = O.rel_err(arr, r)
         worst = max(worst, err)
         assert err < 1e-5, f"{name}: {err:.2e}"
-    record_error(f"strip {nx}x{nv} {kind} H{amp} R{rows} fwd", worst, 1e-5)
+    record_error(f"strip {nx}x{nv} {kind} H{amp} R{rows} C{cols} fwd", worst, 1e-5)
     if nx > 1024:
         return   # the float64 oracle's adjoint at this size is slow; the forward was the point
     w = O.trapezoid_time_weights(T, dt)
@@ -81,7 +85,7 @@ def test_strip_forward_and_adjoint_match_oracle(shape, record_error):
     gf, gH = s._run_backward(f_iv, H, T * dt, None, gff, gfh, gEh, w)
     rf, rH = O.delta_backward(g, dt, f_eq, f_iv, H, T, gff, gfh, gEh, w)
     e = max(O.rel_err(gf, rf), O.rel_err(gH, rH))
-    record_error(f"strip {nx}x{nv} {kind} H{amp} R{rows} adj", e, 5e-5)
+    record_error(f"strip {nx}x{nv} {kind} H{amp} R{rows} C{cols} adj", e, 5e-5)
     assert e < 5e-5, f"adjoint {e:.2e}"
 
 
@@ -91,12 +95,13 @@ def test_strip_checkpoint_recompute_is_bitwise_neutral():
     m, f_eq, f_iv, H = _setup(128, 512, "two_stream", 0.3)
     T, dt = 9, 0.05
     w = O.trapezoid_time_weights(T, dt)
-    outs = []
-    for every in (1, 2, 4, 0):
-        s = _solver(m, dt, f_eq, 8, checkpoint_every=every or None)
-        outs.append(s._run_backward(f_iv, H, T * dt, None, None, None, None, w))
-    for gf, gH in outs[1:]:
-        assert np.array_equal(gf, outs[0][0]) and np.array_equal(gH, outs[0][1])
+    for cols in (256, 128):
+        outs = []
+        for every in (1, 2, 4, 0):
+            s = _solver(m, dt, f_eq, 8, cols, checkpoint_every=every or None)
+            outs.append(s._run_backward(f_iv, H, T * dt, None, None, None, None, w))
+        for gf, gH in outs[1:]:
+            assert np.array_equal(gf, outs[0][0]) and np.array_equal(gH, outs[0][1])
 
 
 def test_strip_agrees_with_persistent_and_is_deterministic():

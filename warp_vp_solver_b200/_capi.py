@@ -23,7 +23,7 @@ VP_SCHEME_STRANG = 0
 VP_SCHEME_MERGED = 1
 VP_STATUS_NONFINITE_INPUT = 1
 VP_STATUS_WAIT_TIMEOUT = 2
-ABI_VERSION = 5   # VP_ABI_VERSION of the header these bindings follow
+ABI_VERSION = 6   # VP_ABI_VERSION of the header these bindings follow
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libvpb200.so")
 
@@ -74,6 +74,8 @@ class LaunchConfig(ctypes.Structure):
         ("strip_rows", c_i32),
         ("strip_ctas", c_i32),
         ("strip_smem_bytes", c_i64),
+        ("strip_cols", c_i32),
+        ("strip_adj_cols", c_i32),
     ]
 
 

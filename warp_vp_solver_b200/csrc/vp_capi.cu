@@ -353,7 +353,7 @@ static WsLayout ws_layout(const vp_plan* p, int n_steps, int every) {
     L.hbuf1 = off; off += align256(nxnv);
     L.seg = off; off += align256(nxnv * (size_t)std::max(0, K - 1));
     const int part_chunks = std::max({p->cfg.n_chunks, p->stage_span > 0 ? p->scfg.n_chunks : 0,
-                                      p->strip.R > 0 ? p->strip.n_chunks : 0});
+                                      p->strip.R > 0 ? std::max(p->strip.n_chunks, p->strip.b_n_chunks) : 0});
     L.part = off; off += align256((size_t)part_chunks * p->nx * real_size(p));
     L.counter = off; off += 256;
     L.vsh = off; off += align256((size_t)p->nx * vshift_size(p));
@@ -436,12 +436,12 @@ static PersistArgs persist_args(const vp_plan* p, unsigned char* ws, const WsLay
 
 // Table arguments of a strip step launch (forward, replay or adjoint).
 template <typename A>
-static void strip_tables(const vp_plan* p, A& a) {
+static void strip_tables(const vp_plan* p, A& a, int gt) {
     a.nx = p->nx;
     a.nv = p->nv;
     a.quad = p->d_pquad;
     a.tq = p->d_ptq;
-    a.chunk = p->d_pchunk;
+    a.chunk = gt == 32 ? p->d_echunk : p->d_pchunk;   // quad shift range per chunk of the group width
     a.dfeq = p->d_dfeq;
     a.vtab = static_cast<const float*>(p->d_vtab);
     a.feq = p->d_feq;
@@ -633,7 +633,7 @@ static int forward_impl(vp_plan* p, const double* f_iv, const T* H, int T_steps,
         } else if (strip) {
             if constexpr (sizeof(T) == 4) {
                 StripFwdArgs sa{};
-                strip_tables(p, sa);
+                strip_tables(p, sa, p->strip.gt);
                 sa.h_in = a.h_in;
                 sa.h_out = a.h_out;
                 sa.vsh = a.vsh;
@@ -720,6 +720,7 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
         r.neg_dt_dv = (T)(-p->dt / p->dv);
         res_halo_rows(p, &r.h_lo, &r.h_hi);
         r.mx_lo = (int)p->mx_lo;
+        r.vrows = p->res_vrows;
         VP_CUDA(launch_res_bwd<T>(r, p->feq2d != 0, p->res_cn, p->res_threads, p->res_smem, s),
                 "cluster-resident backward launch");
         return VP_OK;
@@ -790,7 +791,7 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
                 // the forward's strip kernel, without row sums: bitwise the states it computed
                 if constexpr (sizeof(T) == 4) {
                     StripFwdArgs sa{};
-                    strip_tables(p, sa);
+                    strip_tables(p, sa, p->strip.gt);
                     sa.h_in = fa.h_in;
                     sa.h_out = fa.h_out;
                     sa.vsh = fa.vsh;
@@ -913,7 +914,7 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
         if (strip) {
             if constexpr (sizeof(T) == 4) {
                 StripBwdArgs sb{};
-                strip_tables(p, sb);
+                strip_tables(p, sb, p->strip.bgt);
                 sb.w_in = b.w_in;
                 sb.w_out = b.w_out;
                 sb.grho = grho;
@@ -1299,14 +1300,26 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
     // persistent and strip paths: float32, x-invariant f_eq, nv a multiple of 256, the x shifts of
     // every 4 neighbouring columns within one cell, nx <= 16384 (the circulant table costs O(nx^2)
     // on the host)
-    std::vector<int2> quad, chunk;
+    std::vector<int2> quad, chunk, chunk128;
     std::vector<float> tq;
     if (dtype == VP_F32 && inv && p->d_vtab != nullptr && nx <= 16384 &&
         build_quad_tables(nx, nv, m_signed, tx, quad, tq, chunk)) {
         p->host_msigned = m_signed;
         p->host_tx = tx;
         if (!persist_prepare(p->pst, nx, nv, m_signed, tx, n_sms, 0)) p->pst = PersistHost{};
-        if (!strip_prepare(p->strip, nx, nv, chunk, n_sms, 0)) p->strip = StripHost{};
+        // strip shapes measured on B200 (8192^2): forward 256-column CTAs of two warps, adjoint
+        // 128-column CTAs of one warp
+        std::vector<int2> q2;
+        std::vector<float> t2;
+        const bool c128 = build_quad_tables(nx, nv, m_signed, tx, q2, t2, chunk128, 128);
+        if (!(c128 && strip_prepare(p->strip, nx, nv, chunk, chunk128, n_sms, 0, 64, 32)) &&
+            !strip_prepare(p->strip, nx, nv, chunk, chunk, n_sms, 0, 64, 64))
+            p->strip = StripHost{};
+        if (p->strip.R > 0 && p->strip.bgt == 32 &&
+            (rc = upload_bytes((void**)&p->d_echunk, chunk128.data(), chunk128.size() * sizeof(int2)))) {
+            free_plan(p);
+            return rc;
+        }
     }
     if (p->pst.R > 0 || p->strip.R > 0) {
         std::vector<float> dfeq(nv);
@@ -1371,6 +1384,8 @@ int vp_plan_get_config(const vp_plan* plan, vp_launch_config* out) {
     out->strip_rows = strip ? plan->strip.R : 0;
     out->strip_ctas = strip ? plan->strip.fwd_ctas : 0;
     out->strip_smem_bytes = strip ? (int64_t)plan->strip.fwd_smem : 0;
+    out->strip_cols = strip ? 4 * plan->strip.gt : 0;
+    out->strip_adj_cols = strip ? 4 * plan->strip.bgt : 0;
     return VP_OK;
 }
 
@@ -1430,14 +1445,27 @@ int vp_plan_set_config(vp_plan* plan, const vp_launch_config* cfg) {
         if (plan->d_pquad == nullptr)
             return set_err(VP_ERR_ARG, "strip_rows=%d: the strip path needs a float32 plan with an "
                                        "x-invariant f_eq, nv a multiple of 256 and nx <= 16384", cfg->strip_rows);
-        std::vector<int2> quad, chunk;
+        const int keep_f = plan->strip.gt > 0 ? 4 * plan->strip.gt : 256;
+        const int cols = cfg->strip_cols != 0 ? cfg->strip_cols : (cfg->strip_rows == 16 ? 256 : keep_f);
+        // a width left at 0 keeps the current one where the band height allows it (128-column CTAs
+        // exist for bands of 4 and 8 rows), else 256
+        const int keep_b = plan->strip.bgt > 0 ? 4 * plan->strip.bgt : 256;
+        const int bcols = cfg->strip_adj_cols != 0 ? cfg->strip_adj_cols : (cfg->strip_rows == 16 ? 256 : keep_b);
+        if ((cols != 128 && cols != 256) || (bcols != 128 && bcols != 256))
+            return set_err(VP_ERR_ARG, "strip_cols and strip_adj_cols must be 0, 128 or 256 (got %d, %d)",
+                           cfg->strip_cols, cfg->strip_adj_cols);
+        std::vector<int2> quad, chunk, bchunk;
         std::vector<float> tq;
         StripHost sh;
-        if (!build_quad_tables(plan->nx, plan->nv, plan->host_msigned, plan->host_tx, quad, tq, chunk) ||
-            !strip_prepare(sh, plan->nx, plan->nv, chunk, sms, cfg->strip_rows))
-            return set_err(VP_ERR_ARG, "strip_rows=%d is not usable for a %dx%d grid (4, 8 or 16 dividing nx, "
-                                       "nx a multiple of 32)",
-                           cfg->strip_rows, plan->nx, plan->nv);
+        int rc = VP_OK;
+        if ((cols == 128 || bcols == 128) && !plan_ens_tables(plan, &rc))
+            return rc != VP_OK ? rc : set_err(VP_ERR_ARG, "128-column strip CTAs are not usable for this plan");
+        if (!build_quad_tables(plan->nx, plan->nv, plan->host_msigned, plan->host_tx, quad, tq, chunk, cols) ||
+            !build_quad_tables(plan->nx, plan->nv, plan->host_msigned, plan->host_tx, quad, tq, bchunk, bcols) ||
+            !strip_prepare(sh, plan->nx, plan->nv, chunk, bchunk, sms, cfg->strip_rows, cols / 4, bcols / 4))
+            return set_err(VP_ERR_ARG, "strip_rows=%d with strip_cols=%d, strip_adj_cols=%d is not usable for a %dx%d "
+                                       "grid (4, 8 or 16 dividing nx, 16 only with 256 columns, nx a multiple of 32)",
+                           cfg->strip_rows, cols, bcols, plan->nx, plan->nv);
         plan->strip = sh;
     }
     plan->pst_on = cfg->persist_rows != 0 ? 1 : 0;

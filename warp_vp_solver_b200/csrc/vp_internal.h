@@ -377,13 +377,19 @@ struct StripInst {
 
 struct StripHost {
     int R = 0, n_bands = 0, n_chunks = 0, span_max = 0, ring_rows = 0;
+    int gt = 0;                 // forward: threads of a column group, 64 (256-column chunks) or 32 (128)
+    int bgt = 0, b_n_chunks = 0, b_ring_rows = 0;   // adjoint: its column group, chunks and ring rows
     int fwd_runs = 0, bwd_runs = 0, fwd_ctas = 0, bwd_ctas = 0, field_ctas = 0;
     size_t fwd_smem = 0, bwd_smem = 0;
 };
 constexpr int kStripFieldRows = 32;
 
-// Launch shape of the strip path (force_rows 0: automatic, else 4, 8 or 16); false when not eligible.
-bool strip_prepare(StripHost& sh, int nx, int nv, const std::vector<int2>& chunk, int n_sms, int force_rows);
+// Launch shape of the strip path (force_rows 0: automatic, else 4, 8 or 16) for forward column
+// groups of gt threads and adjoint column groups of bgt threads (64: 256-column chunks, 32:
+// 128-column chunks; chunk / bchunk are the quad shift range tables of those widths); false when
+// not eligible.
+bool strip_prepare(StripHost& sh, int nx, int nv, const std::vector<int2>& chunk, const std::vector<int2>& bchunk,
+                   int n_sms, int force_rows, int gt, int bgt);
 cudaError_t launch_strip_fwd(const StripFwdArgs& a, const StripHost& sh, cudaStream_t s);
 cudaError_t launch_strip_bwd(const StripBwdArgs& a, const StripHost& sh, cudaStream_t s);
 cudaError_t launch_strip_field(const StripFieldArgs& a, const StripHost& sh, cudaStream_t s);
@@ -505,6 +511,8 @@ template <typename T> struct ResBwdArgs {
     T dv, dx, neg_dt_dv;
     int h_lo, h_hi;         // halo rows kept below / above a CTA's own rows
     int mx_lo;              // smallest unreduced x half-step offset (recovers signed offsets)
+    int vrows;              // float32, x-invariant f_eq: V^T + rho^T once per (row, column) into the
+                            // shared plane the launch's shared memory holds for it
 };
 
 template <typename T>

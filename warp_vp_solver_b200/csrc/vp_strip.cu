@@ -38,7 +38,6 @@ namespace vpb {
 
 namespace {
 
-constexpr int kStripThreads = kPstGroup;   // a single-instance CTA: one column group of 256 columns
 constexpr int kFieldThreads = 256;
 constexpr int kFieldWarps = kFieldThreads / 32;
 constexpr int kStripMaxSmem = 200 * 1024;   // dynamic shared memory cap of a strip CTA
@@ -977,37 +976,58 @@ static int strip_occupancy(bool fwd, size_t smem) {
     return n;
 }
 
-bool strip_prepare(StripHost& sh, int nx, int nv, const std::vector<int2>& chunk, int n_sms, int force_rows) {
-    sh = StripHost{};
-    if (nv % kPstC != 0 || nx % kStripFieldRows != 0 || nx < 64 || (int)chunk.size() != nv / kPstC) return false;
+template <int GT>
+static int strip_occupancy_r(int R, bool fwd, size_t smem) {
+    if constexpr (GT == 32) {
+        return R == 8 ? strip_occupancy<8, 32>(fwd, smem) : R == 4 ? strip_occupancy<4, 32>(fwd, smem) : 0;
+    } else {
+        return R == 16 ? strip_occupancy<16, GT>(fwd, smem)
+                       : R == 8 ? strip_occupancy<8, GT>(fwd, smem) : strip_occupancy<4, GT>(fwd, smem);
+    }
+}
+
+// Ring rows of a strip CTA: a band's window (2 dmax + R + 4 rows, at most L slabs of R rows) plus the
+// slab in flight; dmax is the largest spread of quad shifts within one chunk of the table.
+static int strip_ring_rows(const std::vector<int2>& chunk, int R) {
     int dmax = 0;
     for (const int2& c : chunk) dmax = std::max(dmax, c.y - c.x);
+    const int span_max = 2 * dmax + R + 4;
+    return ((span_max + R - 1) / R + 1) * R;
+}
+
+bool strip_prepare(StripHost& sh, int nx, int nv, const std::vector<int2>& chunk, const std::vector<int2>& bchunk,
+                   int n_sms, int force_rows, int gt, int bgt) {
+    sh = StripHost{};
+    if ((gt != 32 && gt != 64) || (bgt != 32 && bgt != 64)) return false;
+    const int cols = 4 * gt, bcols = 4 * bgt;
+    if (nv % cols != 0 || nv % bcols != 0 || nx % kStripFieldRows != 0 || nx < 64 ||
+        (int)chunk.size() != nv / cols || (int)bchunk.size() != nv / bcols)
+        return false;
     for (int R : {4, 8, 16}) {   // automatic: the first that fits (4 measured fastest on B200)
         if (force_rows > 0 && R != force_rows) continue;
-        if (nx % R != 0) continue;
-        const int span_max = 2 * dmax + R + 4;
-        // ring: a band's window (span rows, at most L slabs of R rows) plus the slab in flight
-        const int NR = ((span_max + R - 1) / R + 1) * R;
-        const size_t fb = strip_fwd_bytes(NR, R, kStripThreads), bb = strip_bwd_bytes(NR, R, kStripThreads);
+        if (nx % R != 0 || ((gt == 32 || bgt == 32) && R == 16)) continue;
+        const int NR = strip_ring_rows(chunk, R), NRb = strip_ring_rows(bchunk, R);
+        const size_t fb = strip_fwd_bytes(NR, R, gt), bb = strip_bwd_bytes(NRb, R, bgt);
         if (fb > (size_t)kStripMaxSmem || bb > (size_t)kStripMaxSmem) continue;
-        const int pf = R == 16 ? strip_occupancy<16, kStripThreads>(true, fb) : R == 8 ? strip_occupancy<8, kStripThreads>(true, fb)
-                                                                        : strip_occupancy<4, kStripThreads>(true, fb);
-        const int pb = R == 16 ? strip_occupancy<16, kStripThreads>(false, bb) : R == 8 ? strip_occupancy<8, kStripThreads>(false, bb)
-                                                                         : strip_occupancy<4, kStripThreads>(false, bb);
+        const int pf = gt == 32 ? strip_occupancy_r<32>(R, true, fb) : strip_occupancy_r<64>(R, true, fb);
+        const int pb = bgt == 32 ? strip_occupancy_r<32>(R, false, bb) : strip_occupancy_r<64>(R, false, bb);
         if (pf <= 0 || pb <= 0) continue;
         sh.R = R;
+        sh.gt = gt;
+        sh.bgt = bgt;
         sh.n_bands = nx / R;
-        sh.n_chunks = nv / kPstC;
-        sh.span_max = span_max;
+        sh.n_chunks = nv / cols;
+        sh.b_n_chunks = nv / bcols;
+        sh.span_max = NR - R;
         sh.ring_rows = NR;
+        sh.b_ring_rows = NRb;
         sh.fwd_smem = fb;
         sh.bwd_smem = bb;
         // runs per chunk: as many as fill one wave of CTAs (at least one)
-        const int nch = nv / kPstC;
-        sh.fwd_runs = std::max(1, std::min(nx / R, pf * n_sms / nch));
-        sh.bwd_runs = std::max(1, std::min(nx / R, pb * n_sms / nch));
-        sh.fwd_ctas = nch * sh.fwd_runs;
-        sh.bwd_ctas = nch * sh.bwd_runs;
+        sh.fwd_runs = std::max(1, std::min(nx / R, pf * n_sms / sh.n_chunks));
+        sh.bwd_runs = std::max(1, std::min(nx / R, pb * n_sms / sh.b_n_chunks));
+        sh.fwd_ctas = sh.n_chunks * sh.fwd_runs;
+        sh.bwd_ctas = sh.b_n_chunks * sh.bwd_runs;
         sh.field_ctas = nx / kStripFieldRows;
         return true;
     }
@@ -1020,10 +1040,12 @@ cudaError_t launch_strip_fwd(const StripFwdArgs& args, const StripHost& sh, cuda
     a.n_bands = sh.n_bands;
     a.ring_rows = sh.ring_rows;
     a.runs = sh.fwd_runs;
-    switch (sh.R) {
-        case 4: vp_strip_fwd_kernel<4, kStripThreads><<<sh.fwd_ctas, kStripThreads, sh.fwd_smem, s>>>(a); break;
-        case 8: vp_strip_fwd_kernel<8, kStripThreads><<<sh.fwd_ctas, kStripThreads, sh.fwd_smem, s>>>(a); break;
-        case 16: vp_strip_fwd_kernel<16, kStripThreads><<<sh.fwd_ctas, kStripThreads, sh.fwd_smem, s>>>(a); break;
+    switch (sh.R * 100 + sh.gt) {
+        case 464: vp_strip_fwd_kernel<4, 64><<<sh.fwd_ctas, 64, sh.fwd_smem, s>>>(a); break;
+        case 864: vp_strip_fwd_kernel<8, 64><<<sh.fwd_ctas, 64, sh.fwd_smem, s>>>(a); break;
+        case 1664: vp_strip_fwd_kernel<16, 64><<<sh.fwd_ctas, 64, sh.fwd_smem, s>>>(a); break;
+        case 432: vp_strip_fwd_kernel<4, 32><<<sh.fwd_ctas, 32, sh.fwd_smem, s>>>(a); break;
+        case 832: vp_strip_fwd_kernel<8, 32><<<sh.fwd_ctas, 32, sh.fwd_smem, s>>>(a); break;
         default: return cudaErrorInvalidValue;
     }
     count_launch();
@@ -1032,14 +1054,16 @@ cudaError_t launch_strip_fwd(const StripFwdArgs& args, const StripHost& sh, cuda
 
 cudaError_t launch_strip_bwd(const StripBwdArgs& args, const StripHost& sh, cudaStream_t s) {
     StripBwdArgs a = args;
-    a.n_chunks = sh.n_chunks;
+    a.n_chunks = sh.b_n_chunks;
     a.n_bands = sh.n_bands;
-    a.ring_rows = sh.ring_rows;
+    a.ring_rows = sh.b_ring_rows;
     a.runs = sh.bwd_runs;
-    switch (sh.R) {
-        case 4: vp_strip_bwd_kernel<4, kStripThreads><<<sh.bwd_ctas, kStripThreads, sh.bwd_smem, s>>>(a); break;
-        case 8: vp_strip_bwd_kernel<8, kStripThreads><<<sh.bwd_ctas, kStripThreads, sh.bwd_smem, s>>>(a); break;
-        case 16: vp_strip_bwd_kernel<16, kStripThreads><<<sh.bwd_ctas, kStripThreads, sh.bwd_smem, s>>>(a); break;
+    switch (sh.R * 100 + sh.bgt) {
+        case 464: vp_strip_bwd_kernel<4, 64><<<sh.bwd_ctas, 64, sh.bwd_smem, s>>>(a); break;
+        case 864: vp_strip_bwd_kernel<8, 64><<<sh.bwd_ctas, 64, sh.bwd_smem, s>>>(a); break;
+        case 1664: vp_strip_bwd_kernel<16, 64><<<sh.bwd_ctas, 64, sh.bwd_smem, s>>>(a); break;
+        case 432: vp_strip_bwd_kernel<4, 32><<<sh.bwd_ctas, 32, sh.bwd_smem, s>>>(a); break;
+        case 832: vp_strip_bwd_kernel<8, 32><<<sh.bwd_ctas, 32, sh.bwd_smem, s>>>(a); break;
         default: return cudaErrorInvalidValue;
     }
     count_launch();

@@ -84,10 +84,13 @@ class Plan:
     def set_config(self, rows_per_cta: int | None = None, threads: int | None = None,
                    n_chunks: int | None = None, cluster_size: int | None = None,
                    stage_rows: int | None = None, stage_threads: int | None = None,
-                   persist_rows: int | None = None, strip_rows: int | None = None) -> None:
+                   persist_rows: int | None = None, strip_rows: int | None = None,
+                   strip_cols: int | None = None, strip_adj_cols: int | None = None) -> None:
         """Change the launch shape; arguments left as None keep their current values.
         ``stage_rows=0`` turns the staged forward step off, ``persist_rows=0`` the persistent
-        (one launch per loop) path, ``strip_rows=0`` the strip (two launches per step) path."""
+        (one launch per loop) path, ``strip_rows=0`` the strip (two launches per step) path;
+        ``strip_cols`` / ``strip_adj_cols`` (128 or 256) set the columns a forward / adjoint strip
+        CTA walks."""
         cur = self.get_config()
         c = _capi.LaunchConfig()
         c.rows_per_cta = cur["rows_per_cta"] if rows_per_cta is None else int(rows_per_cta)
@@ -98,6 +101,8 @@ class Plan:
         c.stage_threads = cur["stage_threads"] if stage_threads is None else int(stage_threads)
         c.persist_rows = cur["persist_rows"] if persist_rows is None else int(persist_rows)
         c.strip_rows = cur["strip_rows"] if strip_rows is None else int(strip_rows)
+        c.strip_cols = 0 if strip_cols is None else int(strip_cols)
+        c.strip_adj_cols = 0 if strip_adj_cols is None else int(strip_adj_cols)
         _capi.check(self.lib.vp_plan_set_config(self._h, ctypes.byref(c)))
         self._ws = {}   # workspace size depends on n_chunks and the persistent and strip launch shapes
 
