@@ -720,7 +720,6 @@ static int backward_impl(vp_plan* p, const T* H, int T_steps, const unsigned cha
         r.neg_dt_dv = (T)(-p->dt / p->dv);
         res_halo_rows(p, &r.h_lo, &r.h_hi);
         r.mx_lo = (int)p->mx_lo;
-        r.vrows = p->res_vrows;
         VP_CUDA(launch_res_bwd<T>(r, p->feq2d != 0, p->res_cn, p->res_threads, p->res_smem, s),
                 "cluster-resident backward launch");
         return VP_OK;

@@ -511,8 +511,6 @@ template <typename T> struct ResBwdArgs {
     T dv, dx, neg_dt_dv;
     int h_lo, h_hi;         // halo rows kept below / above a CTA's own rows
     int mx_lo;              // smallest unreduced x half-step offset (recovers signed offsets)
-    int vrows;              // float32, x-invariant f_eq: V^T + rho^T once per (row, column) into the
-                            // shared plane the launch's shared memory holds for it
 };
 
 template <typename T>

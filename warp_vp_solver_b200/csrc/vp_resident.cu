@@ -614,50 +614,6 @@ __global__ void __launch_bounds__(res_max_threads(RPT)) vp_res_fwd_kernel(const 
 // Adjoint
 // ---------------------------------------------------------------------------------------------
 
-// The adjoint's phase A: gh = V^T(w) + rho^T(grho) once per (local row, column) of the plane `cur`
-// (w_n with its halo) into S.po, four columns per thread, one row per thread group at a time.
-// Element by element the same expression as the per-thread window loop:
-// lerp(w[j - m], w[j - m - 1], t) + wr_j * fld[l], wr_j = -dv * trapezoid weight of column j.
-__device__ __forceinline__ void res_vt_rows(const ResSmem<float>& S, const float* cur, int nv, int W, float dv) {
-    const int nq = nv >> 2;
-    const int q = threadIdx.x % nq, j0 = 4 * q;
-    const int lstep = blockDim.x / nq;
-    const int jm = j0 == 0 ? nv - 1 : j0 - 1, jp = j0 + 4 == nv ? 0 : j0 + 4;
-    float wr[4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) wr[e] = -dv * trap_w<float>(j0 + e, nv);
-#pragma unroll 1
-    for (int l = threadIdx.x / nq; l < W; l += lstep) {
-        const VShift<float> v = S.vsh[l];
-        const float* wrow = cur + (size_t)l * nv;
-        const float fl = S.fld[l];
-        float4 o;
-        if (v.m == 0) {   // c0 = j, c1 = j - 1
-            const float4 w = *reinterpret_cast<const float4*>(wrow + j0);
-            o.x = lerp(w.x, wrow[jm], v.t) + wr[0] * fl;
-            o.y = lerp(w.y, w.x, v.t) + wr[1] * fl;
-            o.z = lerp(w.z, w.y, v.t) + wr[2] * fl;
-            o.w = lerp(w.w, w.z, v.t) + wr[3] * fl;
-        } else if (v.m == nv - 1) {   // c0 = j + 1, c1 = j
-            const float4 w = *reinterpret_cast<const float4*>(wrow + j0);
-            o.x = lerp(w.y, w.x, v.t) + wr[0] * fl;
-            o.y = lerp(w.z, w.y, v.t) + wr[1] * fl;
-            o.z = lerp(w.w, w.z, v.t) + wr[2] * fl;
-            o.w = lerp(wrow[jp], w.w, v.t) + wr[3] * fl;
-        } else {
-            float r[4];
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int c0 = wrapneg(j0 + e - v.m, nv);
-                const int c1 = wrapneg(c0 - 1, nv);
-                r[e] = lerp(wrow[c0], wrow[c1], v.t) + wr[e] * fl;
-            }
-            o = make_float4(r[0], r[1], r[2], r[3]);
-        }
-        *reinterpret_cast<float4*>(S.po + (size_t)l * nv + j0) = o;
-    }
-}
-
 // Tape values that the adjoint field of step s reads, loaded into registers ahead of their use:
 // g_E_hist and E_tape of row threadIdx.x and the v shift of local row threadIdx.x. Rows beyond
 // blockDim.x are read in the field itself.
@@ -785,9 +741,7 @@ __global__ void __launch_bounds__(res_max_threads(RPT)) vp_res_bwd_kernel(const 
     const int g = gr0 + rt;
     const bool colv = j < nv;
     const int cw = j >> 5, ncw = NVP >> 5;
-    // the V^T step by rows (phase A) when the host gave the block the plane for it
-    const bool vrows = a.vrows != 0;
-    ResSmem<T> S = res_carve<T>(smem, nx, nv, RC, W, vrows);
+    ResSmem<T> S = res_carve<T>(smem, nx, nv, RC, W, false);
     T* Wb[2] = {S.p0, S.p1};   // cotangent on the v-step output of even / odd steps, local rows
     T* red = S.p2;             // row partials of the warps
     res_init_tables<T>(S, a.P, a.feq, FEQ2D, nx, nv);
@@ -850,35 +804,20 @@ __global__ void __launch_bounds__(res_max_threads(RPT)) vp_res_bwd_kernel(const 
         T prod[RPT];
 #pragma unroll
         for (int k = 0; k < RPT; ++k) prod[k] = T(0);
-        bool from_plane = false;
-        if constexpr (sizeof(T) == 4 && !FEQ2D) {
-            if (vrows) {
-                res_vt_rows(S, cur, nv, W, a.dv);   // phase A: V^T + rho^T once per (row, column)
-                __syncthreads();
-                from_plane = true;
-            }
-        }
         if (colv) {
             // gh = V^T(w_n) + rho^T(grho_n) on rows g-2m-2 .. g-2m+RPT-1 (n = 0: g-m-1 ..), local rows
             const int ng = n == 0 ? RPT + 1 : RPT + 2;   // rows of gh needed
             T gh[RPT + 2];
             const int l0 = n == 0 ? hl + rt - sm - 1 : hl + rt - 2 * sm - 2;
-            if (from_plane) {
-                const T* op = S.po + (size_t)l0 * nv + j;
 #pragma unroll
-                for (int k = 0; k < RPT + 2; ++k)
-                    if (k < ng) gh[k] = op[(size_t)k * nv];
-            } else {
-#pragma unroll
-                for (int k = 0; k < RPT + 2; ++k) {
-                    if (k < ng) {
-                        const int l = l0 + k;
-                        const VShift<T> v = S.vsh[l];
-                        const T* wrow = cur + (size_t)l * nv;
-                        const int c0 = wrapneg(j - v.m, nv);
-                        const int c1 = wrapneg(c0 - 1, nv);
-                        gh[k] = lerp(wrow[c0], wrow[c1], v.t) + wr * S.fld[l];
-                    }
+            for (int k = 0; k < RPT + 2; ++k) {
+                if (k < ng) {
+                    const int l = l0 + k;
+                    const VShift<T> v = S.vsh[l];
+                    const T* wrow = cur + (size_t)l * nv;
+                    const int c0 = wrapneg(j - v.m, nv);
+                    const int c1 = wrapneg(c0 - 1, nv);
+                    gh[k] = lerp(wrow[c0], wrow[c1], v.t) + wr * S.fld[l];
                 }
             }
             if (n == 0) {
