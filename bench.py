@@ -63,7 +63,7 @@ def parse_args():
                     help="force the strip path's band height (0: off); skips autotuning")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
-                    help="c2: skip the 8192^2 roofline and C5 sub-records of the default line")
+                    help="c2: skip the sub-records of the default line (C1, C3, C4, 8192^2 roofline, x slabs, C5)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample duration")
     return ap.parse_args()
@@ -522,6 +522,72 @@ def measure_config(args, rank, local_rank, world, workload):
     return out
 
 
+def measure_slab(args, rank, local_rank, world, nx=2048, n_slabs=2, n_steps=20):
+    """The x-slab decomposition of one grid (two-stream nx x nx, 20 steps, 8-mode H, forward +
+    checkpointed adjoint of J = sum(ee)*dt through SlabSolver.vjp) with every slab on this GPU
+    (LocalRing: the slabs' launches in sequence, ghost exchanges as device copies, the row-sum
+    gather a concatenation), beside the same loop on the one-grid per-column path it is built
+    from; 3 warm-up and 3 timed calls, device-timed."""
+    import torch
+
+    from warp_vp_solver_b200 import make_mesh
+    from warp_vp_solver_b200.plan import Plan
+    from warp_vp_solver_b200.slab import LocalRing, SlabSolver
+    from warp_vp_solver_b200.workloads import fourier_coefficients, fourier_field, two_stream
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dt = 0.05
+    m = make_mesh(10.0 * np.pi, 6.0, nx, nx)
+    f_eq, f_iv = two_stream(m)
+    H = fourier_field(fourier_coefficients(8, 1e-2, 0), m.xs, 2 * np.pi / m.period_x)
+    g_ee = np.full(n_steps, dt)
+    s = SlabSolver(m, dt, f_eq[0], LocalRing(n_slabs), device=dev)
+    f_dev = torch.tensor(f_iv, dtype=torch.float64, device=dev)
+    rows = {k: f_dev[r0:r0 + n] for k, (r0, n) in enumerate(s.bounds)}
+    H_dev = torch.tensor(H, dtype=torch.float32, device=dev)
+    g_dev = torch.tensor(g_ee, dtype=torch.float32, device=dev)
+    plan = Plan(m, dt, f_eq, device=dev)
+    plan.set_config(cluster_size=0, stage_rows=0, persist_rows=0, strip_rows=0)
+    K = int(np.ceil(np.sqrt(n_steps)))
+
+    def slab_call():
+        s.vjp(rows, H_dev, n_steps * dt, g_ee_hist=g_dev)
+
+    def one_grid_call():
+        out = plan.forward(f_dev, H_dev, n_steps, record_history=False, want_tape=True, checkpoint_every=K,
+                           want_f_final=False)
+        plan.backward(H_dev, n_steps, out["tape"], out["every"], g_ee_hist=g_dev)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(3):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        return sum(ms) / len(ms)
+
+    with ClockSampler(local_rank) as clk:
+        ms_slab = timed(slab_call)
+    ms_one = timed(one_grid_call)
+    cells = nx * nx * n_steps
+    return {"workload": f"two-stream {nx}x{nx}, dt {dt}, {n_steps} steps, 8-mode H, forward + checkpointed "
+                        f"adjoint of J = sum(ee)*dt, {n_slabs} x-slabs on one GPU",
+            "value": round(cells / (ms_slab * 1e-3), 1), "unit": "cell-steps/s fwd+adjoint",
+            "ms_per_call": round(ms_slab, 4), "one_grid_per_column_value": round(cells / (ms_one * 1e-3), 1),
+            "one_grid_ms_per_call": round(ms_one, 4), "n_slabs": n_slabs, "ghost_rows": s.ghost,
+            "exchange_bytes_per_step_per_slab": 2 * 2 * s.ghost * nx * 4, "gather_bytes_per_step": nx * 4,
+            "clocks": clk.summary(), "steps": 3, "warmup": 3,
+            "note": "exchanges are device copies here; over NCCL they become point-to-point sends to the two "
+                    "neighbouring ranks and one all_gather of the row sums per step"}
+
+
 def measure_c5(args, rank, local_rank, world):
     """The surrogate-warm-started control against the plain adjoint loop (the C5 workload at
     its full size), per seed, with the one-off data generation and training reported beside the
@@ -963,6 +1029,7 @@ def main():
             if args.workload == "c2" and world == 1 and not args.no_extras:
                 line["roofline_large"] = measure_large(args, rank, local_rank, world)
                 line["configs"] = {w: measure_config(args, rank, local_rank, world, w) for w in ("c1", "c3", "c4")}
+                line["slab"] = measure_slab(args, rank, local_rank, world)
                 line["c5"] = measure_c5(args, rank, local_rank, world)
         if rank == 0 and world == 1 and not args.no_cpu_baseline and base is not None:
             v, cores, kind, sample = base(wl, args.cpu_seconds)

@@ -204,7 +204,22 @@ __device__ __forceinline__ void res_fill_halo(cg::cluster_group& cluster, T* pla
         const T* src = cluster.map_shared_rank(plane, c) + (size_t)(h_lo + q - c * RC) * nv;
         T* dst = plane + (size_t)l * nv;
         if (nv % VE == 0) {
-            for (int v = lane; v < nv / VE; v += 32) reinterpret_cast<V*>(dst)[v] = reinterpret_cast<const V*>(src)[v];
+            // up to four 16-byte loads per lane in flight before their stores (a store followed by
+            // a load that may alias it would serialise the remote round trips)
+            const int nvec = nv / VE;
+            for (int v0 = 0; v0 < nvec; v0 += 128) {
+                V buf[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int v = v0 + 32 * u + lane;
+                    if (v < nvec) buf[u] = reinterpret_cast<const V*>(src)[v];
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int v = v0 + 32 * u + lane;
+                    if (v < nvec) reinterpret_cast<V*>(dst)[v] = buf[u];
+                }
+            }
         } else {
             for (int v = lane; v < nv; v += 32) dst[v] = src[v];
         }
@@ -216,8 +231,8 @@ __device__ __forceinline__ void res_fill_halo(cg::cluster_group& cluster, T* pla
 // and writes one partial per row to red[row][column group] (no block barrier). (2) After a block
 // barrier, res_rows_local sums each row's column-group partials in ascending order into the CTA's
 // own row-sum slot. (3) After the cluster barrier that publishes the slots, every CTA gathers all
-// nx row sums from the owners (res_rows_gather). Only local shared-memory stores precede the
-// barrier; the exchange is one distributed-shared-memory load per row after it.
+// nx row sums from the owners. Only local shared-memory stores precede the
+// barrier; the exchange is one distributed-shared-memory load per row after it (res_exchange).
 template <int N> struct ILog2 { static constexpr int value = 1 + ILog2<N / 2>::value; };
 template <> struct ILog2<1> { static constexpr int value = 0; };
 
@@ -255,11 +270,23 @@ __device__ __forceinline__ void res_rows_local(const T* red, T* slot, int ncw, i
     }
 }
 
-// out[i] = scale * (row sum of row i), read from slot `par` of the owning CTA.
+// The two exchanges after a step's cluster barrier: the halo rows of `plane` (res_fill_halo) and
+// the row sums, out[i] = scale * (row sum of row i) read from slot `par` of the owning CTA. The
+// first row sum of each thread is loaded before the halo rows move and stored after them, so that
+// the two remote round trips overlap instead of following one another (the halo stores could
+// alias the row-sum slots as far as the compiler knows, so it would not hoist the load itself).
 template <typename T, int RC>
-__device__ __forceinline__ void res_rows_gather(cg::cluster_group& cluster, T* own_slots, int par,
-                                                T* out, int nx, T scale) {
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+__device__ __forceinline__ void res_exchange(cg::cluster_group& cluster, T* plane, int nx, int nv, int gr0,
+                                             int h_lo, int h_hi, T* own_slots, int par, T* out, T scale) {
+    const int i0 = threadIdx.x;
+    T first = T(0);
+    if (i0 < nx) {
+        const int c = i0 / RC;
+        first = cluster.map_shared_rank(own_slots, c)[par * RC + (i0 - c * RC)];
+    }
+    res_fill_halo<T, RC>(cluster, plane, nx, nv, gr0, h_lo, h_hi);
+    if (i0 < nx) out[i0] = scale * first;
+    for (int i = i0 + (int)blockDim.x; i < nx; i += blockDim.x) {
         const int c = i / RC;
         out[i] = scale * cluster.map_shared_rank(own_slots, c)[par * RC + (i - c * RC)];
     }
@@ -407,15 +434,17 @@ __device__ void res_fwd_field(const ResFwdArgs<T>& a, ResSmem<T>& S, cg::cluster
                               int par, int gr0, int k, int me, int CN) {
     const int nx = a.nx, nv = a.nv;
     const int W = a.h_lo + RC + a.h_hi;
-    if (me == 0 && k >= 2 && a.ee_hist != nullptr && threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        const double v = lane < CN ? cluster.map_shared_rank(S.eep, lane)[(k - 2) & 3] : 0.0;
+    // warp 0 of CTA 0: the energy partials are loaded before the exchanges and summed after them
+    const bool ee = me == 0 && k >= 2 && a.ee_hist != nullptr && threadIdx.x < 32;
+    const int lane = threadIdx.x & 31;
+    double eev = 0.0;
+    if (ee && lane < CN) eev = cluster.map_shared_rank(S.eep, lane)[(k - 2) & 3];
+    res_exchange<T, RC>(cluster, plane, nx, nv, gr0, a.h_lo, a.h_hi, S.vec1, par, S.vec0, -a.dv);   // halo, rho
+    if (ee) {
         double tot = 0.0;
-        for (int c = 0; c < CN; ++c) tot += __shfl_sync(0xffffffffu, v, c);
+        for (int c = 0; c < CN; ++c) tot += __shfl_sync(0xffffffffu, eev, c);
         if (lane == 0) a.ee_hist[k - 2] = (T)(0.5 * tot * (double)a.dx);
     }
-    res_fill_halo<T, RC>(cluster, plane, nx, nv, gr0, a.h_lo, a.h_hi);
-    res_rows_gather<T, RC>(cluster, S.vec1, par, S.vec0, nx, -a.dv);   // rho
     const int first = res_grow(gr0, a.h_lo, 0, nx);
     res_circ_rows<T>(S.ctab, S.vec0, S.fld, nx, first, W, false, S.vsh, S.aux, a.dtdv, nv);
     __syncthreads();
@@ -645,9 +674,8 @@ __device__ void res_bwd_field(const ResBwdArgs<T>& a, ResSmem<T>& S, cg::cluster
     const int nx = a.nx;
     const int W = a.h_lo + RC + a.h_hi;
     const int me_i = threadIdx.x;
-    res_fill_halo<T, RC>(cluster, plane, nx, a.nv, gr0, a.h_lo, a.h_hi);
     T* sums = S.vec0;
-    res_rows_gather<T, RC>(cluster, S.vec1, par, sums, nx, T(1));
+    res_exchange<T, RC>(cluster, plane, nx, a.nv, gr0, a.h_lo, a.h_hi, S.vec1, par, sums, T(1));
     const T gee = pre.gee;
     for (int i = threadIdx.x; i < nx; i += blockDim.x) {
         const bool own = i == me_i;
