@@ -204,22 +204,7 @@ __device__ __forceinline__ void res_fill_halo(cg::cluster_group& cluster, T* pla
         const T* src = cluster.map_shared_rank(plane, c) + (size_t)(h_lo + q - c * RC) * nv;
         T* dst = plane + (size_t)l * nv;
         if (nv % VE == 0) {
-            // up to four 16-byte loads per lane in flight before their stores (a store followed by
-            // a load that may alias it would serialise the remote round trips)
-            const int nvec = nv / VE;
-            for (int v0 = 0; v0 < nvec; v0 += 128) {
-                V buf[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int v = v0 + 32 * u + lane;
-                    if (v < nvec) buf[u] = reinterpret_cast<const V*>(src)[v];
-                }
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int v = v0 + 32 * u + lane;
-                    if (v < nvec) reinterpret_cast<V*>(dst)[v] = buf[u];
-                }
-            }
+            for (int v = lane; v < nv / VE; v += 32) reinterpret_cast<V*>(dst)[v] = reinterpret_cast<const V*>(src)[v];
         } else {
             for (int v = lane; v < nv; v += 32) dst[v] = src[v];
         }
