@@ -359,50 +359,92 @@ __device__ void res_init_tables(ResSmem<T>& S, const PoissonTables<T>& P, const 
 }
 
 // Phase A of a float32 step with an x-invariant f_eq: o = V(h) + [V(f_eq) - f_eq] of every local
-// row of `cur` into S.po, computed once per (row, column) instead of once per thread window. Thread
-// t takes the 4 columns j0 = 4 (t mod nv/4) .. j0 + 3 and rows t / (nv/4), + blockDim / (nv/4), ...,
-// so a warp works on one row (one shift) at a time. The arithmetic is the per-cell form of the
+// row of `cur` into S.po, computed once per (row, column) instead of once per thread window, so a
+// warp works on one row (one shift) at a time. The arithmetic is the per-cell form of the
 // thread-window code (lerp of the two source cells plus res_vcorr), so the results are the same
-// bits. Needs nv % 4 == 0 and blockDim.x a multiple of nv / 4.
+// bits. Needs nv % 4 == 0 (and, for res_v_rows, blockDim.x a multiple of nv / 4).
+// v step of one local row l (shift v) on four columns j0 .. j0+3 of the plane `cur`, into the
+// phase-A plane: o = V(h) + [V(f_eq) - f_eq] (the fast forms for shifts 0 and -1).
+__device__ __forceinline__ void res_v_quad(const ResSmem<float>& S, const float* cur, int nv, int l, int j0,
+                                           const VShift<float> v) {
+    const int jm = j0 == 0 ? nv - 1 : j0 - 1, jp = j0 + 4 == nv ? 0 : j0 + 4;
+    const float* hr = cur + (size_t)l * nv;
+    float4 o;
+    if (v.m == 0) {
+        const float4 h = *reinterpret_cast<const float4*>(hr + j0);
+        const float4 dd = *reinterpret_cast<const float4*>(S.dfeq + j0);
+        const float t = v.t;
+        o.x = lerp(h.x, h.y, t) + t * dd.x;
+        o.y = lerp(h.y, h.z, t) + t * dd.y;
+        o.z = lerp(h.z, h.w, t) + t * dd.z;
+        o.w = lerp(h.w, hr[jp], t) + t * dd.w;
+    } else if (v.m == nv - 1) {
+        const float4 h = *reinterpret_cast<const float4*>(hr + j0);
+        const float4 dd = *reinterpret_cast<const float4*>(S.dfeq + j0);
+        const float t = v.t, tm = v.t - 1.f;
+        o.x = lerp(hr[jm], h.x, t) + tm * S.dfeq[jm];
+        o.y = lerp(h.x, h.y, t) + tm * dd.x;
+        o.z = lerp(h.y, h.z, t) + tm * dd.y;
+        o.w = lerp(h.z, h.w, t) + tm * dd.z;
+    } else {
+        float r[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int j = j0 + e;
+            const int c0 = wrap1(j + v.m, nv);
+            const int c1 = c0 + 1 == nv ? 0 : c0 + 1;
+            r[e] = lerp(hr[c0], hr[c1], v.t) + res_vcorr<float, false>(S, nullptr, 0, 0, j, c0, c1, v, nv);
+        }
+        o = make_float4(r[0], r[1], r[2], r[3]);
+    }
+    *reinterpret_cast<float4*>(S.po + (size_t)l * nv + j0) = o;
+}
+
+// Phase A of a step as its own pass: the v step once per (local row, column) of the plane `cur`
+// into S.po, four columns per thread, one row per thread group at a time (blockDim.x a multiple
+// of nv / 4).
 __device__ __forceinline__ void res_v_rows(const ResSmem<float>& S, const float* cur, int nv, int W) {
     const int nq = nv >> 2;
     const int q = threadIdx.x % nq, j0 = 4 * q;
     const int lstep = blockDim.x / nq;
-    const int jm = j0 == 0 ? nv - 1 : j0 - 1, jp = j0 + 4 == nv ? 0 : j0 + 4;
 #pragma unroll 1
-    for (int l = threadIdx.x / nq; l < W; l += lstep) {
-        const VShift<float> v = S.vsh[l];
-        const float* hr = cur + (size_t)l * nv;
-        float4 o;
-        if (v.m == 0) {
-            const float4 h = *reinterpret_cast<const float4*>(hr + j0);
-            const float4 dd = *reinterpret_cast<const float4*>(S.dfeq + j0);
-            const float t = v.t;
-            o.x = lerp(h.x, h.y, t) + t * dd.x;
-            o.y = lerp(h.y, h.z, t) + t * dd.y;
-            o.z = lerp(h.z, h.w, t) + t * dd.z;
-            o.w = lerp(h.w, hr[jp], t) + t * dd.w;
-        } else if (v.m == nv - 1) {
-            const float4 h = *reinterpret_cast<const float4*>(hr + j0);
-            const float4 dd = *reinterpret_cast<const float4*>(S.dfeq + j0);
-            const float t = v.t, tm = v.t - 1.f;
-            o.x = lerp(hr[jm], h.x, t) + tm * S.dfeq[jm];
-            o.y = lerp(h.x, h.y, t) + tm * dd.x;
-            o.z = lerp(h.y, h.z, t) + tm * dd.y;
-            o.w = lerp(h.z, h.w, t) + tm * dd.z;
-        } else {
-            float r[4];
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int j = j0 + e;
-                const int c0 = wrap1(j + v.m, nv);
-                const int c1 = c0 + 1 == nv ? 0 : c0 + 1;
-                r[e] = lerp(hr[c0], hr[c1], v.t) + res_vcorr<float, false>(S, nullptr, 0, 0, j, c0, c1, v, nv);
-            }
-            o = make_float4(r[0], r[1], r[2], r[3]);
+    for (int l = threadIdx.x / nq; l < W; l += lstep) res_v_quad(S, cur, nv, l, j0, S.vsh[l]);
+}
+
+// The forward field of the W local rows and phase A of the next step in one pass, one row per warp
+// at a time: the warp sums E of its row over k (each lane k = lane, lane + 32, ... in order, then
+// an xor tree), derives the row's v shift from E + H, stores both and applies the v step to the
+// row's columns of the plane `cur` into S.po. A row stays with one warp from the field to the
+// plane, so no block barrier separates the two. Used for CTAs of at most 8 own rows, whose W
+// local rows number about as many as the CTA's warps (128^2: 11 % faster per forward loop);
+// with 16 own rows and more the rows' uneven split over the warps cost more than the barrier
+// saved (256^2: 4.6 % slower), and phase A stays a pass of its own there.
+// rho in S.vec0; starts and ends with a block barrier.
+__device__ __forceinline__ void res_field_vrows(const ResSmem<float>& S, const float* cur, int nx, int nv,
+                                                int first, int W, float dtdv) {
+    __syncthreads();
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int off = nx + 8;
+    for (int l = (int)(threadIdx.x >> 5); l < W; l += nw) {
+        int i = first + l;
+        while (i >= nx) i -= nx;
+        const float* cp = S.ctab + off + i - lane;   // coefficient of row i at k: ctab[off + i - k]
+        float acc = 0.f;
+#pragma unroll 4
+        for (int k = lane; k < nx; k += 32) {
+            acc += cp[0] * S.vec0[k];
+            cp -= 32;
         }
-        *reinterpret_cast<float4*>(S.po + (size_t)l * nv + j0) = o;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        const VShift<float> v = res_vshift<float>(acc + S.aux[i], dtdv, nv);
+        if (lane == 0) {
+            S.fld[l] = acc;
+            S.vsh[l] = v;
+        }
+        for (int j0 = 4 * lane; j0 < nv; j0 += 128) res_v_quad(S, cur, nv, l, j0, v);
     }
+    __syncthreads();
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -431,6 +473,12 @@ __device__ void res_fwd_field(const ResFwdArgs<T>& a, ResSmem<T>& S, cg::cluster
         if (lane == 0) a.ee_hist[k - 2] = (T)(0.5 * tot * (double)a.dx);
     }
     const int first = res_grow(gr0, a.h_lo, 0, nx);
+    if constexpr (sizeof(T) == 4 && RC <= 8) {
+        if (S.po != nullptr) {   // float32, x-invariant f_eq, plane present: field + phase A of the next step
+            res_field_vrows(S, plane, nx, nv, first, W, a.dtdv);
+            return;
+        }
+    }
     res_circ_rows<T>(S.ctab, S.vec0, S.fld, nx, first, W, false, S.vsh, S.aux, a.dtdv, nv);
     __syncthreads();
 }
@@ -537,7 +585,7 @@ __global__ void __launch_bounds__(res_max_threads(RPT)) vp_res_fwd_kernel(const 
 #pragma unroll
         for (int k = 0; k < RPT; ++k) wv[k] = T(0);
         int dq = 0;
-        if constexpr (sizeof(T) == 4 && !FEQ2D) {
+        if constexpr (sizeof(T) == 4 && !FEQ2D && RC > 8) {
             if (vrows) {
                 res_v_rows(S, cur, nv, W);   // phase A: the v step once per (row, column)
                 __syncthreads();
