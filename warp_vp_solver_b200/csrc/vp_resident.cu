@@ -202,7 +202,7 @@ __device__ __forceinline__ void res_fill_halo(cg::cluster_group& cluster, T* pla
         const int q = res_grow(gr0, h_lo, l, nx);
         const int c = q / RC;   // RC is a power of two known at compile time
         const T* src = cluster.map_shared_rank(plane, c) + (size_t)(h_lo + q - c * RC) * nv;
-        T* dst = plane + (size_t)l * nv;
+        T* dst = plane + l * nv;   // shared-memory offsets in 32-bit arithmetic
         if (nv % VE == 0) {
             for (int v = lane; v < nv / VE; v += 32) reinterpret_cast<V*>(dst)[v] = reinterpret_cast<const V*>(src)[v];
         } else {
@@ -368,7 +368,7 @@ __device__ void res_init_tables(ResSmem<T>& S, const PoissonTables<T>& P, const 
 __device__ __forceinline__ void res_v_quad(const ResSmem<float>& S, const float* cur, int nv, int l, int j0,
                                            const VShift<float> v) {
     const int jm = j0 == 0 ? nv - 1 : j0 - 1, jp = j0 + 4 == nv ? 0 : j0 + 4;
-    const float* hr = cur + (size_t)l * nv;
+    const float* hr = cur + l * nv;
     float4 o;
     if (v.m == 0) {
         const float4 h = *reinterpret_cast<const float4*>(hr + j0);
@@ -397,7 +397,7 @@ __device__ __forceinline__ void res_v_quad(const ResSmem<float>& S, const float*
         }
         o = make_float4(r[0], r[1], r[2], r[3]);
     }
-    *reinterpret_cast<float4*>(S.po + (size_t)l * nv + j0) = o;
+    *reinterpret_cast<float4*>(S.po + (l * nv + j0)) = o;
 }
 
 // Phase A of a step as its own pass: the v step once per (local row, column) of the plane `cur`
@@ -563,7 +563,7 @@ __global__ void __launch_bounds__(res_max_threads(RPT)) vp_res_fwd_kernel(const 
                 const int i = g + k;
                 T h = lerp(d[k], d[k + 1], t);
                 if (FEQ2D) h += (T)res_xcorr(a.feq, a.feq_rs, nx, i, m, t64, j);
-                Hb[0][(size_t)(hl + rt + k) * nv + j] = h;
+                Hb[0][(hl + rt + k) * nv + j] = h;
                 wv[k] = wj * h;
                 if (a.h_tape != nullptr) a.h_tape[(size_t)i * nv + j] = h;
             }
@@ -598,15 +598,15 @@ __global__ void __launch_bounds__(res_max_threads(RPT)) vp_res_fwd_kernel(const 
             bool from_plane = false;
             if constexpr (sizeof(T) == 4 && !FEQ2D) from_plane = vrows;
             if (from_plane) {
-                const T* op = S.po + (size_t)l0 * nv + j;
+                const T* op = S.po + (l0 * nv + j);
 #pragma unroll
-                for (int k = 0; k < RPT + 2; ++k) o[k] = op[(size_t)k * nv];
+                for (int k = 0; k < RPT + 2; ++k) o[k] = op[k * nv];
             } else {
 #pragma unroll
                 for (int k = 0; k < RPT + 2; ++k) {
                     const int l = l0 + k;
                     const VShift<T> v = S.vsh[l];
-                    const T* hr = cur + (size_t)l * nv;
+                    const T* hr = cur + l * nv;
                     const int c0 = wrap1(j + v.m, nv);
                     const int c1 = c0 + 1 == nv ? 0 : c0 + 1;
                     const int q = FEQ2D ? res_grow(gr0, hl, l, nx) : 0;
@@ -626,7 +626,7 @@ __global__ void __launch_bounds__(res_max_threads(RPT)) vp_res_fwd_kernel(const 
                     T h = lerp(d[k], d[k + 1], t);
                     if (FEQ2D) h += (T)res_xcorr(a.feq, a.feq_rs, nx, g + k, m, t64, j);
                     hv[k] = h;
-                    nxt[(size_t)(hl + rt + k) * nv + j] = h;
+                    nxt[(hl + rt + k) * nv + j] = h;
                     wv[k] = wj * h;
                 }
             }
@@ -773,7 +773,7 @@ __device__ __forceinline__ void res_bwd_w(const ResBwdArgs<T>& a, const ResSmem<
     for (int k = 0; k < RPT; ++k) {
         const int i = g + k;
         const T wv = lerp(c[k + 1], c[k], t);
-        own_rows[(size_t)(rt + k) * nv + j] = wv;
+        own_rows[(rt + k) * nv + j] = wv;
         const int d0 = wrap1(j + vs[k].m, nv);
         const int d1 = d0 + 1 == nv ? 0 : d0 + 1;
         T sl = h1[k] - h0[k];
@@ -843,7 +843,7 @@ __global__ void __launch_bounds__(res_max_threads(RPT)) vp_res_bwd_kernel(const 
                 if (a.g_fh != nullptr) v += __ldg(a.g_fh + ((size_t)(T_steps - 1) * nx + q) * nv + j);
                 c[k] = v;
             }
-            res_bwd_w<T, RPT, FEQ2D>(a, S, c, nxt + (size_t)hl * nv, prod, vA, hA0, hA1, g, rt, j, t);
+            res_bwd_w<T, RPT, FEQ2D>(a, S, c, nxt + hl * nv, prod, vA, hA0, hA1, g, rt, j, t);
             // next: slopes of step T-2
 #pragma unroll
             for (int k = 0; k < RPT; ++k) vA[k] = vB[k];
@@ -875,7 +875,7 @@ __global__ void __launch_bounds__(res_max_threads(RPT)) vp_res_bwd_kernel(const 
                 if (k < ng) {
                     const int l = l0 + k;
                     const VShift<T> v = S.vsh[l];
-                    const T* wrow = cur + (size_t)l * nv;
+                    const T* wrow = cur + l * nv;
                     const int c0 = wrapneg(j - v.m, nv);
                     const int c1 = wrapneg(c0 - 1, nv);
                     gh[k] = lerp(wrow[c0], wrow[c1], v.t) + wr * S.fld[l];
@@ -895,7 +895,7 @@ __global__ void __launch_bounds__(res_max_threads(RPT)) vp_res_bwd_kernel(const 
                     if (a.g_fh != nullptr)
                         c[k] += __ldg(a.g_fh + ((size_t)(n - 1) * nx + wrap1(cb + k, nx)) * nv + j);
                 }
-                res_bwd_w<T, RPT, FEQ2D>(a, S, c, nxt + (size_t)hl * nv, prod, vA, hA0, hA1, g, rt, j, t);
+                res_bwd_w<T, RPT, FEQ2D>(a, S, c, nxt + hl * nv, prod, vA, hA0, hA1, g, rt, j, t);
                 // next: slopes of step n-2 (h loads now, shifts of step n-3 for the one after)
 #pragma unroll
                 for (int k = 0; k < RPT; ++k) vA[k] = vB[k];
