@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(kPstThreads, 2) vp_persist_fwd_kernel(const Pe
         *r0 = band_row(bi);
     };
     auto stage_ptr = [&](unsigned k) {
-        return stages + (size_t)(gid * S + (int)(k % (unsigned)S)) * a.span_max * kPstW;
+        return stages + (gid * S + (int)(k % (unsigned)S)) * a.span_max * kPstW;   // 32-bit shared offsets
     };
     auto issue = [&](int j, const float* src) {
         const unsigned mine = tiles_issued++;
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(kPstThreads, 2) vp_persist_fwd_kernel(const Pe
             int col = c0 - 4 + 4 * v;
             col += col < 0 ? nv : 0;
             col -= col >= nv ? nv : 0;
-            pst_cp16(st + (size_t)k * kPstW + 4 * v, src + (size_t)pst_wrap(lo + k, nx) * nv + col);
+            pst_cp16(st + (k * kPstW + 4 * v), src + (size_t)pst_wrap(lo + k, nx) * nv + col);
         }
         pst_cp_commit();
     };
@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(kPstThreads, 2) vp_persist_fwd_kernel(const Pe
                 const float* st = stage_ptr(tiles_used);
                 ++tiles_used;
                 // window row k of this thread: stage row 2*(bm - cm.x) + k, global row r0 + 2*bm + k
-                const float* sb = st + (size_t)(2 * (qi.x - cm.x)) * kPstW + 4 + 4 * gt;
+                const float* sb = st + (2 * (qi.x - cm.x) * kPstW + 4 + 4 * gt);
                 const int ib = bi * a.win_rows + 2 * qi.x - a.win_lo;   // rinfo index of window row 0
                 // rolling over the window rows: after o row k, d row q = k - 3 (o rows q .. q + 3)
                 // and h' row r = k - 4 (d rows r, r + 1) are complete
@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(kPstThreads, 2) vp_persist_fwd_kernel(const Pe
                     float* o = O[k & 3];
                     const int2 ri = rinfo[ib + k];
                     const float tv = __int_as_float(ri.y);
-                    const float* sr = sb + (size_t)k * kPstW;
+                    const float* sr = sb + k * kPstW;
                     if (ri.x == 0) {
                         const float4 h = *reinterpret_cast<const float4*>(sr);
                         const float h4 = sr[4];
@@ -556,7 +556,7 @@ __global__ void __launch_bounds__(kPstThreads, 2) vp_persist_bwd_kernel(const Pe
     constexpr int kPieces = kPstW / 4;
     unsigned tiles_issued = 0, tiles_used = 0;
     auto stage_ptr = [&](unsigned k) {
-        return stages + (size_t)(gid * S + (int)(k % (unsigned)S)) * srows * kPstW;
+        return stages + (gid * S + (int)(k % (unsigned)S)) * srows * kPstW;
     };
     auto issue = [&](int j, const float* w_src, const float* h_src) {
         const unsigned mine = tiles_issued++;
@@ -576,7 +576,7 @@ __global__ void __launch_bounds__(kPstThreads, 2) vp_persist_bwd_kernel(const Pe
             const float* src = wrow ? w_src + (size_t)pst_wrap(lo + k, nx) * nv + col
                                     : h_src + (size_t)(r0 + k - span) * nv + col;
             const int srow = wrow ? k : a.span_max + (k - span);
-            pst_cp16(st + (size_t)srow * kPstW + 4 * v, src);
+            pst_cp16(st + (srow * kPstW + 4 * v), src);
         }
         pst_cp_commit();
     };
@@ -651,8 +651,8 @@ __global__ void __launch_bounds__(kPstThreads, 2) vp_persist_bwd_kernel(const Pe
                 group_sync();
                 const float* st = stage_ptr(tiles_used);
                 ++tiles_used;
-                const float* sb = st + (size_t)(2 * (cm.y - Q.bm)) * kPstW + 4 + 4 * gt;   // window row 0
-                const float* hb = st + (size_t)a.span_max * kPstW + 4 + 4 * gt;            // own row 0
+                const float* sb = st + (2 * (cm.y - Q.bm) * kPstW + 4 + 4 * gt);   // window row 0
+                const float* hb = st + (a.span_max * kPstW + 4 + 4 * gt);            // own row 0
                 const int ib = bi * a.win_rows + (-2 * Q.bm - 4 - a.win_lo);
                 float GH[4][4], cprev[4];
 #pragma unroll
@@ -660,7 +660,7 @@ __global__ void __launch_bounds__(kPstThreads, 2) vp_persist_bwd_kernel(const Pe
                     float* o = GH[k & 3];
                     const int4 ri = rinfo[ib + k];
                     const float tv = __int_as_float(ri.y), gr = __int_as_float(ri.z);
-                    const float* sr = sb + (size_t)k * kPstW;
+                    const float* sr = sb + k * kPstW;
                     float4 v4;
                     if (ri.x == 0) {
                         const float hm = sr[-1];
@@ -703,7 +703,7 @@ __global__ void __launch_bounds__(kPstThreads, 2) vp_persist_bwd_kernel(const Pe
                             *reinterpret_cast<float4*>(w_dst + (size_t)(r0 + r) * nv + j0) =
                                 make_float4(wv[0], wv[1], wv[2], wv[3]);
                             const int ms = hinfo[bi * R + r];
-                            const float* hr = hb + (size_t)r * kPstW;
+                            const float* hr = hb + r * kPstW;
                             float4 sl;
                             if (ms == 0) {
                                 const float4 h = *reinterpret_cast<const float4*>(hr);
