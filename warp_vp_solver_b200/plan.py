@@ -58,6 +58,7 @@ class Plan:
                                                 _DTYPES[self.dtype], ctypes.byref(handle)))
         self._h = handle
         self._ws: dict[tuple[int, int], torch.Tensor] = {}
+        self._sizes: dict = {}   # checkpoint intervals and tape sizes per (n_steps, every), per launch shape
 
     # ---------------------------------------------------------------- housekeeping
     def close(self) -> None:
@@ -105,6 +106,7 @@ class Plan:
         c.strip_adj_cols = 0 if strip_adj_cols is None else int(strip_adj_cols)
         _capi.check(self.lib.vp_plan_set_config(self._h, ctypes.byref(c)))
         self._ws = {}   # workspace size depends on n_chunks and the persistent and strip launch shapes
+        self._sizes = {}
 
     def set_wait_limit(self, ns: int) -> None:
         """Limit of each device-side grid-barrier wait of the persistent launches (ns; 0: no wait)."""
@@ -124,6 +126,7 @@ class Plan:
         path (True)."""
         _capi.check(self.lib.vp_plan_set_scheme(
             self._h, _capi.VP_SCHEME_MERGED if merged else _capi.VP_SCHEME_STRANG))
+        self._sizes = {}
 
     @property
     def merged(self) -> bool:
@@ -137,10 +140,14 @@ class Plan:
         return int(out.value)
 
     def resolve_every(self, n_steps: int, every: int | None) -> int:
-        out = ctypes.c_int32()
-        _capi.check(self.lib.vp_resolve_checkpoint_every(self._h, int(n_steps), int(every or 0),
-                                                         ctypes.byref(out)))
-        return int(out.value)
+        key = ("every", int(n_steps), int(every or 0))
+        hit = self._sizes.get(key)
+        if hit is None:
+            out = ctypes.c_int32()
+            _capi.check(self.lib.vp_resolve_checkpoint_every(self._h, int(n_steps), int(every or 0),
+                                                             ctypes.byref(out)))
+            hit = self._sizes[key] = int(out.value)
+        return hit
 
     def workspace_bytes(self, n_steps: int, every: int) -> int:
         out = ctypes.c_size_t()
@@ -148,9 +155,13 @@ class Plan:
         return int(out.value)
 
     def tape_bytes(self, n_steps: int, every: int) -> int:
-        out = ctypes.c_size_t()
-        _capi.check(self.lib.vp_tape_bytes(self._h, int(n_steps), int(every), ctypes.byref(out)))
-        return int(out.value)
+        key = ("tape", int(n_steps), int(every))
+        hit = self._sizes.get(key)
+        if hit is None:
+            out = ctypes.c_size_t()
+            _capi.check(self.lib.vp_tape_bytes(self._h, int(n_steps), int(every), ctypes.byref(out)))
+            hit = self._sizes[key] = int(out.value)
+        return hit
 
     def workspace(self, n_steps: int, every: int) -> torch.Tensor:
         key = (int(n_steps), int(every))

@@ -283,8 +283,10 @@ class _VPFunction(torch.autograd.Function):
             g_f_hist = None
         g_fiv, g_H = plan.backward(H, ctx.n_steps, tape if tape.numel() else None, ctx.every,
                                    g_f_final, g_f_hist, g_E_hist, g_ee_hist)
-        return (g_fiv.to(device=ctx.f_device, dtype=ctx.f_dtype),
-                g_H.to(device=ctx.H_device, dtype=ctx.H_dtype), None, None, None)
+        # inputs that need no gradient get none (no cast launched for them)
+        return (g_fiv.to(device=ctx.f_device, dtype=ctx.f_dtype) if ctx.needs_input_grad[0] else None,
+                g_H.to(device=ctx.H_device, dtype=ctx.H_dtype) if ctx.needs_input_grad[1] else None,
+                None, None, None)
 
 
 def run_forward_jax_compatible(f_iv, H, t_final, solver_instance: WarpVlasovPoissonSolver):

@@ -25,16 +25,16 @@ _BASIS_CACHE: dict = {}
 
 
 def _fourier_basis(xs: np.ndarray, N: int, k_0: float, dtype, device):
-    """cos(k0 k x) and sin(k0 k x) for k = 1..N on the mesh points, built once per mesh, mode
-    count, dtype and device (a host-to-device copy of the points inside every call would
-    serialise the caller's stream with the host)."""
+    """The stacked basis [cos(k0 k x); sin(k0 k x)] for k = 1..N on the mesh points, shape (2N, nx),
+    built once per mesh, mode count, dtype and device (a host-to-device copy of the points inside
+    every call would serialise the caller's stream with the host)."""
     key = (xs.tobytes(), int(N), float(k_0), dtype, str(device))
     hit = _BASIS_CACHE.get(key)
     if hit is None:
         k = torch.arange(1, N + 1, dtype=dtype, device=device)
         x = torch.as_tensor(xs, dtype=dtype, device=device)
         arg = k_0 * k[:, None] * x[None, :]
-        hit = (torch.cos(arg), torch.sin(arg))
+        hit = torch.cat([torch.cos(arg), torch.sin(arg)], dim=0).contiguous()
         if len(_BASIS_CACHE) >= 32:
             _BASIS_CACHE.clear()
         _BASIS_CACHE[key] = hit
@@ -42,12 +42,13 @@ def _fourier_basis(xs: np.ndarray, N: int, k_0: float, dtype, device):
 
 
 def external_electric_field(ak, mesh, k_0: float) -> torch.Tensor:
-    """H(x) = sum_k a_k cos(k0 k x) + b_k sin(k0 k x) (utils.py:37-48). ``ak`` has shape (2, N)."""
+    """H(x) = sum_k a_k cos(k0 k x) + b_k sin(k0 k x) (utils.py:37-48). ``ak`` has shape (2, N).
+    Evaluated as one product of the flattened coefficients with the stacked basis (one launch
+    forward and one backward on the device)."""
     ak = _as_tensor(ak)
     N = ak.shape[1]
-    cos_b, sin_b = _fourier_basis(np.ascontiguousarray(mesh.xs, dtype=np.float64), N, k_0, ak.dtype,
-                                  ak.device)
-    return ak[0, :] @ cos_b + ak[1, :] @ sin_b
+    basis = _fourier_basis(np.ascontiguousarray(mesh.xs, dtype=np.float64), N, k_0, ak.dtype, ak.device)
+    return ak.reshape(2 * N) @ basis
 
 
 def electric_energy_in_time(ee_array, solver) -> torch.Tensor:
