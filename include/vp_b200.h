@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define VP_ABI_VERSION 6
+#define VP_ABI_VERSION 7
 
 /* status codes */
 #define VP_OK 0
@@ -74,6 +74,12 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
                    vp_plan** out_plan);
 
 /* Releases a plan and its device tables. */
+/* The same plan from one row of f_eq (nv values) that every x row equals: an x-invariant f_eq
+ * without its nx*nv host array, for grids too large for one GPU that x slabs split. No
+ * counterpart in the reference, which always builds the full (nx, nv) f_eq
+ * (warp_vp_solver/solver.py:170-203). */
+int vp_plan_create_from_row(const vp_mesh_desc* mesh, double dt, const double* f_eq_row, int dtype,
+                            vp_plan** out_plan);
 int vp_plan_destroy(vp_plan* plan);
 
 /* Device-side status of a plan: flags that kernels raise without synchronising the host, read

@@ -124,3 +124,20 @@ def test_dist_ring_one_rank_nccl(record_error):
         dist.destroy_process_group()
     bad = {k: v for k, v in diffs.items() if v != 0.0}
     assert not bad, f"slab results differ from the one-grid per-column path: {bad}"
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_plan_from_one_row_equals_plan_from_the_full_array(dtype):
+    """vp_plan_create_from_row (f_eq as its nv-value row) gives the plan vp_plan_create gives for
+    the broadcast (nx, nv) array: the same path and the same results bit for bit."""
+    length_x, nx, nv, dt, T = CASES[0][:5]
+    m, f_eq, f_iv, H, gEh, gff = _problem(length_x, nx, nv, dt, 12)
+    full = Plan(m, dt, np.broadcast_to(f_eq, (nx, nv)), dtype=dtype)
+    row = Plan(m, dt, f_eq, dtype=dtype)
+    assert row.row_only and not full.row_only
+    assert row.get_config() == full.get_config()
+    a = full.forward(f_iv, H, 12, record_history=True)
+    b = row.forward(f_iv, H, 12, record_history=True)
+    torch.cuda.synchronize()
+    for k in ("f_final", "f_hist", "E_hist", "ee_hist"):
+        assert torch.equal(a[k], b[k]), k

@@ -104,7 +104,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_error_reporting_without_device():
     lib = _capi.load()
-    assert lib.vp_abi_version() == _capi.ABI_VERSION == 6
+    assert lib.vp_abi_version() == _capi.ABI_VERSION == 7
     assert lib.vp_plan_destroy(None) == 0
     out = ctypes.c_void_p()
     rc = lib.vp_plan_create(None, 0.1, None, 0, ctypes.byref(out))

@@ -157,3 +157,12 @@ def test_slab_abi_rejects_null_handles_without_a_device():
     assert lib.vp_slab_forward_start(None, None, None, None, None) == _capi.VP_ERR_ARG
     assert lib.vp_slab_backward_finish(None, None, None, None, None, None) == _capi.VP_ERR_ARG
     assert lib.vp_slab_destroy(None) == 0
+
+
+def test_plan_from_row_rejects_null_arguments_without_a_device():
+    import ctypes
+    from warp_vp_solver_b200 import _capi
+    lib = _capi.load()
+    out = ctypes.c_void_p()
+    assert lib.vp_plan_create_from_row(None, 0.1, None, 0, ctypes.byref(out)) == _capi.VP_ERR_ARG
+    assert "must not be NULL" in _capi.last_error()

@@ -23,7 +23,7 @@ VP_SCHEME_STRANG = 0
 VP_SCHEME_MERGED = 1
 VP_STATUS_NONFINITE_INPUT = 1
 VP_STATUS_WAIT_TIMEOUT = 2
-ABI_VERSION = 6   # VP_ABI_VERSION of the header these bindings follow
+ABI_VERSION = 7   # VP_ABI_VERSION of the header these bindings follow
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libvpb200.so")
 
@@ -101,6 +101,8 @@ SIGNATURES = {
     "vp_reset_launch_count": (None, []),
     "vp_plan_create": (c_int, [ctypes.POINTER(MeshDesc), c_dbl, ctypes.POINTER(c_dbl), c_int,
                                ctypes.POINTER(c_vp)]),
+    "vp_plan_create_from_row": (c_int, [ctypes.POINTER(MeshDesc), c_dbl, ctypes.POINTER(c_dbl), c_int,
+                                        ctypes.POINTER(c_vp)]),
     "vp_plan_destroy": (c_int, [c_vp]),
     "vp_plan_get_config": (c_int, [c_vp, ctypes.POINTER(LaunchConfig)]),
     "vp_plan_set_scheme": (c_int, [c_vp, c_i32]),

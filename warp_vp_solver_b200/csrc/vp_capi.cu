@@ -1111,8 +1111,10 @@ int vp_get_last_error(char* buf, size_t buf_len) {
 int64_t vp_launch_count(void) { return g_launches; }
 void vp_reset_launch_count(void) { g_launches = 0; }
 
-int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host, int dtype,
-                   vp_plan** out_plan) {
+// Plan set-up from f_eq given either as nx*nv values (row_only == false) or as one row of nv
+// values that every row of the grid equals (row_only == true: x-invariant, no nx*nv host array).
+static int plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host, bool row_only, int dtype,
+                       vp_plan** out_plan) {
     if (out_plan == nullptr) return set_err(VP_ERR_ARG, "out_plan must not be NULL");
     *out_plan = nullptr;
     if (mesh == nullptr || f_eq_host == nullptr || mesh->xs == nullptr || mesh->vs == nullptr)
@@ -1131,9 +1133,11 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
         if (!std::isfinite(mesh->vs[j])) return set_err(VP_ERR_ARG, "vs[%d] is not finite", j);
     for (int i = 0; i < nx; ++i)
         if (!std::isfinite(mesh->xs[i])) return set_err(VP_ERR_ARG, "xs[%d] is not finite", i);
-    for (size_t c = 0; c < (size_t)nx * nv; ++c)
+    const size_t feq_given = row_only ? (size_t)nv : (size_t)nx * nv;
+    for (size_t c = 0; c < feq_given; ++c)
         if (!std::isfinite(f_eq_host[c]))
-            return set_err(VP_ERR_ARG, "f_eq[%zu, %zu] is not finite", c / (size_t)nv, c % (size_t)nv);
+            return set_err(VP_ERR_ARG, "f_eq[%zu, %zu] is not finite", row_only ? (size_t)0 : c / (size_t)nv,
+                           c % (size_t)nv);
 
     vp_plan* p = new (std::nothrow) vp_plan();
     if (!p) return set_err(VP_ERR_ARG, "out of host memory");
@@ -1155,10 +1159,10 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
 
     // f_eq: x-invariant when every row equals the first one exactly
     bool inv = true;
-    for (int i = 1; i < nx && inv; ++i)
+    for (int i = 1; i < nx && inv && !row_only; ++i)
         inv = std::memcmp(f_eq_host + (size_t)i * nv, f_eq_host, (size_t)nv * sizeof(double)) == 0;
     p->feq2d = inv ? 0 : 1;
-    p->host_feq.assign(f_eq_host, f_eq_host + (size_t)nx * nv);
+    p->host_feq.assign(f_eq_host, f_eq_host + feq_given);
     p->host_vs.assign(mesh->vs, mesh->vs + nv);
 
     // x half-step table: s_j = 0.5*v_j*dt/dx, m_j = floor(-s_j) mod nx, t_j = -s_j - floor(-s_j)
@@ -1346,10 +1350,11 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
         double tot = 0.0;
         for (int i = 0; i < nx; ++i) {
             const double wx = (i == 0 || i == nx - 1) ? 0.5 * mesh->dx : mesh->dx;
+            const double* fr = f_eq_host + (row_only ? (size_t)0 : (size_t)i * nv);
             double row = 0.0;
             for (int j = 0; j < nv; ++j) {
                 const double wv = (j == 0 || j == nv - 1) ? 0.5 * mesh->dv : mesh->dv;
-                row += wv * f_eq_host[(size_t)i * nv + j];
+                row += wv * fr[j];
             }
             tot += wx * row;
         }
@@ -1357,6 +1362,15 @@ int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host,
     }
     *out_plan = p;
     return VP_OK;
+}
+
+int vp_plan_create(const vp_mesh_desc* mesh, double dt, const double* f_eq_host, int dtype, vp_plan** out_plan) {
+    return plan_create(mesh, dt, f_eq_host, false, dtype, out_plan);
+}
+
+int vp_plan_create_from_row(const vp_mesh_desc* mesh, double dt, const double* f_eq_row, int dtype,
+                            vp_plan** out_plan) {
+    return plan_create(mesh, dt, f_eq_row, true, dtype, out_plan);
 }
 
 int vp_plan_get_config(const vp_plan* plan, vp_launch_config* out) {

@@ -44,8 +44,10 @@ class Plan:
         self.nx, self.nv = int(mesh.nx), int(mesh.nv)
         self.dt = float(dt)
         f_eq = np.ascontiguousarray(np.asarray(f_eq, dtype=np.float64))
-        if f_eq.shape != (self.nx, self.nv):
-            raise ValueError(f"f_eq shape {f_eq.shape} != ({self.nx}, {self.nv})")
+        # one row (nv,): an x-invariant f_eq given without its (nx, nv) array
+        self.row_only = f_eq.shape == (self.nv,)
+        if not self.row_only and f_eq.shape != (self.nx, self.nv):
+            raise ValueError(f"f_eq shape {f_eq.shape} != ({self.nx}, {self.nv}) or ({self.nv},)")
         self.f_eq = f_eq
         self._xs = np.ascontiguousarray(np.asarray(mesh.xs, dtype=np.float64))
         self._vs = np.ascontiguousarray(np.asarray(mesh.vs, dtype=np.float64))
@@ -53,9 +55,10 @@ class Plan:
                               float(mesh.dx), float(mesh.dv), float(mesh.period_x),
                               float(mesh.period_v))
         handle = ctypes.c_void_p()
+        create = self.lib.vp_plan_create_from_row if self.row_only else self.lib.vp_plan_create
         with torch.cuda.device(self.device):
-            _capi.check(self.lib.vp_plan_create(ctypes.byref(desc), self.dt, _capi.dbl_ptr(f_eq),
-                                                _DTYPES[self.dtype], ctypes.byref(handle)))
+            _capi.check(create(ctypes.byref(desc), self.dt, _capi.dbl_ptr(f_eq), _DTYPES[self.dtype],
+                               ctypes.byref(handle)))
         self._h = handle
         self._ws: dict[tuple[int, int], torch.Tensor] = {}
         self._sizes: dict = {}   # checkpoint intervals and tape sizes per (n_steps, every), per launch shape

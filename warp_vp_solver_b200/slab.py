@@ -214,8 +214,12 @@ class SlabSolver:
         self.rows = {s: self.bounds[s][1] for s in range(ring.n_slabs)}
         if ops_factory is None:
             f_eq = np.asarray(f_eq, dtype=np.float64)
-            if f_eq.ndim == 1:
-                f_eq = np.broadcast_to(f_eq, (self.nx, self.nv))
+            if f_eq.ndim == 2:   # x slabs need an x-invariant f_eq: keep its first row
+                if not (f_eq == f_eq[:1]).all():
+                    raise ValueError("x slabs need an x-invariant f_eq (every row equal)")
+                f_eq = f_eq[0]
+            # the plan is built from the row alone: no (nx, nv) host array for a grid too large
+            # for one GPU
             self.plan = Plan(mesh, dt, f_eq, dtype=self.dtype, device=device)
             ops_factory = lambda row0, n_rows: CudaSlabOps(self.plan, row0, n_rows)   # noqa: E731
         self.ops = {s: ops_factory(*self.bounds[s]) for s in ring.local}
