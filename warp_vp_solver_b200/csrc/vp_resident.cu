@@ -740,14 +740,18 @@ __device__ __forceinline__ void res_bwd_load_shifts(const ResBwdArgs<T>& a, int 
     for (int k = 0; k < RPT; ++k) vs[k] = a.vsh_tape[(size_t)np * a.nx + g + k];
 }
 
-template <typename T, int RPT>
-__device__ __forceinline__ void res_bwd_load_h(const ResBwdArgs<T>& a, int np, int g, int j,
-                                               const VShift<T> (&vs)[RPT], T (&h0)[RPT], T (&h1)[RPT]) {
+// With an x-invariant f_eq the f_eq slope D[d0] of each row is read here too (fd), so that the
+// step that uses the slopes needs no shifts and no index wraps.
+template <typename T, int RPT, bool FEQ2D>
+__device__ __forceinline__ void res_bwd_load_h(const ResBwdArgs<T>& a, const ResSmem<T>& S, int np, int g, int j,
+                                               const VShift<T> (&vs)[RPT], T (&h0)[RPT], T (&h1)[RPT],
+                                               T (&fd)[RPT]) {
     const int nv = a.nv;
 #pragma unroll
     for (int k = 0; k < RPT; ++k) {
         h0[k] = T(0);
         h1[k] = T(0);
+        fd[k] = T(0);
     }
     if (np < 0) return;
 #pragma unroll
@@ -757,6 +761,7 @@ __device__ __forceinline__ void res_bwd_load_h(const ResBwdArgs<T>& a, int np, i
         const T* hr = a.h_tape + ((size_t)np * a.nx + g + k) * nv;
         h0[k] = __ldg(hr + d0);
         h1[k] = __ldg(hr + d1);
+        if (!FEQ2D) fd[k] = S.dfeq[d0];
     }
 }
 
@@ -767,20 +772,21 @@ template <typename T, int RPT, bool FEQ2D>
 __device__ __forceinline__ void res_bwd_w(const ResBwdArgs<T>& a, const ResSmem<T>& S,
                                           const T (&c)[RPT + 1], T* own_rows, T (&prod)[RPT],
                                           const VShift<T> (&vs)[RPT], const T (&h0)[RPT],
-                                          const T (&h1)[RPT], int g, int rt, int j, T t) {
+                                          const T (&h1)[RPT], const T (&fd)[RPT], int g, int rt, int j, T t) {
     const int nv = a.nv;
 #pragma unroll
     for (int k = 0; k < RPT; ++k) {
-        const int i = g + k;
         const T wv = lerp(c[k + 1], c[k], t);
         own_rows[(rt + k) * nv + j] = wv;
-        const int d0 = wrap1(j + vs[k].m, nv);
-        const int d1 = d0 + 1 == nv ? 0 : d0 + 1;
         T sl = h1[k] - h0[k];
-        if (FEQ2D)
+        if constexpr (FEQ2D) {
+            const int i = g + k;
+            const int d0 = wrap1(j + vs[k].m, nv);
+            const int d1 = d0 + 1 == nv ? 0 : d0 + 1;
             sl += (T)(__ldg(a.feq + (size_t)i * a.feq_rs + d1) - __ldg(a.feq + (size_t)i * a.feq_rs + d0));
-        else
-            sl += S.dfeq[d0];
+        } else {
+            sl += fd[k];
+        }
         prod[k] = sl * wv;
     }
 }
@@ -807,6 +813,7 @@ __global__ void __launch_bounds__(res_max_threads(RPT)) vp_res_bwd_kernel(const 
     T* red = S.p2;             // row partials of the warps
     res_init_tables<T>(S, a.P, a.feq, FEQ2D, nx, nv);
     for (int r = threadIdx.x; r < RC; r += blockDim.x) S.own[r] = T(0);
+    __syncthreads();   // S.dfeq is complete before the first slope loads read it
     int m = 0, sm = 0;
     T t = T(0), wr = T(0);
     if (colv) {
@@ -817,11 +824,11 @@ __global__ void __launch_bounds__(res_max_threads(RPT)) vp_res_bwd_kernel(const 
     }
     // slope inputs: vA/hA of the step whose slopes come next, vB the shifts of the step after it
     VShift<T> vA[RPT], vB[RPT];
-    T hA0[RPT], hA1[RPT];
+    T hA0[RPT], hA1[RPT], fdA[RPT];
     ResBwdPre<T> pre = res_bwd_prefetch<T>(a, T_steps - 1, gr0, W);
     if (colv) {
         res_bwd_load_shifts<T, RPT>(a, T_steps - 1, g, vA);
-        res_bwd_load_h<T, RPT>(a, T_steps - 1, g, j, vA, hA0, hA1);
+        res_bwd_load_h<T, RPT, FEQ2D>(a, S, T_steps - 1, g, j, vA, hA0, hA1, fdA);
         res_bwd_load_shifts<T, RPT>(a, T_steps - 2, g, vB);
     }
     __syncthreads();
@@ -843,11 +850,11 @@ __global__ void __launch_bounds__(res_max_threads(RPT)) vp_res_bwd_kernel(const 
                 if (a.g_fh != nullptr) v += __ldg(a.g_fh + ((size_t)(T_steps - 1) * nx + q) * nv + j);
                 c[k] = v;
             }
-            res_bwd_w<T, RPT, FEQ2D>(a, S, c, nxt + hl * nv, prod, vA, hA0, hA1, g, rt, j, t);
+            res_bwd_w<T, RPT, FEQ2D>(a, S, c, nxt + hl * nv, prod, vA, hA0, hA1, fdA, g, rt, j, t);
             // next: slopes of step T-2
 #pragma unroll
             for (int k = 0; k < RPT; ++k) vA[k] = vB[k];
-            res_bwd_load_h<T, RPT>(a, T_steps - 2, g, j, vA, hA0, hA1);
+            res_bwd_load_h<T, RPT, FEQ2D>(a, S, T_steps - 2, g, j, vA, hA0, hA1, fdA);
             res_bwd_load_shifts<T, RPT>(a, T_steps - 3, g, vB);
         }
         res_warp_rows<T, RPT>(prod, red, rt, cw, ncw);
@@ -895,11 +902,11 @@ __global__ void __launch_bounds__(res_max_threads(RPT)) vp_res_bwd_kernel(const 
                     if (a.g_fh != nullptr)
                         c[k] += __ldg(a.g_fh + ((size_t)(n - 1) * nx + wrap1(cb + k, nx)) * nv + j);
                 }
-                res_bwd_w<T, RPT, FEQ2D>(a, S, c, nxt + hl * nv, prod, vA, hA0, hA1, g, rt, j, t);
+                res_bwd_w<T, RPT, FEQ2D>(a, S, c, nxt + hl * nv, prod, vA, hA0, hA1, fdA, g, rt, j, t);
                 // next: slopes of step n-2 (h loads now, shifts of step n-3 for the one after)
 #pragma unroll
                 for (int k = 0; k < RPT; ++k) vA[k] = vB[k];
-                res_bwd_load_h<T, RPT>(a, n - 2, g, j, vA, hA0, hA1);
+                res_bwd_load_h<T, RPT, FEQ2D>(a, S, n - 2, g, j, vA, hA0, hA1, fdA);
                 res_bwd_load_shifts<T, RPT>(a, n - 3, g, vB);
             }
         }
