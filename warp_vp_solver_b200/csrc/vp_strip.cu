@@ -436,9 +436,9 @@ __device__ __forceinline__ void strip_fwd_body(const StripFwdArgs& a, unsigned c
             a.rho_out[row] = -a.dv * strip_chunk_sum(a.part, nx, a.n_chunks, row);
 }
 
-template <int R, int GT>
 // 640 / GT CTAs per SM: 10 two-warp CTAs (up to 96 registers) measured 4 % faster on 8192^2 than
 // 12 (80 registers), which the shared memory of the ring would also allow
+template <int R, int GT>
 __global__ void __launch_bounds__(GT, 640 / GT) vp_strip_fwd_kernel(const StripFwdArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_last;
