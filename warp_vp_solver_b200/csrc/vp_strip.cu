@@ -794,7 +794,9 @@ __global__ void __launch_bounds__(kFieldThreads) vp_strip_field_kernel(const Str
 // ensemble's packed ones (BatchStep), the tables and offsets each instance's (StripInst).
 // ---------------------------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(kStripEnsThreads, 24)
+// 20 one-warp CTAs per SM (up to 96 registers): the C4 ensemble's forward step 5 % faster than
+// with 24 (80 registers)
+__global__ void __launch_bounds__(kStripEnsThreads, 20)
     vp_strip_ens_fwd_kernel(const StripInst* __restrict__ insts, const int4* __restrict__ map,
                             const BatchStep<float> b) {
     extern __shared__ __align__(16) unsigned char smem[];
